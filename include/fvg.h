@@ -1,0 +1,222 @@
+/*
+ * fvg.h - C ABI of the B200 mode-split time step for FVCOM.
+ *
+ * The library replaces FVCOM's two argument-less time-step subroutines,
+ *   SUBROUTINE EXTERNAL_STEP   (FVCOM_source/external_step.F:30)
+ *   SUBROUTINE INTERNAL_STEP   (FVCOM_source/internal_step.F:29)
+ * which read and write FVCOM's module globals (ALL_VARS, MOD_WD, BCS, MOD_OBCS,
+ * CONTROL).  Here the same state lives in device memory owned by an fvg_handle; the
+ * host hands over the mesh arrays once (fvg_create), copies state in and out by FVCOM
+ * variable name (fvg_set_field / fvg_get_field) and calls fvg_internal_step once per
+ * internal step, as fvcom.F:848-852 calls INTERNAL_STEP.
+ *
+ * Array convention: every per-node, per-cell, per-edge and per-half-edge array uses
+ * FVCOM's 1-based numbering with the ghost row 0 kept, and 2-D arrays are
+ * column-major (Fortran order): element (i, j) of an array with rows 0..len sits at
+ * a[(j-1)*(len+1) + i], j 1-based.  Arrays that FVCOM allocates without a ghost row
+ * (NBSN, NBVE, NBVT, DLTXTRIE..., IEC, IENODE, NIEC, NTRG, DLTXE, DLTYE, DLTXNCVE,
+ * DLTYNCVE) are passed with an unused row 0 as well.  3-D fields are (0:len, 1:KB).
+ *
+ * Every entry point returns an int status (FVG_OK on success) and never aborts the
+ * process, in place of FVCOM's FATAL_ERROR/PSTOP (FVCOM_source/mod_utils.F:270).
+ * One host thread per handle; calls on one handle are not re-entrant; separate handles
+ * are independent and each owns one CUDA stream.
+ */
+#ifndef FVG_H
+#define FVG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FVG_OK 0
+#define FVG_ERR_ARG 1          /* bad argument, size or unknown field name */
+#define FVG_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define FVG_ERR_NAN 3          /* SHUTDOWN_CHECK: non-finite depth (mod_utils.F:320-376) */
+#define FVG_ERR_BOUNDS 4       /* an index in the mesh arrays is out of range */
+#define FVG_ERR_TIMEOUT 5      /* a bounded device wait ran out */
+#define FVG_ERR_UNSUPPORTED 6  /* option outside the supported physics set */
+#define FVG_ERR_NOMEM 7        /* device allocation failed */
+
+/* Mesh arrays as GRID_METRICS builds them (FVCOM_source/grid_metrics.F:29-136). */
+typedef struct fvg_mesh {
+  int32_t m, n, kb;          /* nodes M, cells N, sigma levels KB (KBM1 = KB-1 layers) */
+  int32_t ne, ncv, ncv_i;    /* element edges NE, CV half-edges NCV, interior NCV_I */
+  int32_t nbsn_cols;         /* columns of NBSN (>= max NTSN) */
+  int32_t nbve_cols;         /* columns of NBVE/NBVT (>= max NTVE + 1) */
+  int32_t trie_cols;         /* columns of DLTXTRIE.. DLTYNEC (FVCOM: 12) */
+
+  /* nodes (0:M) */
+  const double *vx, *vy, *h, *art1, *art2, *grav_n, *nn_hvc, *sita_gd, *phpn;
+  const int32_t *isonb, *ntsn, *ntve;
+  const int32_t *nbsn;                 /* NBSN(0:M, nbsn_cols) */
+  const int32_t *nbve, *nbvt;          /* NBVE/NBVT(0:M, nbve_cols) */
+  const double *dltxtrie, *dltytrie;   /* (0:M, trie_cols) */
+  const double *dltxecec, *dltyecec;   /* (0:M, trie_cols) */
+  const double *dltxnec, *dltynec;     /* (0:M, trie_cols) */
+  const double *z, *zz, *dz, *dzz;     /* (0:M, KB) */
+
+  /* cells (0:N) */
+  const double *xc, *yc, *art, *h1, *cor, *grav_e, *cc_hvc, *cc_sponge, *cc_z0b;
+  const double *epor, *iucp, *alpha;
+  const int32_t *nv;                   /* NV(0:N, 3), clockwise */
+  const int32_t *nbe;                  /* NBE(0:N, 3) */
+  const int32_t *isbce;
+  const double *a1u, *a2u;             /* (0:N, 4) */
+  const double *awx, *awy;             /* (0:N, 3) */
+  const double *z1, *zz1, *dz1, *dzz1; /* (0:N, KB) */
+
+  /* element edges (0:NE) */
+  const int32_t *iec, *ienode;         /* (0:NE, 2) */
+  const int32_t *isbc;
+  const double *xijc, *yijc, *dltxc, *dltyc;
+
+  /* control-volume half-edges (0:NCV) */
+  const int32_t *niec;                 /* (0:NCV, 2) */
+  const int32_t *ntrg;
+  const double *dltxe, *dltye;
+  const double *dltxncve, *dltyncve;   /* (0:NCV_I, 2) */
+
+  /* open boundary (1:IOBCN, ghost row 0) - SETUP_OBC (mod_obcs.F:868-1173) */
+  int32_t iobcn;
+  const int32_t *i_obc_n, *type_obc, *next_obc, *nadjc_obc;
+  const int32_t *adjc_obc;             /* (0:IOBCN, 2) */
+  const double *fluxf_obc;             /* (0:IOBCN, 2) */
+  const double *dltn_obc;
+
+  /* rivers (1:NUMQBC, ghost row 0) - SET_RIVER_BNDRY_METRICS (mod_force.F:3447-3581) */
+  int32_t numqbc;
+  const int32_t *inodeq, *icellq;
+  const int32_t *n_icellq;             /* (0:NUMQBC, 2) */
+  const double *rdisq;                 /* (0:NUMQBC, 2) */
+  const double *qarea, *angleq;
+  const double *vqdist;                /* (0:NUMQBC, KBM1) */
+} fvg_mesh;
+
+/* Run-time switches and constants (NML_INTEGRATION, NML_PHYSICS, NML_OPEN_BOUNDARY_CONTROL,
+ * NML_RIVER_TYPE; FVCOM_source/mod_main.F:121-942). */
+typedef struct fvg_params {
+  double dte;                 /* EXTSTEP_SECONDS */
+  int32_t isplit;             /* ISPLIT */
+  int32_t iramp;              /* IRAMP (0: no ramp) */
+  double min_depth;           /* MIN_DEPTH */
+  double static_ssh_adj;      /* STATIC_SSH_ADJ */
+  int32_t horizontal_mixing;  /* 0 'closure', 1 'constant' */
+  double hprnu;               /* HORIZONTAL_PRANDTL_NUMBER */
+  double umol;                /* VERTICAL_MIXING_COEFFICIENT */
+  double vprnu;               /* VERTICAL_PRANDTL_NUMBER */
+  double cbcmin;              /* BOTTOM_ROUGHNESS_MINIMUM */
+  int32_t vertical_mixing;    /* 0 'closure' (MY2.5), 1 'constant' */
+  int32_t wetting_drying_on;
+  int32_t scalar_positivity_control;
+  int32_t barotropic;
+  int32_t temperature_active, salinity_active;
+  int32_t obc_elevation_forcing_on;
+  int32_t obc_ts_type;        /* OBC_TS_TYPE 1..3 */
+  int32_t river_ts_setting;   /* 0 'specified' */
+  int32_t river_location;     /* 0 'node', 1 'edge' */
+  double tide_ref_time;       /* SpecTime: the zero of the tidal phase, seconds */
+} fvg_params;
+
+/* Boundary forcing that is constant in time for the supported cases. */
+typedef struct fvg_forcing {
+  /* spectral tide on the open boundary (BCOND_ASL, mod_obcs.F:554-583) */
+  int32_t ntide;
+  const double *period;       /* (ntide) seconds */
+  const double *apt;          /* (0:IOBCN, ntide) amplitude m */
+  const double *phai;         /* (0:IOBCN, ntide) phase, degrees */
+  const double *emean;        /* (0:IOBCN) mean level m */
+  /* river discharge and its temperature/salinity (UPDATE_RIVERS, mod_force.F:11229) */
+  const double *qdis;         /* (0:NUMQBC) m^3/s before the ramp */
+  const double *tdis, *sdis;  /* (0:NUMQBC) */
+  /* surface wind stress before RAMP*0.001 scaling (UPDATE_WIND / ASIMPLE_DRAG);
+     NULL for no wind.  (0:N) */
+  const double *wstress_x, *wstress_y;
+} fvg_forcing;
+
+typedef struct fvg_handle fvg_handle;
+
+/* Routine identifiers for fvg_run_routine: one FVCOM subroutine on the current state. */
+enum fvg_routine {
+  FVG_R_EXTEL_EDGE = 1,        /* EXTEL_EDGE(K)           extel_edge.F:32       arg: K */
+  FVG_R_BCOND_ELF = 2,         /* BCOND_GCN(1,K)+RK blend external_step.F:253-266 arg: K */
+  FVG_R_N2E2D_ELF = 3,         /* N2E2D(ELF,ELF1)         external_step.F:287 */
+  FVG_R_WET_JUDGE = 4,         /* WET_JUDGE               mod_wd.F:193 */
+  FVG_R_FLUX_OBN = 5,          /* FLUX_OBN(K)             mod_obcs.F:1181       arg: K */
+  FVG_R_ADVAVE = 6,            /* ADVAVE_EDGE_GCN(ADVUA,ADVVA) advave_edge_gcn.F:32 */
+  FVG_R_EXTUV_EDGE = 7,        /* EXTUV_EDGE(K)           extuv_edge.F:33       arg: K */
+  FVG_R_BCOND_UV2D = 8,        /* BCOND_GCN(2,K)          bcond_gcn.F:325 */
+  FVG_R_EXT_UPDATE = 9,        /* external_step.F:333-436 (state shift, K==3/4 sums) arg: K */
+  FVG_R_EXTERNAL_STEP = 10,    /* EXTERNAL_STEP (all 4 stages) arg: IEXT */
+  FVG_R_ADJUST2D3D = 11,       /* ADJUST2D3D(arg)         adjust2d3d.F:29 */
+  FVG_R_BCOND_UV3D_SOLID = 12, /* BCOND_GCN(5,0)          bcond_gcn.F:537 */
+  FVG_R_BROUGH = 13,           /* BOTTOM_ROUGHNESS        brough.F:41 */
+  FVG_R_ADVECTION3D = 14,      /* ADVECTION_EDGE_GCN      advection_edge_gcn.F:30 */
+  FVG_R_BAROPG = 15,           /* BAROPG                  baropg.F:33 */
+  FVG_R_INT_PRE_EXT = 16,      /* internal_step.F:374-416 (2-D sums, ADVAVE, GX/GY) */
+  FVG_R_VERTVL = 17,           /* VERTVL_EDGE             vertvl_edge.F:37 */
+  FVG_R_VISCOFH = 18,          /* VISCOF_H                viscofh.F:33 */
+  FVG_R_ADV_UV = 19,           /* ADV_UV_EDGE_GCN         adv_uv_edge_gcn.F:31 */
+  FVG_R_VDIF_UV = 20,          /* VDIF_UV                 vdif_uv.F:34 */
+  FVG_R_BCOND_UV3D = 21,       /* static-SSH fix + BCOND_GCN(3,0) internal_step.F:660-672 */
+  FVG_R_WREAL = 22,            /* WREAL                   wreal.F:32 */
+  FVG_R_ADV_Q = 23,            /* ADV_Q(Q2,Q2F) arg 0, ADV_Q(Q2L,Q2LF) arg 1  adv_q.F:35 */
+  FVG_R_FCT_Q = 24,            /* FCT_Q2 arg 0, FCT_Q2L arg 1 */
+  FVG_R_VDIF_Q = 25,           /* VDIF_Q                  vdif_q.F:34 */
+  FVG_R_TURB_UPDATE = 26,      /* Q2=Q2F, Q2L=Q2LF, N2E3D(KM,KM1) internal_step.F:1034-1053 */
+  FVG_R_ADV_TS = 27,           /* ADV_T arg 1, ADV_S arg 2 adv_t.F:34 / adv_s.F:34 */
+  FVG_R_FCT_TS = 28,           /* FCT_T arg 1, FCT_S arg 2 */
+  FVG_R_VDIF_TS = 29,          /* VDIF_TS(arg)            vdif_ts.F:42 */
+  FVG_R_BCOND_TS = 30,         /* BCOND_TS(arg)           bcond_ts.F:35 */
+  FVG_R_TS_UPDATE = 31,        /* T1=TF1 + N2E3D arg 1; S1=SF1 + N2E3D arg 2 */
+  FVG_R_DENS2 = 32,            /* DENS2                   eqs_of_state.F:381 */
+  FVG_R_INT_FINAL = 33,        /* U=UF ... WD_UPDATE(3)   internal_step.F:1541-1590 */
+  FVG_R_INTERNAL_STEP = 34,    /* INTERNAL_STEP           internal_step.F:29 */
+  FVG_R_INT_FORCING = 35       /* RAMP, BCOND_GCN(8,0)    internal_step.F:115-265 */
+};
+
+/* Lifecycle.  fvg_create copies the mesh to the device and builds the gather lists;
+   the host arrays may be freed afterwards. */
+int fvg_create(const fvg_mesh* mesh, const fvg_params* params, const fvg_forcing* forcing,
+               fvg_handle** out);
+void fvg_destroy(fvg_handle* h);
+const char* fvg_last_error(const fvg_handle* h);
+
+/* State exchange by FVCOM variable name (lower case, e.g. "el", "ua", "t1", "q2l",
+   "iswetn").  count must equal the field's element count ((len+1) or (len+1)*KB). */
+int fvg_set_field(fvg_handle* h, const char* name, const double* src, int64_t count);
+int fvg_get_field(fvg_handle* h, const char* name, double* dst, int64_t count);
+int fvg_set_ifield(fvg_handle* h, const char* name, const int32_t* src, int64_t count);
+int fvg_get_ifield(fvg_handle* h, const char* name, int32_t* dst, int64_t count);
+/* Element count of a field, or -1 for an unknown name. */
+int64_t fvg_field_size(const fvg_handle* h, const char* name);
+
+/* Model clock: IINT of the last completed internal step and ExtTime in seconds. */
+int fvg_set_clock(fvg_handle* h, int32_t iint, double ext_time);
+int fvg_get_clock(const fvg_handle* h, int32_t* iint, double* ext_time);
+
+/* One INTERNAL_STEP for IINT+1 (fvcom.F:848-852), ISPLIT external steps included. */
+int fvg_internal_step(fvg_handle* h);
+/* n consecutive internal steps; replayed from a captured CUDA graph after the first. */
+int fvg_run(fvg_handle* h, int32_t nsteps);
+/* One reference routine (enum fvg_routine) on the current state, for parity checks. */
+int fvg_run_routine(fvg_handle* h, int32_t routine, int32_t arg);
+/* Wait for all device work of the handle. */
+int fvg_sync(fvg_handle* h);
+
+/* SHUTDOWN_CHECK (mod_utils.F:320-376): FVG_ERR_NAN when the sum of D1 is not finite. */
+int fvg_shutdown_check(fvg_handle* h);
+/* FP64 budgets: out[0] volume (m^3), out[1] heat content (T*volume), out[2] salt
+   content (S*volume) over the node control volumes. */
+int fvg_budget(fvg_handle* h, double out[3]);
+
+/* Library identity for checks that the compiled CUDA path is the one loaded. */
+const char* fvg_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FVG_H */

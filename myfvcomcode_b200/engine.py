@@ -1,0 +1,187 @@
+"""Host-side mirror of FVCOM's time-step interface over the C ABI (include/fvg.h).
+
+``Fvcom(case)`` owns one library handle: the mesh goes to the device once, the
+cold-start state is copied in, and ``internal_step()`` / ``run(n)`` advance the model
+exactly as fvcom.F:848-852 calls INTERNAL_STEP.  ``routine(r, arg)`` runs one reference
+subroutine (enum fvg_routine) for per-routine parity checks; ``get``/``set`` move any
+FVCOM variable by its (lower-case) name.
+
+The CUDA library is required: if libfvg.so is missing or fails to load, construction
+raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .startup import coldstart
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libfvg.so")
+
+ROUTINES = dict(
+    EXTEL_EDGE=1, BCOND_ELF=2, N2E2D_ELF=3, WET_JUDGE=4, FLUX_OBN=5, ADVAVE=6, EXTUV_EDGE=7,
+    BCOND_UV2D=8, EXT_UPDATE=9, EXTERNAL_STEP=10, ADJUST2D3D=11, BCOND_UV3D_SOLID=12,
+    BROUGH=13, ADVECTION3D=14, BAROPG=15, INT_PRE_EXT=16, VERTVL=17, VISCOFH=18, ADV_UV=19,
+    VDIF_UV=20, BCOND_UV3D=21, WREAL=22, ADV_Q=23, FCT_Q=24, VDIF_Q=25, TURB_UPDATE=26,
+    ADV_TS=27, FCT_TS=28, VDIF_TS=29, BCOND_TS=30, TS_UPDATE=31, DENS2=32, INT_FINAL=33,
+    INTERNAL_STEP=34, INT_FORCING=35,
+)
+
+INT_FIELDS = ("iswetn", "iswetnt", "iswetc", "iswetct", "iswetce")
+
+
+class FvgError(RuntimeError):
+    pass
+
+
+def _declare(lib, prefix):
+    P = C.POINTER
+    vp = C.c_void_p
+    fn = lambda n: getattr(lib, prefix + n)
+    fn("create").argtypes = [P(abi.FvgMesh), P(abi.FvgParams), P(abi.FvgForcing), P(vp)]
+    fn("create").restype = C.c_int
+    fn("destroy").argtypes = [vp]
+    fn("destroy").restype = None
+    for n, t in (("set_field", P(C.c_double)), ("get_field", P(C.c_double)),
+                 ("set_ifield", P(C.c_int32)), ("get_ifield", P(C.c_int32))):
+        fn(n).argtypes = [vp, C.c_char_p, t, C.c_int64]
+        fn(n).restype = C.c_int
+    fn("field_size").argtypes = [vp, C.c_char_p]
+    fn("field_size").restype = C.c_int64
+    fn("set_clock").argtypes = [vp, C.c_int32, C.c_double]
+    fn("set_clock").restype = C.c_int
+    fn("get_clock").argtypes = [vp, P(C.c_int32), P(C.c_double)]
+    fn("get_clock").restype = C.c_int
+    fn("internal_step").argtypes = [vp]
+    fn("internal_step").restype = C.c_int
+    fn("run").argtypes = [vp, C.c_int32]
+    fn("run").restype = C.c_int
+    fn("run_routine").argtypes = [vp, C.c_int32, C.c_int32]
+    fn("run_routine").restype = C.c_int
+
+
+class CEngine:
+    """Generic driver of a C library that implements the fvg_* entry-point set."""
+
+    prefix = "fvg_"
+
+    def __init__(self, case, lib, prefix=None, state=None):
+        self.prefix = prefix or self.prefix
+        self.lib = lib
+        _declare(lib, self.prefix)
+        self.case = case
+        g = case["grid"]
+        self.M, self.N, self.KB = g["M"], g["N"], g["KB"]
+        self._ms, self._ps, self._fs, self._bundle = abi.make_structs(case)
+        h = C.c_void_p()
+        rc = self._f("create")(C.byref(self._ms), C.byref(self._ps), C.byref(self._fs), C.byref(h))
+        self._check(rc, "create", handle=False)
+        self.h = h
+        self.set_state(coldstart(case) if state is None else state)
+
+    def _f(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def _check(self, rc, what, handle=True):
+        if rc != 0:
+            msg = ""
+            if handle and hasattr(self.lib, self.prefix + "last_error"):
+                f = self._f("last_error")
+                f.restype = C.c_char_p
+                f.argtypes = [C.c_void_p]
+                m = f(self.h)
+                msg = m.decode() if m else ""
+            raise FvgError("%s%s failed with status %d %s" % (self.prefix, what, rc, msg))
+
+    def size(self, name):
+        return int(self._f("field_size")(self.h, name.encode()))
+
+    def get(self, name):
+        n = self.size(name)
+        if n < 0:
+            raise KeyError(name)
+        if name in INT_FIELDS:
+            out = np.zeros(n, dtype=np.int32)
+            rc = self._f("get_ifield")(self.h, name.encode(), out.ctypes.data_as(C.POINTER(C.c_int32)), n)
+        else:
+            out = np.zeros(n, dtype=np.float64)
+            rc = self._f("get_field")(self.h, name.encode(), out.ctypes.data_as(C.POINTER(C.c_double)), n)
+        self._check(rc, "get_field(%s)" % name)
+        return out
+
+    def get3(self, name):
+        a = self.get(name)
+        rows = a.size // self.KB
+        return a.reshape((rows, self.KB), order="F")
+
+    def set(self, name, arr):
+        if name in INT_FIELDS:
+            a = np.ascontiguousarray(np.asarray(arr, dtype=np.int32).reshape(-1, order="F"))
+            rc = self._f("set_ifield")(self.h, name.encode(), a.ctypes.data_as(C.POINTER(C.c_int32)), a.size)
+        else:
+            a = np.ascontiguousarray(np.asarray(arr, dtype=np.float64).reshape(-1, order="F"))
+            rc = self._f("set_field")(self.h, name.encode(), a.ctypes.data_as(C.POINTER(C.c_double)), a.size)
+        self._check(rc, "set_field(%s)" % name)
+
+    def set_state(self, st):
+        for k, v in st.items():
+            self.set(k, v)
+
+    def clock(self):
+        i = C.c_int32()
+        t = C.c_double()
+        self._check(self._f("get_clock")(self.h, C.byref(i), C.byref(t)), "get_clock")
+        return i.value, t.value
+
+    def set_clock(self, iint, ext_time):
+        self._check(self._f("set_clock")(self.h, int(iint), float(ext_time)), "set_clock")
+
+    def internal_step(self):
+        self._check(self._f("internal_step")(self.h), "internal_step")
+
+    def run(self, n):
+        self._check(self._f("run")(self.h, int(n)), "run")
+
+    def routine(self, name, arg=0):
+        r = ROUTINES[name] if isinstance(name, str) else int(name)
+        self._check(self._f("run_routine")(self.h, r, int(arg)), "run_routine(%s)" % name)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._f("destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_LIB = None
+
+
+def load_library(path=None):
+    """Load the in-tree CUDA library; raise if it is absent (no fallback exists)."""
+    global _LIB
+    if _LIB is None:
+        p = path or LIB_PATH
+        if not os.path.exists(p):
+            raise FvgError("libfvg.so not built at %s (run __graft_entry__.build())" % p)
+        _LIB = C.CDLL(p)
+    return _LIB
+
+
+class Fvcom(CEngine):
+    """The B200 mode-split step for one model (mesh + parameters + forcing)."""
+
+    def __init__(self, case, state=None, lib_path=None):
+        lib = load_library(lib_path)
+        super().__init__(case, lib, "fvg_", state)
+
+    def sync(self):
+        self._check(self.lib.fvg_sync(self.h), "sync")
