@@ -205,6 +205,21 @@ int fvg_run(fvg_handle* h, int32_t nsteps);
 int fvg_run_routine(fvg_handle* h, int32_t routine, int32_t arg);
 /* Wait for all device work of the handle. */
 int fvg_sync(fvg_handle* h);
+/* Override the RAMP factor that fvg_run_routine uses (fvg_run sets it from IINT). */
+int fvg_set_ramp(fvg_handle* h, double ramp);
+/* 1 (default): replay a captured CUDA graph per internal step; 0: plain launches. */
+int fvg_use_graph(fvg_handle* h, int32_t on);
+
+/* Measurement.  fvg_time_steps runs nsteps internal steps and returns their device time
+   (CUDA events on the handle's stream).  fvg_profile runs nsteps with plain launches and
+   events between kernel groups, adding each group's device time to group_ms (length
+   fvg_profile_groups()) and the whole steps' time to *total_ms (may be NULL). */
+int fvg_time_steps(fvg_handle* h, int32_t nsteps, double* ms);
+int32_t fvg_profile_groups(void);
+const char* fvg_profile_group_name(int32_t g);
+int fvg_profile(fvg_handle* h, int32_t nsteps, double* group_ms, double* total_ms);
+/* Number of kernel launches one internal step issues. */
+int32_t fvg_kernels_per_step(const fvg_handle* h);
 
 /* SHUTDOWN_CHECK (mod_utils.F:320-376): FVG_ERR_NAN when the sum of D1 is not finite. */
 int fvg_shutdown_check(fvg_handle* h);

@@ -98,6 +98,21 @@ def _pad_rows(a, rows):
     return out
 
 
+def wind_stress(case):
+    """Surface stress (N/m^2, (0:N)) before FVCOM's RAMP*0.001 scaling, or None."""
+    wind = case["forcing"].get("wind")
+    if wind is None:
+        return None
+    N = case["grid"]["N"]
+    if wind["kind"] == "speed":
+        sx, sy = simple_drag(np.full(N + 1, wind["u"]), np.full(N + 1, wind["v"]))
+    else:
+        sx, sy = np.full(N + 1, float(wind["u"])), np.full(N + 1, float(wind["v"]))
+    sx[0] = 0.0
+    sy[0] = 0.0
+    return sx, sy
+
+
 def make_structs(case):
     """Build (mesh, params, forcing, bundle) ctypes structs for a case dict."""
     g = case["grid"]
@@ -176,14 +191,7 @@ def make_structs(case):
     td = np.zeros(nq + 1); td[1:] = fc["tdis"]
     sd = np.zeros(nq + 1); sd[1:] = fc["sdis"]
     fs.qdis, fs.tdis, fs.sdis = b.d(q), b.d(td), b.d(sd)
-    wind = fc.get("wind")
-    if wind is not None:
-        N = g["N"]
-        if wind["kind"] == "speed":
-            sx, sy = simple_drag(np.full(N + 1, wind["u"]), np.full(N + 1, wind["v"]))
-        else:
-            sx, sy = np.full(N + 1, wind["u"]), np.full(N + 1, wind["v"])
-        sx[0] = 0.0
-        sy[0] = 0.0
-        fs.wstress_x, fs.wstress_y = b.d(sx), b.d(sy)
+    ws = wind_stress(case)
+    if ws is not None:
+        fs.wstress_x, fs.wstress_y = b.d(ws[0]), b.d(ws[1])
     return ms, ps, fs, b

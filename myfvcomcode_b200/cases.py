@@ -74,7 +74,7 @@ def default_params(**kw):
 
 
 def estuary_channel(nx=100, ny=20, kb=11, lx=20000.0, ly=4000.0, river_q=100.0,
-                    river_location="node", lat=30.0, **pkw):
+                    river_location="node", lat=30.0, river=True, **pkw):
     # The lower seaward corner quad is split along its other diagonal so that no cell
     # has one open and one solid side (tge.F:563-580 rejects such cells).
     vx, vy, tri, nid = _structured(nx, ny, lx, ly, flip={(nx - 1, 0)})
@@ -87,15 +87,16 @@ def estuary_channel(nx=100, ny=20, kb=11, lx=20000.0, ly=4000.0, river_q=100.0,
         # Head cell on the x = 0 boundary at mid-channel: cell (i=0, j) second triangle.
         rloc = 2 * (ny // 2) + 2
     kbm1 = kb - 1
-    rivers = [dict(loc=rloc, dist=[1.0 / kbm1] * kbm1)]
+    rivers = [dict(loc=rloc, dist=[1.0 / kbm1] * kbm1)] if river else []
     g = build_grid(vx, vy, nv, h, kb, obc_nodes=obc, obc_types=[1] * len(obc),
                    cor_lat=lat, sponge=(), horcon=0.2, z0b=0.001,
                    rivers=rivers, river_location=river_location)
     n_obc = len(obc)
     tide = dict(period=np.array([M2_PERIOD]), apt=np.full((n_obc, 1), 1.0),
                 phai=np.zeros((n_obc, 1)), emean=np.zeros(n_obc))
-    forcing = dict(tide=tide, qdis=np.array([river_q]), tdis=np.array([15.0]),
-                   sdis=np.array([0.0]), wind=None)
+    nq = len(rivers)
+    forcing = dict(tide=tide, qdis=np.full(nq, river_q), tdis=np.full(nq, 15.0),
+                   sdis=np.zeros(nq), wind=None)
     params = default_params(**pkw)
     init = dict(kind="constant", t=15.0, s=30.0)
     return dict(grid=g, forcing=forcing, params=params, init=init,

@@ -1,0 +1,872 @@
+// fvg_host.cu - C ABI (include/fvg.h) of the B200 mode-split step.
+//
+// fvg_create copies FVCOM's mesh arrays to the device, builds the gather lists that turn
+// the reference's scatter loops into ordered per-target sums, and allocates the state.
+// fvg_internal_step / fvg_run enqueue one INTERNAL_STEP (FVCOM_source/internal_step.F:29)
+// as a fixed kernel sequence; the sequence is captured once into a CUDA graph and
+// replayed, with the per-step scalars (RAMP, tidal phase arguments) supplied through a
+// device schedule table that the host fills ahead of each batch of steps.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "fvg_model.h"
+
+using namespace fvg;
+
+namespace {
+
+const double kPI2 = 2.0 * 3.141592653589793238;
+
+struct FieldDesc {
+  void* d = nullptr;
+  int64_t rows = 0;   // len+1
+  int layers = 1;
+  int64_t stride = 0; // device elements between layers
+  bool is_int = false;
+};
+
+}  // namespace
+
+struct fvg_handle {
+  Dev P{};
+  fvg_params prm{};
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  std::map<std::string, FieldDesc> fields;
+  std::string err;
+  int32_t iint = 0;
+  double ext_time = 0.0;
+  double ramp = 0.0;
+  int ntide = 0;
+  std::vector<double> period;
+  int sched_cap = 0;
+  double* d_sched = nullptr;
+  double* h_sched = nullptr;  // pinned
+  int* h_ctl = nullptr;       // pinned
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t graph = nullptr;
+  bool use_graph = true;
+};
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                    \
+      return FVG_ERR_CUDA;                                                            \
+    }                                                                                 \
+  } while (0)
+
+namespace {
+
+template <class T>
+int dalloc(fvg_handle* h, T** p, size_t n) {
+  void* q = nullptr;
+  size_t bytes = (n == 0 ? 1 : n) * sizeof(T);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    h->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return FVG_ERR_NOMEM;
+  }
+  cudaMemset(q, 0, bytes);
+  h->allocs.push_back(q);
+  *p = (T*)q;
+  return FVG_OK;
+}
+
+template <class T>
+int upload(fvg_handle* h, T** p, const T* src, size_t n) {
+  int rc = dalloc(h, p, n);
+  if (rc) return rc;
+  if (src && n) CK(cudaMemcpy(*p, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return FVG_OK;
+}
+
+// (0:len, 1:KB) Fortran array -> layer-strided device array
+int upload3(fvg_handle* h, double** p, const double* src, size_t rows, int kb, size_t stride) {
+  int rc = dalloc(h, p, stride * kb);
+  if (rc) return rc;
+  if (src)
+    CK(cudaMemcpy2D(*p, stride * sizeof(double), src, rows * sizeof(double), rows * sizeof(double), kb,
+                    cudaMemcpyHostToDevice));
+  return FVG_OK;
+}
+
+inline size_t pad32(size_t n) { return (n + 31) / 32 * 32; }
+
+int build_csr(const std::vector<std::vector<int>>& lists, std::vector<int>& ptr, std::vector<int>& ent) {
+  ptr.assign(lists.size() + 1, 0);
+  for (size_t i = 0; i < lists.size(); ++i) ptr[i + 1] = ptr[i] + (int)lists[i].size();
+  ent.clear();
+  for (auto& l : lists) ent.insert(ent.end(), l.begin(), l.end());
+  return FVG_OK;
+}
+
+// Schedule row for internal step iint (1-based) whose ExtTime before the step is t0.
+void fill_sched_row(const fvg_handle* h, double* row, int32_t iint, double t0) {
+  const fvg_params& p = h->prm;
+  const SchedLayout& sl = h->P.sl;
+  row[sl.ramp_int()] = p.iramp != 0 ? std::tanh((double)iint / (double)p.iramp) : 1.0;
+  double ext = t0;
+  for (int iext = 1; iext <= p.isplit; ++iext) {
+    ext = ext + p.dte;
+    if (p.iramp != 0) {
+      double tmp = (double)(iint - 1) + (double)iext / (double)p.isplit;
+      row[sl.ramp_ext(iext)] = std::tanh(tmp / (double)p.iramp);
+    } else {
+      row[sl.ramp_ext(iext)] = 1.0;
+    }
+    for (int K = 1; K <= 4; ++K) {
+      double rktime = ext + p.dte * (kAlphaRK[K] - 1.0);
+      double te = rktime - p.tide_ref_time;
+      for (int j = 0; j < h->ntide; ++j) row[sl.targ(iext, K, j)] = te * kPI2 / h->period[j];
+    }
+  }
+}
+
+// Row used by fvg_run_routine: current RAMP everywhere, phases from the current ExtTime.
+void fill_routine_row(const fvg_handle* h, double* row) {
+  const fvg_params& p = h->prm;
+  const SchedLayout& sl = h->P.sl;
+  for (int q = 0; q < sl.len; ++q) row[q] = 0.0;
+  row[sl.ramp_int()] = h->ramp;
+  for (int iext = 1; iext <= p.isplit; ++iext) {
+    row[sl.ramp_ext(iext)] = h->ramp;
+    for (int K = 1; K <= 4; ++K) {
+      double rktime = h->ext_time + p.dte * (kAlphaRK[K] - 1.0);
+      double te = rktime - p.tide_ref_time;
+      for (int j = 0; j < h->ntide; ++j) row[sl.targ(iext, K, j)] = te * kPI2 / h->period[j];
+    }
+  }
+}
+
+// Kernel groups reported by fvg_profile (order of enqueue_internal_step).
+const char* kGroupNames[] = {"cell_pre", "advection3d", "baropg", "int_advave", "ext_node", "wet_judge",
+                             "ext_cell", "ext_update", "adjust2", "vertvl_flux", "vertvl_col", "w_viscofh",
+                             "adv_uv", "vdif_uv", "grad_q", "adv_q", "vdif_q", "grad_ts", "adv_ts",
+                             "vdif_ts", "bcond_ts", "final"};
+enum { G_CELL_PRE, G_ADV3D, G_BAROPG, G_INT_ADVAVE, G_EXT_NODE, G_WET, G_EXT_CELL, G_EXT_UPD, G_ADJ2,
+       G_VV_FLUX, G_VV_COL, G_W_VISC, G_ADV_UV, G_VDIF_UV, G_GRAD_Q, G_ADV_Q, G_VDIF_Q, G_GRAD_TS,
+       G_ADV_TS, G_VDIF_TS, G_BCOND_TS, G_FINAL, G_COUNT };
+
+struct Marker {
+  std::vector<cudaEvent_t>* ev = nullptr;
+  std::vector<int>* grp = nullptr;
+  void mark(cudaStream_t s, int g) {
+    if (!ev) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, s);
+    ev->push_back(e);
+    grp->push_back(g);
+  }
+};
+
+// One INTERNAL_STEP as a kernel sequence (internal_step.F:115-1590).
+void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) {
+  const Dev& P = h->P;
+  const fvg_params& p = h->prm;
+  const int spc = p.scalar_positivity_control ? AD_FCT : 0;
+  mk.mark(s, -1);
+  launch_begin_step(P, s);
+  launch_cell_pre(P, s, CP_ADJUST1 | CP_BC5 | CP_BCOND8 | CP_BROUGH);
+  mk.mark(s, G_CELL_PRE);
+  launch_advection3d(P, s);
+  mk.mark(s, G_ADV3D);
+  launch_baropg(P, s, !p.barotropic, 1);
+  mk.mark(s, G_BAROPG);
+  launch_ext_cell(P, s, 1, 1, EC_INT_ADVAVE);
+  launch_int_reset(P, s);
+  mk.mark(s, G_INT_ADVAVE);
+  for (int iext = 1; iext <= p.isplit; ++iext) {
+    for (int K = 1; K <= 4; ++K) {
+      launch_ext_node(P, s, iext, K, EN_EXTEL | EN_BC | (K == 1 ? EN_COPY_ELRK : 0));
+      mk.mark(s, G_EXT_NODE);
+      if (p.wetting_drying_on) {
+        launch_wet_judge(P, s);
+        mk.mark(s, G_WET);
+      }
+      launch_ext_cell(P, s, iext, K,
+                      (p.wetting_drying_on ? 0 : EC_N2E) | EC_FLUXOBN | EC_ADVAVE | EC_EXTUV | EC_BC2 |
+                          (K == 1 ? EC_COPY_RK : 0));
+      mk.mark(s, G_EXT_CELL);
+      launch_ext_update(P, s, K);
+      mk.mark(s, G_EXT_UPD);
+    }
+  }
+  launch_adjust2(P, s);
+  mk.mark(s, G_ADJ2);
+  launch_vertvl_flux(P, s);
+  mk.mark(s, G_VV_FLUX);
+  launch_vertvl_col(P, s, VC_WTS | VC_WD2 | (p.barotropic ? 0 : VC_RHO_ROUNDTRIP) | VC_BOT_NODE);
+  mk.mark(s, G_VV_COL);
+  launch_w_viscofh(P, s, 1, 1);
+  mk.mark(s, G_W_VISC);
+  launch_adv_uv(P, s);
+  mk.mark(s, G_ADV_UV);
+  launch_vdif_uv(P, s, VU_VDIF | VU_BC3 | VU_WREAL);
+  mk.mark(s, G_VDIF_UV);
+  launch_grad(P, s, 0);
+  mk.mark(s, G_GRAD_Q);
+  launch_adv_q(P, s, AD_Q2 | AD_Q2L | spc);
+  mk.mark(s, G_ADV_Q);
+  launch_vdif_q(P, s, 1);
+  mk.mark(s, G_VDIF_Q);
+  int ts = (p.temperature_active ? AD_T : 0) | (p.salinity_active ? AD_S : 0);
+  if (ts) {
+    launch_grad(P, s, 1);
+    mk.mark(s, G_GRAD_TS);
+    launch_adv_ts(P, s, ts | spc);
+    mk.mark(s, G_ADV_TS);
+    launch_vdif_ts(P, s, ts);
+    mk.mark(s, G_VDIF_TS);
+    launch_bcond_ts(P, s, ts);
+    mk.mark(s, G_BCOND_TS);
+  }
+  int fin = FI_KM1 | FI_SHIFT | (p.temperature_active ? FI_T : 0) | (p.salinity_active ? FI_S : 0) |
+            (p.barotropic ? 0 : FI_DENS);
+  launch_final(P, s, fin);
+  mk.mark(s, G_FINAL);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fvg_build_info(void) {
+  return "fvg: B200 mode-split step, sm_100a, FP64, --fmad=false, gather-by-target (no atomics)";
+}
+
+const char* fvg_last_error(const fvg_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, fvg_handle** out) {
+  if (!m || !prm || !out) return FVG_ERR_ARG;
+  *out = nullptr;
+  if (m->m < 3 || m->n < 1 || m->kb < 3 || m->kb > 64) return FVG_ERR_ARG;
+  if (prm->isplit < 1 || prm->dte <= 0.0) return FVG_ERR_ARG;
+  if (prm->vertical_mixing != 0 || prm->river_ts_setting != 0) return FVG_ERR_UNSUPPORTED;
+  if (prm->obc_ts_type < 1 || prm->obc_ts_type > 3) return FVG_ERR_UNSUPPORTED;
+  if (f && f->ntide > kMaxTide) return FVG_ERR_UNSUPPORTED;
+  fvg_handle* h = new fvg_handle();
+  h->prm = *prm;
+  Dev& P = h->P;
+  const int M = m->m, N = m->n, KB = m->kb;
+  P.M = M; P.N = N; P.KB = KB; P.KBM1 = KB - 1; P.KBM2 = KB - 2;
+  P.NE = m->ne; P.NCV = m->ncv; P.NCV_I = m->ncv_i;
+  P.ms = (int)pad32(M + 1);
+  P.ns = (int)pad32(N + 1);
+  P.nbsn_cols = m->nbsn_cols; P.nbve_cols = m->nbve_cols; P.trie_cols = m->trie_cols;
+  P.iobcn = m->iobcn; P.numqbc = m->numqbc;
+  P.isplit = prm->isplit;
+  P.dte = prm->dte;
+  P.dti = prm->dte * (double)prm->isplit;
+  P.min_depth = prm->min_depth;
+  P.static_ssh_adj = prm->static_ssh_adj;
+  P.hprnu = prm->hprnu; P.umol = prm->umol; P.vprnu = prm->vprnu; P.cbcmin = prm->cbcmin;
+  P.fact = prm->horizontal_mixing == 0 ? 1.0 : 0.0;
+  P.fm1 = prm->horizontal_mixing == 0 ? 0.0 : 1.0;
+  P.const1 = std::pow(16.6, .6666667) * 1.00;
+  P.vhp1c = std::pow(15.8 * 100.0, 0.6666667);
+  P.wetting_drying_on = prm->wetting_drying_on;
+  P.river_location = prm->river_location;
+  P.obc_ts_type = prm->obc_ts_type;
+  h->ntide = (f && m->iobcn > 0) ? f->ntide : 0;
+  P.ntide = h->ntide;
+  P.obc_elev_on = prm->obc_elevation_forcing_on && h->ntide > 0;
+  P.have_wind = f && f->wstress_x && f->wstress_y;
+  P.sl.isplit = prm->isplit;
+  P.sl.ntide = h->ntide;
+  P.sl.len = 1 + prm->isplit + prm->isplit * 4 * h->ntide;
+  for (int j = 0; j < h->ntide; ++j) h->period.push_back(f->period[j]);
+
+  int rc = FVG_OK;
+  auto fail = [&](int code) {
+    fvg_destroy(h);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return FVG_ERR_CUDA;
+  }
+  const size_t m1 = M + 1, n1 = N + 1, e1 = m->ne + 1, v1 = m->ncv + 1, vi1 = m->ncv_i + 1;
+  const size_t o1 = m->iobcn + 1, q1 = m->numqbc + 1;
+  const size_t ms = P.ms, ns = P.ns;
+
+  // ---- index validation (FVG_ERR_BOUNDS instead of a device fault) ----
+  for (size_t i = 1; i < n1; ++i)
+    for (int j = 0; j < 3; ++j) {
+      int v = m->nv[j * n1 + i], b = m->nbe[j * n1 + i];
+      if (v < 1 || v > M || b < 0 || b > N) { h->err = "NV/NBE out of range"; return fail(FVG_ERR_BOUNDS); }
+    }
+  for (size_t e = 1; e < e1; ++e) {
+    int a = m->iec[e], b = m->iec[e1 + e], j1 = m->ienode[e], j2 = m->ienode[e1 + e];
+    if (a < 1 || a > N || b < 0 || b > N || j1 < 1 || j1 > M || j2 < 1 || j2 > M) {
+      h->err = "IEC/IENODE out of range";
+      return fail(FVG_ERR_BOUNDS);
+    }
+  }
+  for (size_t e = 1; e < v1; ++e) {
+    int a = m->niec[e], b = m->niec[v1 + e], c = m->ntrg[e];
+    if (a < 1 || a > M || b < 1 || b > M || c < 1 || c > N) { h->err = "NIEC/NTRG out of range"; return fail(FVG_ERR_BOUNDS); }
+  }
+  for (size_t i = 1; i < m1; ++i) {
+    int nt = m->ntsn[i], nv = m->ntve[i];
+    if (nt < 2 || nt > m->nbsn_cols || nv < 1 || nv + 1 > m->nbve_cols || nt - 1 > m->trie_cols || nv > m->trie_cols) {
+      h->err = "NTSN/NTVE out of range";
+      return fail(FVG_ERR_BOUNDS);
+    }
+    for (int j = 0; j < nt; ++j) {
+      int v = m->nbsn[j * m1 + i];
+      if (v < 1 || v > M) { h->err = "NBSN out of range"; return fail(FVG_ERR_BOUNDS); }
+    }
+    for (int j = 0; j < nv; ++j) {
+      int v = m->nbve[j * m1 + i];
+      if (v < 1 || v > N) { h->err = "NBVE out of range"; return fail(FVG_ERR_BOUNDS); }
+    }
+  }
+
+  // ---- mesh upload ----
+#define UPD(dst, src, n) if ((rc = upload(h, (double**)&P.dst, src, n))) return fail(rc)
+#define UPI(dst, src, n) if ((rc = upload(h, (int**)&P.dst, src, n))) return fail(rc)
+#define UP3(dst, src, rows, str) if ((rc = upload3(h, (double**)&P.dst, src, rows, KB, str))) return fail(rc)
+  UPD(vx, m->vx, m1); UPD(vy, m->vy, m1); UPD(h, m->h, m1); UPD(art1, m->art1, m1); UPD(art2, m->art2, m1);
+  UPD(grav_n, m->grav_n, m1); UPD(nn_hvc, m->nn_hvc, m1); UPD(phpn, m->phpn, m1);
+  UPI(isonb, m->isonb, m1); UPI(ntsn, m->ntsn, m1); UPI(ntve, m->ntve, m1);
+  UPI(nbsn, m->nbsn, m1 * m->nbsn_cols); UPI(nbve, m->nbve, m1 * m->nbve_cols); UPI(nbvt, m->nbvt, m1 * m->nbve_cols);
+  UPD(dltxtrie, m->dltxtrie, m1 * m->trie_cols); UPD(dltytrie, m->dltytrie, m1 * m->trie_cols);
+  UPD(dltxecec, m->dltxecec, m1 * m->trie_cols); UPD(dltyecec, m->dltyecec, m1 * m->trie_cols);
+  UPD(dltxnec, m->dltxnec, m1 * m->trie_cols); UPD(dltynec, m->dltynec, m1 * m->trie_cols);
+  UP3(z, m->z, m1, ms); UP3(zz, m->zz, m1, ms); UP3(dz, m->dz, m1, ms); UP3(dzz, m->dzz, m1, ms);
+  UPD(xc, m->xc, n1); UPD(yc, m->yc, n1); UPD(art, m->art, n1); UPD(cor, m->cor, n1);
+  UPD(grav_e, m->grav_e, n1); UPD(cc_hvc, m->cc_hvc, n1); UPD(cc_sponge, m->cc_sponge, n1);
+  UPD(cc_z0b, m->cc_z0b, n1); UPD(epor, m->epor, n1); UPD(iucp, m->iucp, n1);
+  {
+    std::vector<double> h1(m->h1, m->h1 + n1);
+    h1[0] = h1[1];  // extuv_edge.F:73
+    UPD(h1, h1.data(), n1);
+  }
+  UPI(nv, m->nv, n1 * 3); UPI(nbe, m->nbe, n1 * 3); UPI(isbce, m->isbce, n1);
+  UPD(a1u, m->a1u, n1 * 4); UPD(a2u, m->a2u, n1 * 4); UPD(awx, m->awx, n1 * 3); UPD(awy, m->awy, n1 * 3);
+  UP3(z1, m->z1, n1, ns); UP3(zz1, m->zz1, n1, ns); UP3(dz1, m->dz1, n1, ns); UP3(dzz1, m->dzz1, n1, ns);
+  UPI(iec, m->iec, e1 * 2); UPI(ienode, m->ienode, e1 * 2); UPI(isbc, m->isbc, e1);
+  UPD(xijc, m->xijc, e1); UPD(yijc, m->yijc, e1); UPD(dltxc, m->dltxc, e1); UPD(dltyc, m->dltyc, e1);
+  UPI(niec, m->niec, v1 * 2); UPI(ntrg, m->ntrg, v1); UPD(dltxe, m->dltxe, v1); UPD(dltye, m->dltye, v1);
+  UPD(dltxncve, m->dltxncve, vi1 * 2); UPD(dltyncve, m->dltyncve, vi1 * 2);
+  // Loop-invariant transcendental factors, formed on the host with the C library so they
+  // equal the values the reference recomputes each call.
+  {
+    std::vector<double> sa(n1), ca(n1), cs(m1), ss(m1);
+    for (size_t i = 0; i < n1; ++i) { sa[i] = std::sin(m->alpha[i]); ca[i] = std::cos(m->alpha[i]); }
+    for (size_t i = 0; i < m1; ++i) { cs[i] = std::cos(m->sita_gd[i]); ss[i] = std::sin(m->sita_gd[i]); }
+    UPD(sin_alpha, sa.data(), n1); UPD(cos_alpha, ca.data(), n1);
+    UPD(cos_sita, cs.data(), m1); UPD(sin_sita, ss.data(), m1);
+  }
+
+  // ---- gather lists ----
+  {
+    std::vector<std::vector<int>> nl(m1), cl(n1);
+    for (int he = 1; he <= m->ncv; ++he) {
+      nl[m->niec[he]].push_back(he * 2 + 0);
+      nl[m->niec[v1 + he]].push_back(he * 2 + 1);
+    }
+    for (int e = 1; e <= m->ne; ++e) {
+      cl[m->iec[e]].push_back(e * 2 + 0);
+      int b = m->iec[e1 + e];
+      if (b > 0) cl[b].push_back(e * 2 + 1);
+    }
+    std::vector<int> ptr, ent;
+    build_csr(nl, ptr, ent);
+    UPI(node_he_ptr, ptr.data(), ptr.size()); UPI(node_he, ent.data(), ent.size());
+    std::vector<int> ce(3 * n1, 0);
+    for (size_t i = 1; i < n1; ++i) {
+      if (cl[i].size() != 3) { h->err = "cell without exactly three edges"; return fail(FVG_ERR_BOUNDS); }
+      for (int s = 0; s < 3; ++s) ce[3 * i + s] = cl[i][s];
+    }
+    UPI(cell_edge, ce.data(), ce.size());
+  }
+  // open boundary
+  {
+    std::vector<int> node_obc(m1, 0), kind(o1, 0);
+    std::vector<std::vector<int>> co(n1);
+    for (int ob = 1; ob <= m->iobcn; ++ob) {
+      int nd = m->i_obc_n[ob];
+      if (nd < 1 || nd > M) { h->err = "I_OBC_N out of range"; return fail(FVG_ERR_BOUNDS); }
+      node_obc[nd] = ob;
+      int t = m->type_obc[ob];
+      if (t == 1 || t == 2) kind[ob] = 1;
+      else if (t == 3 || t == 4) kind[ob] = 2;
+      else { h->err = "open-boundary TYPE_OBC 5-10 not supported"; return fail(FVG_ERR_UNSUPPORTED); }
+      int na = m->nadjc_obc[ob];
+      for (int s = 0; s < na && s < 2; ++s) {
+        int c = m->adjc_obc[s * o1 + ob];
+        if (c < 1 || c > N) { h->err = "ADJC_OBC out of range"; return fail(FVG_ERR_BOUNDS); }
+        co[c].push_back(ob * 2 + s);
+      }
+      int nx = m->next_obc[ob];
+      if (nx < 1 || nx > M) { h->err = "NEXT_OBC out of range"; return fail(FVG_ERR_BOUNDS); }
+    }
+    std::vector<int> ptr, ent;
+    build_csr(co, ptr, ent);
+    UPI(node_obc, node_obc.data(), m1); UPI(obc_kind, kind.data(), o1);
+    UPI(cell_obc_ptr, ptr.data(), ptr.size()); UPI(cell_obc, ent.data(), ent.size());
+    UPI(i_obc_n, m->i_obc_n, o1); UPI(next_obc, m->next_obc, o1);
+    UPD(dltn_obc, m->dltn_obc, o1); UPD(fluxf_obc, m->fluxf_obc, o1 * 2);
+    size_t nt = h->ntide;
+    std::vector<double> apt(o1 * (nt ? nt : 1), 0.0), ph(o1 * (nt ? nt : 1), 0.0), em(o1, 0.0);
+    if (nt) {
+      for (size_t q = 0; q < o1 * nt; ++q) { apt[q] = f->apt[q]; ph[q] = f->phai[q] * kPI2 / 360.0; }
+      for (size_t q = 0; q < o1; ++q) em[q] = f->emean ? f->emean[q] : 0.0;
+    }
+    UPD(apt, apt.data(), apt.size()); UPD(phai_rad, ph.data(), ph.size()); UPD(emean, em.data(), o1);
+  }
+  // rivers
+  {
+    const int nq = m->numqbc;
+    std::vector<std::vector<int>> nr(m1), cr(n1);
+    std::vector<int> bcriv(n1, 0), skip(m1, 0);
+    for (int ob = 1; ob <= m->iobcn; ++ob) skip[m->i_obc_n[ob]] = 1;
+    for (int j = 1; j <= nq; ++j) {
+      if (prm->river_location == 0) {
+        int nd = m->inodeq[j];
+        if (nd < 1 || nd > M) { h->err = "INODEQ out of range"; return fail(FVG_ERR_BOUNDS); }
+        nr[nd].push_back(j * 2);
+        skip[nd] = 1;
+        int i1 = m->nbve[nd], i2 = m->nbve[(m->ntve[nd] - 1) * m1 + nd];
+        cr[i1].push_back(j * 2);
+        cr[i2].push_back(j * 2 + 1);
+      } else {
+        int c = m->icellq[j], a = m->n_icellq[j], b = m->n_icellq[q1 + j];
+        if (c < 1 || c > N || a < 1 || a > M || b < 1 || b > M) { h->err = "river cell out of range"; return fail(FVG_ERR_BOUNDS); }
+        nr[a].push_back(j * 2);
+        nr[b].push_back(j * 2 + 1);
+        skip[a] = 1;
+        skip[b] = 1;
+        cr[c].push_back(j * 2);
+      }
+    }
+    for (size_t i = 1; i < n1; ++i)
+      for (int j = 1; j <= nq && !bcriv[i]; ++j) {
+        bool hit;
+        if (prm->river_location == 0) {
+          int i1 = m->inodeq[j];
+          hit = (int)i == m->nbve[i1] || (int)i == m->nbve[(m->ntve[i1] - 1) * m1 + i1];
+        } else {
+          hit = (int)i == m->icellq[j];
+        }
+        if (hit) bcriv[i] = j;
+      }
+    std::vector<int> ptr, ent;
+    build_csr(nr, ptr, ent);
+    UPI(node_riv_ptr, ptr.data(), ptr.size()); UPI(node_riv, ent.data(), ent.size());
+    build_csr(cr, ptr, ent);
+    UPI(cell_riv_ptr, ptr.data(), ptr.size()); UPI(cell_riv, ent.data(), ent.size());
+    UPI(cell_bcriv, bcriv.data(), n1); UPI(riv_skip, skip.data(), m1);
+    UPI(inodeq, m->inodeq, q1); UPI(icellq, m->icellq, q1); UPI(n_icellq, m->n_icellq, q1 * 2);
+    UPD(rdisq, m->rdisq, q1 * 2); UPD(qarea, m->qarea, q1); UPD(vqdist, m->vqdist, q1 * (KB - 1));
+    std::vector<double> sq(q1), cq(q1);
+    for (size_t j = 0; j < q1; ++j) { sq[j] = std::sin(m->angleq[j]); cq[j] = std::cos(m->angleq[j]); }
+    UPD(sin_angleq, sq.data(), q1); UPD(cos_angleq, cq.data(), q1);
+    UPD(qdis0, f ? f->qdis : nullptr, q1); UPD(tdis, f ? f->tdis : nullptr, q1); UPD(sdis, f ? f->sdis : nullptr, q1);
+  }
+  UPD(wsx, P.have_wind ? f->wstress_x : nullptr, n1);
+  UPD(wsy, P.have_wind ? f->wstress_y : nullptr, n1);
+
+  // ---- state ----
+  auto reg = [&](const char* name, double** p, size_t rows, int layers, size_t stride) -> int {
+    int r = dalloc(h, p, layers == 1 ? rows : stride * layers);
+    if (r) return r;
+    h->fields[name] = FieldDesc{*p, (int64_t)rows, layers, (int64_t)(layers == 1 ? rows : stride), false};
+    return FVG_OK;
+  };
+  auto regi = [&](const char* name, int** p, size_t rows) -> int {
+    int r = dalloc(h, p, rows);
+    if (r) return r;
+    std::vector<int> ones(rows, 1);
+    cudaMemcpy(*p, ones.data(), rows * sizeof(int), cudaMemcpyHostToDevice);
+    h->fields[name] = FieldDesc{*p, (int64_t)rows, 1, (int64_t)rows, true};
+    return FVG_OK;
+  };
+#define RN2(x) if ((rc = reg(#x, &P.x, m1, 1, 0))) return fail(rc)
+#define RN3(x) if ((rc = reg(#x, &P.x, m1, KB, ms))) return fail(rc)
+#define RC2(x) if ((rc = reg(#x, &P.x, n1, 1, 0))) return fail(rc)
+#define RC3(x) if ((rc = reg(#x, &P.x, n1, KB, ns))) return fail(rc)
+  RN2(el); RN2(elf); RN2(elrk); RN2(et); RN2(d); RN2(dt); RN2(dtfa); RN2(egf); RN2(wubot_n); RN2(wvbot_n); RN2(taubm_n);
+  RN2(pfpxb_t); RN2(pfpyb_t); RN2(ah_bottom_t); RN2(pfpxb_s); RN2(pfpyb_s); RN2(ah_bottom_s);
+  RN3(t1); RN3(s1); RN3(tf1); RN3(sf1); RN3(rho1); RN3(tmean1); RN3(smean1); RN3(rmean1);
+  RN3(q2); RN3(q2l); RN3(q2f); RN3(q2lf); RN3(l); RN3(km); RN3(kh); RN3(kq); RN3(wts); RN3(viscofh);
+  RC2(el1); RC2(elf1); RC2(elrk1); RC2(et1); RC2(d1); RC2(dt1); RC2(ua); RC2(va); RC2(uaf); RC2(vaf);
+  RC2(uark); RC2(vark); RC2(uard); RC2(vard); RC2(adx2d); RC2(ady2d); RC2(drx2d); RC2(dry2d);
+  RC2(advua); RC2(advva); RC2(pstx); RC2(psty); RC2(wubot); RC2(wvbot); RC2(cbc); RC2(tps); RC2(fluxobn);
+  RC2(taubm); RC2(wusurf); RC2(wvsurf);
+  RC3(u); RC3(v); RC3(uf); RC3(vf); RC3(w); RC3(ww); RC3(advx); RC3(advy); RC3(drhox); RC3(drhoy);
+  RC3(rho); RC3(t); RC3(s); RC3(rmean); RC3(km1); RC3(viscofm);
+  if ((rc = regi("iswetn", &P.iswetn, m1))) return fail(rc);
+  if ((rc = regi("iswetnt", &P.iswetnt, m1))) return fail(rc);
+  if ((rc = regi("iswetc", &P.iswetc, n1))) return fail(rc);
+  if ((rc = regi("iswetct", &P.iswetct, n1))) return fail(rc);
+  if ((rc = regi("iswetce", &P.iswetce, n1))) return fail(rc);
+  if ((rc = reg("xflux_obcn", &P.xflux_obcn, o1, 1, 0))) return fail(rc);
+  if ((rc = reg("uard_obcn", &P.uard_obcn, o1, 1, 0))) return fail(rc);
+  if ((rc = reg("xflux_obc_t", &P.xflux_obc_t, o1, KB - 1, o1))) return fail(rc);
+  if ((rc = reg("xflux_obc_s", &P.xflux_obc_s, o1, KB - 1, o1))) return fail(rc);
+  if ((rc = reg("qdis", &P.qdis, q1, 1, 0))) return fail(rc);
+  h->fields["h1"] = FieldDesc{P.h1, (int64_t)n1, 1, (int64_t)n1, false};
+  // surface stress before the RAMP*0.001 scaling: a per-step forcing input
+  h->fields["wstress_x"] = FieldDesc{(void*)P.wsx, (int64_t)n1, 1, (int64_t)n1, false};
+  h->fields["wstress_y"] = FieldDesc{(void*)P.wsy, (int64_t)n1, 1, (int64_t)n1, false};
+  if ((rc = dalloc(h, &P.scr_xflux, ms * KB))) return fail(rc);
+  for (int t = 0; t < 2; ++t)
+    for (int g = 0; g < 6; ++g) {
+      if ((rc = dalloc(h, &P.gq[t][g], ms * KB))) return fail(rc);
+      if ((rc = dalloc(h, &P.gt[t][g], ms * KB))) return fail(rc);
+    }
+  if ((rc = dalloc(h, &P.budget, 3 + 3 * 148))) return fail(rc);
+
+  // ---- schedule ----
+  h->sched_cap = 256;
+  if ((rc = dalloc(h, &h->d_sched, (size_t)(h->sched_cap + 1) * P.sl.len))) return fail(rc);
+  if (cudaMallocHost(&h->h_sched, (size_t)(h->sched_cap + 1) * P.sl.len * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&h->h_ctl, 4 * sizeof(int)) != cudaSuccess) {
+    h->err = "cudaMallocHost failed";
+    return fail(FVG_ERR_NOMEM);
+  }
+  {
+    int* ctl;
+    if ((rc = dalloc(h, &ctl, 4))) return fail(rc);
+    P.ctl = ctl;
+  }
+  P.sched = h->d_sched;
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    h->err = "device synchronize failed after create";
+    return fail(FVG_ERR_CUDA);
+  }
+  *out = h;
+  return FVG_OK;
+}
+
+void fvg_destroy(fvg_handle* h) {
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->h_sched) cudaFreeHost(h->h_sched);
+  if (h->h_ctl) cudaFreeHost(h->h_ctl);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int64_t fvg_field_size(const fvg_handle* h, const char* name) {
+  if (!h || !name) return -1;
+  auto it = h->fields.find(name);
+  if (it == h->fields.end()) return -1;
+  return it->second.rows * it->second.layers;
+}
+
+static int field_copy(fvg_handle* h, const char* name, void* host, int64_t count, bool to_dev, bool is_int) {
+  if (!h || !name || !host) return FVG_ERR_ARG;
+  auto it = h->fields.find(name);
+  if (it == h->fields.end()) { h->err = std::string("unknown field ") + name; return FVG_ERR_ARG; }
+  const FieldDesc& fd = it->second;
+  if (fd.is_int != is_int || count != fd.rows * fd.layers) {
+    h->err = std::string("size/type mismatch for field ") + name;
+    return FVG_ERR_ARG;
+  }
+  size_t es = is_int ? sizeof(int32_t) : sizeof(double);
+  CK(cudaStreamSynchronize(h->stream));
+  if (fd.layers == 1) {
+    CK(cudaMemcpy(to_dev ? fd.d : host, to_dev ? host : fd.d, fd.rows * es,
+                  to_dev ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost));
+  } else if (to_dev) {
+    CK(cudaMemcpy2D(fd.d, fd.stride * es, host, fd.rows * es, fd.rows * es, fd.layers, cudaMemcpyHostToDevice));
+  } else {
+    CK(cudaMemcpy2D(host, fd.rows * es, fd.d, fd.stride * es, fd.rows * es, fd.layers, cudaMemcpyDeviceToHost));
+  }
+  return FVG_OK;
+}
+
+int fvg_set_field(fvg_handle* h, const char* name, const double* src, int64_t count) {
+  return field_copy(h, name, (void*)src, count, true, false);
+}
+int fvg_get_field(fvg_handle* h, const char* name, double* dst, int64_t count) {
+  return field_copy(h, name, dst, count, false, false);
+}
+int fvg_set_ifield(fvg_handle* h, const char* name, const int32_t* src, int64_t count) {
+  return field_copy(h, name, (void*)src, count, true, true);
+}
+int fvg_get_ifield(fvg_handle* h, const char* name, int32_t* dst, int64_t count) {
+  return field_copy(h, name, dst, count, false, true);
+}
+
+int fvg_set_clock(fvg_handle* h, int32_t iint, double ext_time) {
+  if (!h) return FVG_ERR_ARG;
+  h->iint = iint;
+  h->ext_time = ext_time;
+  return FVG_OK;
+}
+int fvg_get_clock(const fvg_handle* h, int32_t* iint, double* ext_time) {
+  if (!h || !iint || !ext_time) return FVG_ERR_ARG;
+  *iint = h->iint;
+  *ext_time = h->ext_time;
+  return FVG_OK;
+}
+int fvg_set_ramp(fvg_handle* h, double ramp) {
+  if (!h) return FVG_ERR_ARG;
+  h->ramp = ramp;
+  return FVG_OK;
+}
+
+// mode 0: graph replay (or plain launches when graphs are off); mode 1: plain launches
+// with events between kernel groups, accumulated into group_ms; total_ms gets the device
+// time of all steps measured with events on the handle's stream.
+static int run_steps(fvg_handle* h, int32_t nsteps, int mode, double* group_ms, double* total_ms) {
+  if (!h || nsteps < 0) return FVG_ERR_ARG;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (total_ms) {
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+  }
+  double total = 0.0;
+  const int len = h->P.sl.len;
+  int done = 0;
+  while (done < nsteps) {
+    int c = std::min(h->sched_cap, nsteps - done);
+    CK(cudaStreamSynchronize(h->stream));
+    int32_t iint = h->iint;
+    double t = h->ext_time;
+    for (int s = 0; s < c; ++s) {
+      fill_sched_row(h, h->h_sched + (size_t)s * len, iint + 1, t);
+      iint += 1;
+      for (int iext = 1; iext <= h->prm.isplit; ++iext) t = t + h->prm.dte;
+    }
+    CK(cudaMemcpyAsync(h->d_sched, h->h_sched, (size_t)c * len * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    h->h_ctl[0] = -1;
+    CK(cudaMemcpyAsync(h->P.ctl, h->h_ctl, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    if (total_ms) CK(cudaEventRecord(t0, h->stream));
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> grp;
+    for (int s = 0; s < c; ++s) {
+      if (mode == 1) {
+        Marker mk;
+        mk.ev = &ev;
+        mk.grp = &grp;
+        enqueue_internal_step(h, h->stream, mk);
+      } else if (h->use_graph) {
+        if (!h->gexec) {
+          CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+          enqueue_internal_step(h, h->stream);
+          cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
+          if (e != cudaSuccess) { h->err = std::string("graph capture: ") + cudaGetErrorString(e); return FVG_ERR_CUDA; }
+          CK(cudaGraphInstantiate(&h->gexec, h->graph, 0));
+        }
+        CK(cudaGraphLaunch(h->gexec, h->stream));
+      } else {
+        enqueue_internal_step(h, h->stream);
+      }
+    }
+    CK(cudaGetLastError());
+    if (total_ms) {
+      CK(cudaEventRecord(t1, h->stream));
+      CK(cudaEventSynchronize(t1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, t0, t1));
+      total += ms;
+    }
+    if (mode == 1) {
+      CK(cudaStreamSynchronize(h->stream));
+      for (size_t q = 1; q < ev.size(); ++q) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[q - 1], ev[q]);
+        if (grp[q] >= 0 && group_ms) group_ms[grp[q]] += ms;
+      }
+      for (auto e : ev) cudaEventDestroy(e);
+    }
+    // advance the host clock exactly as the reference accumulates ExtTime
+    for (int s = 0; s < c; ++s) {
+      h->iint += 1;
+      for (int iext = 1; iext <= h->prm.isplit; ++iext) h->ext_time = h->ext_time + h->prm.dte;
+    }
+    h->ramp = h->prm.iramp != 0 ? std::tanh((double)h->iint / (double)h->prm.iramp) : 1.0;
+    done += c;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  if (total_ms) {
+    *total_ms = total;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+  }
+  return FVG_OK;
+}
+
+int fvg_run(fvg_handle* h, int32_t nsteps) { return run_steps(h, nsteps, 0, nullptr, nullptr); }
+
+int fvg_internal_step(fvg_handle* h) { return fvg_run(h, 1); }
+
+int fvg_time_steps(fvg_handle* h, int32_t nsteps, double* ms) {
+  if (!ms) return FVG_ERR_ARG;
+  return run_steps(h, nsteps, 0, nullptr, ms);
+}
+
+int32_t fvg_profile_groups(void) { return G_COUNT; }
+
+int32_t fvg_kernels_per_step(const fvg_handle* h) {
+  if (!h) return -1;
+  const fvg_params& p = h->prm;
+  int n = 1 + 1 + 1 + 1 + 2;                                // begin, cell_pre, adv3d, baropg, int advave+reset
+  n += p.isplit * 4 * (3 + (p.wetting_drying_on ? 2 : 0)); // RK stages
+  n += 1 + 1 + 1 + 1 + 1 + 1;                              // adjust2, vertvl x2, w/viscofh, adv_uv, vdif_uv
+  n += 3;                                                  // grad_q, adv_q, vdif_q
+  if (p.temperature_active || p.salinity_active) n += 4;   // grad_ts, adv_ts, vdif_ts, bcond_ts
+  n += 1;                                                  // final
+  return n;
+}
+const char* fvg_profile_group_name(int32_t g) { return (g >= 0 && g < G_COUNT) ? kGroupNames[g] : ""; }
+
+int fvg_profile(fvg_handle* h, int32_t nsteps, double* group_ms, double* total_ms) {
+  if (!group_ms) return FVG_ERR_ARG;
+  for (int g = 0; g < G_COUNT; ++g) group_ms[g] = 0.0;
+  return run_steps(h, nsteps, 1, group_ms, total_ms);
+}
+
+int fvg_sync(fvg_handle* h) {
+  if (!h) return FVG_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  return FVG_OK;
+}
+
+int fvg_use_graph(fvg_handle* h, int32_t on) {
+  if (!h) return FVG_ERR_ARG;
+  h->use_graph = on != 0;
+  return FVG_OK;
+}
+
+int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
+  if (!h) return FVG_ERR_ARG;
+  if (r == FVG_R_INTERNAL_STEP) return fvg_run(h, 1);
+  const Dev& P = h->P;
+  const fvg_params& p = h->prm;
+  cudaStream_t s = h->stream;
+  const int len = P.sl.len;
+  const int R = h->sched_cap;
+  int iext = 1;
+  if (r == FVG_R_EXTERNAL_STEP) {
+    iext = arg;
+    h->ext_time = h->ext_time + p.dte;
+    if (p.iramp != 0) {
+      double tmp = (double)(h->iint - 1) + (double)arg / (double)p.isplit;
+      h->ramp = std::tanh(tmp / (double)p.iramp);
+    } else {
+      h->ramp = 1.0;
+    }
+  } else if (r == FVG_R_INT_FORCING) {
+    h->ramp = p.iramp != 0 ? std::tanh((double)h->iint / (double)p.iramp) : 1.0;
+  }
+  CK(cudaStreamSynchronize(s));
+  double* row = h->h_sched + (size_t)R * len;
+  fill_routine_row(h, row);
+  CK(cudaMemcpyAsync(h->d_sched + (size_t)R * len, row, len * sizeof(double), cudaMemcpyHostToDevice, s));
+  h->h_ctl[0] = R;
+  CK(cudaMemcpyAsync(P.ctl, h->h_ctl, sizeof(int), cudaMemcpyHostToDevice, s));
+  const int spc = 0;
+  switch (r) {
+    case FVG_R_EXTEL_EDGE: launch_ext_node(P, s, 1, arg, EN_EXTEL); break;
+    case FVG_R_BCOND_ELF: launch_ext_node(P, s, 1, arg, EN_BC); break;
+    case FVG_R_N2E2D_ELF: launch_ext_cell(P, s, 1, 1, EC_N2E); break;
+    case FVG_R_WET_JUDGE: launch_wet_judge(P, s); break;
+    case FVG_R_FLUX_OBN: launch_ext_cell(P, s, 1, arg, EC_FLUXOBN); break;
+    case FVG_R_ADVAVE: launch_ext_cell(P, s, 1, 1, EC_ADVAVE); break;
+    case FVG_R_EXTUV_EDGE: launch_ext_cell(P, s, 1, arg, EC_EXTUV); break;
+    case FVG_R_BCOND_UV2D: launch_ext_cell(P, s, 1, 1, EC_BC2); break;
+    case FVG_R_EXT_UPDATE: launch_ext_update(P, s, arg); break;
+    case FVG_R_EXTERNAL_STEP:
+      for (int K = 1; K <= 4; ++K) {
+        launch_ext_node(P, s, iext, K, EN_EXTEL | EN_BC | (K == 1 ? EN_COPY_ELRK : 0));
+        if (p.wetting_drying_on) launch_wet_judge(P, s);
+        launch_ext_cell(P, s, iext, K,
+                        (p.wetting_drying_on ? 0 : EC_N2E) | EC_FLUXOBN | EC_ADVAVE | EC_EXTUV | EC_BC2 |
+                            (K == 1 ? EC_COPY_RK : 0));
+        launch_ext_update(P, s, K);
+      }
+      break;
+    case FVG_R_ADJUST2D3D:
+      if (arg == 1) launch_cell_pre(P, s, CP_ADJUST1);
+      else launch_adjust2(P, s);
+      break;
+    case FVG_R_BCOND_UV3D_SOLID: launch_cell_pre(P, s, CP_BC5); break;
+    case FVG_R_BROUGH:
+      launch_cell_pre(P, s, CP_BROUGH);
+      launch_vertvl_col(P, s, VC_BOT_NODE);
+      break;
+    case FVG_R_ADVECTION3D: launch_advection3d(P, s); break;
+    case FVG_R_BAROPG:
+      launch_baropg(P, s, 1, 0);
+      launch_vertvl_col(P, s, VC_RHO_ROUNDTRIP);
+      break;
+    case FVG_R_INT_PRE_EXT:
+      launch_baropg(P, s, 0, 1);
+      launch_ext_cell(P, s, 1, 1, EC_INT_ADVAVE);
+      launch_int_reset(P, s);
+      break;
+    case FVG_R_VERTVL:
+      launch_vertvl_flux(P, s);
+      launch_vertvl_col(P, s, VC_WTS);
+      launch_w_viscofh(P, s, 1, 0);
+      break;
+    case FVG_R_VISCOFH: launch_w_viscofh(P, s, 0, 1); break;
+    case FVG_R_ADV_UV: launch_adv_uv(P, s); break;
+    case FVG_R_VDIF_UV: launch_vdif_uv(P, s, VU_VDIF); break;
+    case FVG_R_BCOND_UV3D: launch_vdif_uv(P, s, VU_BC3); break;
+    case FVG_R_WREAL: launch_vdif_uv(P, s, VU_WREAL); break;
+    case FVG_R_ADV_Q:
+      launch_grad(P, s, 0);
+      launch_adv_q(P, s, (arg == 0 ? AD_Q2 : AD_Q2L) | spc);
+      break;
+    case FVG_R_FCT_Q: launch_fct_q(P, s, arg == 0 ? AD_Q2 : AD_Q2L); break;
+    case FVG_R_VDIF_Q: launch_vdif_q(P, s, 0); break;
+    case FVG_R_TURB_UPDATE: launch_turb_update(P, s); break;
+    case FVG_R_ADV_TS:
+      launch_grad(P, s, 1);
+      launch_adv_ts(P, s, arg == 1 ? AD_T : AD_S);
+      break;
+    case FVG_R_FCT_TS: launch_fct_ts(P, s, arg == 1 ? AD_T : AD_S); break;
+    case FVG_R_VDIF_TS: launch_vdif_ts(P, s, arg == 1 ? AD_T : AD_S); break;
+    case FVG_R_BCOND_TS: launch_bcond_ts(P, s, arg == 1 ? AD_T : AD_S); break;
+    case FVG_R_TS_UPDATE: launch_final(P, s, arg == 1 ? FI_T : FI_S); break;
+    case FVG_R_DENS2: launch_final(P, s, FI_DENS); break;
+    case FVG_R_INT_FINAL: launch_final(P, s, FI_SHIFT); break;
+    case FVG_R_INT_FORCING:
+      launch_set_qdis(P, s);
+      launch_cell_pre(P, s, CP_BCOND8);
+      break;
+    default: h->err = "unknown routine"; return FVG_ERR_ARG;
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  return FVG_OK;
+}
+
+int fvg_shutdown_check(fvg_handle* h) {
+  if (!h) return FVG_ERR_ARG;
+  std::vector<double> d1(h->P.N + 1);
+  int rc = fvg_get_field(h, "d1", d1.data(), (int64_t)d1.size());
+  if (rc) return rc;
+  double s = 0.0;
+  for (int i = 1; i <= h->P.N; ++i) s = s + d1[i];
+  if (!std::isfinite(s)) { h->err = "non-finite depth (SHUTDOWN_CHECK)"; return FVG_ERR_NAN; }
+  return FVG_OK;
+}
+
+int fvg_budget(fvg_handle* h, double out[3]) {
+  if (!h || !out) return FVG_ERR_ARG;
+  launch_budget(h->P, h->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, h->P.budget, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return FVG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+// fvg_model.h - device data of one fvg_handle and the kernel entry points.
+//
+// Layout in HBM: every field keeps FVCOM's 1-based index with its ghost slot 0.  3-D
+// fields are stored layer-major ("SoA, layer-contiguous"): element (i, k) of a node
+// field at a[(k-1)*ms + i], of a cell field at a[(k-1)*ns + i], where the layer strides
+// ms >= M+1 and ns >= N+1 are rounded up to 32 elements so every layer starts on a
+// 256-byte boundary and a warp's 32 consecutive nodes/cells in one layer are one
+// coalesced 256-byte transaction.
+//
+// Scatter loops of the reference (edge -> cell, half-edge -> node) run as gathers: each
+// target owns a list of its contributing edges in ascending edge number (CSR), so every
+// sum is accumulated in exactly the reference's order and no atomics are used.
+//
+// Time-dependent scalars (RAMP of the internal and of each external step, tidal phase
+// arguments of each Runge-Kutta stage) are read from a device schedule table indexed by
+// a device step counter, so one captured CUDA graph of an internal step replays for any
+// step.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/fvg.h"
+
+namespace fvg {
+
+constexpr int kMaxTide = 8;
+
+// Per-step schedule: [ramp_int, ramp_ext[1..isplit], targ[iext][K][j]].
+struct SchedLayout {
+  int isplit, ntide, len;
+  __host__ __device__ int ramp_int() const { return 0; }
+  __host__ __device__ int ramp_ext(int iext) const { return iext; }
+  __host__ __device__ int targ(int iext, int K, int j) const {
+    return 1 + isplit + ((iext - 1) * 4 + (K - 1)) * ntide + j;
+  }
+};
+
+// Device pointers and sizes, passed by value to kernels.
+struct Dev {
+  int M, N, KB, KBM1, KBM2, NE, NCV, NCV_I, ms, ns;
+  int nbsn_cols, nbve_cols, trie_cols;
+  int iobcn, numqbc, ntide;
+  int isplit;
+  double dte, dti, min_depth, static_ssh_adj, hprnu, umol, vprnu, cbcmin;
+  double fact, fm1;
+  double const1, vhp1c;  // 16.6**0.6666667 and (15.8*100)**0.6666667 (vdif_q.F:172,227)
+  int wetting_drying_on, river_location, obc_ts_type, obc_elev_on, have_wind;
+  SchedLayout sl;
+  const double* sched;  // schedule table
+  int* ctl;             // ctl[0] = current schedule slot; ctl[1] = error word
+
+  // ----- mesh, nodes -----
+  const double *vx, *vy, *h, *art1, *art2, *grav_n, *nn_hvc, *cos_sita, *sin_sita, *phpn;
+  const int *isonb, *ntsn, *ntve, *nbsn, *nbve, *nbvt;
+  const double *dltxtrie, *dltytrie, *dltxecec, *dltyecec, *dltxnec, *dltynec;
+  const double *z, *zz, *dz, *dzz;  // 3-D node (ms stride)
+  // ----- mesh, cells -----
+  const double *xc, *yc, *art, *cor, *grav_e, *cc_hvc, *cc_sponge, *cc_z0b, *epor, *iucp;
+  const double *sin_alpha, *cos_alpha;
+  double* h1;  // H1(0) is reset by EXTUV_EDGE
+  const int *nv, *nbe, *isbce;
+  const double *a1u, *a2u, *awx, *awy;
+  const double *z1, *zz1, *dz1, *dzz1;  // 3-D cell (ns stride)
+  // ----- edges / half-edges -----
+  const int *iec, *ienode, *isbc;
+  const double *xijc, *yijc, *dltxc, *dltyc;
+  const int *niec, *ntrg;
+  const double *dltxe, *dltye, *dltxncve, *dltyncve;
+  // ----- gather lists -----
+  const int *node_he_ptr, *node_he;   // node -> half-edges (id*2 + side), ascending id
+  const int *cell_edge;               // cell -> its 3 edges (id*2 + side), ascending id
+  // ----- open boundary -----
+  const int *i_obc_n, *next_obc, *node_obc;  // node_obc[node] = OBC index (0 = none)
+  const int *obc_kind;                        // 1: specified elevation, 2: clamped
+  const double *dltn_obc;
+  const int *cell_obc_ptr, *cell_obc;         // cell -> (obc index*2 + slot)
+  const double *fluxf_obc;                    // (0:IOBCN, 2)
+  const double *apt, *phai_rad, *emean;       // (0:IOBCN, ntide)
+  // ----- rivers -----
+  const int *node_riv_ptr, *node_riv;         // node -> (river*2 + which) in order
+  const int *cell_riv_ptr, *cell_riv;         // cell -> river momentum entries in order
+  const int *inodeq, *icellq, *n_icellq;
+  const double *rdisq, *qarea, *sin_angleq, *cos_angleq, *vqdist, *qdis0, *tdis, *sdis;
+  const int *riv_skip;                        // node is an OBC or river node (FCT skip)
+  const int *cell_bcriv;                      // first river whose inflow cell this is (BCOND_GCN 2/3/5)
+  // ----- forcing -----
+  const double *wsx, *wsy;
+
+  // ----- state, node 2-D -----
+  double *el, *elf, *elrk, *et, *d, *dt, *dtfa, *egf, *wubot_n, *wvbot_n, *taubm_n;
+  double *pfpxb_t, *pfpyb_t, *ah_bottom_t, *pfpxb_s, *pfpyb_s, *ah_bottom_s;
+  // node 3-D
+  double *t1, *s1, *tf1, *sf1, *rho1, *tmean1, *smean1, *rmean1;
+  double *q2, *q2l, *q2f, *q2lf, *l, *km, *kh, *kq, *wts, *viscofh;
+  // cell 2-D
+  double *el1, *elf1, *elrk1, *et1, *d1, *dt1, *ua, *va, *uaf, *vaf, *uark, *vark;
+  double *uard, *vard, *adx2d, *ady2d, *drx2d, *dry2d, *advua, *advva, *pstx, *psty;
+  double *wubot, *wvbot, *cbc, *tps, *fluxobn, *taubm, *wusurf, *wvsurf;
+  // cell 3-D
+  double *u, *v, *uf, *vf, *w, *ww, *advx, *advy, *drhox, *drhoy, *rho, *t, *s, *rmean;
+  double *km1, *viscofm;
+  // wet/dry
+  int *iswetn, *iswetnt, *iswetc, *iswetct, *iswetce;
+  // open boundary
+  double *xflux_obcn, *uard_obcn, *xflux_obc_t, *xflux_obc_s;
+  // river discharge after the ramp
+  double* qdis;
+  // scratch (node 3-D)
+  double *scr_xflux;                         // VERTVL flux
+  double *gq[2][6];  // ADV_Q of Q2 / Q2L: PQPX, PQPY, PQPXD, PQPYD, ring min, ring max
+  double *gt[2][6];  // ADV_T / ADV_S: the same six per tracer
+  double* budget;                            // 3 doubles
+};
+
+// index helpers
+__host__ __device__ inline size_t N3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ms + i; }
+__host__ __device__ inline size_t C3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ns + i; }
+
+// Fortran SIGN(1.0, x) for a processor that does not distinguish negative zero.
+__host__ __device__ inline double fsign1(double x) { return x >= 0.0 ? 1.0 : -1.0; }
+
+extern const double kAlphaRK[5];
+
+// ---------------- external mode (k_ext.cu) ----------------
+enum ExtNodeParts { EN_EXTEL = 1, EN_BC = 2, EN_COPY_ELRK = 4 };
+enum ExtCellParts { EC_N2E = 1, EC_FLUXOBN = 2, EC_ADVAVE = 4, EC_EXTUV = 8, EC_BC2 = 16, EC_COPY_RK = 32,
+                    EC_INT_ADVAVE = 64 };
+void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts);
+void launch_wet_judge(const Dev& P, cudaStream_t s);
+void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts);
+void launch_ext_update(const Dev& P, cudaStream_t s, int K);
+void launch_begin_step(const Dev& P, cudaStream_t s);
+void launch_set_qdis(const Dev& P, cudaStream_t s);
+
+// ---------------- 3-D momentum (k_mom3d.cu) ----------------
+enum CellPreParts { CP_ADJUST1 = 1, CP_BC5 = 2, CP_BCOND8 = 4, CP_BROUGH = 8 };
+void launch_cell_pre(const Dev& P, cudaStream_t s, int parts);
+void launch_advection3d(const Dev& P, cudaStream_t s);
+void launch_baropg(const Dev& P, cudaStream_t s, int do_baropg, int do_sums);
+void launch_int_reset(const Dev& P, cudaStream_t s);
+void launch_adjust2(const Dev& P, cudaStream_t s);
+void launch_vertvl_flux(const Dev& P, cudaStream_t s);
+enum VertvlColParts { VC_WTS = 1, VC_WD2 = 2, VC_RHO_ROUNDTRIP = 4, VC_BOT_NODE = 8 };
+void launch_vertvl_col(const Dev& P, cudaStream_t s, int parts);
+void launch_w_viscofh(const Dev& P, cudaStream_t s, int do_w, int do_visc);
+void launch_adv_uv(const Dev& P, cudaStream_t s);
+enum VdifUvParts { VU_VDIF = 1, VU_BC3 = 2, VU_WREAL = 4 };
+void launch_vdif_uv(const Dev& P, cudaStream_t s, int parts);
+
+// ---------------- scalars and turbulence (k_scalar.cu) ----------------
+void launch_grad(const Dev& P, cudaStream_t s, int which);  // 0: q2+q2l, 1: T+S
+enum AdvParts { AD_Q2 = 1, AD_Q2L = 2, AD_FCT = 4, AD_T = 8, AD_S = 16 };
+void launch_adv_q(const Dev& P, cudaStream_t s, int parts);
+void launch_fct_q(const Dev& P, cudaStream_t s, int parts);
+void launch_vdif_q(const Dev& P, cudaStream_t s, int copy_back);
+void launch_turb_update(const Dev& P, cudaStream_t s);
+void launch_adv_ts(const Dev& P, cudaStream_t s, int parts);
+void launch_fct_ts(const Dev& P, cudaStream_t s, int parts);
+void launch_vdif_ts(const Dev& P, cudaStream_t s, int parts);
+void launch_bcond_ts(const Dev& P, cudaStream_t s, int parts);
+enum FinalParts { FI_T = 1, FI_S = 2, FI_DENS = 4, FI_KM1 = 8, FI_SHIFT = 16 };
+void launch_final(const Dev& P, cudaStream_t s, int parts);
+void launch_budget(const Dev& P, cudaStream_t s);
+
+}  // namespace fvg

@@ -1,0 +1,379 @@
+// k_ext.cu - external (2-D) mode kernels: one EXTERNAL_STEP Runge-Kutta stage is
+//   k_ext_node   EXTEL_EDGE(K) + BCOND_GCN(1,K) + RK blend      (per node, half-edge gather)
+//   k_wet_*      WET_JUDGE                                      (wetting/drying only)
+//   k_ext_cell   N2E2D + FLUX_OBN + ADVAVE_EDGE_GCN + EXTUV_EDGE + BCOND_GCN(2,K)  (per cell)
+//   k_ext_update external_step.F:333-436 (EL=ELF, D, D1, UA=UAF, UARD/EGF sums)
+// Reference: FVCOM_source/external_step.F:30-443 and the routines cited per kernel.
+// Arithmetic is kept in the reference's expression order; the library is compiled with
+// --fmad=false so no multiply-add is contracted.
+#include "fvg_model.h"
+
+namespace fvg {
+
+__device__ __constant__ double dAlphaRK[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
+const double kAlphaRK[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
+#define ONE_THIRD (1.0 / 3.0)
+
+__device__ inline const double* sched_row(const Dev& P) {
+  return P.sched + (size_t)P.ctl[0] * P.sl.len;
+}
+
+// -------------------------------------------------------------------------------------
+// EXTEL_EDGE(K) (extel_edge.F:76-180) and BCOND_GCN(1,K) -> BCOND_ASL/BCOND_ASL_CLP
+// (mod_obcs.F:509-617) with the Runge-Kutta blend of the specified-elevation nodes
+// (external_step.F:262-266).  One thread per node; the node's control-volume half-edges
+// are gathered in ascending half-edge number, the order of the reference's scatter.
+// -------------------------------------------------------------------------------------
+__global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  if (parts & EN_COPY_ELRK) P.elrk[i] = P.el[i];
+  const double alpha = dAlphaRK[K];
+  int ob = P.node_obc[i];
+  if (parts & EN_EXTEL) {
+    double x = 0.0;
+    for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
+      int e = P.node_he[q];
+      int he = e >> 1;
+      int c = P.ntrg[he];
+      double exflux = P.d1[c] * (-P.ua[c] * P.dltye[he] + P.va[c] * P.dltxe[he]);
+      x = (e & 1) ? x + exflux : x - exflux;
+    }
+    if (ob > 0) {
+      P.xflux_obcn[ob] = x;
+      x = 0.0;
+    }
+    for (int q = P.node_riv_ptr[i]; q < P.node_riv_ptr[i + 1]; ++q) {
+      int r = P.node_riv[q];
+      int j = r >> 1;
+      if (P.river_location == 0)
+        x = x - P.qdis[j];
+      else
+        x = x - P.qdis[j] * P.rdisq[(size_t)(r & 1) * (P.numqbc + 1) + j];
+    }
+    double dtk = alpha * P.dte;
+    P.elf[i] = P.elrk[i] - dtk * x / P.art1[i];
+  }
+  if ((parts & EN_BC) && ob > 0) {
+    int kind = P.obc_kind[ob];
+    if (kind == 1) {
+      if (P.obc_elev_on) {
+        const double* row = sched_row(P);
+        double force = 0.0;
+        for (int j = 0; j < P.ntide; ++j) {
+          size_t q = (size_t)j * (P.iobcn + 1) + ob;
+          double targ = row[P.sl.targ(iext, K, j)];
+          force = P.apt[q] * cos(targ - P.phai_rad[q]) + force;
+        }
+        force = force + P.emean[ob];
+        P.elf[i] = force * row[P.sl.ramp_ext(iext)];
+      }
+      P.elf[i] = P.elrk[i] + alpha * (P.elf[i] - P.elrk[i]);
+    } else if (kind == 2) {
+      P.elf[i] = 0.0;
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// WET_JUDGE (mod_wd.F:193-284) in two passes.  Cells first: the cell flag uses the
+// unclamped ELF of its nodes, and ELF1 is the mean of the clamped ELF, which each cell
+// forms itself from h and ELF.  Then nodes: the node flag and the clamp of ELF.
+// -------------------------------------------------------------------------------------
+__global__ void k_wet_cells(const Dev P) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  int n1 = P.nv[i], n2 = P.nv[(size_t)(P.N + 1) + i], n3 = P.nv[(size_t)2 * (P.N + 1) + i];
+  double e1 = P.elf[n1], e2 = P.elf[n2], e3 = P.elf[n3];
+  double dtmp = fmax(fmax(e1, e2), e3) + fmin(fmin(P.h[n1], P.h[n2]), P.h[n3]);
+  P.iswetc[i] = ((dtmp - P.min_depth) < 1.0e-5) ? 0 : 1;
+  double c1 = fmax(e1, -P.h[n1] + P.min_depth);
+  double c2 = fmax(e2, -P.h[n2] + P.min_depth);
+  double c3 = fmax(e3, -P.h[n3] + P.min_depth);
+  P.elf1[i] = ONE_THIRD * (c1 + c2 + c3);
+}
+
+__global__ void k_wet_nodes(const Dev P) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  double e = P.elf[i];
+  int wet = ((P.h[i] + e - P.min_depth) < 1.0e-5) ? 0 : 1;
+  int s = 0;
+  for (int j = 1; j <= P.ntve[i]; ++j) s += P.iswetc[P.nbve[(size_t)(j - 1) * (P.M + 1) + i]];
+  if (s == 0) wet = 0;
+  P.iswetn[i] = wet;
+  P.elf[i] = fmax(e, -P.h[i] + P.min_depth);
+}
+
+// -------------------------------------------------------------------------------------
+// Least-squares velocity gradient of one cell from itself and its three neighbours
+// (advave_edge_gcn.F:634-637, 699-702): COFA1/COFA2 for UA, COFA5/COFA6 for VA.
+// -------------------------------------------------------------------------------------
+struct Grad {
+  double ux, uy, vx, vy;
+};
+
+__device__ inline Grad cell_grad(const Dev& P, int c, const double* U, const double* V) {
+  const size_t n1 = P.N + 1;
+  int k1 = P.nbe[c], k2 = P.nbe[n1 + c], k3 = P.nbe[2 * n1 + c];
+  double a1 = P.a1u[c], a2 = P.a1u[n1 + c], a3 = P.a1u[2 * n1 + c], a4 = P.a1u[3 * n1 + c];
+  double b1 = P.a2u[c], b2 = P.a2u[n1 + c], b3 = P.a2u[2 * n1 + c], b4 = P.a2u[3 * n1 + c];
+  double u0 = U[c], u1 = U[k1], u2 = U[k2], u3 = U[k3];
+  double v0 = V[c], v1 = V[k1], v2 = V[k2], v3 = V[k3];
+  Grad g;
+  g.ux = a1 * u0 + a2 * u1 + a3 * u2 + a4 * u3;
+  g.uy = b1 * u0 + b2 * u1 + b3 * u2 + b4 * u3;
+  g.vx = a1 * v0 + a2 * v1 + a3 * v2 + a4 * v3;
+  g.vy = b1 * v0 + b2 * v1 + b3 * v2 + b4 * v3;
+  return g;
+}
+
+// ADVAVE_EDGE_GCN for one cell (advave_edge_gcn.F:115-1003, LIMITED_NO branch).
+__device__ inline void advave_cell(const Dev& P, int i, double& xf, double& yf, double& px, double& py) {
+  xf = 0.0; yf = 0.0; px = 0.0; py = 0.0;
+  const size_t e1 = P.NE + 1;
+  for (int s = 0; s < 3; ++s) {
+    int code = P.cell_edge[3 * i + s];
+    int e = code >> 1;
+    int side = code & 1;
+    int ia = P.iec[e], ib = P.iec[e1 + e];
+    int j1 = P.ienode[e], j2 = P.ienode[e1 + e];
+    double dij = 0.5 * (P.d[j1] + P.d[j2]);
+    double elij = 0.5 * (P.el[j1] + P.el[j2]);
+    if (P.iswetce[ia] * P.iswetc[ia] == 1 || P.iswetce[ib] * P.iswetc[ib] == 1) {
+      Grad ga = cell_grad(P, ia, P.ua, P.va);
+      double xij = P.xijc[e] - P.xc[ia];
+      double yij = P.yijc[e] - P.yc[ia];
+      double uij1 = P.ua[ia] + ga.ux * xij + ga.uy * yij;
+      double vij1 = P.va[ia] + ga.vx * xij + ga.vy * yij;
+      Grad gb = cell_grad(P, ib, P.ua, P.va);
+      xij = P.xijc[e] - P.xc[ib];
+      yij = P.yijc[e] - P.yc[ib];
+      double uij2 = P.ua[ib] + gb.ux * xij + gb.uy * yij;
+      double vij2 = P.va[ib] + gb.vx * xij + gb.vy * yij;
+      double uij = 0.5 * (uij1 + uij2);
+      double vij = 0.5 * (vij1 + vij2);
+      double un = -uij * P.dltyc[e] + vij * P.dltxc[e];
+      double viscof1 = P.art[ia] * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + 0.5 * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
+      double viscof2 = P.art[ib] * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + 0.5 * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
+      double viscof = (P.fact * 0.5 * (viscof1 * P.cc_hvc[ia] + viscof2 * P.cc_hvc[ib]) +
+                       P.fm1 * 0.5 * (P.cc_hvc[ia] + P.cc_hvc[ib])) / P.hprnu;
+      double txx = (ga.ux + gb.ux) * viscof;
+      double tyy = (ga.vy + gb.vy) * viscof;
+      double txy = 0.5 * (ga.uy + gb.uy + ga.vx + gb.vx) * viscof;
+      double fxx = dij * (txx * P.dltyc[e] - txy * P.dltxc[e]);
+      double fyy = dij * (txy * P.dltyc[e] - tyy * P.dltxc[e]);
+      double sg = fsign1(un);
+      double xadv = dij * un * ((1.0 - sg) * uij2 + (1.0 + sg) * uij1) * 0.5;
+      double yadv = dij * un * ((1.0 - sg) * vij2 + (1.0 + sg) * vij1) * 0.5;
+      double nb = 1.0 - (double)P.isbc[e];
+      if (side == 0) {
+        xf = xf + (xadv + fxx * P.epor[i]) * nb * P.iucp[i];
+        yf = yf + (yadv + fyy * P.epor[i]) * nb * P.iucp[i];
+      } else {
+        xf = xf - (xadv + fxx * P.epor[i]) * nb * P.iucp[i];
+        yf = yf - (yadv + fyy * P.epor[i]) * nb * P.iucp[i];
+      }
+    }
+    if (side == 0) {
+      px = px - P.grav_e[i] * P.d1[i] * elij * P.dltyc[e];
+      py = py + P.grav_e[i] * P.d1[i] * elij * P.dltxc[e];
+    } else {
+      px = px + P.grav_e[i] * P.d1[i] * elij * P.dltyc[e];
+      py = py - P.grav_e[i] * P.d1[i] * elij * P.dltxc[e];
+    }
+  }
+  double w = (double)(P.iswetce[i] * P.iswetc[i]);
+  xf = xf * w;
+  yf = yf * w;
+}
+
+// FLUX_OBN (mod_obcs.F:1181-1215) value on one open-boundary cell.
+__device__ inline double fluxobn_cell(const Dev& P, int i, int K) {
+  double f = 0.0;
+  for (int q = P.cell_obc_ptr[i]; q < P.cell_obc_ptr[i + 1]; ++q) {
+    int code = P.cell_obc[q];
+    int ob = code >> 1, slot = code & 1;
+    int j = P.i_obc_n[ob];
+    double flux = -(P.elf[j] - P.elrk[j]) * P.art1[j] / (dAlphaRK[K] * P.dte) - P.xflux_obcn[ob];
+    f = f + P.fluxf_obc[(size_t)slot * (P.iobcn + 1) + ob] * flux;
+  }
+  return f;
+}
+
+// River clamp / tangential projection of a solid-boundary cell (bcond_gcn.F:345-405).
+__device__ inline void bc_solid(const Dev& P, int i, int rj, double& uu, double& vv) {
+  if (rj > 0) {
+    double ca = P.cos_angleq[rj], sa = P.sin_angleq[rj];
+    double untmp = uu * ca + vv * sa;
+    double vntmp = -uu * sa + vv * ca;
+    untmp = fmax(untmp, 0.0);
+    uu = untmp * ca - vntmp * sa;
+    vv = untmp * sa + vntmp * ca;
+  } else {
+    double sa = P.sin_alpha[i], ca = P.cos_alpha[i];
+    double ui = uu * (sa * sa) - vv * sa * ca;
+    double vi = -uu * sa * ca + vv * (ca * ca);
+    uu = ui;
+    vv = vi;
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Per-cell part of one RK stage.  EC_INT_ADVAVE is the internal-step call of ADVAVE
+// followed by ADX2D -= ADVUA (internal_step.F:387-392).
+// -------------------------------------------------------------------------------------
+__global__ void k_ext_cell(const Dev P, int iext, int K, int parts) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  const size_t n1 = P.N + 1;
+  if (parts & EC_COPY_RK) {
+    P.uark[i] = P.ua[i];
+    P.vark[i] = P.va[i];
+    P.elrk1[i] = P.el1[i];
+  }
+  if (parts & EC_N2E)
+    P.elf1[i] = ONE_THIRD * (P.elf[P.nv[i]] + P.elf[P.nv[n1 + i]] + P.elf[P.nv[2 * n1 + i]]);
+  double fob = 0.0;
+  if (parts & EC_FLUXOBN) {
+    fob = fluxobn_cell(P, i, K);
+    P.fluxobn[i] = fob;
+  } else if (P.isbce[i] == 2) {
+    fob = P.fluxobn[i];
+  }
+  double xf, yf, px, py;
+  if (parts & (EC_ADVAVE | EC_INT_ADVAVE)) {
+    advave_cell(P, i, xf, yf, px, py);
+    if (P.isbce[i] == 2) {
+      xf = (xf + fob * P.ua[i]) * P.iucp[i];
+      yf = (yf + fob * P.va[i]) * P.iucp[i];
+    }
+    for (int q = P.cell_riv_ptr[i]; q < P.cell_riv_ptr[i + 1]; ++q) {
+      int k = P.cell_riv[q] >> 1;
+      double vlctyq = P.qdis[k] / P.qarea[k];
+      if (P.river_location == 0) {
+        xf = xf - 0.5 * P.qdis[k] * vlctyq * P.cos_angleq[k];
+        yf = yf - 0.5 * P.qdis[k] * vlctyq * P.sin_angleq[k];
+      } else {
+        double temp = P.qdis[k] * vlctyq;
+        xf = xf - temp * P.cos_angleq[k];
+        yf = yf - temp * P.sin_angleq[k];
+      }
+    }
+    P.advua[i] = xf;
+    P.advva[i] = yf;
+    P.pstx[i] = px;
+    P.psty[i] = py;
+    if (parts & EC_INT_ADVAVE) {
+      P.adx2d[i] = P.adx2d[i] - xf;
+      P.ady2d[i] = P.ady2d[i] - yf;
+    }
+  } else {
+    xf = P.advua[i];
+    yf = P.advva[i];
+    px = P.pstx[i];
+    py = P.psty[i];
+  }
+  if (parts & (EC_EXTUV | EC_BC2)) {
+    double uaf, vaf;
+    if (parts & EC_EXTUV) {
+      // EXTUV_EDGE(K) (extuv_edge.F:106-163)
+      if (P.iswetce[i] * P.iswetc[i] == 1) {
+        double ramp = sched_row(P)[P.sl.ramp_ext(iext)];
+        double wus = P.have_wind ? P.wsx[i] * ramp * 0.001 : 0.0;
+        double wvs = P.have_wind ? P.wsy[i] * ramp * 0.001 : 0.0;
+        double resx = P.adx2d[i] + xf + P.drx2d[i] + px - P.cor[i] * P.va[i] * P.d1[i] * P.art[i] -
+                      (wus + P.wubot[i]) * P.art[i];
+        double resy = P.ady2d[i] + yf + P.dry2d[i] + py + P.cor[i] * P.ua[i] * P.d1[i] * P.art[i] -
+                      (wvs + P.wvbot[i]) * P.art[i];
+        double a = dAlphaRK[K];
+        uaf = (P.uark[i] * (P.h1[i] + P.elrk1[i]) - a * P.dte * resx / P.art[i]) / (P.h1[i] + P.elf1[i]);
+        vaf = (P.vark[i] * (P.h1[i] + P.elrk1[i]) - a * P.dte * resy / P.art[i]) / (P.h1[i] + P.elf1[i]);
+      } else {
+        uaf = 0.0;
+        vaf = 0.0;
+      }
+      uaf = uaf / (1.0 + P.cc_sponge[i] * (uaf * uaf));
+      vaf = vaf / (1.0 + P.cc_sponge[i] * (vaf * vaf));
+    } else {
+      uaf = P.uaf[i];
+      vaf = P.vaf[i];
+    }
+    if (parts & EC_BC2) {
+      // BCOND_GCN(2,K) (bcond_gcn.F:325-406)
+      int b = P.isbce[i];
+      if (b == 3) { uaf = 0.0; vaf = 0.0; }
+      if (b == 1) bc_solid(P, i, P.cell_bcriv[i], uaf, vaf);
+    }
+    P.uaf[i] = uaf;
+    P.vaf[i] = vaf;
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// external_step.F:333-436: EL=ELF, EL1=N2E2D(EL), D, D1, UA=UAF, DTFA, the K==3 sums
+// for the 3-D correction, the K==4 open-boundary transport and WD_UPDATE(1).
+// -------------------------------------------------------------------------------------
+__global__ void k_ext_update(const Dev P, int K) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i <= P.M) {
+    double e = P.elf[i];
+    P.el[i] = e;
+    double dd = P.h[i] + e;
+    P.d[i] = dd;
+    P.dtfa[i] = dd;
+    if (K == 3) P.egf[i] = P.egf[i] + e / (double)P.isplit;
+    if (K == 4) {
+      int ob = P.node_obc[i];
+      if (ob > 0) {
+        double tmp = -(P.elf[i] - P.elrk[i]) * P.art1[i] / P.dte - P.xflux_obcn[ob];
+        P.uard_obcn[ob] = P.uard_obcn[ob] + tmp / (double)(float)P.isplit;
+      }
+    }
+  }
+  if (i <= P.N) {
+    double e1 = P.elf1[i];
+    P.el1[i] = e1;
+    double dd1 = P.h1[i] + e1;
+    P.d1[i] = dd1;
+    double u = P.uaf[i], v = P.vaf[i];
+    P.ua[i] = u;
+    P.va[i] = v;
+    if (K == 3) {
+      P.uard[i] = P.uard[i] + u * dd1;
+      P.vard[i] = P.vard[i] + v * dd1;
+    }
+    if (P.wetting_drying_on) P.iswetce[i] = P.iswetc[i];
+  }
+}
+
+// Start of an internal step: advance the schedule slot, then BCOND_GCN(8,0)'s river ramp
+// QDIS = QDIS*RAMP (bcond_gcn.F:645-648).
+__global__ void k_begin_step(const Dev P, int advance) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int slot = P.ctl[0] + advance;
+  P.ctl[0] = slot;
+  double ramp = P.sched[(size_t)slot * P.sl.len];
+  for (int j = 1; j <= P.numqbc; ++j) P.qdis[j] = P.qdis0[j] * ramp;
+}
+
+static inline int nblk(int n, int b) { return (n + b - 1) / b; }
+
+void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
+  k_ext_node<<<nblk(P.M, 256), 256, 0, s>>>(P, iext, K, parts);
+}
+void launch_wet_judge(const Dev& P, cudaStream_t s) {
+  k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);
+  k_wet_nodes<<<nblk(P.M, 256), 256, 0, s>>>(P);
+}
+void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
+  k_ext_cell<<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
+}
+void launch_ext_update(const Dev& P, cudaStream_t s, int K) {
+  int n = P.M > P.N ? P.M : P.N;
+  k_ext_update<<<nblk(n, 256), 256, 0, s>>>(P, K);
+}
+void launch_begin_step(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 1); }
+void launch_set_qdis(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 0); }
+
+}  // namespace fvg

@@ -1,0 +1,716 @@
+// k_mom3d.cu - internal-mode (3-D) momentum kernels of INTERNAL_STEP
+// (FVCOM_source/internal_step.F:29-1607): ADJUST2D3D, BCOND_GCN(5/8), BOTTOM_ROUGHNESS,
+// ADVECTION_EDGE_GCN, BAROPG, VERTVL_EDGE, VISCOF_H, ADV_UV_EDGE_GCN, VDIF_UV,
+// BCOND_GCN(3), WREAL.
+//
+// Thread shapes: column kernels (vertical prefix sums and tridiagonal solves) run one
+// thread per cell or node looping over the layers; layer-parallel gathers run on 32 x 8
+// blocks (32 consecutive cells/nodes of one layer per warp, 8 layers per block) so a warp
+// reads one coalesced 256-byte row of each field and the 2-D mesh metrics it needs are
+// shared by the eight warps through L1.
+#include "fvg_model.h"
+
+namespace fvg {
+
+#define ONE_THIRD (1.0 / 3.0)
+constexpr int kMaxKB = 64;
+__device__ __constant__ double dAlpha3[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
+
+static inline int nblk(int n, int b) { return (n + b - 1) / b; }
+
+__device__ inline double ramp_int(const Dev& P) { return P.sched[(size_t)P.ctl[0] * P.sl.len]; }
+
+// River clamp / tangential projection (bcond_gcn.F:345-405, 443-499, 552-608).
+__device__ inline void bc_solid3(const Dev& P, int i, double& uu, double& vv) {
+  int rj = P.cell_bcriv[i];
+  if (rj > 0) {
+    double ca = P.cos_angleq[rj], sa = P.sin_angleq[rj];
+    double untmp = uu * ca + vv * sa;
+    double vntmp = -uu * sa + vv * ca;
+    untmp = fmax(untmp, 0.0);
+    uu = untmp * ca - vntmp * sa;
+    vv = untmp * sa + vntmp * ca;
+  } else {
+    double sa = P.sin_alpha[i], ca = P.cos_alpha[i];
+    double ui = uu * (sa * sa) - vv * sa * ca;
+    double vi = -uu * sa * ca + vv * (ca * ca);
+    uu = ui;
+    vv = vi;
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// ADJUST2D3D(1) (adjust2d3d.F:57-63), BCOND_GCN(5,0) (bcond_gcn.F:537-611),
+// BCOND_GCN(8,0) wind (bcond_gcn.F:661-683), BOTTOM_ROUGHNESS cell part (brough.F:76-193).
+// One thread per cell column.
+// -------------------------------------------------------------------------------------
+__global__ void k_cell_pre(const Dev P, int parts) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  const int KBM1 = P.KBM1;
+  if (parts & CP_ADJUST1) {
+    double uac = 0.0, vac = 0.0;
+    for (int k = 1; k <= KBM1; ++k) uac = uac + P.u[C3(P, i, k)] * P.dz1[C3(P, i, k)];
+    for (int k = 1; k <= KBM1; ++k) vac = vac + P.v[C3(P, i, k)] * P.dz1[C3(P, i, k)];
+    double du = 1.0 * (P.ua[i] - uac), dv = 1.0 * (P.va[i] - vac);
+    for (int k = 1; k <= KBM1; ++k) {
+      P.u[C3(P, i, k)] = P.u[C3(P, i, k)] + du;
+      P.v[C3(P, i, k)] = P.v[C3(P, i, k)] + dv;
+    }
+  }
+  if (parts & CP_BC5) {
+    int b = P.isbce[i];
+    if (b == 3 || b == 1) {
+      for (int k = 1; k <= KBM1; ++k) {
+        size_t q = C3(P, i, k);
+        double uu = P.u[q], vv = P.v[q];
+        if (b == 3) { uu = 0.0; vv = 0.0; }
+        else bc_solid3(P, i, uu, vv);
+        P.u[q] = uu;
+        P.v[q] = vv;
+      }
+    }
+  }
+  if ((parts & CP_BCOND8) && P.have_wind) {
+    double ramp = ramp_int(P);
+    P.wusurf[i] = -P.wsx[i] * ramp * 0.001;
+    P.wvsurf[i] = -P.wsy[i] * ramp * 0.001;
+  }
+  if (parts & CP_BROUGH) {
+    const double VK2 = 0.160;
+    double zb = P.zz1[C3(P, i, KBM1)] - P.z1[C3(P, i, P.KB)];
+    double lg = (P.dt1[i] > 3.0) ? log(zb * P.dt1[i] / P.cc_z0b[i]) : log(zb * 3.0 / P.cc_z0b[i]);
+    double cbc = VK2 / (lg * lg);
+    if (cbc < P.cbcmin) cbc = P.cbcmin;
+    P.cbc[i] = cbc;
+    double ub = P.u[C3(P, i, KBM1)], vb = P.v[C3(P, i, KBM1)];
+    double btps = cbc * sqrt(ub * ub + vb * vb);
+    double wu = -btps * ub, wv = -btps * vb;
+    double cff = 0.75 * P.dz1[C3(P, i, KBM1)] * P.d1[i];
+    wu = (wu >= 0.0 ? 1.0 : -1.0) * fmin(fabs(wu), fabs(ub * cff / P.dti));
+    wv = (wv >= 0.0 ? 1.0 : -1.0) * fmin(fabs(wv), fabs(vb * cff / P.dti));
+    P.wubot[i] = wu;
+    P.wvbot[i] = wv;
+    P.taubm[i] = sqrt(wu * wu + wv * wv);
+  }
+}
+
+// Least-squares gradient of U,V on layer k (advection_edge_gcn.F:533-536).
+struct G3 {
+  double ux, uy, vx, vy;
+};
+__device__ inline G3 grad3(const Dev& P, int c, const double* U, const double* V) {
+  const size_t n1 = P.N + 1;
+  int k1 = P.nbe[c], k2 = P.nbe[n1 + c], k3 = P.nbe[2 * n1 + c];
+  double a1 = P.a1u[c], a2 = P.a1u[n1 + c], a3 = P.a1u[2 * n1 + c], a4 = P.a1u[3 * n1 + c];
+  double b1 = P.a2u[c], b2 = P.a2u[n1 + c], b3 = P.a2u[2 * n1 + c], b4 = P.a2u[3 * n1 + c];
+  double u0 = U[c], u1 = U[k1], u2 = U[k2], u3 = U[k3];
+  double v0 = V[c], v1 = V[k1], v2 = V[k2], v3 = V[k3];
+  G3 g;
+  g.ux = a1 * u0 + a2 * u1 + a3 * u2 + a4 * u3;
+  g.uy = b1 * u0 + b2 * u1 + b3 * u2 + b4 * u3;
+  g.vx = a1 * v0 + a2 * v1 + a3 * v2 + a4 * v3;
+  g.vy = b1 * v0 + b2 * v1 + b3 * v2 + b4 * v3;
+  return g;
+}
+
+// Horizontal flux of one edge on one layer (advection_edge_gcn.F:449-603 and
+// adv_uv_edge_gcn.F:580-779 share this body).  Returns whether the edge is active
+// (at least one wet side) and its upwind/viscous pieces.
+struct EdgeFlux {
+  double xadv, yadv, fxx, fyy, viscof;
+};
+
+__device__ inline EdgeFlux edge_flux3(const Dev& P, int e, int ia, int ib, int k, double dij, bool exflux_form) {
+  const double* U = P.u + C3(P, 0, k);
+  const double* V = P.v + C3(P, 0, k);
+  double xija = P.xijc[e] - P.xc[ia], yija = P.yijc[e] - P.yc[ia];
+  double xijb = P.xijc[e] - P.xc[ib], yijb = P.yijc[e] - P.yc[ib];
+  G3 ga = grad3(P, ia, U, V);
+  double uij1 = U[ia] + ga.ux * xija + ga.uy * yija;
+  double vij1 = V[ia] + ga.vx * xija + ga.vy * yija;
+  G3 gb = grad3(P, ib, U, V);
+  double uij2 = U[ib] + gb.ux * xijb + gb.uy * yijb;
+  double vij2 = V[ib] + gb.vx * xijb + gb.vy * yijb;
+  double uij = 0.5 * (uij1 + uij2);
+  double vij = 0.5 * (vij1 + vij2);
+  double viscof1 = P.art[ia] * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + 0.5 * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
+  double viscof2 = P.art[ib] * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + 0.5 * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
+  double viscof = (P.fact * 0.5 * (viscof1 * P.cc_hvc[ia] + viscof2 * P.cc_hvc[ib]) +
+                   P.fm1 * 0.5 * (P.cc_hvc[ia] + P.cc_hvc[ib])) / P.hprnu;
+  double txx = (ga.ux + gb.ux) * viscof;
+  double tyy = (ga.vy + gb.vy) * viscof;
+  double txy = 0.5 * (ga.uy + gb.uy + ga.vx + gb.vx) * viscof;
+  EdgeFlux f;
+  f.fxx = dij * (txx * P.dltyc[e] - txy * P.dltxc[e]);
+  f.fyy = dij * (txy * P.dltyc[e] - tyy * P.dltxc[e]);
+  f.viscof = viscof;
+  if (exflux_form) {
+    // adv_uv_edge_gcn.F:730, 752-753
+    double exflux = dij * (-uij * P.dltyc[e] + vij * P.dltxc[e]);
+    double sg = fsign1(exflux);
+    f.xadv = exflux * ((1.0 - sg) * uij2 + (1.0 + sg) * uij1) * 0.5;
+    f.yadv = exflux * ((1.0 - sg) * vij2 + (1.0 + sg) * vij1) * 0.5;
+  } else {
+    // advection_edge_gcn.F:559, 576-577
+    double un = vij * P.dltxc[e] - uij * P.dltyc[e];
+    double sg = fsign1(un);
+    f.xadv = dij * un * ((1.0 - sg) * uij2 + (1.0 + sg) * uij1) * 0.5;
+    f.yadv = dij * un * ((1.0 - sg) * vij2 + (1.0 + sg) * vij1) * 0.5;
+  }
+  return f;
+}
+
+// River momentum source on one cell and layer (advection_edge_gcn.F:674-708).
+__device__ inline void river3(const Dev& P, int i, int k, double& x, double& y) {
+  for (int q = P.cell_riv_ptr[i]; q < P.cell_riv_ptr[i + 1]; ++q) {
+    int ii = P.cell_riv[q] >> 1;
+    double vq = P.vqdist[(size_t)(k - 1) * (P.numqbc + 1) + ii];
+    double vlctyq = P.qdis[ii] / P.qarea[ii];
+    double temp;
+    if (P.river_location == 0) {
+      int j = P.inodeq[ii];
+      temp = 0.5 * P.qdis[ii] * vq * vq * vlctyq / P.dz[N3(P, j, k)];
+    } else {
+      int i1 = P.icellq[ii];
+      temp = P.qdis[ii] * vq * vq * vlctyq / P.dz1[C3(P, i1, k)];
+    }
+    x = x - temp * P.cos_angleq[ii];
+    y = y - temp * P.sin_angleq[ii];
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// ADVECTION_EDGE_GCN (advection_edge_gcn.F:397-708): per cell and layer, the cell's three
+// edges in ascending edge number.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (i > P.N || k > P.KBM1) return;
+  const size_t e1 = P.NE + 1;
+  double x = 0.0, y = 0.0;
+  for (int s = 0; s < 3; ++s) {
+    int code = P.cell_edge[3 * i + s];
+    int e = code >> 1, side = code & 1;
+    int ia = P.iec[e], ib = P.iec[e1 + e];
+    if (!(P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1)) continue;
+    int j1 = P.ienode[e], j2 = P.ienode[e1 + e];
+    double dij = 0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]);
+    EdgeFlux f = edge_flux3(P, e, ia, ib, k, dij, false);
+    double isb = (double)P.isbc[e];
+    double tp = (double)(float)(1 - P.isbc[e]) * P.epor[i];
+    if (side == 0) {
+      x = x + f.xadv * tp + (f.fxx + 3.0 * f.fxx * isb) * P.epor[i];
+      y = y + f.yadv * tp + (f.fyy + 3.0 * f.fyy * isb) * P.epor[i];
+    } else {
+      x = x - f.xadv * tp - (f.fxx + 3.0 * f.fxx * isb) * P.epor[i];
+      y = y - f.yadv * tp - (f.fyy + 3.0 * f.fyy * isb) * P.epor[i];
+    }
+  }
+  double w = (double)(P.iswetct[i] * P.iswetc[i]);
+  x = x * w;
+  y = y * w;
+  if (P.isbce[i] == 2) { x = 0.0; y = 0.0; }
+  river3(P, i, k, x, y);
+  P.advx[C3(P, i, k)] = x;
+  P.advy[C3(P, i, k)] = y;
+}
+
+// -------------------------------------------------------------------------------------
+// BAROPG, sigma levels (baropg.F:56-161), then the vertical sums of ADVX/DRHOX into the
+// 2-D forcing (internal_step.F:374-384).  One thread per cell column; the density
+// anomalies RHO1-RMEAN1 of the three nodes are formed on the fly and the cell's
+// RHO = (RHO-RMEAN)+RMEAN round trip is written back as the reference does.
+// -------------------------------------------------------------------------------------
+__global__ void k_baropg(const Dev P, int do_baropg, int do_sums) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  const size_t n1 = P.N + 1;
+  const int KBM1 = P.KBM1;
+  if (do_baropg) {
+    int nvv[4] = {0, P.nv[i], P.nv[n1 + i], P.nv[2 * n1 + i]};
+    double ramp = ramp_int(P);
+    bool active = P.iswetct[i] * P.iswetc[i] == 1 &&
+                  (P.h[nvv[1]] > P.static_ssh_adj || P.h[nvv[2]] > P.static_ssh_adj || P.h[nvv[3]] > P.static_ssh_adj);
+    double dx[4], dyv[4], dij[4];
+    for (int j = 1; j <= 3; ++j) {
+      int J1 = j + 1 - ((j + 1) / 4) * 3, J2 = j + 2 - ((j + 2) / 4) * 3;
+      dyv[j] = P.vy[nvv[J1]] - P.vy[nvv[J2]];
+      dx[j] = P.vx[nvv[J2]] - P.vx[nvv[J1]];
+      dij[j] = 0.5 * (P.dt[nvv[J1]] + P.dt[nvv[J2]]);
+    }
+    double rprev[4] = {0, 0, 0, 0}, d1p[4] = {0, 0, 0, 0};
+    double d2 = 0.0, rhoc_prev = 0.0;
+    double dt1 = P.dt1[i], ge = P.grav_e[i];
+    for (int k = 1; k <= KBM1; ++k) {
+      double rij[4];
+      for (int j = 1; j <= 3; ++j) {
+        int J1 = j + 1 - ((j + 1) / 4) * 3, J2 = j + 2 - ((j + 2) / 4) * 3;
+        size_t q1 = N3(P, nvv[J1], k), q2 = N3(P, nvv[J2], k);
+        rij[j] = 0.5 * ((P.rho1[q1] - P.rmean1[q1]) + (P.rho1[q2] - P.rmean1[q2]));
+      }
+      double rhoc = P.rho[C3(P, i, k)] - P.rmean[C3(P, i, k)];
+      if (k == 1) {
+        for (int j = 1; j <= 3; ++j) d1p[j] = rij[j] * (-P.zz1[C3(P, i, 1)]);
+        d2 = 0.0;
+      } else {
+        double zkm = P.zz1[C3(P, i, k - 1)], zk = P.zz1[C3(P, i, k)];
+        for (int j = 1; j <= 3; ++j) d1p[j] = 0.5 * (rprev[j] + rij[j]) * (zkm - zk) + d1p[j];
+        d2 = d2 + 0.5 * (zkm + zk) * (rhoc - rhoc_prev);
+      }
+      double drhox = 0.0, drhoy = 0.0;
+      if (active) {
+        for (int j = 1; j <= 3; ++j) {
+          double drho1 = dyv[j] * d1p[j] * dt1;
+          double drho2 = dyv[j] * dij[j] * d2;
+          drhox = drhox + drho1 + drho2;
+          drho1 = dx[j] * d1p[j] * dt1;
+          drho2 = dx[j] * dij[j] * d2;
+          drhoy = drhoy + drho1 + drho2;
+        }
+      }
+      double dz1 = P.dz1[C3(P, i, k)];
+      P.drhox[C3(P, i, k)] = drhox * dt1 * dz1 * ge * ramp;
+      P.drhoy[C3(P, i, k)] = drhoy * dt1 * dz1 * ge * ramp;
+      for (int j = 1; j <= 3; ++j) rprev[j] = rij[j];
+      rhoc_prev = rhoc;
+    }
+    for (int k = 1; k <= P.KB; ++k) {
+      size_t q = C3(P, i, k);
+      P.rho[q] = (P.rho[q] - P.rmean[q]) + P.rmean[q];
+    }
+  }
+  if (do_sums) {
+    double ax = 0.0, ay = 0.0, rx = 0.0, ry = 0.0;
+    for (int k = 1; k <= KBM1; ++k) {
+      size_t q = C3(P, i, k);
+      ax = ax + P.advx[q];
+      ay = ay + P.advy[q];
+      rx = rx + P.drhox[q];
+      ry = ry + P.drhoy[q];
+    }
+    P.adx2d[i] = ax;
+    P.ady2d[i] = ay;
+    P.drx2d[i] = rx;
+    P.dry2d[i] = ry;
+  }
+}
+
+// internal_step.F:395-416: UARD=VARD=EGF=0, UARD_OBCN=0 before the external loop.
+__global__ void k_int_reset(const Dev P) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= P.N) { P.uard[i] = 0.0; P.vard[i] = 0.0; }
+  if (i <= P.M) P.egf[i] = 0.0;
+  if (i >= 1 && i <= P.iobcn) P.uard_obcn[i] = 0.0;
+}
+
+// ADJUST2D3D(2) (adjust2d3d.F:65-92), one thread per cell column.
+__global__ void k_adjust2(const Dev P) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > P.N) return;
+  double ud = P.uard[i] / (double)(float)P.isplit;
+  double vd = P.vard[i] / (double)(float)P.isplit;
+  P.uard[i] = ud;
+  P.vard[i] = vd;
+  if (i == 0) return;
+  if (P.iswetct[i] * P.iswetc[i] != 1) return;
+  double ut = 0.0, vt = 0.0;
+  for (int k = 1; k <= P.KBM1; ++k) {
+    size_t q = C3(P, i, k);
+    ut = ut + P.u[q] * P.dz1[q];
+    vt = vt + P.v[q] * P.dz1[q];
+  }
+  double dt1 = P.dt1[i];
+  ut = ut * dt1;
+  vt = vt * dt1;
+  for (int k = 1; k <= P.KBM1; ++k) {
+    size_t q = C3(P, i, k);
+    P.u[q] = P.u[q] - (ut - ud) / dt1;
+    P.v[q] = P.v[q] - (vt - vd) / dt1;
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// VERTVL_EDGE horizontal divergence (vertvl_edge.F:68-220): per node and layer, the
+// node's half-edges in ascending order.  Result in the scratch field.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_vertvl_flux(const Dev P) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (i > P.M || k > P.KBM1) return;
+  double x = 0.0;
+  if (P.isonb[i] != 2) {
+    for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
+      int e = P.node_he[q];
+      int he = e >> 1;
+      int c = P.ntrg[he];
+      double dij = P.dt1[c] * P.dz1[C3(P, c, k)];
+      double exflux = dij * (-P.u[C3(P, c, k)] * P.dltye[he] + P.v[C3(P, c, k)] * P.dltxe[he]);
+      x = (e & 1) ? x + exflux : x - exflux;
+    }
+  }
+  for (int q = P.node_riv_ptr[i]; q < P.node_riv_ptr[i + 1]; ++q) {
+    int r = P.node_riv[q];
+    int j = r >> 1;
+    double vq = P.vqdist[(size_t)(k - 1) * (P.numqbc + 1) + j];
+    if (P.river_location == 0)
+      x = x - P.qdis[j] * vq;
+    else
+      x = x - P.qdis[j] * P.rdisq[(size_t)(r & 1) * (P.numqbc + 1) + j] * vq;
+  }
+  P.scr_xflux[N3(P, i, k)] = x;
+}
+
+// -------------------------------------------------------------------------------------
+// VERTVL_EDGE vertical integration and mass-conservation adjustment
+// (vertvl_edge.F:236-539), WD_UPDATE(2) (mod_wd.F:311-317), the RHO1 round trip of BAROPG
+// (baropg.F:56,160) and E2N2D of the bottom stress (brough.F:193-206).  Node columns.
+// -------------------------------------------------------------------------------------
+__global__ void k_vertvl_col(const Dev P, int parts) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  const int KB = P.KB, KBM1 = P.KBM1;
+  if (parts & VC_WTS) {
+    const double ROFVROS = 0.9775171065;
+    double wb = 0.0 / P.art1[i];
+    double wk = -(0.0 + 0.0) * ROFVROS;
+    P.wts[N3(P, i, 1)] = wk;
+    if (P.iswetnt[i] * P.iswetn[i] == 1) {
+      double dd = P.d[i] - P.dt[i];
+      for (int k = 1; k <= KBM1; ++k) {
+        wk = wk + P.scr_xflux[N3(P, i, k)] / P.art1[i] + P.dz[N3(P, i, k)] * dd / P.dti;
+        P.wts[N3(P, i, k + 1)] = wk;
+      }
+    } else {
+      for (int k = 1; k <= KBM1; ++k) P.wts[N3(P, i, k + 1)] = 0.0;
+      wk = 0.0;
+    }
+    double wkb = wk;
+    if (fabs(wkb - wb) > 1.0e-8 && P.isonb[i] != 2) {
+      double tmp1 = P.elf[i] * (double)(float)KBM1 - (wkb - wb) * P.dti / P.dz[N3(P, i, 1)];
+      tmp1 = tmp1 / (double)(float)KBM1;
+      P.dtfa[i] = tmp1 + P.h[i];
+      for (int k = 2; k <= KB; ++k) {
+        double cur = P.wts[N3(P, i, k)];
+        double wkb_now = (k == KB) ? cur : wkb;
+        P.wts[N3(P, i, k)] = cur - (double)((float)(k - 1) / (float)KBM1) * (wkb_now - wb);
+      }
+    }
+  }
+  if ((parts & VC_WD2) && P.wetting_drying_on) {
+    if (P.dtfa[i] - P.min_depth <= 1.0e-5) P.iswetn[i] = 0;
+  }
+  if (parts & VC_RHO_ROUNDTRIP) {
+    for (int k = 1; k <= KBM1; ++k) {
+      size_t q = N3(P, i, k);
+      P.rho1[q] = (P.rho1[q] - P.rmean1[q]) + P.rmean1[q];
+    }
+  }
+  if (parts & VC_BOT_NODE) {
+    double su = 0.0, sv = 0.0;
+    int nt = P.ntve[i];
+    for (int j = 1; j <= nt; ++j) {
+      int c = P.nbve[(size_t)(j - 1) * (P.M + 1) + i];
+      su = su + P.wubot[c];
+      sv = sv + P.wvbot[c];
+    }
+    double fn = (double)(float)nt;
+    su = su / fn;
+    sv = sv / fn;
+    P.wubot_n[i] = su;
+    P.wvbot_n[i] = sv;
+    P.taubm_n[i] = sqrt(su * su + sv * sv);
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// W = N2E(WTS)*ISWETC (vertvl_edge.F:552-563) on cells, and VISCOF_H (viscofh.F:58-122)
+// on nodes, one thread per (entity, layer).
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_w_viscofh(const Dev P, int do_w, int do_visc) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (k > P.KB) return;
+  const size_t n1 = P.N + 1, m1 = P.M + 1;
+  if (do_w && i <= P.N) {
+    double w = ONE_THIRD * (P.wts[N3(P, P.nv[i], k)] + P.wts[N3(P, P.nv[n1 + i], k)] + P.wts[N3(P, P.nv[2 * n1 + i], k)]);
+    P.w[C3(P, i, k)] = (double)(float)P.iswetc[i] * w;
+  }
+  if (do_visc && i <= P.M && k <= P.KBM1) {
+    const double* U = P.u + C3(P, 0, k);
+    const double* V = P.v + C3(P, 0, k);
+    double pupx = 0.0, pupy = 0.0, pvpx = 0.0, pvpy = 0.0;
+    int nt = P.ntve[i];
+    bool bnd = P.isonb[i] != 0;
+    // J=1, then J=2..NTVE-1, then J=NTVE (viscofh.F:65-111); a node with one cell adds
+    // that cell's edge term twice, as the reference does.
+    auto ecec = [&](int j) {
+      size_t q = (size_t)(j - 1) * m1 + i;
+      int c = P.nbve[q];
+      double ey = P.dltyecec[q], ex = P.dltxecec[q];
+      pupx = pupx + U[c] * ey;
+      pupy = pupy + U[c] * ex;
+      pvpx = pvpx + V[c] * ey;
+      pvpy = pvpy + V[c] * ex;
+    };
+    auto nec = [&](int j, double sgn) {
+      size_t q = (size_t)(j - 1) * m1 + i;
+      int c = P.nbve[q];
+      double ny = sgn * P.dltynec[q], nx = sgn * P.dltxnec[q];
+      pupx = pupx + U[c] * ny;
+      pupy = pupy + U[c] * nx;
+      pvpx = pvpx + V[c] * ny;
+      pvpy = pvpy + V[c] * nx;
+    };
+    ecec(1);
+    if (bnd) nec(1, 1.0);
+    for (int j = 2; j <= nt - 1; ++j) ecec(j);
+    ecec(nt);
+    if (bnd) nec(nt, -1.0);
+    double a1 = P.art1[i];
+    pupx = pupx / a1;
+    pupy = pupy / a1;
+    pvpx = pvpx / a1;
+    pvpy = pvpy / a1;
+    double tmp1 = pupx * pupx + pvpy * pvpy;
+    double tmp2 = 0.5 * ((pupy + pvpx) * (pupy + pvpx));
+    P.viscofh[N3(P, i, k)] = sqrt(tmp1 + tmp2) * a1;
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// ADV_UV_EDGE_GCN (adv_uv_edge_gcn.F:124-1193): horizontal advection/diffusion, the
+// internal barotropic pressure gradient from EGF, vertical advection, baroclinic
+// pressure gradient, Coriolis, river momentum and the explicit update to UF/VF.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (i > P.N || k > P.KBM1) return;
+  const size_t e1 = P.NE + 1;
+  double x = 0.0, y = 0.0, px = 0.0, py = 0.0, vm = 0.0;
+  const double dz1i = P.dz1[C3(P, i, k)];
+  const double gdd = P.grav_e[i] * P.dt1[i] * dz1i;
+  for (int s = 0; s < 3; ++s) {
+    int code = P.cell_edge[3 * i + s];
+    int e = code >> 1, side = code & 1;
+    int ia = P.iec[e], ib = P.iec[e1 + e];
+    int j1 = P.ienode[e], j2 = P.ienode[e1 + e];
+    double elij = 0.5 * (P.egf[j1] + P.egf[j2]);
+    double dij = 0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]);
+    if (P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1) {
+      EdgeFlux f = edge_flux3(P, e, ia, ib, k, dij, true);
+      vm = vm + f.viscof;
+      double isb = (double)P.isbc[e];
+      double tp = (double)(float)(1 - P.isbc[e]) * P.epor[i];
+      if (side == 0) {
+        x = x + f.xadv * tp + (f.fxx + 3.0 * f.fxx * isb) * P.epor[i];
+        y = y + f.yadv * tp + (f.fyy + 3.0 * f.fyy * isb) * P.epor[i];
+      } else {
+        x = x - f.xadv * tp - (f.fxx + 3.0 * f.fxx * isb) * P.epor[i];
+        y = y - f.yadv * tp - (f.fyy + 3.0 * f.fyy * isb) * P.epor[i];
+      }
+    }
+    if (side == 0) {
+      px = px - gdd * elij * P.dltyc[e];
+      py = py + gdd * elij * P.dltxc[e];
+    } else {
+      px = px + gdd * elij * P.dltyc[e];
+      py = py - gdd * elij * P.dltxc[e];
+    }
+  }
+  bool wet = P.iswetct[i] * P.iswetc[i] == 1;
+  double w = (double)(P.iswetct[i] * P.iswetc[i]);
+  x = x * w;
+  y = y * w;
+  px = px * w;
+  py = py * w;
+  x = x + px;
+  y = y + py;
+  size_t q = C3(P, i, k);
+  if (wet) {
+    const double *U = P.u, *V = P.v, *W = P.w, *DZ1 = P.dz1;
+    double xfv, yfv;
+    if (k == 1) {
+      size_t qp = C3(P, i, k + 1);
+      xfv = -W[qp] * (U[q] * DZ1[qp] + U[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
+      yfv = -W[qp] * (V[q] * DZ1[qp] + V[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
+    } else if (k == P.KBM1) {
+      size_t qm = C3(P, i, k - 1);
+      xfv = W[q] * (U[q] * DZ1[qm] + U[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]);
+      yfv = W[q] * (V[q] * DZ1[qm] + V[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]);
+    } else {
+      size_t qm = C3(P, i, k - 1), qp = C3(P, i, k + 1);
+      xfv = W[q] * (U[q] * DZ1[qm] + U[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]) -
+            W[qp] * (U[q] * DZ1[qp] + U[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
+      yfv = W[q] * (V[q] * DZ1[qm] + V[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]) -
+            W[qp] * (V[q] * DZ1[qp] + V[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
+    }
+    x = x + xfv * P.art[i] + P.drhox[q] - P.cor[i] * V[q] * P.dt1[i] * DZ1[q] * P.art[i];
+    y = y + yfv * P.art[i] + P.drhoy[q] + P.cor[i] * U[q] * P.dt1[i] * DZ1[q] * P.art[i];
+  }
+  if (P.isbce[i] == 2) { x = 0.0; y = 0.0; }
+  river3(P, i, k, x, y);
+  double uf, vf;
+  if (wet) {
+    double d1 = P.d1[i];
+    uf = P.u[q] * P.dt1[i] / d1 - P.dti * x / P.art[i] / (d1 * dz1i);
+    vf = P.v[q] * P.dt1[i] / d1 - P.dti * y / P.art[i] / (d1 * dz1i);
+  } else {
+    uf = 0.0;
+    vf = 0.0;
+  }
+  P.uf[q] = uf;
+  P.vf[q] = vf;
+  P.viscofm[q] = vm / P.art[i];
+}
+
+// -------------------------------------------------------------------------------------
+// VDIF_UV (vdif_uv.F:56-182), the static-SSH fix and BCOND_GCN(3,0)
+// (internal_step.F:660-672, bcond_gcn.F:424-502), WREAL (wreal.F:57-129).
+// One thread per cell column; the Thomas sweep keeps its coefficients in registers and
+// local memory.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_vdif_uv(const Dev P, int parts) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  const int KB = P.KB, KBM1 = P.KBM1, KBM2 = P.KBM2;
+  const double DTI = P.dti;
+  if (parts & VU_VDIF) {
+    if (P.iswetc[i] == 1) {
+      double vhu[kMaxKB], vhpu[kMaxKB], vhv[kMaxKB], vhpv[kMaxKB];
+      const double d1 = P.d1[i];
+      // A(K) uses KM1(K+1) with DZ1(K), DZZ1(K); C(K) uses KM1(K) with DZ1(K), DZZ1(K-1).
+      auto Acoef = [&](int kk) {
+        return -DTI * (P.km1[C3(P, i, kk + 1)] + P.umol) / (P.dz1[C3(P, i, kk)] * P.dzz1[C3(P, i, kk)] * d1 * d1);
+      };
+      auto Ccoef = [&](int kk) {
+        return -DTI * (P.km1[C3(P, i, kk)] + P.umol) / (P.dz1[C3(P, i, kk)] * P.dzz1[C3(P, i, kk - 1)] * d1 * d1);
+      };
+      int n1 = P.N + 1;
+      int it1 = P.isonb[P.nv[i]], it2 = P.isonb[P.nv[n1 + i]], it3 = P.isonb[P.nv[2 * n1 + i]];
+      double tmp = (it1 == 2 || it2 == 2 || it3 == 2) ? 0.0 : 1.0;
+      double a1 = Acoef(1);
+      double wus = P.wusurf[i], wvs = P.wvsurf[i];
+      vhu[1] = a1 / (a1 - 1.0);
+      vhv[1] = a1 / (a1 - 1.0);
+      vhpu[1] = (-DTI * wus * tmp / (-P.dz1[C3(P, i, 1)] * d1) - P.uf[C3(P, i, 1)]) / (a1 - 1.0);
+      vhpv[1] = (-DTI * wvs * tmp / (-P.dz1[C3(P, i, 1)] * d1) - P.vf[C3(P, i, 1)]) / (a1 - 1.0);
+      for (int k = 2; k <= KBM2; ++k) {
+        double ak = Acoef(k), ck = Ccoef(k);
+        double pu = 1.0 / (ak + ck * (1.0 - vhu[k - 1]) - 1.0);
+        double pv = 1.0 / (ak + ck * (1.0 - vhv[k - 1]) - 1.0);
+        vhu[k] = ak * pu;
+        vhv[k] = ak * pv;
+        vhpu[k] = (ck * vhpu[k - 1] - P.uf[C3(P, i, k)]) * pu;
+        vhpv[k] = (ck * vhpv[k - 1] - P.vf[C3(P, i, k)]) * pv;
+      }
+      double ub = P.u[C3(P, i, KBM1)], vb = P.v[C3(P, i, KBM1)];
+      double tps = P.cbc[i] * sqrt(ub * ub + vb * vb);
+      P.tps[i] = tps;
+      double cb = Ccoef(KBM1);
+      double dzb = P.dz1[C3(P, i, KBM1)];
+      double ufk = (cb * vhpu[KBM2] - P.uf[C3(P, i, KBM1)]) / (tps * DTI / (-dzb * d1) - 1.0 - (vhu[KBM2] - 1.0) * cb);
+      double vfk = (cb * vhpv[KBM2] - P.vf[C3(P, i, KBM1)]) / (tps * DTI / (-dzb * d1) - 1.0 - (vhv[KBM2] - 1.0) * cb);
+      P.uf[C3(P, i, KBM1)] = ufk;
+      P.vf[C3(P, i, KBM1)] = vfk;
+      for (int k = 2; k <= KBM1; ++k) {
+        int ki = KB - k;
+        ufk = (vhu[ki] * ufk + vhpu[ki]);
+        vfk = (vhv[ki] * vfk + vhpv[ki]);
+        P.uf[C3(P, i, ki)] = ufk;
+        P.vf[C3(P, i, ki)] = vfk;
+      }
+      P.wubot[i] = -tps * ub;
+      P.wvbot[i] = -tps * vb;
+    } else {
+      for (int k = 2; k <= KBM1; ++k) {
+        int ki = KB - k;
+        P.uf[C3(P, i, ki)] = 0.0;
+        P.vf[C3(P, i, ki)] = 0.0;
+      }
+      P.wubot[i] = 0.0;
+      P.wvbot[i] = 0.0;
+    }
+    double sp = P.cc_sponge[i];
+    for (int k = 1; k <= KBM1; ++k) {
+      size_t q = C3(P, i, k);
+      double uu = P.uf[q], vv = P.vf[q];
+      P.uf[q] = uu / (1.0 + sp * (uu * uu));
+      P.vf[q] = vv / (1.0 + sp * (vv * vv));
+    }
+  }
+  if (parts & VU_BC3) {
+    bool fix = P.h1[i] <= P.static_ssh_adj;
+    int b = P.isbce[i];
+    for (int k = 1; k <= KBM1; ++k) {
+      size_t q = C3(P, i, k);
+      double uu = P.uf[q], vv = P.vf[q];
+      if (fix) { uu = P.ua[i]; vv = P.va[i]; }
+      if (b == 3) { uu = 0.0; vv = 0.0; }
+      if (b == 1) bc_solid3(P, i, uu, vv);
+      P.uf[q] = uu;
+      P.vf[q] = vv;
+    }
+  }
+  if (parts & VU_WREAL) {
+    if (P.iswetc[i] == 1) {
+      const size_t n1 = P.N + 1;
+      int j1 = P.nv[i], j2 = P.nv[n1 + i], j3 = P.nv[2 * n1 + i];
+      double ax1 = P.awx[i], ax2 = P.awx[n1 + i], ax3 = P.awx[2 * n1 + i];
+      double ay1 = P.awy[i], ay2 = P.awy[n1 + i], ay3 = P.awy[2 * n1 + i];
+      double dddx = ax1 * P.d[j1] + ax2 * P.d[j2] + ax3 * P.d[j3];
+      double dddy = ay1 * P.d[j1] + ay2 * P.d[j2] + ay3 * P.d[j3];
+      double dedx = ax1 * P.elf[j1] + ax2 * P.elf[j2] + ax3 * P.elf[j3];
+      double dedy = ay1 * P.elf[j1] + ay2 * P.elf[j2] + ay3 * P.elf[j3];
+      double etf1aa = ONE_THIRD * (P.el[j1] + P.el[j2] + P.el[j3]);
+      for (int k = 1; k <= KBM1; ++k) {
+        size_t q = C3(P, i, k);
+        double zz = P.zz1[q];
+        double ww1 = 0.5 * (P.w[q] + P.w[C3(P, i, k + 1)]) + P.u[q] * (zz * dddx + dedx) + P.v[q] * (zz * dddy + dedy);
+        double ww2 = (zz + 1.0) * (etf1aa - P.et1[i]) / DTI;
+        P.ww[q] = ww1 + ww2;
+      }
+    } else {
+      for (int k = 1; k <= KBM1; ++k) P.ww[C3(P, i, k)] = 0.0;
+    }
+  }
+}
+
+void launch_cell_pre(const Dev& P, cudaStream_t s, int parts) {
+  k_cell_pre<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);
+}
+void launch_advection3d(const Dev& P, cudaStream_t s) {
+  dim3 b(32, 8), g(nblk(P.N, 32), nblk(P.KBM1, 8));
+  k_advection3d<<<g, b, 0, s>>>(P);
+}
+void launch_baropg(const Dev& P, cudaStream_t s, int do_baropg, int do_sums) {
+  k_baropg<<<nblk(P.N, 128), 128, 0, s>>>(P, do_baropg, do_sums);
+}
+void launch_int_reset(const Dev& P, cudaStream_t s) {
+  int n = (P.M > P.N ? P.M : P.N) + 1;
+  k_int_reset<<<nblk(n, 256), 256, 0, s>>>(P);
+}
+void launch_adjust2(const Dev& P, cudaStream_t s) { k_adjust2<<<nblk(P.N + 1, 128), 128, 0, s>>>(P); }
+void launch_vertvl_flux(const Dev& P, cudaStream_t s) {
+  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));
+  k_vertvl_flux<<<g, b, 0, s>>>(P);
+}
+void launch_vertvl_col(const Dev& P, cudaStream_t s, int parts) {
+  k_vertvl_col<<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
+}
+void launch_w_viscofh(const Dev& P, cudaStream_t s, int do_w, int do_visc) {
+  int n = P.M > P.N ? P.M : P.N;
+  dim3 b(32, 8), g(nblk(n, 32), nblk(P.KB, 8));
+  k_w_viscofh<<<g, b, 0, s>>>(P, do_w, do_visc);
+}
+void launch_adv_uv(const Dev& P, cudaStream_t s) {
+  dim3 b(32, 8), g(nblk(P.N, 32), nblk(P.KBM1, 8));
+  k_adv_uv<<<g, b, 0, s>>>(P);
+}
+void launch_vdif_uv(const Dev& P, cudaStream_t s, int parts) {
+  k_vdif_uv<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);
+}
+
+}  // namespace fvg

@@ -1,0 +1,792 @@
+// k_scalar.cu - node-centred scalar transport and turbulence of INTERNAL_STEP:
+// ADV_Q/FCT_Q2/FCT_Q2L (adv_q.F, fct_q2.F, fct_q2l.F), VDIF_Q with the MY2.5 closure
+// (vdif_q.F), ADV_T/ADV_S with FCT_T/FCT_S (adv_t.F, adv_s.F, fct_t.F, fct_s.F), VDIF_TS
+// (vdif_ts.F), BCOND_TS (bcond_ts.F, mod_obcs.F:1223-1373), DENS2 (eqs_of_state.F) and the
+// end-of-step shifts (internal_step.F:1034-1590).
+//
+// The node-ring gradients (PTPX.. over NBSN) and the ring extrema of the advected field
+// are formed once per (node, layer) by k_grad into scratch fields; the flux kernels then
+// gather each node's control-volume half-edges in ascending order and read both ends'
+// gradients, reproducing the reference's scatter sums.  T and S (and Q2 and Q2L) are
+// transported in the same launch since neither reads the other's update.
+#include "fvg_model.h"
+
+namespace fvg {
+
+#define ONE_THIRD (1.0 / 3.0)
+constexpr int kMaxKBs = 64;
+
+static inline int nblk(int n, int b) { return (n + b - 1) / b; }
+
+__device__ inline double F4(double x) { return (double)(float)x; }
+__device__ inline int NBSN(const Dev& P, int i, int j) { return P.nbsn[(size_t)(j - 1) * (P.M + 1) + i]; }
+__device__ inline double TRIEX(const Dev& P, int i, int j) { return P.dltxtrie[(size_t)(j - 1) * (P.M + 1) + i]; }
+__device__ inline double TRIEY(const Dev& P, int i, int j) { return P.dltytrie[(size_t)(j - 1) * (P.M + 1) + i]; }
+
+// -------------------------------------------------------------------------------------
+// Ring gradients and extrema.  which == 0: Q2 and Q2L on K=2..KBM1 (adv_q.F:161-235);
+// which == 1: T1 and S1 on K=1..KBM1 with the wet/dry substitution of adv_t.F:214-376,
+// plus PFPXB/PFPYB and AH_BOTTOM at K=KBM1 (adv_t.F:394-408).
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_grad(const Dev P, int which) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (i > P.M || k > P.KBM1) return;
+  if (which == 0 && k < 2) return;
+  const int nt = P.ntsn[i];
+  const double art2 = P.art2[i];
+  for (int t = 0; t < 2; ++t) {
+    const double* Q;
+    const double* QM = nullptr;
+    double** G;
+    if (which == 0) {
+      Q = (t == 0 ? P.q2 : P.q2l) + N3(P, 0, k);
+      G = (double**)P.gq[t];
+    } else {
+      Q = (t == 0 ? P.t1 : P.s1) + N3(P, 0, k);
+      QM = (t == 0 ? P.tmean1 : P.smean1) + N3(P, 0, k);
+      G = (double**)P.gt[t];
+    }
+    const double qmean = F4(1.e-8);
+    double px = 0.0, py = 0.0, pxd = 0.0, pyd = 0.0;
+    double rmin = Q[NBSN(P, i, 1)], rmax = rmin;
+    for (int j = 1; j <= nt - 1; ++j) {
+      int i1 = NBSN(P, i, j), i2 = NBSN(P, i, j + 1);
+      if (j >= 2) {
+        rmin = fmin(rmin, Q[i1]);
+        rmax = fmax(rmax, Q[i1]);
+      }
+      double ffd, ff1;
+      if (which == 0) {
+        ffd = 0.5 * (Q[i1] + Q[i2] - qmean - qmean);
+        ff1 = 0.5 * (Q[i1] + Q[i2]);
+      } else {
+        int w1 = P.iswetn[i1], w2 = P.iswetn[i2];
+        int a = i1, b = i2;
+        if (w1 == 0 && w2 == 1) { a = i; b = i2; }
+        else if (w1 == 1 && w2 == 0) { a = i1; b = i; }
+        else if (w1 == 0 && w2 == 0) { a = i; b = i; }
+        ffd = 0.5 * (Q[a] + Q[b] - QM[a] - QM[b]);
+        ff1 = 0.5 * (Q[a] + Q[b]);
+      }
+      double ty = TRIEY(P, i, j), tx = TRIEX(P, i, j);
+      px = px + ff1 * ty;
+      py = py + ff1 * tx;
+      pxd = pxd + ffd * ty;
+      pyd = pyd + ffd * tx;
+    }
+    px = px / art2;
+    py = py / art2;
+    pxd = pxd / art2;
+    pyd = pyd / art2;
+    size_t q = N3(P, i, k);
+    G[0][q] = px;
+    G[1][q] = py;
+    G[2][q] = pxd;
+    G[3][q] = pyd;
+    G[4][q] = rmin;
+    G[5][q] = rmax;
+    if (which == 1 && k == P.KBM1) {
+      if (t == 0) { P.pfpxb_t[i] = px; P.pfpyb_t[i] = py; }
+      else { P.pfpxb_s[i] = px; P.pfpyb_s[i] = py; }
+      double ah = (P.fact * P.viscofh[N3(P, i, P.KBM1)] + P.fm1) * P.nn_hvc[i];
+      if (t == 0) P.ah_bottom_t[i] = ah;
+      else P.ah_bottom_s[i] = ah;
+    }
+  }
+}
+
+// Vertical-neighbour bound of FCT on sigma layers (fct_t.F:78-97) and on interfaces
+// (fct_q2.F:73-92).
+__device__ inline void fct_layer_bounds(const Dev& P, int i, int k, const double* F, double& fmax_, double& fmin_) {
+  const double* DZ = P.dz;
+  size_t q = N3(P, i, k);
+  if (k == 1) {
+    size_t qp = N3(P, i, k + 1);
+    double a = (F[q] * DZ[qp] + F[qp] * DZ[q]) / (DZ[q] + DZ[qp]);
+    fmax_ = fmax(fmax_, a);
+    fmin_ = fmin(fmin_, a);
+  } else if (k == P.KBM1) {
+    size_t qm = N3(P, i, k - 1);
+    double a = (F[q] * DZ[qm] + F[qm] * DZ[q]) / (DZ[q] + DZ[qm]);
+    fmax_ = fmax(fmax_, a);
+    fmin_ = fmin(fmin_, a);
+  } else {
+    size_t qm = N3(P, i, k - 1), qp = N3(P, i, k + 1);
+    double a = (F[q] * DZ[qm] + F[qm] * DZ[q]) / (DZ[q] + DZ[qm]);
+    double b = (F[q] * DZ[qp] + F[qp] * DZ[q]) / (DZ[q] + DZ[qp]);
+    fmax_ = fmax(fmax(fmax_, a), b);
+    fmin_ = fmin(fmin(fmin_, a), b);
+  }
+}
+__device__ inline void fct_level_bounds(const Dev& P, int i, int k, const double* F, double& fmax_, double& fmin_) {
+  const double* DZZ = P.dzz;
+  size_t q = N3(P, i, k), qm = N3(P, i, k - 1), qp = N3(P, i, k + 1);
+  if (k == 2) {
+    double a = (F[q] * DZZ[q] + F[qp] * DZZ[qm]) / (DZZ[q] + DZZ[qm]);
+    fmax_ = fmax(fmax_, a);
+    fmin_ = fmin(fmin_, a);
+  } else if (k == P.KBM1) {
+    size_t qmm = N3(P, i, k - 2);
+    double a = (F[q] * DZZ[qmm] + F[qm] * DZZ[qm]) / (DZZ[qm] + DZZ[qmm]);
+    fmax_ = fmax(fmax_, a);
+    fmin_ = fmin(fmin_, a);
+  } else {
+    size_t qmm = N3(P, i, k - 2);
+    double a = (F[q] * DZZ[qmm] + F[qm] * DZZ[qm]) / (DZZ[qm] + DZZ[qmm]);
+    double b = (F[q] * DZZ[q] + F[qp] * DZZ[qm]) / (DZZ[q] + DZZ[qm]);
+    fmax_ = fmax(fmax(fmax_, a), b);
+    fmin_ = fmin(fmin(fmin_, a), b);
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// ADV_Q(Q2,Q2F) and ADV_Q(Q2L,Q2LF) (adv_q.F:114-401), then FCT_Q2/FCT_Q2L.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_adv_q(const Dev P, int parts) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 2;
+  if (i > P.M || k > P.KBM1) return;
+  const size_t v1 = P.NCV + 1, vi1 = P.NCV_I + 1;
+  const bool wet = P.iswetn[i] * P.iswetnt[i] == 1;
+  for (int t = 0; t < 2; ++t) {
+    if (!(parts & (t == 0 ? AD_Q2 : AD_Q2L))) continue;
+    const double* Q = (t == 0 ? P.q2 : P.q2l);
+    double* QF = (t == 0 ? P.q2f : P.q2lf);
+    double* const* G = P.gq[t];
+    const double* Qk = Q + N3(P, 0, k);
+    double x = 0.0;
+    for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
+      int code = P.node_he[q];
+      int he = code >> 1;
+      int ia = P.niec[he], ib = P.niec[v1 + he];
+      int c = P.ntrg[he];
+      size_t ck = C3(P, c, k), ckm = C3(P, c, k - 1);
+      double uq = (P.u[ck] * P.dz1[ckm] + P.u[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]);
+      double vq = (P.v[ck] * P.dz1[ckm] + P.v[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]);
+      double dtij = P.dt1[c] * P.dzz1[ckm];
+      double un = vq * P.dltxe[he] - uq * P.dltye[he];
+      size_t qa = N3(P, ia, k), qb = N3(P, ib, k);
+      double fij1 = Qk[ia] + P.dltxncve[he] * G[0][qa] + P.dltyncve[he] * G[1][qa];
+      double fij2 = Qk[ib] + P.dltxncve[vi1 + he] * G[0][qb] + P.dltyncve[vi1 + he] * G[1][qb];
+      double q1min = fmin(G[4][qa], Qk[ia]), q1max = fmax(G[5][qa], Qk[ia]);
+      double q2min = fmin(G[4][qb], Qk[ib]), q2max = fmax(G[5][qb], Qk[ib]);
+      if (fij1 < q1min) fij1 = q1min;
+      if (fij1 > q1max) fij1 = q1max;
+      if (fij2 < q2min) fij2 = q2min;
+      if (fij2 > q2max) fij2 = q2max;
+      size_t qam = N3(P, ia, k - 1), qbm = N3(P, ib, k - 1);
+      double vfa = (P.viscofh[qa] * P.dz[qam] + P.viscofh[qam] * P.dz[qa]) / (P.dz[qa] + P.dz[qam]);
+      double vfb = (P.viscofh[qb] * P.dz[qbm] + P.viscofh[qbm] * P.dz[qb]) / (P.dz[qb] + P.dz[qbm]);
+      double viscof = (P.fact * 0.5 * (vfa * P.nn_hvc[ia] + vfb * P.nn_hvc[ib]) +
+                       P.fm1 * 0.5 * (P.nn_hvc[ia] + P.nn_hvc[ib])) / P.hprnu;
+      double txx = 0.5 * (G[2][qa] + G[2][qb]) * viscof;
+      double tyy = 0.5 * (G[3][qa] + G[3][qb]) * viscof;
+      double fxx = -dtij * txx * P.dltye[he];
+      double fyy = dtij * tyy * P.dltxe[he];
+      double sg = fsign1(un);
+      double exflux = -un * dtij * ((1.0 + sg) * fij2 + (1.0 - sg) * fij1) * 0.5 + fxx + fyy;
+      x = (code & 1) ? x - exflux : x + exflux;
+    }
+    size_t q = N3(P, i, k);
+    double qf;
+    if (wet) {
+      size_t qm = N3(P, i, k - 1), qp = N3(P, i, k + 1);
+      double temp = P.wts[qm] * Q[qm] - P.wts[qp] * Q[qp];
+      x = x + temp * P.art1[i] * P.dzz[qm] / (P.dz[qm] + P.dz[q]);
+      qf = (Q[q] - x / P.art1[i] * (P.dti / (P.dt[i] * P.dzz[qm]))) * (P.dt[i] / P.d[i]);
+    } else {
+      qf = Q[q];
+    }
+    if ((parts & AD_FCT) && !P.riv_skip[i]) {
+      double qmax = G[5][q], qmin = G[4][q];
+      fct_level_bounds(P, i, k, Q, qmax, qmin);
+      if (qmin - qf > 0.0) qf = qmin;
+      if (qf - qmax > 0.0) qf = qmax;
+    }
+    QF[q] = qf;
+  }
+}
+
+// FCT_Q2 / FCT_Q2L alone (fct_q2.F:51-99) on QF already in memory.
+__global__ void __launch_bounds__(256) k_fct_q(const Dev P, int parts) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 2;
+  if (i > P.M || k > P.KBM1 || P.riv_skip[i]) return;
+  for (int t = 0; t < 2; ++t) {
+    if (!(parts & (t == 0 ? AD_Q2 : AD_Q2L))) continue;
+    const double* Q = (t == 0 ? P.q2 : P.q2l);
+    double* QF = (t == 0 ? P.q2f : P.q2lf);
+    size_t q = N3(P, i, k);
+    double qmax = Q[N3(P, NBSN(P, i, 1), k)], qmin = qmax;
+    for (int j = 2; j <= P.ntsn[i]; ++j) {
+      double v = Q[N3(P, NBSN(P, i, j), k)];
+      qmax = fmax(qmax, v);
+      qmin = fmin(qmin, v);
+    }
+    fct_level_bounds(P, i, k, Q, qmax, qmin);
+    double qf = QF[q];
+    if (qmin - qf > 0.0) qf = qmin;
+    if (qf - qmax > 0.0) qf = qmax;
+    QF[q] = qf;
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// VDIF_Q, MY2.5 (vdif_q.F:119-513), one thread per node column.  With copy_back the
+// end-of-closure shift Q2=Q2F, Q2L=Q2LF (internal_step.F:1034-1035) follows.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_vdif_q(const Dev P, int copy_back) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  const double A1 = 0.92, B1 = 16.6, A2 = 0.74, B2 = 10.1, C1 = 0.08;
+  const double E1 = 1.80, E2 = 1.33, SEF = 1.00, KAPPA = 0.40;
+  const double SMALL = 1.e-8, GH_MAX = .0233, GH_MIN = -.281;
+  const double SURFL = 2.e+5, GHC = -6.0;
+  const double COEF4 = 18.0 * A1 * A1 + 9.0 * A1 * A2;
+  const double COEF5 = 9.0 * A1 * A2;
+  const int KB = P.KB, KBM1 = P.KBM1;
+  const double DTI = P.dti;
+  const double d = P.d[i];
+  const bool wet = P.iswetn[i] == 1;
+  double boygr[kMaxKBs], prod[kMaxKBs], gh[kMaxKBs], dtef[kMaxKBs], vh[kMaxKBs], vhp[kMaxKBs];
+  for (int k = 0; k <= KB; ++k) { boygr[k] = 0.0; prod[k] = 0.0; gh[k] = 0.0; dtef[k] = 0.0; vh[k] = 0.0; vhp[k] = 0.0; }
+  double* Q2 = P.q2;
+  double* Q2L = P.q2l;
+  double* Q2F = P.q2f;
+  double* Q2LF = P.q2lf;
+  double* L = P.l;
+  auto n3 = [&](int k) { return N3(P, i, k); };
+  for (int k = 2; k <= KBM1; ++k)
+    if (Q2F[n3(k)] <= SMALL || Q2LF[n3(k)] <= SMALL) { Q2F[n3(k)] = SMALL; Q2LF[n3(k)] = SMALL; }
+  auto Acoef = [&](int k) {
+    return wet ? -0.5 * DTI * (P.kq[n3(k + 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k)] * d * d) : 0.0;
+  };
+  auto Ccoef = [&](int k) {
+    return wet ? -0.5 * DTI * (P.kq[n3(k - 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k - 1)] * d * d) : 0.0;
+  };
+  // Surface and bottom boundary values (vdif_q.F:172-246).
+  const size_t m1 = P.M + 1;
+  const int nt = P.ntve[i];
+  double wus = 0.0, wvs = 0.0, wub = 0.0, wvb = 0.0;
+  for (int j = 1; j <= nt; ++j) {
+    int c = P.nbve[(size_t)(j - 1) * m1 + i];
+    wus = wus + P.wusurf[c];
+    wvs = wvs + P.wvsurf[c];
+  }
+  double fn = (double)(float)nt;
+  wus = wus / fn;
+  wvs = wvs / fn;
+  double utau2 = sqrt(wus * wus + wvs * wvs);
+  vhp[1] = P.vhp1c * utau2;
+  vh[1] = 0.0;
+  double l0 = SURFL * utau2 / P.grav_n[i];
+  for (int j = 1; j <= nt; ++j) {
+    int c = P.nbve[(size_t)(j - 1) * m1 + i];
+    wub = wub + P.wubot[c];
+    wvb = wvb + P.wvbot[c];
+  }
+  wub = wub / fn;
+  wvb = wvb / fn;
+  Q2F[n3(KB)] = sqrt(wub * wub + wvb * wvb) * P.const1;
+  for (int k = 1; k <= KB; ++k) {
+    Q2[n3(k)] = fabs(Q2[n3(k)] + SMALL);
+    Q2L[n3(k)] = fabs(Q2L[n3(k)]);
+  }
+  if (wet) {
+    for (int k = 2; k <= KBM1; ++k) {
+      boygr[k] = P.grav_n[i] * (P.rho1[n3(k - 1)] - P.rho1[n3(k)]) / (P.dzz[n3(k - 1)] * d);
+      prod[k] = P.km[n3(k)] * 0.0 * pow(.5 * (-boygr[k] + fabs(boygr[k])), 1.5);
+    }
+    for (int k = 2; k <= KBM1; ++k) {
+      double uk = 0.0, vk = 0.0, ukm1 = 0.0, vkm1 = 0.0;
+      for (int j = 1; j <= nt; ++j) {
+        int c = P.nbve[(size_t)(j - 1) * m1 + i];
+        uk = uk + P.u[C3(P, c, k)];
+        vk = vk + P.v[C3(P, c, k)];
+        ukm1 = ukm1 + P.u[C3(P, c, k - 1)];
+        vkm1 = vkm1 + P.v[C3(P, c, k - 1)];
+      }
+      uk = uk / fn; vk = vk / fn; ukm1 = ukm1 / fn; vkm1 = vkm1 / fn;
+      double den = P.dzz[n3(k - 1)] * d;
+      prod[k] = prod[k] + P.km[n3(k)] * SEF * ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den);
+      prod[k] = prod[k] + P.kh[n3(k)] * boygr[k];
+    }
+  }
+  for (int k = 2; k <= KBM1; ++k) L[n3(k)] = Q2L[n3(k)] / Q2[n3(k)];
+  for (int k = 2; k <= KBM1; ++k) {
+    if (P.z[n3(k)] > -0.5) L[n3(k)] = fmax(L[n3(k)], KAPPA * l0);
+    if (boygr[k] < 0.0) {
+      double lmax = sqrt(fabs(GH_MIN) * Q2[n3(k)] / (-boygr[k] + SMALL));
+      L[n3(k)] = fmin(L[n3(k)], lmax);
+      Q2L[n3(k)] = Q2[n3(k)] * L[n3(k)];
+    }
+  }
+  for (int k = 1; k <= KBM1; ++k) gh[k] = (L[n3(k)] * L[n3(k)] / Q2[n3(k)]) * boygr[k];
+  for (int k = 1; k <= KB; ++k) gh[k] = fmin(gh[k], GH_MAX);
+  L[n3(1)] = KAPPA * l0;
+  L[n3(KB)] = 0.0;
+  gh[1] = 0.0;
+  gh[KB] = 0.0;
+  // STF (vdif_q.F:358-367) is recomputed from GH where it is needed.
+  auto stf_of = [&](int k) {
+    double s = 1.0;
+    if (gh[k] < 0.0) s = 1.0 - F4(0.9) * pow(gh[k] / GHC, 1.5);
+    if (gh[k] < GHC) s = F4(0.1);
+    return s;
+  };
+  for (int k = 1; k <= KB; ++k) dtef[k] = sqrt(Q2[n3(k)]) / (B1 * L[n3(k)] + SMALL) * stf_of(k);
+  // q2 equation (vdif_q.F:372-391)
+  for (int k = 2; k <= KBM1; ++k) {
+    double a = Acoef(k), c = Ccoef(k);
+    double p = 1. / (a + c * (1. - vh[k - 1]) - (2. * DTI * dtef[k] + 1.));
+    vh[k] = a * p;
+    vhp[k] = (-2. * DTI * prod[k] + c * vhp[k - 1] - Q2F[n3(k)]) * p;
+  }
+  if (wet)
+    for (int k = 1; k <= KBM1; ++k) {
+      int ki = KB - k;
+      Q2F[n3(ki)] = vh[ki] * Q2F[n3(ki + 1)] + vhp[ki];
+    }
+  // q2l equation (vdif_q.F:398-431)
+  vh[1] = 0.0;
+  vhp[1] = 0.0;
+  if (wet) {
+    for (int k = 2; k <= KBM1; ++k) {
+      double x = (1. / fabs(P.z[n3(k)] - P.z[n3(1)]) + 1. / fabs(P.z[n3(k)] - P.z[n3(KB)])) * L[n3(k)] / (d * KAPPA);
+      dtef[k] = dtef[k] * (1. + E2 * (x * x));
+      double a = Acoef(k), c = Ccoef(k);
+      double p = 1. / (a + c * (1. - vh[k - 1]) - (DTI * dtef[k] + 1.));
+      vh[k] = a * p;
+      vhp[k] = (DTI * (-prod[k] * L[n3(k)] * E1) + c * vhp[k - 1] - Q2LF[n3(k)]) * p;
+    }
+    for (int k = 1; k <= KBM1; ++k) {
+      int ki = KB - k;
+      Q2LF[n3(ki)] = vh[ki] * Q2LF[n3(ki + 1)] + vhp[ki];
+    }
+  }
+  for (int k = 2; k <= KBM1; ++k)
+    if (Q2F[n3(k)] <= SMALL || Q2LF[n3(k)] <= SMALL) { Q2F[n3(k)] = SMALL; Q2LF[n3(k)] = SMALL; }
+  // Stability functions and mixing coefficients (vdif_q.F:470-491)
+  for (int k = 1; k <= KB; ++k) {
+    double stf = stf_of(k);
+    double coef1 = A2 * (1.0 - 6.0 * A1 / B1 * stf);
+    double coef2 = 3.0 * A2 * B2 / stf + 18.0 * A1 * A2;
+    double coef3 = A1 * (1.0 - 3.0 * C1 - 6.0 * A1 / B1 * stf);
+    double sh = coef1 / (1.0 - coef2 * gh[k]);
+    double sm = (coef3 + sh * COEF4 * gh[k]) / (1. - COEF5 * gh[k]);
+    double kn = L[n3(k)] * sqrt(Q2[n3(k)]);
+    size_t q = n3(k);
+    P.kq[q] = 0.5 * (kn * KAPPA * sm + P.kq[q]);
+    P.km[q] = 0.5 * (kn * sm + P.km[q]);
+    P.kh[q] = 0.5 * (kn * sh * P.vprnu + P.kh[q]);
+  }
+  if (P.h[i] <= P.static_ssh_adj) {
+    double kqt = 0.0, kmt = 0.0, kht = 0.0;
+    for (int k = 2; k <= KBM1; ++k) { kqt = kqt + P.kq[n3(k)]; kmt = kmt + P.km[n3(k)]; kht = kht + P.kh[n3(k)]; }
+    kqt = kqt / (double)(KBM1 - 1);
+    kmt = kmt / (double)(KBM1 - 1);
+    kht = kht / (double)(KBM1 - 1);
+    for (int k = 2; k <= KBM1; ++k) { P.kq[n3(k)] = kqt; P.km[n3(k)] = kmt; P.kh[n3(k)] = kht; }
+  }
+  if (copy_back)
+    for (int k = 1; k <= KB; ++k) { Q2[n3(k)] = Q2F[n3(k)]; Q2L[n3(k)] = Q2LF[n3(k)]; }
+}
+
+// Q2=Q2F, Q2L=Q2LF on every node and level; N2E3D(KM,KM1) (internal_step.F:1034-1053).
+__global__ void __launch_bounds__(256) k_turb_update(const Dev P) {
+  int i = blockIdx.x * 32 + threadIdx.x;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (k > P.KB) return;
+  if (i <= P.M) {
+    size_t q = N3(P, i, k);
+    P.q2[q] = P.q2f[q];
+    P.q2l[q] = P.q2lf[q];
+  }
+  if (i >= 1 && i <= P.N) {
+    const size_t n1 = P.N + 1;
+    P.km1[C3(P, i, k)] = ONE_THIRD * (P.km[N3(P, P.nv[i], k)] + P.km[N3(P, P.nv[n1 + i], k)] + P.km[N3(P, P.nv[2 * n1 + i], k)]);
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// ADV_T / ADV_S (adv_t.F:124-1042, adv_s.F) with FCT_T / FCT_S (fct_t.F:51-104,
+// fct_s.F:50-108) on the same (node, layer) thread.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_adv_ts(const Dev P, int parts) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (i > P.M || k > P.KBM1) return;
+  const size_t v1 = P.NCV + 1, vi1 = P.NCV_I + 1;
+  const bool wet = P.iswetn[i] * P.iswetnt[i] == 1;
+  const int ob = P.node_obc[i];
+  for (int t = 0; t < 2; ++t) {
+    if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
+    const double* F1 = (t == 0 ? P.t1 : P.s1);
+    double* FF1 = (t == 0 ? P.tf1 : P.sf1);
+    double* const* G = P.gt[t];
+    const double* Fk = F1 + N3(P, 0, k);
+    double x = 0.0, xa = 0.0;
+    for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
+      int code = P.node_he[q];
+      int he = code >> 1;
+      int ia = P.niec[he], ib = P.niec[v1 + he];
+      int c = P.ntrg[he];
+      size_t ck = C3(P, c, k);
+      double dtij = P.dt1[c] * P.dz1[ck];
+      double un = P.v[ck] * P.dltxe[he] - P.u[ck] * P.dltye[he];
+      size_t qa = N3(P, ia, k), qb = N3(P, ib, k);
+      double fij1 = Fk[ia] + P.dltxncve[he] * G[0][qa] + P.dltyncve[he] * G[1][qa];
+      double fij2 = Fk[ib] + P.dltxncve[vi1 + he] * G[0][qb] + P.dltyncve[vi1 + he] * G[1][qb];
+      double t1min = fmin(G[4][qa], Fk[ia]), t1max = fmax(G[5][qa], Fk[ia]);
+      double t2min = fmin(G[4][qb], Fk[ib]), t2max = fmax(G[5][qb], Fk[ib]);
+      if (fij1 < t1min) fij1 = t1min;
+      if (fij1 > t1max) fij1 = t1max;
+      if (fij2 < t2min) fij2 = t2min;
+      if (fij2 > t2max) fij2 = t2max;
+      double viscof = P.fact * 0.5 * (P.viscofh[qa] * P.nn_hvc[ia] + P.viscofh[qb] * P.nn_hvc[ib]) +
+                      P.fm1 * 0.5 * (P.nn_hvc[ia] + P.nn_hvc[ib]);
+      double txx = 0.5 * (G[2][qa] + G[2][qb]) * viscof;
+      double tyy = 0.5 * (G[3][qa] + G[3][qb]) * viscof;
+      double fxx = -dtij * txx * P.dltye[he];
+      double fyy = dtij * tyy * P.dltxe[he];
+      double sg = fsign1(un);
+      double exflux = -un * dtij * ((1.0 + sg) * fij2 + (1.0 - sg) * fij1) * 0.5 + fxx + fyy;
+      if (code & 1) {
+        x = x - exflux;
+        xa = xa - (exflux - fxx - fyy);
+      } else {
+        x = x + exflux;
+        xa = xa + (exflux - fxx - fyy);
+      }
+    }
+    if (ob > 0) (t == 0 ? P.xflux_obc_t : P.xflux_obc_s)[(size_t)(k - 1) * (P.iobcn + 1) + ob] = xa;
+    size_t q = N3(P, i, k);
+    double ff;
+    if (wet) {
+      const double* DZ = P.dz;
+      double temp;
+      if (k == 1) {
+        size_t qp = N3(P, i, k + 1);
+        temp = -P.wts[qp] * (F1[q] * DZ[qp] + F1[qp] * DZ[q]) / (DZ[q] + DZ[qp]);
+      } else if (k == P.KBM1) {
+        size_t qm = N3(P, i, k - 1);
+        temp = P.wts[q] * (F1[q] * DZ[qm] + F1[qm] * DZ[q]) / (DZ[q] + DZ[qm]);
+      } else {
+        size_t qm = N3(P, i, k - 1), qp = N3(P, i, k + 1);
+        temp = P.wts[q] * (F1[q] * DZ[qm] + F1[qm] * DZ[q]) / (DZ[q] + DZ[qm]) -
+               P.wts[qp] * (F1[q] * DZ[qp] + F1[qp] * DZ[q]) / (DZ[q] + DZ[qp]);
+      }
+      if (P.isonb[i] == 2)
+        x = temp * P.art1[i];
+      else
+        x = x + temp * P.art1[i];
+      ff = (F1[q] - x / P.art1[i] * (P.dti / (P.dt[i] * DZ[q]))) * (P.dt[i] / P.dtfa[i]);
+    } else {
+      ff = F1[q];
+    }
+    if (parts & AD_FCT) {
+      if (!P.riv_skip[i]) {
+        double fmx = G[5][q], fmn = G[4][q];
+        fct_layer_bounds(P, i, k, F1, fmx, fmn);
+        if (fmn - ff > 0.0) ff = fmn;
+        if (ff - fmx > 0.0) ff = fmx;
+      }
+      if (t == 1 && ff < 0.0) ff = 0.0;
+    }
+    FF1[q] = ff;
+  }
+}
+
+// FCT_T / FCT_S alone (fct_t.F:51-104, fct_s.F:50-108) on TF1/SF1 in memory.
+__global__ void __launch_bounds__(256) k_fct_ts(const Dev P, int parts) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (i > P.M || k > P.KBM1) return;
+  for (int t = 0; t < 2; ++t) {
+    if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
+    const double* F1 = (t == 0 ? P.t1 : P.s1);
+    double* FF1 = (t == 0 ? P.tf1 : P.sf1);
+    size_t q = N3(P, i, k);
+    double ff = FF1[q];
+    if (!P.riv_skip[i]) {
+      double fmx = F1[N3(P, NBSN(P, i, 1), k)], fmn = fmx;
+      for (int j = 2; j <= P.ntsn[i]; ++j) {
+        double v = F1[N3(P, NBSN(P, i, j), k)];
+        fmx = fmax(fmx, v);
+        fmn = fmin(fmn, v);
+      }
+      fct_layer_bounds(P, i, k, F1, fmx, fmn);
+      if (fmn - ff > 0.0) ff = fmn;
+      if (ff - fmx > 0.0) ff = fmx;
+    }
+    if (t == 1 && ff < 0.0) ff = 0.0;
+    FF1[q] = ff;
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// VDIF_TS(1,TF1) and VDIF_TS(2,SF1) (vdif_ts.F:78-337) with heating off (the surface
+// heat and short-wave terms are zero), one thread per node column.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_vdif_ts(const Dev P, int parts) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M || P.iswetn[i] != 1) return;
+  const int KB = P.KB, KBM1 = P.KBM1, KBM2 = P.KBM2;
+  const double DTI = P.dti, UMOLPR = P.umol * 1.e0, GW = 0.0;
+  const double d = P.d[i];
+  auto n3 = [&](int k) { return N3(P, i, k); };
+  auto AF = [&](int k) { double fkh = P.kh[n3(k + 1)]; return -DTI * (fkh + UMOLPR) / (P.dz[n3(k)] * P.dzz[n3(k)] * d * d); };
+  auto CF = [&](int k) { double fkh = P.kh[n3(k)]; return -DTI * (fkh + UMOLPR) / (P.dz[n3(k)] * P.dzz[n3(k - 1)] * d * d); };
+  const double khbottom = P.kh[n3(KBM1)];
+  const bool update = P.iswetn[i] * P.iswetnt[i] == 1;
+  for (int t = 0; t < 2; ++t) {
+    if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
+    double* F = (t == 0 ? P.tf1 : P.sf1);
+    double vhf[kMaxKBs], vhpf[kMaxKBs];
+    const double rad = 0.0, wfsurf = 0.0, swradf = 0.0, sasurf = 0.0;
+    double af1 = AF(1);
+    vhf[1] = af1 / (af1 - 1.);
+    vhpf[1] = -DTI * (sasurf + wfsurf - swradf + rad - rad) / (-P.dz[n3(1)] * d) - F[n3(1)];
+    vhpf[1] = vhpf[1] / (af1 - 1.);
+    for (int k = 2; k <= KBM2; ++k) {
+      double af = AF(k), cf = CF(k);
+      double p = 1. / (af + cf * (1. - vhf[k - 1]) - 1.);
+      vhf[k] = af * p;
+      vhpf[k] = (cf * vhpf[k - 1] - F[n3(k)] + DTI * (rad - rad) / (d * P.dz[n3(k)])) * p;
+    }
+    if (P.isonb[i] != 2 && update) {
+      double pfx = t == 0 ? P.pfpxb_t[i] : P.pfpxb_s[i];
+      double pfy = t == 0 ? P.pfpyb_t[i] : P.pfpyb_s[i];
+      double ah = t == 0 ? P.ah_bottom_t[i] : P.ah_bottom_s[i];
+      double tmp1 = pfx * P.cos_sita[i] + pfy * P.sin_sita[i];
+      double tmp2 = ah * P.phpn[i];
+      double tmp3 = khbottom + UMOLPR + ah * P.phpn[i] * P.phpn[i];
+      double tmp = tmp1 * tmp2 / tmp3 * (khbottom + UMOLPR);
+      if (t == 0) {
+        if (tmp1 > 0.0) tmp = 0.0;
+      } else {
+        if (tmp1 < 0.0) tmp = 0.0;
+        tmp = -tmp;
+      }
+      double cfb = CF(KBM1);
+      double ff = (cfb * vhpf[KBM2] - F[n3(KBM1)] - GW + DTI * (rad - rad - tmp) / (d * P.dz[n3(KBM1)])) /
+                  (cfb * (1. - vhf[KBM2]) - 1.);
+      F[n3(KBM1)] = ff;
+      for (int k = 2; k <= KBM1; ++k) {
+        int ki = KB - k;
+        ff = (vhf[ki] * ff + vhpf[ki]);
+        F[n3(ki)] = ff;
+      }
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// BCOND_TS(1) and BCOND_TS(2) (bcond_ts.F:60-262): river nodes take the river T/S; open
+// boundary nodes take the outflow estimate with the radiation perturbation of
+// OBC_TS_TYPE and the neighbour clamp, or keep T1/S1 on inflow.  One block.
+// -------------------------------------------------------------------------------------
+__global__ void k_bcond_ts(const Dev P, int parts) {
+  const int KBM1 = P.KBM1;
+  for (int r = threadIdx.x + 1; r <= P.numqbc; r += blockDim.x) {
+    int n1 = P.river_location == 0 ? P.inodeq[r] : P.n_icellq[r];
+    int n2 = P.river_location == 0 ? 0 : P.n_icellq[(size_t)(P.numqbc + 1) + r];
+    for (int k = 1; k <= KBM1; ++k) {
+      P.tf1[N3(P, n1, k)] = P.tdis[r];
+      P.sf1[N3(P, n1, k)] = P.sdis[r];
+      if (n2 > 0) {
+        P.tf1[N3(P, n2, k)] = P.tdis[r];
+        P.sf1[N3(P, n2, k)] = P.sdis[r];
+      }
+    }
+  }
+  __syncthreads();
+  for (int ob = threadIdx.x + 1; ob <= P.iobcn; ob += blockDim.x) {
+    int j = P.i_obc_n[ob], j1 = P.next_obc[ob];
+    for (int t = 0; t < 2; ++t) {
+      if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
+      const double* F1 = t == 0 ? P.t1 : P.s1;
+      double* FF1 = t == 0 ? P.tf1 : P.sf1;
+      const double* XO = t == 0 ? P.xflux_obc_t : P.xflux_obc_s;
+      double t2d = 0.0, t2dn = 0.0, xf2d = 0.0;
+      for (int k = 1; k <= KBM1; ++k) {
+        t2d = t2d + F1[N3(P, j, k)] * P.dz[N3(P, j, k)];
+        t2dn = t2dn + FF1[N3(P, j1, k)] * P.dz[N3(P, j1, k)];
+        xf2d = xf2d + XO[(size_t)(k - 1) * (P.iobcn + 1) + ob];
+      }
+      if (P.uard_obcn[ob] > 0.0) {
+        double tmp = xf2d + t2d * P.uard_obcn[ob];
+        double t2d_obc = (t2d * P.dt[j] - tmp * P.dti / P.art1[j]) / P.d[j];
+        double cc = 0.0, cp = 1.0;
+        if (P.obc_ts_type != 1) {
+          cc = sqrt(P.grav_n[j] * P.h[j]) * P.dti / P.dltn_obc[ob];
+          cp = cc + 1.0;
+        }
+        for (int k = 1; k <= KBM1; ++k) {
+          double ttmp;
+          double pert_next = FF1[N3(P, j1, k)] - t2dn;
+          if (P.obc_ts_type == 1) {
+            ttmp = pert_next;
+          } else if (P.obc_ts_type == 2) {
+            double pert = F1[N3(P, j, k)] - t2d;
+            ttmp = (cc * pert_next + pert) / cp;
+          } else {
+            double pert = F1[N3(P, j, k)] - t2d;
+            ttmp = (cc * pert_next + pert * (1.0 - P.dti / 10800.0)) / cp;
+          }
+          FF1[N3(P, j, k)] = t2d_obc + ttmp;
+        }
+        for (int k = 1; k <= KBM1; ++k) {
+          double fmx = F1[N3(P, NBSN(P, j, 1), k)], fmn = fmx;
+          for (int jj = 2; jj <= P.ntsn[j]; ++jj) {
+            double v = F1[N3(P, NBSN(P, j, jj), k)];
+            fmx = fmax(fmx, v);
+            fmn = fmin(fmn, v);
+          }
+          fct_layer_bounds(P, j, k, F1, fmx, fmn);
+          double ff = FF1[N3(P, j, k)];
+          if (fmn - ff > 0.0) ff = fmn;
+          if (ff - fmx > 0.0) ff = fmx;
+          FF1[N3(P, j, k)] = ff;
+        }
+      } else {
+        for (int k = 1; k <= KBM1; ++k) FF1[N3(P, j, k)] = F1[N3(P, j, k)];
+      }
+    }
+  }
+}
+
+// DENS2_2D (eqs_of_state.F:290-319), same operation order.
+__device__ inline double dens2(double S, double T) {
+  double r = S * S * S * 6.76786136E-6 - S * S * 4.8249614E-4 + S * 8.14876577E-1 - 0.22584586E0;
+  r = r * (T * T * T * 1.667E-8 - T * T * 8.164E-7 + T * 1.803E-5);
+  r = r + 1.0 - T * T * T * 1.0843E-6 + T * T * 9.8185E-5 - T * 4.786E-3;
+  r = r * (S * S * S * 6.76786136E-6 - S * S * 4.8249614E-4 + S * 8.14876577E-1 + 3.895414E-2);
+  r = r - (T - 3.98) * (T - 3.98) * (T + 283.0) / (503.57 * (T + 67.26));
+  return r * 1.e-3;
+}
+
+// -------------------------------------------------------------------------------------
+// End of the internal step: T1=TF1, S1=SF1, N2E3D to T/S, DENS2 with N2E3D(RHO1,RHO),
+// N2E3D(KM,KM1), U=UF, V=VF, ET=EL, DT=D, ET1=EL1, DT1=D1, WD_UPDATE(3)
+// (internal_step.F:1053-1590).  Threads over (max(M,N)+1) x KB.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_final(const Dev P, int parts) {
+  int i = blockIdx.x * 32 + threadIdx.x;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (k > P.KB) return;
+  const double* Tn = (parts & FI_T) ? P.tf1 : P.t1;
+  const double* Sn = (parts & FI_S) ? P.sf1 : P.s1;
+  if (i <= P.M) {
+    size_t q = N3(P, i, k);
+    if (parts & FI_T) P.t1[q] = P.tf1[q];
+    if (parts & FI_S) P.s1[q] = P.sf1[q];
+    if (parts & FI_DENS) P.rho1[q] = (k == P.KB || i == 0) ? 0.0 : dens2(Sn[q], Tn[q]);
+    if ((parts & FI_SHIFT) && k == 1) {
+      P.et[i] = P.el[i];
+      P.dt[i] = P.d[i];
+      if (P.wetting_drying_on) P.iswetnt[i] = P.iswetn[i];
+    }
+  }
+  if (i >= 1 && i <= P.N) {
+    const size_t n1 = P.N + 1;
+    int a = P.nv[i], b = P.nv[n1 + i], c = P.nv[2 * n1 + i];
+    size_t qa = N3(P, a, k), qb = N3(P, b, k), qc = N3(P, c, k);
+    size_t q = C3(P, i, k);
+    if (parts & FI_T) P.t[q] = ONE_THIRD * (P.tf1[qa] + P.tf1[qb] + P.tf1[qc]);
+    if (parts & FI_S) P.s[q] = ONE_THIRD * (P.sf1[qa] + P.sf1[qb] + P.sf1[qc]);
+    if (parts & FI_DENS) {
+      double ra = k == P.KB ? 0.0 : dens2(Sn[qa], Tn[qa]);
+      double rb = k == P.KB ? 0.0 : dens2(Sn[qb], Tn[qb]);
+      double rc = k == P.KB ? 0.0 : dens2(Sn[qc], Tn[qc]);
+      P.rho[q] = ONE_THIRD * (ra + rb + rc);
+    }
+    if (parts & FI_KM1) P.km1[q] = ONE_THIRD * (P.km[qa] + P.km[qb] + P.km[qc]);
+    if (parts & FI_SHIFT) {
+      P.u[q] = P.uf[q];
+      P.v[q] = P.vf[q];
+      if (k == 1) {
+        P.et1[i] = P.el1[i];
+        P.dt1[i] = P.d1[i];
+        if (P.wetting_drying_on) P.iswetct[i] = P.iswetc[i];
+      }
+    }
+  }
+}
+
+// FP64 budgets over node control volumes, fixed-order two-level reduction.
+__global__ void k_budget_partial(const Dev P, double* part) {
+  __shared__ double sv[256], sh[256], ss[256];
+  int tid = threadIdx.x;
+  double v = 0.0, hh = 0.0, s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + tid + 1; i <= P.M; i += gridDim.x * blockDim.x) {
+    double dd = P.d[i] * P.art1[i];
+    double ct = 0.0, cs = 0.0;
+    for (int k = 1; k <= P.KBM1; ++k) {
+      ct = ct + P.t1[N3(P, i, k)] * P.dz[N3(P, i, k)];
+      cs = cs + P.s1[N3(P, i, k)] * P.dz[N3(P, i, k)];
+    }
+    v = v + dd;
+    hh = hh + ct * dd;
+    s = s + cs * dd;
+  }
+  sv[tid] = v; sh[tid] = hh; ss[tid] = s;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (tid < st) { sv[tid] += sv[tid + st]; sh[tid] += sh[tid + st]; ss[tid] += ss[tid + st]; }
+    __syncthreads();
+  }
+  if (tid == 0) { part[3 * blockIdx.x] = sv[0]; part[3 * blockIdx.x + 1] = sh[0]; part[3 * blockIdx.x + 2] = ss[0]; }
+}
+__global__ void k_budget_final(const double* part, int nb, double* out) {
+  if (threadIdx.x != 0) return;
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int j = 0; j < nb; ++j) { a += part[3 * j]; b += part[3 * j + 1]; c += part[3 * j + 2]; }
+  out[0] = a; out[1] = b; out[2] = c;
+}
+
+void launch_grad(const Dev& P, cudaStream_t s, int which) {
+  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));
+  k_grad<<<g, b, 0, s>>>(P, which);
+}
+void launch_adv_q(const Dev& P, cudaStream_t s, int parts) {
+  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1 - 1, 8));
+  k_adv_q<<<g, b, 0, s>>>(P, parts);
+}
+void launch_fct_q(const Dev& P, cudaStream_t s, int parts) {
+  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1 - 1, 8));
+  k_fct_q<<<g, b, 0, s>>>(P, parts);
+}
+void launch_vdif_q(const Dev& P, cudaStream_t s, int copy_back) {
+  k_vdif_q<<<nblk(P.M, 128), 128, 0, s>>>(P, copy_back);
+}
+void launch_turb_update(const Dev& P, cudaStream_t s) {
+  int n = (P.M > P.N ? P.M : P.N) + 1;
+  dim3 b(32, 8), g(nblk(n, 32), nblk(P.KB, 8));
+  k_turb_update<<<g, b, 0, s>>>(P);
+}
+void launch_adv_ts(const Dev& P, cudaStream_t s, int parts) {
+  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));
+  k_adv_ts<<<g, b, 0, s>>>(P, parts);
+}
+void launch_fct_ts(const Dev& P, cudaStream_t s, int parts) {
+  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));
+  k_fct_ts<<<g, b, 0, s>>>(P, parts);
+}
+void launch_vdif_ts(const Dev& P, cudaStream_t s, int parts) {
+  k_vdif_ts<<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
+}
+void launch_bcond_ts(const Dev& P, cudaStream_t s, int parts) { k_bcond_ts<<<1, 256, 0, s>>>(P, parts); }
+void launch_final(const Dev& P, cudaStream_t s, int parts) {
+  int n = (P.M > P.N ? P.M : P.N) + 1;
+  dim3 b(32, 8), g(nblk(n, 32), nblk(P.KB, 8));
+  k_final<<<g, b, 0, s>>>(P, parts);
+}
+void launch_budget(const Dev& P, cudaStream_t s) {
+  const int nb = 148;
+  k_budget_partial<<<nb, 256, 0, s>>>(P, P.budget + 3);
+  k_budget_final<<<1, 32, 0, s>>>(P.budget + 3, nb, P.budget);
+}
+
+}  // namespace fvg

@@ -185,3 +185,20 @@ class Fvcom(CEngine):
 
     def sync(self):
         self._check(self.lib.fvg_sync(self.h), "sync")
+
+    def set_ramp(self, r):
+        self.lib.fvg_set_ramp.argtypes = [C.c_void_p, C.c_double]
+        self._check(self.lib.fvg_set_ramp(self.h, float(r)), "set_ramp")
+
+    def use_graph(self, on):
+        self.lib.fvg_use_graph.argtypes = [C.c_void_p, C.c_int32]
+        self._check(self.lib.fvg_use_graph(self.h, int(bool(on))), "use_graph")
+
+    def budget(self):
+        out = (C.c_double * 3)()
+        self.lib.fvg_budget.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        self._check(self.lib.fvg_budget(self.h, out), "budget")
+        return tuple(out)
+
+    def shutdown_check(self):
+        return int(self.lib.fvg_shutdown_check(self.h))
