@@ -155,6 +155,11 @@ __global__ void __launch_bounds__(256) k_adv_q(const Dev P, int parts) {
     double* QF = (t == 0 ? P.q2f : P.q2lf);
     double* const* G = P.gq[t];
     const double* Qk = Q + N3(P, 0, k);
+    if (k == 2) {
+      // QF = 0 on every level before the interior levels are set (adv_q.F:114)
+      QF[N3(P, i, 1)] = 0.0;
+      QF[N3(P, i, P.KB)] = 0.0;
+    }
     double x = 0.0;
     for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
       int code = P.node_he[q];
