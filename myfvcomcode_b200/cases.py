@@ -6,7 +6,8 @@ shapes, sizes and forcing the workloads call for:
 * ``estuary_channel``: the idealised estuary channel, 20 km x 4 km, a 100 x 20 structured
   grid split diagonally (2,121 nodes, 4,000 cells), depth linear 5 -> 20 m seaward, M2
   tide of 1.0 m on the 21 seaward nodes, one 100 m^3/s fresh river at the head,
-  T = 15 C / S = 30 initially, MY2.5, DTE = 2 s, ISPLIT = 10, no wetting and drying.
+  T = 15 C / S = 30 initially, MY2.5, DTE = 2 s, ISPLIT = 10, no wetting and drying,
+  a sponge layer (radius 6 km, coefficient 0.01) at the open boundary.
   ``nx``/``ny``/``kb`` shrink it for quick tests.
 * ``coastal_mesh``: the large coastal mesh, a Delaunay triangulation of jittered lattice
   points in a 200 km x 100 km box (200,000 points by default), bathymetry
@@ -74,7 +75,7 @@ def default_params(**kw):
 
 
 def estuary_channel(nx=100, ny=20, kb=11, lx=20000.0, ly=4000.0, river_q=100.0,
-                    river_location="node", lat=30.0, river=True, **pkw):
+                    river_location="node", lat=30.0, river=True, sponge=True, **pkw):
     # The lower seaward corner quad is split along its other diagonal so that no cell
     # has one open and one solid side (tge.F:563-580 rejects such cells).
     vx, vy, tri, nid = _structured(nx, ny, lx, ly, flip={(nx - 1, 0)})
@@ -88,8 +89,13 @@ def estuary_channel(nx=100, ny=20, kb=11, lx=20000.0, ly=4000.0, river_q=100.0,
         rloc = 2 * (ny // 2) + 2
     kbm1 = kb - 1
     rivers = [dict(loc=rloc, dist=[1.0 / kbm1] * kbm1)] if river else []
+    # Sponge layer at the open boundary, as FVCOM's Estuary example carries one
+    # (Examples/Estuary/tstinp/tst_spg.dat): centred on the middle open-boundary node,
+    # radius 0.3 of the channel length, coefficient 0.01.  Without it the corner where
+    # the open boundary meets the wall grows grid-scale noise after about 0.6 day.
+    spg = [(obc[len(obc) // 2], 0.3 * lx, 0.01)] if sponge else ()
     g = build_grid(vx, vy, nv, h, kb, obc_nodes=obc, obc_types=[1] * len(obc),
-                   cor_lat=lat, sponge=(), horcon=0.2, z0b=0.001,
+                   cor_lat=lat, sponge=spg, horcon=0.2, z0b=0.001,
                    rivers=rivers, river_location=river_location)
     n_obc = len(obc)
     tide = dict(period=np.array([M2_PERIOD]), apt=np.full((n_obc, 1), 1.0),
@@ -152,6 +158,12 @@ def coastal_mesh(npts=200000, kb=41, lx=200000.0, ly=100000.0, seed=1234, lat=40
     tri = tri[keep]
     cross = cross[keep]
     tri = np.where((cross < 0)[:, None], tri[:, [0, 2, 1]], tri)
+    # Number the cells in the same column-major lattice order as the nodes (x strip, then
+    # y), as mesh generators emit them; Delaunay returns triangles in arbitrary order.
+    cxs = (vx[tri[:, 0]] + vx[tri[:, 1]] + vx[tri[:, 2]]) / 3.0
+    cys = (vy[tri[:, 0]] + vy[tri[:, 1]] + vy[tri[:, 2]]) / 3.0
+    order = np.lexsort((cys, np.floor(cxs / dx)))
+    tri = tri[order]
     nv = _ccw_to_fvcom(tri)
     f, res = _grf(rng, lx, ly, 10000.0)
     h = 5.0 + 195.0 * _bilinear(f, res, vx, vy)

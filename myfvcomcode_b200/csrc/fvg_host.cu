@@ -175,16 +175,18 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   launch_begin_step(P, s);
   launch_cell_pre(P, s, CP_ADJUST1 | CP_BC5 | CP_BCOND8 | CP_BROUGH);
   mk.mark(s, G_CELL_PRE);
+  launch_grad3(P, s);
   launch_advection3d(P, s);
   mk.mark(s, G_ADV3D);
   launch_baropg(P, s, !p.barotropic, 1);
+  launch_ext_prep(P, s);
   mk.mark(s, G_BAROPG);
   launch_ext_cell(P, s, 1, 1, EC_INT_ADVAVE);
   launch_int_reset(P, s);
   mk.mark(s, G_INT_ADVAVE);
   for (int iext = 1; iext <= p.isplit; ++iext) {
     for (int K = 1; K <= 4; ++K) {
-      launch_ext_node(P, s, iext, K, EN_EXTEL | EN_BC | (K == 1 ? EN_COPY_ELRK : 0));
+      launch_ext_node(P, s, iext, K, EN_EXTEL | EN_BC | EN_GRAD | (K == 1 ? EN_COPY_ELRK : 0));
       mk.mark(s, G_EXT_NODE);
       if (p.wetting_drying_on) {
         launch_wet_judge(P, s);
@@ -206,6 +208,7 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   mk.mark(s, G_VV_COL);
   launch_w_viscofh(P, s, 1, 1);
   mk.mark(s, G_W_VISC);
+  launch_grad3(P, s);
   launch_adv_uv(P, s);
   mk.mark(s, G_ADV_UV);
   launch_vdif_uv(P, s, VU_VDIF | VU_BC3 | VU_WREAL);
@@ -387,6 +390,24 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
       for (int s = 0; s < 3; ++s) ce[3 * i + s] = cl[i][s];
     }
     UPI(cell_edge, ce.data(), ce.size());
+    std::vector<std::vector<int>> ch(n1);
+    for (int he = 1; he <= m->ncv; ++he) ch[m->ntrg[he]].push_back(he);
+    std::vector<int> chv(3 * n1, 0);
+    for (size_t i = 1; i < n1; ++i) {
+      if (ch[i].size() != 3) { h->err = "cell without exactly three half-edges"; return fail(FVG_ERR_BOUNDS); }
+      for (int s2 = 0; s2 < 3; ++s2) {
+        int he = ch[i][s2];
+        int a = m->niec[he], b = m->niec[v1 + he];
+        bool ok_a = false, ok_b = false;
+        for (int j = 0; j < 3; ++j) {
+          ok_a |= m->nv[j * n1 + i] == a;
+          ok_b |= m->nv[j * n1 + i] == b;
+        }
+        if (!ok_a || !ok_b) { h->err = "half-edge nodes not on its cell"; return fail(FVG_ERR_BOUNDS); }
+        chv[3 * i + s2] = he;
+      }
+    }
+    UPI(cell_he, chv.data(), chv.size());
   }
   // open boundary
   {
@@ -525,6 +546,14 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
       if ((rc = dalloc(h, &P.gt[t][g], ms * KB))) return fail(rc);
     }
   if ((rc = dalloc(h, &P.budget, 3 + 3 * 148))) return fail(rc);
+  P.ncvs = (int)pad32(m->ncv + 1);
+  for (int q = 0; q < 4; ++q) {
+    if ((rc = dalloc(h, &P.g2d[q], n1))) return fail(rc);
+    if ((rc = dalloc(h, &P.g3[q], ns * KB))) return fail(rc);
+  }
+  if ((rc = dalloc(h, &P.exf2d, v1))) return fail(rc);
+  for (int t = 0; t < 2; ++t)
+    if ((rc = dalloc(h, &P.ex[t], (size_t)P.ncvs * KB))) return fail(rc);
 
   // ---- schedule ----
   h->sched_cap = 256;
@@ -716,11 +745,11 @@ int32_t fvg_profile_groups(void) { return G_COUNT; }
 int32_t fvg_kernels_per_step(const fvg_handle* h) {
   if (!h) return -1;
   const fvg_params& p = h->prm;
-  int n = 1 + 1 + 1 + 1 + 2;                                // begin, cell_pre, adv3d, baropg, int advave+reset
+  int n = 1 + 1 + 2 + 2 + 2;                                // begin, cell_pre, grad3+adv3d, baropg+prep, int advave+reset
   n += p.isplit * 4 * (3 + (p.wetting_drying_on ? 2 : 0)); // RK stages
-  n += 1 + 1 + 1 + 1 + 1 + 1;                              // adjust2, vertvl x2, w/viscofh, adv_uv, vdif_uv
-  n += 3;                                                  // grad_q, adv_q, vdif_q
-  if (p.temperature_active || p.salinity_active) n += 4;   // grad_ts, adv_ts, vdif_ts, bcond_ts
+  n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv
+  n += 4;                                                  // grad_q, adv_q (2 phases), vdif_q
+  if (p.temperature_active || p.salinity_active) n += 5;   // grad_ts, adv_ts (2 phases), vdif_ts, bcond_ts
   n += 1;                                                  // final
   return n;
 }
@@ -773,18 +802,25 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
   CK(cudaMemcpyAsync(P.ctl, h->h_ctl, sizeof(int), cudaMemcpyHostToDevice, s));
   const int spc = 0;
   switch (r) {
-    case FVG_R_EXTEL_EDGE: launch_ext_node(P, s, 1, arg, EN_EXTEL); break;
+    case FVG_R_EXTEL_EDGE:
+      launch_ext_prep(P, s);
+      launch_ext_node(P, s, 1, arg, EN_EXTEL);
+      break;
     case FVG_R_BCOND_ELF: launch_ext_node(P, s, 1, arg, EN_BC); break;
     case FVG_R_N2E2D_ELF: launch_ext_cell(P, s, 1, 1, EC_N2E); break;
     case FVG_R_WET_JUDGE: launch_wet_judge(P, s); break;
     case FVG_R_FLUX_OBN: launch_ext_cell(P, s, 1, arg, EC_FLUXOBN); break;
-    case FVG_R_ADVAVE: launch_ext_cell(P, s, 1, 1, EC_ADVAVE); break;
+    case FVG_R_ADVAVE:
+      launch_ext_prep(P, s);
+      launch_ext_cell(P, s, 1, 1, EC_ADVAVE);
+      break;
     case FVG_R_EXTUV_EDGE: launch_ext_cell(P, s, 1, arg, EC_EXTUV); break;
     case FVG_R_BCOND_UV2D: launch_ext_cell(P, s, 1, 1, EC_BC2); break;
     case FVG_R_EXT_UPDATE: launch_ext_update(P, s, arg); break;
     case FVG_R_EXTERNAL_STEP:
+      launch_ext_prep(P, s);
       for (int K = 1; K <= 4; ++K) {
-        launch_ext_node(P, s, iext, K, EN_EXTEL | EN_BC | (K == 1 ? EN_COPY_ELRK : 0));
+        launch_ext_node(P, s, iext, K, EN_EXTEL | EN_BC | EN_GRAD | (K == 1 ? EN_COPY_ELRK : 0));
         if (p.wetting_drying_on) launch_wet_judge(P, s);
         launch_ext_cell(P, s, iext, K,
                         (p.wetting_drying_on ? 0 : EC_N2E) | EC_FLUXOBN | EC_ADVAVE | EC_EXTUV | EC_BC2 |
@@ -801,13 +837,17 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
       launch_cell_pre(P, s, CP_BROUGH);
       launch_vertvl_col(P, s, VC_BOT_NODE);
       break;
-    case FVG_R_ADVECTION3D: launch_advection3d(P, s); break;
+    case FVG_R_ADVECTION3D:
+      launch_grad3(P, s);
+      launch_advection3d(P, s);
+      break;
     case FVG_R_BAROPG:
       launch_baropg(P, s, 1, 0);
       launch_vertvl_col(P, s, VC_RHO_ROUNDTRIP);
       break;
     case FVG_R_INT_PRE_EXT:
       launch_baropg(P, s, 0, 1);
+      launch_ext_prep(P, s);
       launch_ext_cell(P, s, 1, 1, EC_INT_ADVAVE);
       launch_int_reset(P, s);
       break;
@@ -817,7 +857,10 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
       launch_w_viscofh(P, s, 1, 0);
       break;
     case FVG_R_VISCOFH: launch_w_viscofh(P, s, 0, 1); break;
-    case FVG_R_ADV_UV: launch_adv_uv(P, s); break;
+    case FVG_R_ADV_UV:
+      launch_grad3(P, s);
+      launch_adv_uv(P, s);
+      break;
     case FVG_R_VDIF_UV: launch_vdif_uv(P, s, VU_VDIF); break;
     case FVG_R_BCOND_UV3D: launch_vdif_uv(P, s, VU_BC3); break;
     case FVG_R_WREAL: launch_vdif_uv(P, s, VU_WREAL); break;

@@ -69,6 +69,7 @@ struct Dev {
   // ----- gather lists -----
   const int *node_he_ptr, *node_he;   // node -> half-edges (id*2 + side), ascending id
   const int *cell_edge;               // cell -> its 3 edges (id*2 + side), ascending id
+  const int *cell_he;                 // cell -> its 3 control-volume half-edges (NTRG(he) == cell)
   // ----- open boundary -----
   const int *i_obc_n, *next_obc, *node_obc;  // node_obc[node] = OBC index (0 = none)
   const int *obc_kind;                        // 1: specified elevation, 2: clamped
@@ -110,6 +111,11 @@ struct Dev {
   double *gq[2][6];  // ADV_Q of Q2 / Q2L: PQPX, PQPY, PQPXD, PQPYD, ring min, ring max
   double *gt[2][6];  // ADV_T / ADV_S: the same six per tracer
   double* budget;                            // 3 doubles
+  double* ex[2];                             // half-edge fluxes of the two advected tracers (ncvs x KB)
+  double* g2d[4];                            // least-squares gradient of UA, VA per cell (COFA1/2/5/6)
+  double* exf2d;                             // EXTEL_EDGE flux of each half-edge (NCV+1)
+  double* g3[4];                             // least-squares gradient of U, V per cell and layer (ns x KB)
+  int ncvs;                                  // layer stride of ex (>= NCV+1)
 };
 
 // index helpers
@@ -122,7 +128,7 @@ __host__ __device__ inline double fsign1(double x) { return x >= 0.0 ? 1.0 : -1.
 extern const double kAlphaRK[5];
 
 // ---------------- external mode (k_ext.cu) ----------------
-enum ExtNodeParts { EN_EXTEL = 1, EN_BC = 2, EN_COPY_ELRK = 4 };
+enum ExtNodeParts { EN_EXTEL = 1, EN_BC = 2, EN_COPY_ELRK = 4, EN_GRAD = 8 };
 enum ExtCellParts { EC_N2E = 1, EC_FLUXOBN = 2, EC_ADVAVE = 4, EC_EXTUV = 8, EC_BC2 = 16, EC_COPY_RK = 32,
                     EC_INT_ADVAVE = 64 };
 void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts);
@@ -130,11 +136,13 @@ void launch_wet_judge(const Dev& P, cudaStream_t s);
 void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts);
 void launch_ext_update(const Dev& P, cudaStream_t s, int K);
 void launch_begin_step(const Dev& P, cudaStream_t s);
+void launch_ext_prep(const Dev& P, cudaStream_t s);
 void launch_set_qdis(const Dev& P, cudaStream_t s);
 
 // ---------------- 3-D momentum (k_mom3d.cu) ----------------
 enum CellPreParts { CP_ADJUST1 = 1, CP_BC5 = 2, CP_BCOND8 = 4, CP_BROUGH = 8 };
 void launch_cell_pre(const Dev& P, cudaStream_t s, int parts);
+void launch_grad3(const Dev& P, cudaStream_t s);
 void launch_advection3d(const Dev& P, cudaStream_t s);
 void launch_baropg(const Dev& P, cudaStream_t s, int do_baropg, int do_sums);
 void launch_int_reset(const Dev& P, cudaStream_t s);

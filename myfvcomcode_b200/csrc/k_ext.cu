@@ -19,6 +19,54 @@ __device__ inline const double* sched_row(const Dev& P) {
 }
 
 // -------------------------------------------------------------------------------------
+// Least-squares velocity gradient of one cell from itself and its three neighbours
+// (advave_edge_gcn.F:634-637, 699-702): COFA1/COFA2 for UA, COFA5/COFA6 for VA.
+// -------------------------------------------------------------------------------------
+struct Grad {
+  double ux, uy, vx, vy;
+};
+
+__device__ inline Grad cell_grad(const Dev& P, int c, const double* U, const double* V) {
+  const size_t n1 = P.N + 1;
+  int k1 = P.nbe[c], k2 = P.nbe[n1 + c], k3 = P.nbe[2 * n1 + c];
+  double a1 = P.a1u[c], a2 = P.a1u[n1 + c], a3 = P.a1u[2 * n1 + c], a4 = P.a1u[3 * n1 + c];
+  double b1 = P.a2u[c], b2 = P.a2u[n1 + c], b3 = P.a2u[2 * n1 + c], b4 = P.a2u[3 * n1 + c];
+  double u0 = U[c], u1 = U[k1], u2 = U[k2], u3 = U[k3];
+  double v0 = V[c], v1 = V[k1], v2 = V[k2], v3 = V[k3];
+  Grad g;
+  g.ux = a1 * u0 + a2 * u1 + a3 * u2 + a4 * u3;
+  g.uy = b1 * u0 + b2 * u1 + b3 * u2 + b4 * u3;
+  g.vx = a1 * v0 + a2 * v1 + a3 * v2 + a4 * v3;
+  g.vy = b1 * v0 + b2 * v1 + b3 * v2 + b4 * v3;
+  return g;
+}
+
+__device__ inline void store_grad(const Dev& P, int c) {
+  Grad g = cell_grad(P, c, P.ua, P.va);
+  P.g2d[0][c] = g.ux;
+  P.g2d[1][c] = g.uy;
+  P.g2d[2][c] = g.vx;
+  P.g2d[3][c] = g.vy;
+}
+__device__ inline Grad load_grad(const Dev& P, int c) {
+  Grad g;
+  g.ux = P.g2d[0][c];
+  g.uy = P.g2d[1][c];
+  g.vx = P.g2d[2][c];
+  g.vy = P.g2d[3][c];
+  return g;
+}
+// EXTEL_EDGE half-edge flux EXFLUX = DIJ*(-UIJ*DLTYE+VIJ*DLTXE) (extel_edge.F:86-94) of the
+// three half-edges owned by cell c, from the cell's own D1, UA, VA.
+__device__ inline void store_exf(const Dev& P, int c) {
+  double d1 = P.d1[c], u = P.ua[c], v = P.va[c];
+  for (int s = 0; s < 3; ++s) {
+    int he = P.cell_he[3 * c + s];
+    P.exf2d[he] = d1 * (-u * P.dltye[he] + v * P.dltxe[he]);
+  }
+}
+
+// -------------------------------------------------------------------------------------
 // EXTEL_EDGE(K) (extel_edge.F:76-180) and BCOND_GCN(1,K) -> BCOND_ASL/BCOND_ASL_CLP
 // (mod_obcs.F:509-617) with the Runge-Kutta blend of the specified-elevation nodes
 // (external_step.F:262-266).  One thread per node; the node's control-volume half-edges
@@ -26,6 +74,8 @@ __device__ inline const double* sched_row(const Dev& P) {
 // -------------------------------------------------------------------------------------
 __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  // cell part: least-squares gradient of the current UA, VA for ADVAVE of this stage
+  if ((parts & EN_GRAD) && i <= P.N) store_grad(P, i);
   if (i > P.M) return;
   if (parts & EN_COPY_ELRK) P.elrk[i] = P.el[i];
   const double alpha = dAlphaRK[K];
@@ -34,9 +84,7 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
     double x = 0.0;
     for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
       int e = P.node_he[q];
-      int he = e >> 1;
-      int c = P.ntrg[he];
-      double exflux = P.d1[c] * (-P.ua[c] * P.dltye[he] + P.va[c] * P.dltxe[he]);
+      double exflux = P.exf2d[e >> 1];
       x = (e & 1) ? x + exflux : x - exflux;
     }
     if (ob > 0) {
@@ -105,29 +153,6 @@ __global__ void k_wet_nodes(const Dev P) {
   P.elf[i] = fmax(e, -P.h[i] + P.min_depth);
 }
 
-// -------------------------------------------------------------------------------------
-// Least-squares velocity gradient of one cell from itself and its three neighbours
-// (advave_edge_gcn.F:634-637, 699-702): COFA1/COFA2 for UA, COFA5/COFA6 for VA.
-// -------------------------------------------------------------------------------------
-struct Grad {
-  double ux, uy, vx, vy;
-};
-
-__device__ inline Grad cell_grad(const Dev& P, int c, const double* U, const double* V) {
-  const size_t n1 = P.N + 1;
-  int k1 = P.nbe[c], k2 = P.nbe[n1 + c], k3 = P.nbe[2 * n1 + c];
-  double a1 = P.a1u[c], a2 = P.a1u[n1 + c], a3 = P.a1u[2 * n1 + c], a4 = P.a1u[3 * n1 + c];
-  double b1 = P.a2u[c], b2 = P.a2u[n1 + c], b3 = P.a2u[2 * n1 + c], b4 = P.a2u[3 * n1 + c];
-  double u0 = U[c], u1 = U[k1], u2 = U[k2], u3 = U[k3];
-  double v0 = V[c], v1 = V[k1], v2 = V[k2], v3 = V[k3];
-  Grad g;
-  g.ux = a1 * u0 + a2 * u1 + a3 * u2 + a4 * u3;
-  g.uy = b1 * u0 + b2 * u1 + b3 * u2 + b4 * u3;
-  g.vx = a1 * v0 + a2 * v1 + a3 * v2 + a4 * v3;
-  g.vy = b1 * v0 + b2 * v1 + b3 * v2 + b4 * v3;
-  return g;
-}
-
 // ADVAVE_EDGE_GCN for one cell (advave_edge_gcn.F:115-1003, LIMITED_NO branch).
 __device__ inline void advave_cell(const Dev& P, int i, double& xf, double& yf, double& px, double& py) {
   xf = 0.0; yf = 0.0; px = 0.0; py = 0.0;
@@ -141,12 +166,12 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xf, double& yf, 
     double dij = 0.5 * (P.d[j1] + P.d[j2]);
     double elij = 0.5 * (P.el[j1] + P.el[j2]);
     if (P.iswetce[ia] * P.iswetc[ia] == 1 || P.iswetce[ib] * P.iswetc[ib] == 1) {
-      Grad ga = cell_grad(P, ia, P.ua, P.va);
+      Grad ga = load_grad(P, ia);
       double xij = P.xijc[e] - P.xc[ia];
       double yij = P.yijc[e] - P.yc[ia];
       double uij1 = P.ua[ia] + ga.ux * xij + ga.uy * yij;
       double vij1 = P.va[ia] + ga.vx * xij + ga.vy * yij;
-      Grad gb = cell_grad(P, ib, P.ua, P.va);
+      Grad gb = load_grad(P, ib);
       xij = P.xijc[e] - P.xc[ib];
       yij = P.yijc[e] - P.yc[ib];
       double uij2 = P.ua[ib] + gb.ux * xij + gb.uy * yij;
@@ -344,7 +369,17 @@ __global__ void k_ext_update(const Dev P, int K) {
       P.vard[i] = P.vard[i] + v * dd1;
     }
     if (P.wetting_drying_on) P.iswetce[i] = P.iswetc[i];
+    store_exf(P, i);
   }
+}
+
+// Gradients and half-edge continuity fluxes of the current UA, VA, D1 for every cell
+// (start of the external mode, and before single-routine calls).
+__global__ void k_ext_prep(const Dev P) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  store_grad(P, i);
+  store_exf(P, i);
 }
 
 // Start of an internal step: advance the schedule slot, then BCOND_GCN(8,0)'s river ramp
@@ -360,8 +395,10 @@ __global__ void k_begin_step(const Dev P, int advance) {
 static inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
 void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
-  k_ext_node<<<nblk(P.M, 256), 256, 0, s>>>(P, iext, K, parts);
+  int n = (parts & EN_GRAD) ? (P.M > P.N ? P.M : P.N) : P.M;
+  k_ext_node<<<nblk(n, 256), 256, 0, s>>>(P, iext, K, parts);
 }
+void launch_ext_prep(const Dev& P, cudaStream_t s) { k_ext_prep<<<nblk(P.N, 256), 256, 0, s>>>(P); }
 void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);
   k_wet_nodes<<<nblk(P.M, 256), 256, 0, s>>>(P);

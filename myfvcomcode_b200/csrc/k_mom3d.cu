@@ -121,15 +121,39 @@ struct EdgeFlux {
   double xadv, yadv, fxx, fyy, viscof;
 };
 
+__device__ inline G3 load_g3(const Dev& P, int c, int k) {
+  size_t q = C3(P, c, k);
+  G3 g;
+  g.ux = P.g3[0][q];
+  g.uy = P.g3[1][q];
+  g.vx = P.g3[2][q];
+  g.vy = P.g3[3][q];
+  return g;
+}
+
+// Least-squares gradient of U, V of every cell and layer (the COFA1..COFA8 inputs of
+// advection_edge_gcn.F:533-548 and adv_uv_edge_gcn.F:704-719), evaluated once per cell.
+__global__ void __launch_bounds__(256) k_grad3(const Dev P) {
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (i > P.N || k > P.KBM1) return;
+  G3 g = grad3(P, i, P.u + C3(P, 0, k), P.v + C3(P, 0, k));
+  size_t q = C3(P, i, k);
+  P.g3[0][q] = g.ux;
+  P.g3[1][q] = g.uy;
+  P.g3[2][q] = g.vx;
+  P.g3[3][q] = g.vy;
+}
+
 __device__ inline EdgeFlux edge_flux3(const Dev& P, int e, int ia, int ib, int k, double dij, bool exflux_form) {
   const double* U = P.u + C3(P, 0, k);
   const double* V = P.v + C3(P, 0, k);
   double xija = P.xijc[e] - P.xc[ia], yija = P.yijc[e] - P.yc[ia];
   double xijb = P.xijc[e] - P.xc[ib], yijb = P.yijc[e] - P.yc[ib];
-  G3 ga = grad3(P, ia, U, V);
+  G3 ga = load_g3(P, ia, k);
   double uij1 = U[ia] + ga.ux * xija + ga.uy * yija;
   double vij1 = V[ia] + ga.vx * xija + ga.vy * yija;
-  G3 gb = grad3(P, ib, U, V);
+  G3 gb = load_g3(P, ib, k);
   double uij2 = U[ib] + gb.ux * xijb + gb.uy * yijb;
   double vij2 = V[ib] + gb.vx * xijb + gb.vy * yijb;
   double uij = 0.5 * (uij1 + uij2);
@@ -680,6 +704,10 @@ __global__ void __launch_bounds__(128) k_vdif_uv(const Dev P, int parts) {
 
 void launch_cell_pre(const Dev& P, cudaStream_t s, int parts) {
   k_cell_pre<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);
+}
+void launch_grad3(const Dev& P, cudaStream_t s) {
+  dim3 b(32, 8), g(nblk(P.N, 32), nblk(P.KBM1, 8));
+  k_grad3<<<g, b, 0, s>>>(P);
 }
 void launch_advection3d(const Dev& P, cudaStream_t s) {
   dim3 b(32, 8), g(nblk(P.N, 32), nblk(P.KBM1, 8));

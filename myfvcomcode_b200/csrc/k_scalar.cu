@@ -5,10 +5,12 @@
 // end-of-step shifts (internal_step.F:1034-1590).
 //
 // The node-ring gradients (PTPX.. over NBSN) and the ring extrema of the advected field
-// are formed once per (node, layer) by k_grad into scratch fields; the flux kernels then
-// gather each node's control-volume half-edges in ascending order and read both ends'
-// gradients, reproducing the reference's scatter sums.  T and S (and Q2 and Q2L) are
-// transported in the same launch since neither reads the other's update.
+// are formed once per (node, layer) by k_grad into scratch fields.  Horizontal advection
+// then runs in two phases: k_he_adv evaluates each control-volume half-edge flux once
+// (one thread per cell and layer, the cell's three half-edges), and k_gather_q/_ts sum
+// each node's half-edge fluxes with their signs in ascending half-edge order, which
+// reproduces the reference's scatter sums bit for bit.  T and S (and Q2 and Q2L) are
+// transported in the same launches since neither reads the other's update.
 #include "fvg_model.h"
 
 namespace fvg {
@@ -141,57 +143,162 @@ __device__ inline void fct_level_bounds(const Dev& P, int i, int k, const double
 }
 
 // -------------------------------------------------------------------------------------
-// ADV_Q(Q2,Q2F) and ADV_Q(Q2L,Q2LF) (adv_q.F:114-401), then FCT_Q2/FCT_Q2L.
+// Half-edge fluxes of ADV_Q (adv_q.F:250-342) and ADV_T/ADV_S (adv_t.F:411-556).
+//
+// Phase 1 (k_he_adv, one thread per cell and layer): a cell's three control-volume
+// half-edges run from its centroid to its edge midpoints and each separates two of the
+// cell's own nodes, so the node data (tracer value, ring gradients and extrema, mixing
+// coefficient) is loaded once for the three half-edges.  Each half-edge flux EXFLUX is
+// evaluated once, in the reference's expression order, and stored by half-edge number.
+// Phase 2 (k_gather_*, one thread per node and layer) sums the node's half-edge fluxes
+// with their signs in ascending half-edge order -- the order of the reference's scatter --
+// and applies the vertical flux, the update and the FCT clamp.
+// MODE 0: Q2 and Q2L on interfaces K=2..KBM1; MODE 1: T and S on layers K=1..KBM1.
 // -------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_adv_q(const Dev P, int parts) {
+struct HeCell {
+  double uq, vq, dtij;
+  int nd[3];
+  double vf[3], nn[3];
+};
+
+template <int MODE>
+__device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell& hc) {
+  const size_t n1 = P.N + 1;
+  size_t ck = C3(P, c, k);
+  if (MODE == 0) {
+    size_t ckm = C3(P, c, k - 1);
+    hc.uq = (P.u[ck] * P.dz1[ckm] + P.u[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]);
+    hc.vq = (P.v[ck] * P.dz1[ckm] + P.v[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]);
+    hc.dtij = P.dt1[c] * P.dzz1[ckm];
+  } else {
+    hc.uq = P.u[ck];
+    hc.vq = P.v[ck];
+    hc.dtij = P.dt1[c] * P.dz1[ck];
+  }
+  for (int j = 0; j < 3; ++j) {
+    int n = P.nv[j * n1 + c];
+    hc.nd[j] = n;
+    size_t q = N3(P, n, k);
+    if (MODE == 0) {
+      size_t qm = N3(P, n, k - 1);
+      hc.vf[j] = (P.viscofh[q] * P.dz[qm] + P.viscofh[qm] * P.dz[q]) / (P.dz[q] + P.dz[qm]);
+    } else {
+      hc.vf[j] = P.viscofh[q];
+    }
+    hc.nn[j] = P.nn_hvc[n];
+  }
+}
+
+// EXFLUX of half-edge he on layer k for tracer t; a and b are the positions of NIEC(he,1)
+// and NIEC(he,2) among the cell's nodes.  xadv receives EXFLUX-FXX-FYY.
+template <int MODE>
+__device__ inline double he_flux(const Dev& P, const HeCell& hc, int he, int k, int t, int a, int b,
+                                 const double* qv, const double* const* gv, double* xadv) {
+  const size_t vi1 = P.NCV_I + 1;
+  double un = hc.vq * P.dltxe[he] - hc.uq * P.dltye[he];
+  double fij1 = qv[a] + P.dltxncve[he] * gv[0][a] + P.dltyncve[he] * gv[1][a];
+  double fij2 = qv[b] + P.dltxncve[vi1 + he] * gv[0][b] + P.dltyncve[vi1 + he] * gv[1][b];
+  double q1min = fmin(gv[4][a], qv[a]), q1max = fmax(gv[5][a], qv[a]);
+  double q2min = fmin(gv[4][b], qv[b]), q2max = fmax(gv[5][b], qv[b]);
+  if (fij1 < q1min) fij1 = q1min;
+  if (fij1 > q1max) fij1 = q1max;
+  if (fij2 < q2min) fij2 = q2min;
+  if (fij2 > q2max) fij2 = q2max;
+  double viscof = P.fact * 0.5 * (hc.vf[a] * hc.nn[a] + hc.vf[b] * hc.nn[b]) + P.fm1 * 0.5 * (hc.nn[a] + hc.nn[b]);
+  if (MODE == 0) viscof = viscof / P.hprnu;
+  double txx = 0.5 * (gv[2][a] + gv[2][b]) * viscof;
+  double tyy = 0.5 * (gv[3][a] + gv[3][b]) * viscof;
+  double fxx = -hc.dtij * txx * P.dltye[he];
+  double fyy = hc.dtij * tyy * P.dltxe[he];
+  double sg = fsign1(un);
+  double exflux = -un * hc.dtij * ((1.0 + sg) * fij2 + (1.0 - sg) * fij1) * 0.5 + fxx + fyy;
+  if (xadv) *xadv = exflux - fxx - fyy;
+  return exflux;
+}
+
+template <int MODE>
+__device__ inline void tracer_nodes(const Dev& P, const HeCell& hc, int k, int t, double* qv, double gv[6][3]) {
+  const double* Q = MODE == 0 ? (t == 0 ? P.q2 : P.q2l) : (t == 0 ? P.t1 : P.s1);
+  double* const* G = MODE == 0 ? P.gq[t] : P.gt[t];
+  for (int j = 0; j < 3; ++j) {
+    size_t q = N3(P, hc.nd[j], k);
+    qv[j] = Q[q];
+    for (int g = 0; g < 6; ++g) gv[g][j] = G[g][q];
+  }
+}
+
+__device__ inline int pos3(const HeCell& hc, int n) { return n == hc.nd[0] ? 0 : (n == hc.nd[1] ? 1 : 2); }
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_he_adv(const Dev P, int parts) {
+  int c = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + (MODE == 0 ? 2 : 1);
+  if (c > P.N || k > P.KBM1) return;
+  HeCell hc;
+  he_cell_load<MODE>(P, c, k, hc);
+  const size_t v1 = P.NCV + 1;
+  int hes[3], pa[3], pb[3];
+  for (int s = 0; s < 3; ++s) {
+    int he = P.cell_he[3 * c + s];
+    hes[s] = he;
+    pa[s] = pos3(hc, P.niec[he]);
+    pb[s] = pos3(hc, P.niec[v1 + he]);
+  }
+  for (int t = 0; t < 2; ++t) {
+    int bit = MODE == 0 ? (t == 0 ? AD_Q2 : AD_Q2L) : (t == 0 ? AD_T : AD_S);
+    if (!(parts & bit)) continue;
+    double qv[3], gv[6][3];
+    tracer_nodes<MODE>(P, hc, k, t, qv, gv);
+    const double* gp[6] = {gv[0], gv[1], gv[2], gv[3], gv[4], gv[5]};
+    double* EX = P.ex[t] + (size_t)(k - 1) * P.ncvs;
+    for (int s = 0; s < 3; ++s)
+      EX[hes[s]] = he_flux<MODE>(P, hc, hes[s], k, t, pa[s], pb[s], qv, gp, nullptr);
+  }
+}
+
+// XFLUX_ADV of one open-boundary node (adv_t.F:510-511, 572-579): the advective parts of
+// its half-edge fluxes, recomputed with the same arithmetic as phase 1.
+__device__ inline double obc_xflux_adv(const Dev& P, int i, int k, int t) {
+  const size_t v1 = P.NCV + 1;
+  double xa = 0.0;
+  for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
+    int code = P.node_he[q];
+    int he = code >> 1;
+    int c = P.ntrg[he];
+    HeCell hc;
+    he_cell_load<1>(P, c, k, hc);
+    double qv[3], gv[6][3];
+    tracer_nodes<1>(P, hc, k, t, qv, gv);
+    const double* gp[6] = {gv[0], gv[1], gv[2], gv[3], gv[4], gv[5]};
+    double part;
+    he_flux<1>(P, hc, he, k, t, pos3(hc, P.niec[he]), pos3(hc, P.niec[v1 + he]), qv, gp, &part);
+    xa = (code & 1) ? xa - part : xa + part;
+  }
+  return xa;
+}
+
+// Phase 2 of ADV_Q(Q2,Q2F)/ADV_Q(Q2L,Q2LF) (adv_q.F:114-401) with FCT_Q2/FCT_Q2L.
+__global__ void __launch_bounds__(256) k_gather_q(const Dev P, int parts) {
   int i = blockIdx.x * 32 + threadIdx.x + 1;
   int k = blockIdx.y * 8 + threadIdx.y + 2;
   if (i > P.M || k > P.KBM1) return;
-  const size_t v1 = P.NCV + 1, vi1 = P.NCV_I + 1;
   const bool wet = P.iswetn[i] * P.iswetnt[i] == 1;
+  const int q0 = P.node_he_ptr[i], q1 = P.node_he_ptr[i + 1];
   for (int t = 0; t < 2; ++t) {
     if (!(parts & (t == 0 ? AD_Q2 : AD_Q2L))) continue;
     const double* Q = (t == 0 ? P.q2 : P.q2l);
     double* QF = (t == 0 ? P.q2f : P.q2lf);
-    double* const* G = P.gq[t];
-    const double* Qk = Q + N3(P, 0, k);
     if (k == 2) {
       // QF = 0 on every level before the interior levels are set (adv_q.F:114)
       QF[N3(P, i, 1)] = 0.0;
       QF[N3(P, i, P.KB)] = 0.0;
     }
+    const double* EX = P.ex[t] + (size_t)(k - 1) * P.ncvs;
     double x = 0.0;
-    for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
+    for (int q = q0; q < q1; ++q) {
       int code = P.node_he[q];
-      int he = code >> 1;
-      int ia = P.niec[he], ib = P.niec[v1 + he];
-      int c = P.ntrg[he];
-      size_t ck = C3(P, c, k), ckm = C3(P, c, k - 1);
-      double uq = (P.u[ck] * P.dz1[ckm] + P.u[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]);
-      double vq = (P.v[ck] * P.dz1[ckm] + P.v[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]);
-      double dtij = P.dt1[c] * P.dzz1[ckm];
-      double un = vq * P.dltxe[he] - uq * P.dltye[he];
-      size_t qa = N3(P, ia, k), qb = N3(P, ib, k);
-      double fij1 = Qk[ia] + P.dltxncve[he] * G[0][qa] + P.dltyncve[he] * G[1][qa];
-      double fij2 = Qk[ib] + P.dltxncve[vi1 + he] * G[0][qb] + P.dltyncve[vi1 + he] * G[1][qb];
-      double q1min = fmin(G[4][qa], Qk[ia]), q1max = fmax(G[5][qa], Qk[ia]);
-      double q2min = fmin(G[4][qb], Qk[ib]), q2max = fmax(G[5][qb], Qk[ib]);
-      if (fij1 < q1min) fij1 = q1min;
-      if (fij1 > q1max) fij1 = q1max;
-      if (fij2 < q2min) fij2 = q2min;
-      if (fij2 > q2max) fij2 = q2max;
-      size_t qam = N3(P, ia, k - 1), qbm = N3(P, ib, k - 1);
-      double vfa = (P.viscofh[qa] * P.dz[qam] + P.viscofh[qam] * P.dz[qa]) / (P.dz[qa] + P.dz[qam]);
-      double vfb = (P.viscofh[qb] * P.dz[qbm] + P.viscofh[qbm] * P.dz[qb]) / (P.dz[qb] + P.dz[qbm]);
-      double viscof = (P.fact * 0.5 * (vfa * P.nn_hvc[ia] + vfb * P.nn_hvc[ib]) +
-                       P.fm1 * 0.5 * (P.nn_hvc[ia] + P.nn_hvc[ib])) / P.hprnu;
-      double txx = 0.5 * (G[2][qa] + G[2][qb]) * viscof;
-      double tyy = 0.5 * (G[3][qa] + G[3][qb]) * viscof;
-      double fxx = -dtij * txx * P.dltye[he];
-      double fyy = dtij * tyy * P.dltxe[he];
-      double sg = fsign1(un);
-      double exflux = -un * dtij * ((1.0 + sg) * fij2 + (1.0 - sg) * fij1) * 0.5 + fxx + fyy;
-      x = (code & 1) ? x - exflux : x + exflux;
+      double e = EX[code >> 1];
+      x = (code & 1) ? x - e : x + e;
     }
     size_t q = N3(P, i, k);
     double qf;
@@ -204,6 +311,7 @@ __global__ void __launch_bounds__(256) k_adv_q(const Dev P, int parts) {
       qf = Q[q];
     }
     if ((parts & AD_FCT) && !P.riv_skip[i]) {
+      double* const* G = P.gq[t];
       double qmax = G[5][q], qmin = G[4][q];
       fct_level_bounds(P, i, k, Q, qmax, qmin);
       if (qmin - qf > 0.0) qf = qmin;
@@ -415,57 +523,28 @@ __global__ void __launch_bounds__(256) k_turb_update(const Dev P) {
 }
 
 // -------------------------------------------------------------------------------------
-// ADV_T / ADV_S (adv_t.F:124-1042, adv_s.F) with FCT_T / FCT_S (fct_t.F:51-104,
+// Phase 2 of ADV_T / ADV_S (adv_t.F:124-1042, adv_s.F) with FCT_T / FCT_S (fct_t.F:51-104,
 // fct_s.F:50-108) on the same (node, layer) thread.
 // -------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_adv_ts(const Dev P, int parts) {
+__global__ void __launch_bounds__(256) k_gather_ts(const Dev P, int parts) {
   int i = blockIdx.x * 32 + threadIdx.x + 1;
   int k = blockIdx.y * 8 + threadIdx.y + 1;
   if (i > P.M || k > P.KBM1) return;
-  const size_t v1 = P.NCV + 1, vi1 = P.NCV_I + 1;
   const bool wet = P.iswetn[i] * P.iswetnt[i] == 1;
   const int ob = P.node_obc[i];
+  const int q0 = P.node_he_ptr[i], q1 = P.node_he_ptr[i + 1];
   for (int t = 0; t < 2; ++t) {
     if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
     const double* F1 = (t == 0 ? P.t1 : P.s1);
     double* FF1 = (t == 0 ? P.tf1 : P.sf1);
-    double* const* G = P.gt[t];
-    const double* Fk = F1 + N3(P, 0, k);
-    double x = 0.0, xa = 0.0;
-    for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
+    const double* EX = P.ex[t] + (size_t)(k - 1) * P.ncvs;
+    double x = 0.0;
+    for (int q = q0; q < q1; ++q) {
       int code = P.node_he[q];
-      int he = code >> 1;
-      int ia = P.niec[he], ib = P.niec[v1 + he];
-      int c = P.ntrg[he];
-      size_t ck = C3(P, c, k);
-      double dtij = P.dt1[c] * P.dz1[ck];
-      double un = P.v[ck] * P.dltxe[he] - P.u[ck] * P.dltye[he];
-      size_t qa = N3(P, ia, k), qb = N3(P, ib, k);
-      double fij1 = Fk[ia] + P.dltxncve[he] * G[0][qa] + P.dltyncve[he] * G[1][qa];
-      double fij2 = Fk[ib] + P.dltxncve[vi1 + he] * G[0][qb] + P.dltyncve[vi1 + he] * G[1][qb];
-      double t1min = fmin(G[4][qa], Fk[ia]), t1max = fmax(G[5][qa], Fk[ia]);
-      double t2min = fmin(G[4][qb], Fk[ib]), t2max = fmax(G[5][qb], Fk[ib]);
-      if (fij1 < t1min) fij1 = t1min;
-      if (fij1 > t1max) fij1 = t1max;
-      if (fij2 < t2min) fij2 = t2min;
-      if (fij2 > t2max) fij2 = t2max;
-      double viscof = P.fact * 0.5 * (P.viscofh[qa] * P.nn_hvc[ia] + P.viscofh[qb] * P.nn_hvc[ib]) +
-                      P.fm1 * 0.5 * (P.nn_hvc[ia] + P.nn_hvc[ib]);
-      double txx = 0.5 * (G[2][qa] + G[2][qb]) * viscof;
-      double tyy = 0.5 * (G[3][qa] + G[3][qb]) * viscof;
-      double fxx = -dtij * txx * P.dltye[he];
-      double fyy = dtij * tyy * P.dltxe[he];
-      double sg = fsign1(un);
-      double exflux = -un * dtij * ((1.0 + sg) * fij2 + (1.0 - sg) * fij1) * 0.5 + fxx + fyy;
-      if (code & 1) {
-        x = x - exflux;
-        xa = xa - (exflux - fxx - fyy);
-      } else {
-        x = x + exflux;
-        xa = xa + (exflux - fxx - fyy);
-      }
+      double e = EX[code >> 1];
+      x = (code & 1) ? x - e : x + e;
     }
-    if (ob > 0) (t == 0 ? P.xflux_obc_t : P.xflux_obc_s)[(size_t)(k - 1) * (P.iobcn + 1) + ob] = xa;
+    if (ob > 0) (t == 0 ? P.xflux_obc_t : P.xflux_obc_s)[(size_t)(k - 1) * (P.iobcn + 1) + ob] = obc_xflux_adv(P, i, k, t);
     size_t q = N3(P, i, k);
     double ff;
     if (wet) {
@@ -492,6 +571,7 @@ __global__ void __launch_bounds__(256) k_adv_ts(const Dev P, int parts) {
     }
     if (parts & AD_FCT) {
       if (!P.riv_skip[i]) {
+        double* const* G = P.gt[t];
         double fmx = G[5][q], fmn = G[4][q];
         fct_layer_bounds(P, i, k, F1, fmx, fmn);
         if (fmn - ff > 0.0) ff = fmn;
@@ -756,8 +836,9 @@ void launch_grad(const Dev& P, cudaStream_t s, int which) {
   k_grad<<<g, b, 0, s>>>(P, which);
 }
 void launch_adv_q(const Dev& P, cudaStream_t s, int parts) {
-  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1 - 1, 8));
-  k_adv_q<<<g, b, 0, s>>>(P, parts);
+  dim3 b(32, 8);
+  k_he_adv<0><<<dim3(nblk(P.N, 32), nblk(P.KBM1 - 1, 8)), b, 0, s>>>(P, parts);
+  k_gather_q<<<dim3(nblk(P.M, 32), nblk(P.KBM1 - 1, 8)), b, 0, s>>>(P, parts);
 }
 void launch_fct_q(const Dev& P, cudaStream_t s, int parts) {
   dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1 - 1, 8));
@@ -772,8 +853,9 @@ void launch_turb_update(const Dev& P, cudaStream_t s) {
   k_turb_update<<<g, b, 0, s>>>(P);
 }
 void launch_adv_ts(const Dev& P, cudaStream_t s, int parts) {
-  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));
-  k_adv_ts<<<g, b, 0, s>>>(P, parts);
+  dim3 b(32, 8);
+  k_he_adv<1><<<dim3(nblk(P.N, 32), nblk(P.KBM1, 8)), b, 0, s>>>(P, parts);
+  k_gather_ts<<<dim3(nblk(P.M, 32), nblk(P.KBM1, 8)), b, 0, s>>>(P, parts);
 }
 void launch_fct_ts(const Dev& P, cudaStream_t s, int parts) {
   dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));
