@@ -39,6 +39,7 @@ extern "C" {
 #define FVG_ERR_TIMEOUT 5      /* a bounded device wait ran out */
 #define FVG_ERR_UNSUPPORTED 6  /* option outside the supported physics set */
 #define FVG_ERR_NOMEM 7        /* device allocation failed */
+#define FVG_ERR_CAPACITY 8     /* input larger than a fixed-size device buffer */
 
 /* Mesh arrays as GRID_METRICS builds them (FVCOM_source/grid_metrics.F:29-136). */
 typedef struct fvg_mesh {
@@ -226,6 +227,20 @@ int fvg_shutdown_check(fvg_handle* h);
 /* FP64 budgets: out[0] volume (m^3), out[1] heat content (T*volume), out[2] salt
    content (S*volume) over the node control volumes. */
 int fvg_budget(fvg_handle* h, double out[3]);
+
+/* The budgets of fvg_budget computed from caller-owned device arrays, with no handle and
+   no memory allocation (no counterpart in the reference, which sums its host arrays).
+   For callers that keep their own FVCOM state on the device and cannot allocate when
+   they check it: cudaMalloc/cudaFree would synchronise the device on every call, and a
+   run that fills HBM may have nothing left to allocate.  d and art1 are (0:M); t1, s1
+   and dz are (0:M, >=KBM1) column-major with leading dimension M+1 (FVCOM's layout, ghost
+   row 0), all in device memory of the current device.  The scratch is a fixed 393,240-
+   byte device array: M above 4,194,304 returns FVG_ERR_CAPACITY; KBM1 must be 1..63.
+   Runs on `stream` (a cudaStream_t; NULL for the default stream) and waits for it.  The
+   first call on a device sets up the scratch address; make it before any stream capture.
+   Calls that overlap on one device share the scratch and race. */
+int fvg_budget_fields(const double* d, const double* art1, const double* t1, const double* s1,
+                      const double* dz, int32_t m, int32_t kbm1, void* stream, double out[3]);
 
 /* Library identity for checks that the compiled CUDA path is the one loaded. */
 const char* fvg_build_info(void);
