@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shape instead of autotuning it")
     return ap.parse_args()
 
 
@@ -231,6 +233,13 @@ def main():
     lib.fvg_profile_group_name.argtypes = [C.c_int32]
     lib.fvg_kernels_per_step.argtypes = [C.c_void_p]
     lib.fvg_kernels_per_step.restype = C.c_int32
+
+    if not args.no_tune:
+        from myfvcomcode_b200 import autotune
+        tuned = autotune.autotune(case, steps=2, warmup=1, engine=f)
+        autotune.apply(f, tuned)
+    cfg["tiling"] = {"col_threads": f.get_tuning("col_threads"), "col_layers": f.get_tuning("col_layers"),
+                     "autotuned": not args.no_tune}
 
     f.run(args.warmup)
     barrier(pg, local)

@@ -210,6 +210,11 @@ int fvg_sync(fvg_handle* h);
 int fvg_set_ramp(fvg_handle* h, double ramp);
 /* 1 (default): replay a captured CUDA graph per internal step; 0: plain launches. */
 int fvg_use_graph(fvg_handle* h, int32_t on);
+/* Launch shape of the 3-D gather kernels (results do not depend on it):
+   "col_threads" = entities (threads) per block, 32..256 in steps of 32 (default 128);
+   "col_layers"  = consecutive layers each thread walks, 1..KB (default 8). */
+int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value);
+int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value);
 
 /* Measurement.  fvg_time_steps runs nsteps internal steps and returns their device time
    (CUDA events on the handle's stream).  fvg_profile runs nsteps with plain launches and

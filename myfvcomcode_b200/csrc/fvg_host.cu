@@ -262,6 +262,8 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   P.NE = m->ne; P.NCV = m->ncv; P.NCV_I = m->ncv_i;
   P.ms = (int)pad32(M + 1);
   P.ns = (int)pad32(N + 1);
+  P.col_bc = 128;
+  P.col_lc = 8;
   P.nbsn_cols = m->nbsn_cols; P.nbve_cols = m->nbve_cols; P.trie_cols = m->trie_cols;
   P.iobcn = m->iobcn; P.numqbc = m->numqbc;
   P.isplit = prm->isplit;
@@ -549,11 +551,11 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   P.ncvs = (int)pad32(m->ncv + 1);
   for (int q = 0; q < 4; ++q) {
     if ((rc = dalloc(h, &P.g2d[q], n1))) return fail(rc);
-    if ((rc = dalloc(h, &P.g3[q], ns * KB))) return fail(rc);
   }
   if ((rc = dalloc(h, &P.exf2d, v1))) return fail(rc);
-  for (int t = 0; t < 2; ++t)
-    if ((rc = dalloc(h, &P.ex[t], (size_t)P.ncvs * KB))) return fail(rc);
+  for (int q = 0; q < 4; ++q)
+    if ((rc = dalloc(h, &P.g3[q], ns * KB))) return fail(rc);
+  if ((rc = dalloc(h, (double**)&P.ex2, (size_t)P.ncvs * KB * 2))) return fail(rc);
 
   // ---- schedule ----
   h->sched_cap = 256;
@@ -770,6 +772,35 @@ int fvg_sync(fvg_handle* h) {
 int fvg_use_graph(fvg_handle* h, int32_t on) {
   if (!h) return FVG_ERR_ARG;
   h->use_graph = on != 0;
+  return FVG_OK;
+}
+
+int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value) {
+  if (!h || !key) return FVG_ERR_ARG;
+  std::string k(key);
+  if (k == "col_threads") {
+    if (value < 32 || value > 256 || value % 32 != 0) { h->err = "col_threads must be 32..256, a multiple of 32"; return FVG_ERR_ARG; }
+    h->P.col_bc = value;
+  } else if (k == "col_layers") {
+    if (value < 1 || value > h->P.KB) { h->err = "col_layers must be 1..KB"; return FVG_ERR_ARG; }
+    h->P.col_lc = value;
+  } else {
+    h->err = "unknown tuning key " + k;
+    return FVG_ERR_ARG;
+  }
+  // The captured step holds the old launch shapes: capture again on the next step.
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  return FVG_OK;
+}
+
+int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value) {
+  if (!h || !key || !value) return FVG_ERR_ARG;
+  std::string k(key);
+  if (k == "col_threads") *value = h->P.col_bc;
+  else if (k == "col_layers") *value = h->P.col_lc;
+  else return FVG_ERR_ARG;
   return FVG_OK;
 }
 

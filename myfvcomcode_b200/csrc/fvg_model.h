@@ -111,12 +111,28 @@ struct Dev {
   double *gq[2][6];  // ADV_Q of Q2 / Q2L: PQPX, PQPY, PQPXD, PQPYD, ring min, ring max
   double *gt[2][6];  // ADV_T / ADV_S: the same six per tracer
   double* budget;                            // 3 doubles
-  double* ex[2];                             // half-edge fluxes of the two advected tracers (ncvs x KB)
+  double2* ex2;                              // half-edge fluxes of both advected tracers (ncvs x KB)
   double* g2d[4];                            // least-squares gradient of UA, VA per cell (COFA1/2/5/6)
   double* exf2d;                             // EXTEL_EDGE flux of each half-edge (NCV+1)
   double* g3[4];                             // least-squares gradient of U, V per cell and layer (ns x KB)
   int ncvs;                                  // layer stride of ex (>= NCV+1)
+  // Column tiling of the 3-D gather kernels: col_bc threads (entities) per block, each
+  // walking col_lc consecutive layers, so the entity's index chain (cell -> edge ->
+  // neighbour) is resolved from cache after the first layer.  Results do not depend on it.
+  int col_bc, col_lc;
 };
+
+// Grid of a column-tiled kernel over n entities and nl layers.
+inline dim3 col_grid(const Dev& P, int n, int nl) {
+  return dim3((unsigned)((n + P.col_bc - 1) / P.col_bc), (unsigned)((nl + P.col_lc - 1) / P.col_lc));
+}
+// First and last layer of this thread's chunk, layers k0..klast.
+__device__ inline void col_range(const Dev& P, int k0, int klast, int& kb, int& ke) {
+  kb = k0 + (int)blockIdx.y * P.col_lc;
+  ke = kb + P.col_lc - 1;
+  if (ke > klast) ke = klast;
+}
+
 
 // index helpers
 __host__ __device__ inline size_t N3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ms + i; }

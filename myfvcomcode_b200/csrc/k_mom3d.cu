@@ -134,15 +134,18 @@ __device__ inline G3 load_g3(const Dev& P, int c, int k) {
 // Least-squares gradient of U, V of every cell and layer (the COFA1..COFA8 inputs of
 // advection_edge_gcn.F:533-548 and adv_uv_edge_gcn.F:704-719), evaluated once per cell.
 __global__ void __launch_bounds__(256) k_grad3(const Dev P) {
-  int i = blockIdx.x * 32 + threadIdx.x + 1;
-  int k = blockIdx.y * 8 + threadIdx.y + 1;
-  if (i > P.N || k > P.KBM1) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  int kb, ke;
+  col_range(P, 1, P.KBM1, kb, ke);
+  for (int k = kb; k <= ke; ++k) {
   G3 g = grad3(P, i, P.u + C3(P, 0, k), P.v + C3(P, 0, k));
   size_t q = C3(P, i, k);
   P.g3[0][q] = g.ux;
   P.g3[1][q] = g.uy;
   P.g3[2][q] = g.vx;
   P.g3[3][q] = g.vy;
+  }
 }
 
 __device__ inline EdgeFlux edge_flux3(const Dev& P, int e, int ia, int ib, int k, double dij, bool exflux_form) {
@@ -209,9 +212,11 @@ __device__ inline void river3(const Dev& P, int i, int k, double& x, double& y) 
 // edges in ascending edge number.
 // -------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
-  int i = blockIdx.x * 32 + threadIdx.x + 1;
-  int k = blockIdx.y * 8 + threadIdx.y + 1;
-  if (i > P.N || k > P.KBM1) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  int kb, ke;
+  col_range(P, 1, P.KBM1, kb, ke);
+  for (int k = kb; k <= ke; ++k) {
   const size_t e1 = P.NE + 1;
   double x = 0.0, y = 0.0;
   for (int s = 0; s < 3; ++s) {
@@ -239,6 +244,7 @@ __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
   river3(P, i, k, x, y);
   P.advx[C3(P, i, k)] = x;
   P.advy[C3(P, i, k)] = y;
+  }
 }
 
 // -------------------------------------------------------------------------------------
@@ -360,9 +366,11 @@ __global__ void k_adjust2(const Dev P) {
 // node's half-edges in ascending order.  Result in the scratch field.
 // -------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_vertvl_flux(const Dev P) {
-  int i = blockIdx.x * 32 + threadIdx.x + 1;
-  int k = blockIdx.y * 8 + threadIdx.y + 1;
-  if (i > P.M || k > P.KBM1) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  int kb, ke;
+  col_range(P, 1, P.KBM1, kb, ke);
+  for (int k = kb; k <= ke; ++k) {
   double x = 0.0;
   if (P.isonb[i] != 2) {
     for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
@@ -384,6 +392,7 @@ __global__ void __launch_bounds__(256) k_vertvl_flux(const Dev P) {
       x = x - P.qdis[j] * P.rdisq[(size_t)(r & 1) * (P.numqbc + 1) + j] * vq;
   }
   P.scr_xflux[N3(P, i, k)] = x;
+  }
 }
 
 // -------------------------------------------------------------------------------------
@@ -453,9 +462,10 @@ __global__ void k_vertvl_col(const Dev P, int parts) {
 // on nodes, one thread per (entity, layer).
 // -------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_w_viscofh(const Dev P, int do_w, int do_visc) {
-  int i = blockIdx.x * 32 + threadIdx.x + 1;
-  int k = blockIdx.y * 8 + threadIdx.y + 1;
-  if (k > P.KB) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int kb, ke;
+  col_range(P, 1, P.KB, kb, ke);
+  for (int k = kb; k <= ke; ++k) {
   const size_t n1 = P.N + 1, m1 = P.M + 1;
   if (do_w && i <= P.N) {
     double w = ONE_THIRD * (P.wts[N3(P, P.nv[i], k)] + P.wts[N3(P, P.nv[n1 + i], k)] + P.wts[N3(P, P.nv[2 * n1 + i], k)]);
@@ -501,6 +511,7 @@ __global__ void __launch_bounds__(256) k_w_viscofh(const Dev P, int do_w, int do
     double tmp2 = 0.5 * ((pupy + pvpx) * (pupy + pvpx));
     P.viscofh[N3(P, i, k)] = sqrt(tmp1 + tmp2) * a1;
   }
+  }
 }
 
 // -------------------------------------------------------------------------------------
@@ -509,9 +520,11 @@ __global__ void __launch_bounds__(256) k_w_viscofh(const Dev P, int do_w, int do
 // pressure gradient, Coriolis, river momentum and the explicit update to UF/VF.
 // -------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
-  int i = blockIdx.x * 32 + threadIdx.x + 1;
-  int k = blockIdx.y * 8 + threadIdx.y + 1;
-  if (i > P.N || k > P.KBM1) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  int kb, ke;
+  col_range(P, 1, P.KBM1, kb, ke);
+  for (int k = kb; k <= ke; ++k) {
   const size_t e1 = P.NE + 1;
   double x = 0.0, y = 0.0, px = 0.0, py = 0.0, vm = 0.0;
   const double dz1i = P.dz1[C3(P, i, k)];
@@ -588,6 +601,7 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
   P.uf[q] = uf;
   P.vf[q] = vf;
   P.viscofm[q] = vm / P.art[i];
+  }
 }
 
 // -------------------------------------------------------------------------------------
@@ -706,12 +720,10 @@ void launch_cell_pre(const Dev& P, cudaStream_t s, int parts) {
   k_cell_pre<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);
 }
 void launch_grad3(const Dev& P, cudaStream_t s) {
-  dim3 b(32, 8), g(nblk(P.N, 32), nblk(P.KBM1, 8));
-  k_grad3<<<g, b, 0, s>>>(P);
+  k_grad3<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_advection3d(const Dev& P, cudaStream_t s) {
-  dim3 b(32, 8), g(nblk(P.N, 32), nblk(P.KBM1, 8));
-  k_advection3d<<<g, b, 0, s>>>(P);
+  k_advection3d<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_baropg(const Dev& P, cudaStream_t s, int do_baropg, int do_sums) {
   k_baropg<<<nblk(P.N, 128), 128, 0, s>>>(P, do_baropg, do_sums);
@@ -722,20 +734,17 @@ void launch_int_reset(const Dev& P, cudaStream_t s) {
 }
 void launch_adjust2(const Dev& P, cudaStream_t s) { k_adjust2<<<nblk(P.N + 1, 128), 128, 0, s>>>(P); }
 void launch_vertvl_flux(const Dev& P, cudaStream_t s) {
-  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));
-  k_vertvl_flux<<<g, b, 0, s>>>(P);
+  k_vertvl_flux<<<col_grid(P, P.M, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_vertvl_col(const Dev& P, cudaStream_t s, int parts) {
   k_vertvl_col<<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
 }
 void launch_w_viscofh(const Dev& P, cudaStream_t s, int do_w, int do_visc) {
   int n = P.M > P.N ? P.M : P.N;
-  dim3 b(32, 8), g(nblk(n, 32), nblk(P.KB, 8));
-  k_w_viscofh<<<g, b, 0, s>>>(P, do_w, do_visc);
+  k_w_viscofh<<<col_grid(P, n, P.KB), P.col_bc, 0, s>>>(P, do_w, do_visc);
 }
 void launch_adv_uv(const Dev& P, cudaStream_t s) {
-  dim3 b(32, 8), g(nblk(P.N, 32), nblk(P.KBM1, 8));
-  k_adv_uv<<<g, b, 0, s>>>(P);
+  k_adv_uv<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_vdif_uv(const Dev& P, cudaStream_t s, int parts) {
   k_vdif_uv<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);

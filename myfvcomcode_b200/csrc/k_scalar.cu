@@ -31,69 +31,71 @@ __device__ inline double TRIEY(const Dev& P, int i, int j) { return P.dltytrie[(
 // plus PFPXB/PFPYB and AH_BOTTOM at K=KBM1 (adv_t.F:394-408).
 // -------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_grad(const Dev P, int which) {
-  int i = blockIdx.x * 32 + threadIdx.x + 1;
-  int k = blockIdx.y * 8 + threadIdx.y + 1;
-  if (i > P.M || k > P.KBM1) return;
-  if (which == 0 && k < 2) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  int kb, ke;
+  col_range(P, which == 0 ? 2 : 1, P.KBM1, kb, ke);
   const int nt = P.ntsn[i];
   const double art2 = P.art2[i];
-  for (int t = 0; t < 2; ++t) {
-    const double* Q;
-    const double* QM = nullptr;
-    double** G;
-    if (which == 0) {
-      Q = (t == 0 ? P.q2 : P.q2l) + N3(P, 0, k);
-      G = (double**)P.gq[t];
-    } else {
-      Q = (t == 0 ? P.t1 : P.s1) + N3(P, 0, k);
-      QM = (t == 0 ? P.tmean1 : P.smean1) + N3(P, 0, k);
-      G = (double**)P.gt[t];
-    }
-    const double qmean = F4(1.e-8);
-    double px = 0.0, py = 0.0, pxd = 0.0, pyd = 0.0;
-    double rmin = Q[NBSN(P, i, 1)], rmax = rmin;
-    for (int j = 1; j <= nt - 1; ++j) {
-      int i1 = NBSN(P, i, j), i2 = NBSN(P, i, j + 1);
-      if (j >= 2) {
-        rmin = fmin(rmin, Q[i1]);
-        rmax = fmax(rmax, Q[i1]);
-      }
-      double ffd, ff1;
+  for (int k = kb; k <= ke; ++k) {
+    for (int t = 0; t < 2; ++t) {
+      const double* Q;
+      const double* QM = nullptr;
+      double* const* G;
       if (which == 0) {
-        ffd = 0.5 * (Q[i1] + Q[i2] - qmean - qmean);
-        ff1 = 0.5 * (Q[i1] + Q[i2]);
+        Q = (t == 0 ? P.q2 : P.q2l) + N3(P, 0, k);
+        G = P.gq[t];
       } else {
-        int w1 = P.iswetn[i1], w2 = P.iswetn[i2];
-        int a = i1, b = i2;
-        if (w1 == 0 && w2 == 1) { a = i; b = i2; }
-        else if (w1 == 1 && w2 == 0) { a = i1; b = i; }
-        else if (w1 == 0 && w2 == 0) { a = i; b = i; }
-        ffd = 0.5 * (Q[a] + Q[b] - QM[a] - QM[b]);
-        ff1 = 0.5 * (Q[a] + Q[b]);
+        Q = (t == 0 ? P.t1 : P.s1) + N3(P, 0, k);
+        QM = (t == 0 ? P.tmean1 : P.smean1) + N3(P, 0, k);
+        G = P.gt[t];
       }
-      double ty = TRIEY(P, i, j), tx = TRIEX(P, i, j);
-      px = px + ff1 * ty;
-      py = py + ff1 * tx;
-      pxd = pxd + ffd * ty;
-      pyd = pyd + ffd * tx;
-    }
-    px = px / art2;
-    py = py / art2;
-    pxd = pxd / art2;
-    pyd = pyd / art2;
-    size_t q = N3(P, i, k);
-    G[0][q] = px;
-    G[1][q] = py;
-    G[2][q] = pxd;
-    G[3][q] = pyd;
-    G[4][q] = rmin;
-    G[5][q] = rmax;
-    if (which == 1 && k == P.KBM1) {
-      if (t == 0) { P.pfpxb_t[i] = px; P.pfpyb_t[i] = py; }
-      else { P.pfpxb_s[i] = px; P.pfpyb_s[i] = py; }
-      double ah = (P.fact * P.viscofh[N3(P, i, P.KBM1)] + P.fm1) * P.nn_hvc[i];
-      if (t == 0) P.ah_bottom_t[i] = ah;
-      else P.ah_bottom_s[i] = ah;
+      const double qmean = F4(1.e-8);
+      double px = 0.0, py = 0.0, pxd = 0.0, pyd = 0.0;
+      double rmin = Q[NBSN(P, i, 1)], rmax = rmin;
+      for (int j = 1; j <= nt - 1; ++j) {
+        int i1 = NBSN(P, i, j), i2 = NBSN(P, i, j + 1);
+        if (j >= 2) {
+          rmin = fmin(rmin, Q[i1]);
+          rmax = fmax(rmax, Q[i1]);
+        }
+        double ffd, ff1;
+        if (which == 0) {
+          ffd = 0.5 * (Q[i1] + Q[i2] - qmean - qmean);
+          ff1 = 0.5 * (Q[i1] + Q[i2]);
+        } else {
+          int w1 = P.iswetn[i1], w2 = P.iswetn[i2];
+          int a = i1, b = i2;
+          if (w1 == 0 && w2 == 1) { a = i; b = i2; }
+          else if (w1 == 1 && w2 == 0) { a = i1; b = i; }
+          else if (w1 == 0 && w2 == 0) { a = i; b = i; }
+          ffd = 0.5 * (Q[a] + Q[b] - QM[a] - QM[b]);
+          ff1 = 0.5 * (Q[a] + Q[b]);
+        }
+        double ty = TRIEY(P, i, j), tx = TRIEX(P, i, j);
+        px = px + ff1 * ty;
+        py = py + ff1 * tx;
+        pxd = pxd + ffd * ty;
+        pyd = pyd + ffd * tx;
+      }
+      px = px / art2;
+      py = py / art2;
+      pxd = pxd / art2;
+      pyd = pyd / art2;
+      size_t q = N3(P, i, k);
+      G[0][q] = px;
+      G[1][q] = py;
+      G[2][q] = pxd;
+      G[3][q] = pyd;
+      G[4][q] = rmin;
+      G[5][q] = rmax;
+      if (which == 1 && k == P.KBM1) {
+        if (t == 0) { P.pfpxb_t[i] = px; P.pfpyb_t[i] = py; }
+        else { P.pfpxb_s[i] = px; P.pfpyb_s[i] = py; }
+        double ah = (P.fact * P.viscofh[N3(P, i, P.KBM1)] + P.fm1) * P.nn_hvc[i];
+        if (t == 0) P.ah_bottom_t[i] = ah;
+        else P.ah_bottom_s[i] = ah;
+      }
     }
   }
 }
@@ -189,25 +191,43 @@ __device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell& hc) {
   }
 }
 
-// EXFLUX of half-edge he on layer k for tracer t; a and b are the positions of NIEC(he,1)
-// and NIEC(he,2) among the cell's nodes.  xadv receives EXFLUX-FXX-FYY.
+// v[j] for a run-time slot j in 0..2, by selects, so v stays in registers.
+__device__ inline double sel3(const double* v, int j) { return j == 0 ? v[0] : (j == 1 ? v[1] : v[2]); }
+__device__ inline int sel3i(const int* v, int j) { return j == 0 ? v[0] : (j == 1 ? v[1] : v[2]); }
+
+// One tracer's node data on layer k: value, ring gradients, ring extrema.
+struct TRec {
+  double q, px, py, pxd, pyd, rmin, rmax;
+};
 template <int MODE>
-__device__ inline double he_flux(const Dev& P, const HeCell& hc, int he, int k, int t, int a, int b,
-                                 const double* qv, const double* const* gv, double* xadv) {
+__device__ inline TRec load_trec(const Dev& P, int n, int k, int t) {
+  const double* Q = MODE == 0 ? (t == 0 ? P.q2 : P.q2l) : (t == 0 ? P.t1 : P.s1);
+  double* const* G = MODE == 0 ? P.gq[t] : P.gt[t];
+  const size_t q = N3(P, n, k);
+  return TRec{Q[q], G[0][q], G[1][q], G[2][q], G[3][q], G[4][q], G[5][q]};
+}
+
+// EXFLUX of half-edge he for tracer t; a and b are the positions of NIEC(he,1) and
+// NIEC(he,2) among the cell's nodes, ra and rb their records.  xadv receives
+// EXFLUX-FXX-FYY.
+template <int MODE>
+__device__ inline double he_flux(const Dev& P, const HeCell& hc, int he, int a, int b, const TRec& ra,
+                                 const TRec& rb, double* xadv) {
   const size_t vi1 = P.NCV_I + 1;
   double un = hc.vq * P.dltxe[he] - hc.uq * P.dltye[he];
-  double fij1 = qv[a] + P.dltxncve[he] * gv[0][a] + P.dltyncve[he] * gv[1][a];
-  double fij2 = qv[b] + P.dltxncve[vi1 + he] * gv[0][b] + P.dltyncve[vi1 + he] * gv[1][b];
-  double q1min = fmin(gv[4][a], qv[a]), q1max = fmax(gv[5][a], qv[a]);
-  double q2min = fmin(gv[4][b], qv[b]), q2max = fmax(gv[5][b], qv[b]);
+  double fij1 = ra.q + P.dltxncve[he] * ra.px + P.dltyncve[he] * ra.py;
+  double fij2 = rb.q + P.dltxncve[vi1 + he] * rb.px + P.dltyncve[vi1 + he] * rb.py;
+  double q1min = fmin(ra.rmin, ra.q), q1max = fmax(ra.rmax, ra.q);
+  double q2min = fmin(rb.rmin, rb.q), q2max = fmax(rb.rmax, rb.q);
   if (fij1 < q1min) fij1 = q1min;
   if (fij1 > q1max) fij1 = q1max;
   if (fij2 < q2min) fij2 = q2min;
   if (fij2 > q2max) fij2 = q2max;
-  double viscof = P.fact * 0.5 * (hc.vf[a] * hc.nn[a] + hc.vf[b] * hc.nn[b]) + P.fm1 * 0.5 * (hc.nn[a] + hc.nn[b]);
+  const double vfa = sel3(hc.vf, a), vfb = sel3(hc.vf, b), nna = sel3(hc.nn, a), nnb = sel3(hc.nn, b);
+  double viscof = P.fact * 0.5 * (vfa * nna + vfb * nnb) + P.fm1 * 0.5 * (nna + nnb);
   if (MODE == 0) viscof = viscof / P.hprnu;
-  double txx = 0.5 * (gv[2][a] + gv[2][b]) * viscof;
-  double tyy = 0.5 * (gv[3][a] + gv[3][b]) * viscof;
+  double txx = 0.5 * (ra.pxd + rb.pxd) * viscof;
+  double tyy = 0.5 * (ra.pyd + rb.pyd) * viscof;
   double fxx = -hc.dtij * txx * P.dltye[he];
   double fyy = hc.dtij * tyy * P.dltxe[he];
   double sg = fsign1(un);
@@ -216,43 +236,38 @@ __device__ inline double he_flux(const Dev& P, const HeCell& hc, int he, int k, 
   return exflux;
 }
 
-template <int MODE>
-__device__ inline void tracer_nodes(const Dev& P, const HeCell& hc, int k, int t, double* qv, double gv[6][3]) {
-  const double* Q = MODE == 0 ? (t == 0 ? P.q2 : P.q2l) : (t == 0 ? P.t1 : P.s1);
-  double* const* G = MODE == 0 ? P.gq[t] : P.gt[t];
-  for (int j = 0; j < 3; ++j) {
-    size_t q = N3(P, hc.nd[j], k);
-    qv[j] = Q[q];
-    for (int g = 0; g < 6; ++g) gv[g][j] = G[g][q];
-  }
-}
-
 __device__ inline int pos3(const HeCell& hc, int n) { return n == hc.nd[0] ? 0 : (n == hc.nd[1] ? 1 : 2); }
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_he_adv(const Dev P, int parts) {
-  int c = blockIdx.x * 32 + threadIdx.x + 1;
-  int k = blockIdx.y * 8 + threadIdx.y + (MODE == 0 ? 2 : 1);
-  if (c > P.N || k > P.KBM1) return;
-  HeCell hc;
-  he_cell_load<MODE>(P, c, k, hc);
+  int c = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (c > P.N) return;
+  int kb, ke;
+  col_range(P, MODE == 0 ? 2 : 1, P.KBM1, kb, ke);
   const size_t v1 = P.NCV + 1;
+  const bool do0 = parts & (MODE == 0 ? AD_Q2 : AD_T), do1 = parts & (MODE == 0 ? AD_Q2L : AD_S);
   int hes[3], pa[3], pb[3];
-  for (int s = 0; s < 3; ++s) {
-    int he = P.cell_he[3 * c + s];
-    hes[s] = he;
-    pa[s] = pos3(hc, P.niec[he]);
-    pb[s] = pos3(hc, P.niec[v1 + he]);
+  {
+    int nd0 = P.nv[c], nd1 = P.nv[(size_t)(P.N + 1) + c];
+    for (int s = 0; s < 3; ++s) {
+      int he = P.cell_he[3 * c + s];
+      hes[s] = he;
+      int na = P.niec[he], nb = P.niec[v1 + he];
+      pa[s] = na == nd0 ? 0 : (na == nd1 ? 1 : 2);
+      pb[s] = nb == nd0 ? 0 : (nb == nd1 ? 1 : 2);
+    }
   }
-  for (int t = 0; t < 2; ++t) {
-    int bit = MODE == 0 ? (t == 0 ? AD_Q2 : AD_Q2L) : (t == 0 ? AD_T : AD_S);
-    if (!(parts & bit)) continue;
-    double qv[3], gv[6][3];
-    tracer_nodes<MODE>(P, hc, k, t, qv, gv);
-    const double* gp[6] = {gv[0], gv[1], gv[2], gv[3], gv[4], gv[5]};
-    double* EX = P.ex[t] + (size_t)(k - 1) * P.ncvs;
-    for (int s = 0; s < 3; ++s)
-      EX[hes[s]] = he_flux<MODE>(P, hc, hes[s], k, t, pa[s], pb[s], qv, gp, nullptr);
+  for (int k = kb; k <= ke; ++k) {
+    HeCell hc;
+    he_cell_load<MODE>(P, c, k, hc);
+    double2* EX = P.ex2 + (size_t)(k - 1) * P.ncvs;
+    for (int s = 0; s < 3; ++s) {
+      const int na = sel3i(hc.nd, pa[s]), nb = sel3i(hc.nd, pb[s]);
+      double e0 = 0.0, e1 = 0.0;
+      if (do0) e0 = he_flux<MODE>(P, hc, hes[s], pa[s], pb[s], load_trec<MODE>(P, na, k, 0), load_trec<MODE>(P, nb, k, 0), nullptr);
+      if (do1) e1 = he_flux<MODE>(P, hc, hes[s], pa[s], pb[s], load_trec<MODE>(P, na, k, 1), load_trec<MODE>(P, nb, k, 1), nullptr);
+      EX[hes[s]] = make_double2(e0, e1);
+    }
   }
 }
 
@@ -267,23 +282,43 @@ __device__ inline double obc_xflux_adv(const Dev& P, int i, int k, int t) {
     int c = P.ntrg[he];
     HeCell hc;
     he_cell_load<1>(P, c, k, hc);
-    double qv[3], gv[6][3];
-    tracer_nodes<1>(P, hc, k, t, qv, gv);
-    const double* gp[6] = {gv[0], gv[1], gv[2], gv[3], gv[4], gv[5]};
+    const int na = P.niec[he], nb = P.niec[v1 + he];
     double part;
-    he_flux<1>(P, hc, he, k, t, pos3(hc, P.niec[he]), pos3(hc, P.niec[v1 + he]), qv, gp, &part);
+    he_flux<1>(P, hc, he, pos3(hc, na), pos3(hc, nb), load_trec<1>(P, na, k, t), load_trec<1>(P, nb, k, t), &part);
     xa = (code & 1) ? xa - part : xa + part;
   }
   return xa;
 }
 
+// Signed sum of a node's half-edge fluxes on layer k, both tracers, in ascending
+// half-edge order (the order of the reference's scatter into XFLUX).
+__device__ inline double2 gather_he(const Dev& P, int q0, int q1, int k) {
+  const double2* EX = P.ex2 + (size_t)(k - 1) * P.ncvs;
+  double x0 = 0.0, x1 = 0.0;
+  for (int q = q0; q < q1; ++q) {
+    int code = P.node_he[q];
+    double2 e = EX[code >> 1];
+    if (code & 1) {
+      x0 = x0 - e.x;
+      x1 = x1 - e.y;
+    } else {
+      x0 = x0 + e.x;
+      x1 = x1 + e.y;
+    }
+  }
+  return make_double2(x0, x1);
+}
+
 // Phase 2 of ADV_Q(Q2,Q2F)/ADV_Q(Q2L,Q2LF) (adv_q.F:114-401) with FCT_Q2/FCT_Q2L.
 __global__ void __launch_bounds__(256) k_gather_q(const Dev P, int parts) {
-  int i = blockIdx.x * 32 + threadIdx.x + 1;
-  int k = blockIdx.y * 8 + threadIdx.y + 2;
-  if (i > P.M || k > P.KBM1) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  int kb, ke;
+  col_range(P, 2, P.KBM1, kb, ke);
   const bool wet = P.iswetn[i] * P.iswetnt[i] == 1;
   const int q0 = P.node_he_ptr[i], q1 = P.node_he_ptr[i + 1];
+  for (int k = kb; k <= ke; ++k) {
+  const double2 xs = gather_he(P, q0, q1, k);
   for (int t = 0; t < 2; ++t) {
     if (!(parts & (t == 0 ? AD_Q2 : AD_Q2L))) continue;
     const double* Q = (t == 0 ? P.q2 : P.q2l);
@@ -293,13 +328,7 @@ __global__ void __launch_bounds__(256) k_gather_q(const Dev P, int parts) {
       QF[N3(P, i, 1)] = 0.0;
       QF[N3(P, i, P.KB)] = 0.0;
     }
-    const double* EX = P.ex[t] + (size_t)(k - 1) * P.ncvs;
-    double x = 0.0;
-    for (int q = q0; q < q1; ++q) {
-      int code = P.node_he[q];
-      double e = EX[code >> 1];
-      x = (code & 1) ? x - e : x + e;
-    }
+    double x = t == 0 ? xs.x : xs.y;
     size_t q = N3(P, i, k);
     double qf;
     if (wet) {
@@ -318,6 +347,7 @@ __global__ void __launch_bounds__(256) k_gather_q(const Dev P, int parts) {
       if (qf - qmax > 0.0) qf = qmax;
     }
     QF[q] = qf;
+  }
   }
 }
 
@@ -527,23 +557,20 @@ __global__ void __launch_bounds__(256) k_turb_update(const Dev P) {
 // fct_s.F:50-108) on the same (node, layer) thread.
 // -------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_gather_ts(const Dev P, int parts) {
-  int i = blockIdx.x * 32 + threadIdx.x + 1;
-  int k = blockIdx.y * 8 + threadIdx.y + 1;
-  if (i > P.M || k > P.KBM1) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  int kb, ke;
+  col_range(P, 1, P.KBM1, kb, ke);
   const bool wet = P.iswetn[i] * P.iswetnt[i] == 1;
   const int ob = P.node_obc[i];
   const int q0 = P.node_he_ptr[i], q1 = P.node_he_ptr[i + 1];
+  for (int k = kb; k <= ke; ++k) {
+  const double2 xs = gather_he(P, q0, q1, k);
   for (int t = 0; t < 2; ++t) {
     if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
     const double* F1 = (t == 0 ? P.t1 : P.s1);
     double* FF1 = (t == 0 ? P.tf1 : P.sf1);
-    const double* EX = P.ex[t] + (size_t)(k - 1) * P.ncvs;
-    double x = 0.0;
-    for (int q = q0; q < q1; ++q) {
-      int code = P.node_he[q];
-      double e = EX[code >> 1];
-      x = (code & 1) ? x - e : x + e;
-    }
+    double x = t == 0 ? xs.x : xs.y;
     if (ob > 0) (t == 0 ? P.xflux_obc_t : P.xflux_obc_s)[(size_t)(k - 1) * (P.iobcn + 1) + ob] = obc_xflux_adv(P, i, k, t);
     size_t q = N3(P, i, k);
     double ff;
@@ -580,6 +607,7 @@ __global__ void __launch_bounds__(256) k_gather_ts(const Dev P, int parts) {
       if (t == 1 && ff < 0.0) ff = 0.0;
     }
     FF1[q] = ff;
+  }
   }
 }
 
@@ -832,13 +860,11 @@ __global__ void k_budget_final(const double* part, int nb, double* out) {
 }
 
 void launch_grad(const Dev& P, cudaStream_t s, int which) {
-  dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));
-  k_grad<<<g, b, 0, s>>>(P, which);
+  k_grad<<<col_grid(P, P.M, which == 0 ? P.KBM1 - 1 : P.KBM1), P.col_bc, 0, s>>>(P, which);
 }
 void launch_adv_q(const Dev& P, cudaStream_t s, int parts) {
-  dim3 b(32, 8);
-  k_he_adv<0><<<dim3(nblk(P.N, 32), nblk(P.KBM1 - 1, 8)), b, 0, s>>>(P, parts);
-  k_gather_q<<<dim3(nblk(P.M, 32), nblk(P.KBM1 - 1, 8)), b, 0, s>>>(P, parts);
+  k_he_adv<0><<<col_grid(P, P.N, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
+  k_gather_q<<<col_grid(P, P.M, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
 }
 void launch_fct_q(const Dev& P, cudaStream_t s, int parts) {
   dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1 - 1, 8));
@@ -853,9 +879,8 @@ void launch_turb_update(const Dev& P, cudaStream_t s) {
   k_turb_update<<<g, b, 0, s>>>(P);
 }
 void launch_adv_ts(const Dev& P, cudaStream_t s, int parts) {
-  dim3 b(32, 8);
-  k_he_adv<1><<<dim3(nblk(P.N, 32), nblk(P.KBM1, 8)), b, 0, s>>>(P, parts);
-  k_gather_ts<<<dim3(nblk(P.M, 32), nblk(P.KBM1, 8)), b, 0, s>>>(P, parts);
+  k_he_adv<1><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P, parts);
+  k_gather_ts<<<col_grid(P, P.M, P.KBM1), P.col_bc, 0, s>>>(P, parts);
 }
 void launch_fct_ts(const Dev& P, cudaStream_t s, int parts) {
   dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));

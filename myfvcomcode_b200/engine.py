@@ -202,3 +202,20 @@ class Fvcom(CEngine):
 
     def shutdown_check(self):
         return int(self.lib.fvg_shutdown_check(self.h))
+
+    def set_tuning(self, key, value):
+        self.lib.fvg_set_tuning.argtypes = [C.c_void_p, C.c_char_p, C.c_int32]
+        self._check(self.lib.fvg_set_tuning(self.h, key.encode(), int(value)), "set_tuning(%s)" % key)
+
+    def get_tuning(self, key):
+        v = C.c_int32()
+        self.lib.fvg_get_tuning.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_int32)]
+        self._check(self.lib.fvg_get_tuning(self.h, key.encode(), C.byref(v)), "get_tuning(%s)" % key)
+        return v.value
+
+    def time_steps(self, n):
+        """Run n internal steps; device milliseconds (CUDA events on the handle's stream)."""
+        ms = C.c_double()
+        self.lib.fvg_time_steps.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]
+        self._check(self.lib.fvg_time_steps(self.h, int(n), C.byref(ms)), "time_steps")
+        return ms.value

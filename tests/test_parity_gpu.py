@@ -152,3 +152,24 @@ def test_graph_replay_equals_plain_launches(small_channel):
     b.run(5)
     for n in ("el", "ua", "u", "t1", "s1", "q2l", "kh"):
         assert np.array_equal(a.get(n), b.get(n)), n
+
+
+@pytest.mark.parametrize("threads,layers", [(32, 1), (64, 3), (256, 7)])
+def test_launch_shape_does_not_change_results(small_coastal, threads, layers):
+    from myfvcomcode_b200.engine import Fvcom
+    a = Fvcom(small_coastal)
+    b = Fvcom(small_coastal)
+    b.set_tuning("col_threads", threads)
+    b.set_tuning("col_layers", layers)
+    assert (b.get_tuning("col_threads"), b.get_tuning("col_layers")) == (threads, layers)
+    a.run(4)
+    b.run(4)
+    for n in ("el", "ua", "u", "v", "w", "t1", "s1", "q2", "q2l", "km", "viscofh", "wts"):
+        assert np.array_equal(a.get(n), b.get(n)), n
+
+
+def test_autotuner_returns_a_timed_shape(small_channel):
+    from myfvcomcode_b200 import autotune
+    r = autotune.autotune(small_channel, cands=[(64, 1), (128, 5)], steps=2, warmup=1)
+    assert (r["col_threads"], r["col_layers"]) in [(64, 1), (128, 5)]
+    assert len(r["table"]) == 2 and all(t[0] > 0 for t in r["table"])
