@@ -751,7 +751,8 @@ int32_t fvg_kernels_per_step(const fvg_handle* h) {
   n += p.isplit * 4 * (3 + (p.wetting_drying_on ? 2 : 0)); // RK stages
   n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv
   n += 4;                                                  // grad_q, adv_q (2 phases), vdif_q
-  if (p.temperature_active || p.salinity_active) n += 5;   // grad_ts, adv_ts (2 phases), vdif_ts, bcond_ts
+  if (p.temperature_active || p.salinity_active)           // grad_ts, adv_ts (2 phases), vdif_ts,
+    n += 5 + (h->P.iobcn > 0 ? 1 : 0);                     // bcond_ts (rivers, open boundary)
   n += 1;                                                  // final
   return n;
 }

@@ -441,19 +441,28 @@ __global__ void __launch_bounds__(128) k_vdif_q(const Dev P, int copy_back) {
       boygr[k] = P.grav_n[i] * (P.rho1[n3(k - 1)] - P.rho1[n3(k)]) / (P.dzz[n3(k - 1)] * d);
       prod[k] = P.km[n3(k)] * 0.0 * pow(.5 * (-boygr[k] + fabs(boygr[k])), 1.5);
     }
-    for (int k = 2; k <= KBM1; ++k) {
-      double uk = 0.0, vk = 0.0, ukm1 = 0.0, vkm1 = 0.0;
+    // Ring means of U and V on layer k; the layer k-1 means of the reference's loop are
+    // the same sums in the same order, carried from the previous iteration.
+    auto ring_mean = [&](int k, double& um, double& vm) {
+      double su = 0.0, sv = 0.0;
       for (int j = 1; j <= nt; ++j) {
         int c = P.nbve[(size_t)(j - 1) * m1 + i];
-        uk = uk + P.u[C3(P, c, k)];
-        vk = vk + P.v[C3(P, c, k)];
-        ukm1 = ukm1 + P.u[C3(P, c, k - 1)];
-        vkm1 = vkm1 + P.v[C3(P, c, k - 1)];
+        su = su + P.u[C3(P, c, k)];
+        sv = sv + P.v[C3(P, c, k)];
       }
-      uk = uk / fn; vk = vk / fn; ukm1 = ukm1 / fn; vkm1 = vkm1 / fn;
+      um = su / fn;
+      vm = sv / fn;
+    };
+    double ukm1, vkm1;
+    ring_mean(1, ukm1, vkm1);
+    for (int k = 2; k <= KBM1; ++k) {
+      double uk, vk;
+      ring_mean(k, uk, vk);
       double den = P.dzz[n3(k - 1)] * d;
       prod[k] = prod[k] + P.km[n3(k)] * SEF * ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den);
       prod[k] = prod[k] + P.kh[n3(k)] * boygr[k];
+      ukm1 = uk;
+      vkm1 = vk;
     }
   }
   for (int k = 2; k <= KBM1; ++k) L[n3(k)] = Q2L[n3(k)] / Q2[n3(k)];
@@ -700,7 +709,7 @@ __global__ void __launch_bounds__(128) k_vdif_ts(const Dev P, int parts) {
 // boundary nodes take the outflow estimate with the radiation perturbation of
 // OBC_TS_TYPE and the neighbour clamp, or keep T1/S1 on inflow.  One block.
 // -------------------------------------------------------------------------------------
-__global__ void k_bcond_ts(const Dev P, int parts) {
+__global__ void k_bcond_ts_riv(const Dev P) {
   const int KBM1 = P.KBM1;
   for (int r = threadIdx.x + 1; r <= P.numqbc; r += blockDim.x) {
     int n1 = P.river_location == 0 ? P.inodeq[r] : P.n_icellq[r];
@@ -714,11 +723,20 @@ __global__ void k_bcond_ts(const Dev P, int parts) {
       }
     }
   }
-  __syncthreads();
-  for (int ob = threadIdx.x + 1; ob <= P.iobcn; ob += blockDim.x) {
+}
+
+// Open-boundary part: one thread per (open-boundary node, tracer).  The nodes are
+// independent: each reads the old field, its own XFLUX_OBC and TF1/SF1 of its interior
+// neighbour NEXT_OBC, which is not an open-boundary node.
+__global__ void k_bcond_ts_obc(const Dev P, int parts) {
+  const int KBM1 = P.KBM1;
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ob = id / 2 + 1, t = id % 2;
+  if (ob > P.iobcn) return;
+  {
     int j = P.i_obc_n[ob], j1 = P.next_obc[ob];
-    for (int t = 0; t < 2; ++t) {
-      if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
+    {
+      if (!(parts & (t == 0 ? AD_T : AD_S))) return;
       const double* F1 = t == 0 ? P.t1 : P.s1;
       double* FF1 = t == 0 ? P.tf1 : P.sf1;
       const double* XO = t == 0 ? P.xflux_obc_t : P.xflux_obc_s;
@@ -889,7 +907,10 @@ void launch_fct_ts(const Dev& P, cudaStream_t s, int parts) {
 void launch_vdif_ts(const Dev& P, cudaStream_t s, int parts) {
   k_vdif_ts<<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
 }
-void launch_bcond_ts(const Dev& P, cudaStream_t s, int parts) { k_bcond_ts<<<1, 256, 0, s>>>(P, parts); }
+void launch_bcond_ts(const Dev& P, cudaStream_t s, int parts) {
+  k_bcond_ts_riv<<<1, 128, 0, s>>>(P);
+  if (P.iobcn > 0) k_bcond_ts_obc<<<nblk(2 * P.iobcn, 64), 64, 0, s>>>(P, parts);
+}
 void launch_final(const Dev& P, cudaStream_t s, int parts) {
   int n = (P.M > P.N ? P.M : P.N) + 1;
   dim3 b(32, 8), g(nblk(n, 32), nblk(P.KB, 8));
