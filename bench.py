@@ -43,6 +43,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shape instead of autotuning it")
+    ap.add_argument("--precision", default="fp32flux", choices=["fp64", "fp32flux"],
+                    help="form timed for the headline value (fp32flux: FP32 edge fluxes and advection)")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip timing the plain FP64 path beside the chosen form")
     return ap.parse_args()
 
 
@@ -224,38 +228,62 @@ def main():
         import torch  # noqa: F401  (pinned host buffers for the end-to-end leg)
     import torch
     torch.cuda.set_device(local)
-    f = Fvcom(case)
+    lib = None
+
+    def timed_handle(precision):
+        """A handle of the case in ``precision``, autotuned and warmed up, and its device
+        time over ``args.steps`` internal steps (max over ranks) with the clocks seen."""
+        f = Fvcom(case)
+        f.set_precision(precision)
+        if not args.no_tune:
+            from myfvcomcode_b200 import autotune
+            tuned = autotune.autotune(case, steps=2, warmup=1, engine=f)
+            autotune.apply(f, tuned)
+        f.run(args.warmup)
+        barrier(pg, local)
+        sampler = ClockSampler(local)
+        sampler.start()
+        time.sleep(0.3)
+        t = f.time_steps(args.steps)
+        clocks = sampler.stop()
+        barrier(pg, local)
+        t = reduce_max(pg, t, local)
+        if f.shutdown_check() != 0:
+            raise SystemExit("non-finite state after the timed steps (%s)" % precision)
+        return f, t, clocks
+
+    f, t_ms, clocks = timed_handle(args.precision)
     lib = f.lib
-    lib.fvg_time_steps.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]
     lib.fvg_profile.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.fvg_profile_groups.restype = C.c_int32
     lib.fvg_profile_group_name.restype = C.c_char_p
     lib.fvg_profile_group_name.argtypes = [C.c_int32]
     lib.fvg_kernels_per_step.argtypes = [C.c_void_p]
     lib.fvg_kernels_per_step.restype = C.c_int32
-
-    if not args.no_tune:
-        from myfvcomcode_b200 import autotune
-        tuned = autotune.autotune(case, steps=2, warmup=1, engine=f)
-        autotune.apply(f, tuned)
+    cfg["precision"] = {"fp64": "plain FP64",
+                        "fp32flux": "FP32 edge fluxes/advection/FCT; FP64 elevation update, "
+                                    "column solves, state and budgets"}[args.precision]
     cfg["tiling"] = {"col_threads": f.get_tuning("col_threads"), "col_layers": f.get_tuning("col_layers"),
                      "autotuned": not args.no_tune}
-
-    f.run(args.warmup)
-    barrier(pg, local)
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
-    ms = C.c_double()
-    rc = lib.fvg_time_steps(f.h, args.steps, C.byref(ms))
-    clocks = sampler.stop()
-    if rc != 0:
-        raise SystemExit("fvg_time_steps failed: %d" % rc)
-    barrier(pg, local)
-    t_ms = reduce_max(pg, ms.value, local)
     value = cells_layers * args.steps * world / (t_ms / 1e3)
-    if f.shutdown_check() != 0:
-        raise SystemExit("non-finite state after the timed steps")
+
+    plain = None
+    if args.precision != "fp64" and not args.no_plain:
+        fp, tp_ms, _ = timed_handle("fp64")
+        plain = {"value": cells_layers * args.steps * world / (tp_ms / 1e3), "ms_per_step": tp_ms / args.steps,
+                 "tiling": [fp.get_tuning("col_threads"), fp.get_tuning("col_layers")]}
+        # Both handles ran the same steps from the same cold start: live error of the
+        # chosen form against FP64 at this point of the run.
+        from myfvcomcode_b200.precision_report import compare
+        n_done = fp.clock()[0]
+        if f.clock()[0] == n_done:
+            plain["error_of_chosen_form"] = dict(compare(fp, f), internal_steps=n_done)
+        fp.close()
+        day = os.path.join(ROOT, "profiles", "precision_error_coastal200k_k40_1day.json")
+        if os.path.exists(day):
+            with open(day) as fh:
+                plain["error_after_1_day"] = json.load(fh).get("errors_vs_fp64")
+        cfg["plain_fp64"] = plain
 
     # per-kernel-group device time (plain launches with events between groups)
     ng = lib.fvg_profile_groups()
@@ -264,7 +292,7 @@ def main():
     nprof = 2
     lib.fvg_profile(f.h, nprof, gms, C.byref(tot))
     names = [lib.fvg_profile_group_name(i).decode() for i in range(ng)]
-    led = bytes_model.ledger(g, p["ISPLIT"], bool(p["WETTING_DRYING_ON"]))
+    led = bytes_model.ledger(g, p["ISPLIT"], bool(p["WETTING_DRYING_ON"]), args.precision)
     groups = {names[i]: gms[i] / nprof for i in range(ng) if gms[i] > 0}
     dom = max(groups, key=groups.get)
     b_launch, n_launch = led[dom]
@@ -272,7 +300,7 @@ def main():
     achieved = b_launch / (dur / 1e3) / 1e9
     peak, peak_kind = peak_hbm()
     traffic = traffic_table().get((dom, case["name"]))
-    step_b = bytes_model.step_bytes(g, p["ISPLIT"], bool(p["WETTING_DRYING_ON"]))
+    step_b = bytes_model.step_bytes(g, p["ISPLIT"], bool(p["WETTING_DRYING_ON"]), args.precision)
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
             "algorithmic_bytes_per_launch": b_launch, "launch_ms": dur,
@@ -323,7 +351,8 @@ def main():
     if rank == 0:
         line = {"metric": metric, "value": value, "unit": "cell-layer updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32 fluxes, f64 state",
                 "data": "synthetic", "config": cfg, "clocks": clocks, "e2e": e2e, "roofline": roof,
                 "cpu_baseline": cpu, "gpu_launches": int(lib.fvg_kernels_per_step(f.h)) * args.steps}
         print(json.dumps(line), flush=True)

@@ -210,6 +210,17 @@ int fvg_sync(fvg_handle* h);
 int fvg_set_ramp(fvg_handle* h, double ramp);
 /* 1 (default): replay a captured CUDA graph per internal step; 0: plain launches. */
 int fvg_use_graph(fvg_handle* h, int32_t on);
+/* Precision form.  FVG_PREC_FP64 (default): FP64 everywhere, bitwise equal to the
+   oracle.  FVG_PREC_FP32_FLUX: the edge fluxes and advection -- ADVAVE's edge loop, the
+   3-D momentum edge fluxes of ADVECTION_EDGE_GCN/ADV_UV_EDGE_GCN, ADV_Q and ADV_T/ADV_S
+   with FCT and their node-ring and cell gradients -- in FP32 arithmetic over FP32 scratch
+   and FP32 copies of their mesh metrics; the free-surface update (EXTEL_EDGE), the
+   vertical continuity, the tridiagonal solves, the state and the budgets stay FP64.
+   The first switch to FP32 allocates its scratch. */
+#define FVG_PREC_FP64 0
+#define FVG_PREC_FP32_FLUX 1
+int fvg_set_precision(fvg_handle* h, int32_t mode);
+int32_t fvg_get_precision(const fvg_handle* h);
 /* Launch shape of the 3-D gather kernels (results do not depend on it):
    "col_threads" = entities (threads) per block, 32..256 in steps of 32 (default 128);
    "col_layers"  = consecutive layers each thread walks, 1..KB (default 8). */

@@ -22,42 +22,55 @@ def sizes(grid):
                 K=grid["KB"] - 1, ntsn=int(grid["NTSN"][1:].sum()), ntve=int(grid["NTVE"][1:].sum()))
 
 
-def ledger(grid, isplit, wet_dry):
-    """{group: (bytes per launch, launches per internal step)}"""
+def ledger(grid, isplit, wet_dry, precision="fp64"):
+    """{group: (bytes per launch, launches per internal step)}
+
+    ``precision`` "fp32flux" counts the arrays that form keeps in FP32 at 4 bytes: the
+    least-squares and node-ring gradients (A1U/A2U, the 2-D and 3-D cell gradients,
+    PTPX.. with the ring extrema), the edge offsets, DLTXC/DLTYC, ART, CC_HVC and the
+    control-volume metrics read by the flux kernels.  FP64 state is counted at 8 bytes.
+    """
     s = sizes(grid)
     M, N, NE, NCV, K, KB = s["M"], s["N"], s["NE"], s["NCV"], s["K"], s["KB"]
     ntsn, ntve = s["ntsn"], s["ntve"]
+    X = 4 if precision == "fp32flux" else D  # width of the flux kernels' scratch and metrics
     st = 4 * isplit
     ring = I * ntsn + 2 * D * ntsn          # NBSN + DLTXTRIE/DLTYTRIE entries
     halfedge_csr = I * 2 * NCV + I * (M + 1)
-    halfedge_geo = NCV * (I + 2 * D) + NCV * (2 * I + 4 * D)  # NTRG, DLTXE/YE, NIEC, DLTXNCVE/YNCVE
-    edge_geo = NE * (4 * I + I + 4 * D)     # IEC, IENODE, ISBC, XIJC/YIJC/DLTXC/DLTYC
-    cell_lsq = N * (3 * I + 8 * D + 3 * I)  # NBE, A1U/A2U, CELL_EDGE
+    halfedge_geo = NCV * (I + 2 * X) + NCV * (2 * I + 4 * X)  # NTRG, DLTXE/YE, NIEC, DLTXNCVE/YNCVE
+    # IEC, IENODE, ISBC, and the edge offsets (XIJC/YIJC with XC/YC) and DLTXC/DLTYC
+    edge_off = NE * 2 * D + N * 2 * D if X == D else NE * 4 * X
+    edge_geo = NE * (4 * I + I + 2 * X) + edge_off
+    cell_lsq = N * (3 * I + 8 * X + 3 * I)  # NBE, A1U/A2U, CELL_EDGE
+    pg_extra = 0 if X == D else NE * 2 * D  # FP64 DLTXC/DLTYC of the surface-slope term
     g = {}
     # ---- external mode, per RK stage ----
     g["ext_node"] = (M * (I + I + 3 * D) + halfedge_csr + NCV * (I + 2 * D) + N * 3 * D, st)
-    g["ext_cell"] = (N * (cell_lsq // N + 26 * D + 6 * I) + N * 8 * D + edge_geo + M * 4 * D, st)
+    g["ext_cell"] = (N * (cell_lsq // N + 22 * D + 4 * X + 6 * I) + N * 8 * D + edge_geo + pg_extra
+                     + M * 4 * D, st)
     g["ext_update"] = (M * (6 * D + I) + N * (10 * D + (2 * I if wet_dry else 0)), st)
     if wet_dry:
         g["wet_judge"] = (N * (3 * I + I + D) + M * (4 * D + 2 * I) + I * ntve, st)
     # ---- 3-D, once per internal step ----
     g["cell_pre"] = (N * K * 4 * D + N * K * D + N * 12 * D, 1)              # U,V rw; DZ1; 2-D
-    g["advection3d"] = (N * K * 4 * D + M * K * D + cell_lsq + N * 10 * D + edge_geo + M * D, 1)
+    g["advection3d"] = (N * K * 2 * D + N * K * 2 * X + M * K * D + cell_lsq + N * 6 * D + N * 4 * X
+                        + edge_geo + M * D, 1)
     g["baropg"] = (M * K * 2 * D + N * KB * 2 * D + N * K * 7 * D + N * 10 * D + M * 3 * D, 1)
-    g["int_advave"] = (N * (cell_lsq // N + 20 * D) + edge_geo + M * 3 * D, 1)
+    g["int_advave"] = (N * (cell_lsq // N + 16 * D + 4 * X) + edge_geo + pg_extra + M * 3 * D, 1)
     g["adjust2"] = (N * K * 5 * D + N * 6 * D, 1)
     g["vertvl_flux"] = (N * K * 3 * D + M * K * D + halfedge_csr + NCV * (I + 2 * D) + N * D, 1)
     g["vertvl_col"] = (M * K * 2 * D + M * KB * D + M * K * 2 * D + M * 10 * D + I * ntve + N * 2 * D, 1)
     g["w_viscofh"] = (M * KB * D + N * KB * D + N * K * 2 * D + M * K * D + M * 3 * D
                       + ntve * (I + 4 * D) + N * I, 1)
-    g["adv_uv"] = (N * K * 9 * D + N * D + M * K * D + cell_lsq + N * 14 * D + edge_geo + M * 2 * D, 1)
+    g["adv_uv"] = (N * K * 7 * D + N * K * 2 * X + N * D + M * K * D + cell_lsq + N * 10 * D + N * 4 * X
+                   + edge_geo + M * 2 * D, 1)
     g["vdif_uv"] = (N * KB * D + N * K * 10 * D + N * 20 * D + M * 3 * D, 1)
-    g["grad_q"] = (M * K * 2 * D + M * K * 12 * D + ring + M * 2 * D, 1)
-    g["adv_q"] = (M * K * (12 * D + 6 * D + 2 * D) + N * K * 4 * D + halfedge_csr + halfedge_geo
+    g["grad_q"] = (M * K * 2 * D + M * K * 12 * X + ring + M * 2 * D, 1)
+    g["adv_q"] = (M * K * (12 * X + 6 * D + 2 * D) + N * K * 4 * D + halfedge_csr + halfedge_geo
                   + M * 6 * D, 1)
     g["vdif_q"] = (M * KB * 14 * D + N * K * 2 * D + N * 4 * D + I * ntve + M * 6 * D, 1)
-    g["grad_ts"] = (M * K * 4 * D + M * K * 12 * D + ring + M * 8 * D, 1)
-    g["adv_ts"] = (M * K * (12 * D + 6 * D + 2 * D) + N * K * 3 * D + halfedge_csr + halfedge_geo
+    g["grad_ts"] = (M * K * 4 * D + M * K * 12 * X + ring + M * 8 * D, 1)
+    g["adv_ts"] = (M * K * (12 * X + 6 * D + 2 * D) + N * K * 3 * D + halfedge_csr + halfedge_geo
                    + M * 6 * D, 1)
     g["vdif_ts"] = (M * K * 5 * D + M * 12 * D, 1)
     g["bcond_ts"] = (grid["IOBCN"] * K * 8 * D, 1)
@@ -65,5 +78,5 @@ def ledger(grid, isplit, wet_dry):
     return g
 
 
-def step_bytes(grid, isplit, wet_dry):
-    return sum(b * n for b, n in ledger(grid, isplit, wet_dry).values())
+def step_bytes(grid, isplit, wet_dry, precision="fp64"):
+    return sum(b * n for b, n in ledger(grid, isplit, wet_dry, precision).values())

@@ -264,6 +264,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   P.ns = (int)pad32(N + 1);
   P.col_bc = 128;
   P.col_lc = 8;
+  P.prec = FVG_PREC_FP64;
   P.nbsn_cols = m->nbsn_cols; P.nbve_cols = m->nbve_cols; P.trie_cols = m->trie_cols;
   P.iobcn = m->iobcn; P.numqbc = m->numqbc;
   P.isplit = prm->isplit;
@@ -775,6 +776,52 @@ int fvg_use_graph(fvg_handle* h, int32_t on) {
   h->use_graph = on != 0;
   return FVG_OK;
 }
+
+int fvg_set_precision(fvg_handle* h, int32_t mode) {
+  if (!h) return FVG_ERR_ARG;
+  if (mode != FVG_PREC_FP64 && mode != FVG_PREC_FP32_FLUX) { h->err = "unknown precision mode"; return FVG_ERR_ARG; }
+  Dev& P = h->P;
+  CK(cudaStreamSynchronize(h->stream));
+  if (mode == FVG_PREC_FP32_FLUX && !P.f.ex2) {
+    int rc;
+    const size_t ms = P.ms, ns = P.ns, KB = P.KB, n1 = P.N + 1, e1 = P.NE + 1;
+    const size_t v1 = P.NCV + 1, vi1 = P.NCV_I + 1;
+    F32& f = P.f;
+    auto fail = [&](int r) { return r; };
+    for (int q = 0; q < 4; ++q) {
+      if ((rc = dalloc(h, &f.g2d[q], n1))) return fail(rc);
+      if ((rc = dalloc(h, &f.g3[q], ns * KB))) return fail(rc);
+    }
+    for (int t = 0; t < 2; ++t)
+      for (int g = 0; g < 6; ++g) {
+        if ((rc = dalloc(h, &f.gq[t][g], ms * KB))) return fail(rc);
+        if ((rc = dalloc(h, &f.gt[t][g], ms * KB))) return fail(rc);
+      }
+    if ((rc = dalloc(h, (float**)&f.ex2, (size_t)P.ncvs * KB * 2))) return fail(rc);
+    if ((rc = dalloc(h, &f.xo, 2 * e1))) return fail(rc);
+    if ((rc = dalloc(h, &f.yo, 2 * e1))) return fail(rc);
+    if ((rc = dalloc(h, &f.dltxc, e1))) return fail(rc);
+    if ((rc = dalloc(h, &f.dltyc, e1))) return fail(rc);
+    if ((rc = dalloc(h, &f.art, n1))) return fail(rc);
+    if ((rc = dalloc(h, &f.cc_hvc, n1))) return fail(rc);
+    if ((rc = dalloc(h, &f.a1u, 4 * n1))) return fail(rc);
+    if ((rc = dalloc(h, &f.a2u, 4 * n1))) return fail(rc);
+    if ((rc = dalloc(h, &f.dltxe, v1))) return fail(rc);
+    if ((rc = dalloc(h, &f.dltye, v1))) return fail(rc);
+    if ((rc = dalloc(h, &f.dltxncve, 2 * vi1))) return fail(rc);
+    if ((rc = dalloc(h, &f.dltyncve, 2 * vi1))) return fail(rc);
+    launch_make_f32(P, h->stream);
+    CK(cudaGetLastError());
+  }
+  P.prec = mode;
+  // The captured step holds the other precision's kernels: capture again.
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  return FVG_OK;
+}
+
+int32_t fvg_get_precision(const fvg_handle* h) { return h ? h->P.prec : -1; }
 
 int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value) {
   if (!h || !key) return FVG_ERR_ARG;

@@ -35,6 +35,17 @@ struct SchedLayout {
   }
 };
 
+// FP32 scratch and mesh metrics of the precision form.  Edge offsets are formed in FP64
+// and rounded once: xo[e] = XIJC(e)-XC(IEC(e,1)), xo[NE+1+e] = XIJC(e)-XC(IEC(e,2)), the
+// same for y.
+struct F32 {
+  float *g2d[4], *g3[4];
+  float *gq[2][6], *gt[2][6];
+  float2* ex2;
+  float *xo, *yo, *dltxc, *dltyc, *art, *cc_hvc, *a1u, *a2u;
+  float *dltxe, *dltye, *dltxncve, *dltyncve;
+};
+
 // Device pointers and sizes, passed by value to kernels.
 struct Dev {
   int M, N, KB, KBM1, KBM2, NE, NCV, NCV_I, ms, ns;
@@ -116,6 +127,11 @@ struct Dev {
   double* exf2d;                             // EXTEL_EDGE flux of each half-edge (NCV+1)
   double* g3[4];                             // least-squares gradient of U, V per cell and layer (ns x KB)
   int ncvs;                                  // layer stride of ex (>= NCV+1)
+  // Precision form (fvg_set_precision): 0 = FP64 everywhere; 1 = the edge fluxes and
+  // advection (ADVAVE's edge loop, the 3-D momentum edge fluxes, ADV_Q/ADV_T/ADV_S with
+  // FCT) in FP32 arithmetic over FP32 scratch and FP32 copies of their mesh metrics.
+  int prec;
+  F32 f;
   // Column tiling of the 3-D gather kernels: col_bc threads (entities) per block, each
   // walking col_lc consecutive layers, so the entity's index chain (cell -> edge ->
   // neighbour) is resolved from cache after the first layer.  Results do not depend on it.
@@ -138,8 +154,60 @@ __device__ inline void col_range(const Dev& P, int k0, int klast, int& kb, int& 
 __host__ __device__ inline size_t N3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ms + i; }
 __host__ __device__ inline size_t C3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ns + i; }
 
+// Mesh metrics and scratch of the edge-flux kernels by arithmetic type R.  The FP64
+// instantiation reads the FP64 arrays and forms the edge offsets as the reference does;
+// the FP32 one reads the FP32 copies of the precision form.
+template <typename R> struct Mesh;
+template <> struct Mesh<double> {
+  typedef double2 R2;
+  __device__ static double xoa(const Dev& P, int e, int ia) { return P.xijc[e] - P.xc[ia]; }
+  __device__ static double yoa(const Dev& P, int e, int ia) { return P.yijc[e] - P.yc[ia]; }
+  __device__ static double xob(const Dev& P, int e, int ib) { return P.xijc[e] - P.xc[ib]; }
+  __device__ static double yob(const Dev& P, int e, int ib) { return P.yijc[e] - P.yc[ib]; }
+  __device__ static double dltxc(const Dev& P, int e) { return P.dltxc[e]; }
+  __device__ static double dltyc(const Dev& P, int e) { return P.dltyc[e]; }
+  __device__ static double art(const Dev& P, int c) { return P.art[c]; }
+  __device__ static double cc_hvc(const Dev& P, int c) { return P.cc_hvc[c]; }
+  __device__ static double a1u(const Dev& P, size_t q) { return P.a1u[q]; }
+  __device__ static double a2u(const Dev& P, size_t q) { return P.a2u[q]; }
+  __device__ static double dltxe(const Dev& P, size_t q) { return P.dltxe[q]; }
+  __device__ static double dltye(const Dev& P, size_t q) { return P.dltye[q]; }
+  __device__ static double dltxncve(const Dev& P, size_t q) { return P.dltxncve[q]; }
+  __device__ static double dltyncve(const Dev& P, size_t q) { return P.dltyncve[q]; }
+  __device__ static double* g2d(const Dev& P, int q) { return P.g2d[q]; }
+  __device__ static double* g3(const Dev& P, int q) { return P.g3[q]; }
+  __device__ static double* const* gq(const Dev& P, int t) { return P.gq[t]; }
+  __device__ static double* const* gt(const Dev& P, int t) { return P.gt[t]; }
+  __device__ static double2* ex2(const Dev& P) { return P.ex2; }
+};
+template <> struct Mesh<float> {
+  typedef float2 R2;
+  __device__ static float xoa(const Dev& P, int e, int) { return P.f.xo[e]; }
+  __device__ static float yoa(const Dev& P, int e, int) { return P.f.yo[e]; }
+  __device__ static float xob(const Dev& P, int e, int) { return P.f.xo[(size_t)P.NE + 1 + e]; }
+  __device__ static float yob(const Dev& P, int e, int) { return P.f.yo[(size_t)P.NE + 1 + e]; }
+  __device__ static float dltxc(const Dev& P, int e) { return P.f.dltxc[e]; }
+  __device__ static float dltyc(const Dev& P, int e) { return P.f.dltyc[e]; }
+  __device__ static float art(const Dev& P, int c) { return P.f.art[c]; }
+  __device__ static float cc_hvc(const Dev& P, int c) { return P.f.cc_hvc[c]; }
+  __device__ static float a1u(const Dev& P, size_t q) { return P.f.a1u[q]; }
+  __device__ static float a2u(const Dev& P, size_t q) { return P.f.a2u[q]; }
+  __device__ static float dltxe(const Dev& P, size_t q) { return P.f.dltxe[q]; }
+  __device__ static float dltye(const Dev& P, size_t q) { return P.f.dltye[q]; }
+  __device__ static float dltxncve(const Dev& P, size_t q) { return P.f.dltxncve[q]; }
+  __device__ static float dltyncve(const Dev& P, size_t q) { return P.f.dltyncve[q]; }
+  __device__ static float* g2d(const Dev& P, int q) { return P.f.g2d[q]; }
+  __device__ static float* g3(const Dev& P, int q) { return P.f.g3[q]; }
+  __device__ static float* const* gq(const Dev& P, int t) { return P.f.gq[t]; }
+  __device__ static float* const* gt(const Dev& P, int t) { return P.f.gt[t]; }
+  __device__ static float2* ex2(const Dev& P) { return P.f.ex2; }
+};
+__device__ inline double2 mk2(double a, double b) { return make_double2(a, b); }
+__device__ inline float2 mk2(float a, float b) { return make_float2(a, b); }
+
 // Fortran SIGN(1.0, x) for a processor that does not distinguish negative zero.
 __host__ __device__ inline double fsign1(double x) { return x >= 0.0 ? 1.0 : -1.0; }
+__host__ __device__ inline float fsign1(float x) { return x >= 0.0f ? 1.0f : -1.0f; }
 
 extern const double kAlphaRK[5];
 
@@ -153,6 +221,7 @@ void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts);
 void launch_ext_update(const Dev& P, cudaStream_t s, int K);
 void launch_begin_step(const Dev& P, cudaStream_t s);
 void launch_ext_prep(const Dev& P, cudaStream_t s);
+void launch_make_f32(const Dev& P, cudaStream_t s);
 void launch_set_qdis(const Dev& P, cudaStream_t s);
 
 // ---------------- 3-D momentum (k_mom3d.cu) ----------------

@@ -22,38 +22,48 @@ __device__ inline const double* sched_row(const Dev& P) {
 // Least-squares velocity gradient of one cell from itself and its three neighbours
 // (advave_edge_gcn.F:634-637, 699-702): COFA1/COFA2 for UA, COFA5/COFA6 for VA.
 // -------------------------------------------------------------------------------------
+template <typename R>
 struct Grad {
-  double ux, uy, vx, vy;
+  R ux, uy, vx, vy;
 };
 
-__device__ inline Grad cell_grad(const Dev& P, int c, const double* U, const double* V) {
+template <typename R>
+__device__ inline Grad<R> cell_grad(const Dev& P, int c, const double* U, const double* V) {
+  typedef Mesh<R> Mh;
   const size_t n1 = P.N + 1;
   int k1 = P.nbe[c], k2 = P.nbe[n1 + c], k3 = P.nbe[2 * n1 + c];
-  double a1 = P.a1u[c], a2 = P.a1u[n1 + c], a3 = P.a1u[2 * n1 + c], a4 = P.a1u[3 * n1 + c];
-  double b1 = P.a2u[c], b2 = P.a2u[n1 + c], b3 = P.a2u[2 * n1 + c], b4 = P.a2u[3 * n1 + c];
-  double u0 = U[c], u1 = U[k1], u2 = U[k2], u3 = U[k3];
-  double v0 = V[c], v1 = V[k1], v2 = V[k2], v3 = V[k3];
-  Grad g;
+  R a1 = Mh::a1u(P, c), a2 = Mh::a1u(P, n1 + c), a3 = Mh::a1u(P, 2 * n1 + c), a4 = Mh::a1u(P, 3 * n1 + c);
+  R b1 = Mh::a2u(P, c), b2 = Mh::a2u(P, n1 + c), b3 = Mh::a2u(P, 2 * n1 + c), b4 = Mh::a2u(P, 3 * n1 + c);
+  R u0 = (R)U[c], u1 = (R)U[k1], u2 = (R)U[k2], u3 = (R)U[k3];
+  R v0 = (R)V[c], v1 = (R)V[k1], v2 = (R)V[k2], v3 = (R)V[k3];
+  Grad<R> g;
   g.ux = a1 * u0 + a2 * u1 + a3 * u2 + a4 * u3;
   g.uy = b1 * u0 + b2 * u1 + b3 * u2 + b4 * u3;
   g.vx = a1 * v0 + a2 * v1 + a3 * v2 + a4 * v3;
   g.vy = b1 * v0 + b2 * v1 + b3 * v2 + b4 * v3;
   return g;
 }
-
-__device__ inline void store_grad(const Dev& P, int c) {
-  Grad g = cell_grad(P, c, P.ua, P.va);
-  P.g2d[0][c] = g.ux;
-  P.g2d[1][c] = g.uy;
-  P.g2d[2][c] = g.vx;
-  P.g2d[3][c] = g.vy;
+// Least-squares gradient of UA, VA of cell c (advave_edge_gcn.F:634-637, 699-702), stored
+// for the edge loop of the next ADVAVE call in the handle's precision.
+template <typename R>
+__device__ inline void store_grad_t(const Dev& P, int c) {
+  Grad<R> g = cell_grad<R>(P, c, P.ua, P.va);
+  Mesh<R>::g2d(P, 0)[c] = g.ux;
+  Mesh<R>::g2d(P, 1)[c] = g.uy;
+  Mesh<R>::g2d(P, 2)[c] = g.vx;
+  Mesh<R>::g2d(P, 3)[c] = g.vy;
 }
-__device__ inline Grad load_grad(const Dev& P, int c) {
-  Grad g;
-  g.ux = P.g2d[0][c];
-  g.uy = P.g2d[1][c];
-  g.vx = P.g2d[2][c];
-  g.vy = P.g2d[3][c];
+__device__ inline void store_grad(const Dev& P, int c) {
+  if (P.prec) store_grad_t<float>(P, c);
+  else store_grad_t<double>(P, c);
+}
+template <typename R>
+__device__ inline Grad<R> load_grad(const Dev& P, int c) {
+  Grad<R> g;
+  g.ux = Mesh<R>::g2d(P, 0)[c];
+  g.uy = Mesh<R>::g2d(P, 1)[c];
+  g.vx = Mesh<R>::g2d(P, 2)[c];
+  g.vy = Mesh<R>::g2d(P, 3)[c];
   return g;
 }
 // EXTEL_EDGE half-edge flux EXFLUX = DIJ*(-UIJ*DLTYE+VIJ*DLTXE) (extel_edge.F:86-94) of the
@@ -153,51 +163,58 @@ __global__ void k_wet_nodes(const Dev P) {
   P.elf[i] = fmax(e, -P.h[i] + P.min_depth);
 }
 
-// ADVAVE_EDGE_GCN for one cell (advave_edge_gcn.F:115-1003, LIMITED_NO branch).
-__device__ inline void advave_cell(const Dev& P, int i, double& xf, double& yf, double& px, double& py) {
-  xf = 0.0; yf = 0.0; px = 0.0; py = 0.0;
+// ADVAVE_EDGE_GCN for one cell (advave_edge_gcn.F:115-1003, LIMITED_NO branch).  The
+// edge fluxes are evaluated in R; the surface-slope pressure gradient PSTX/PSTY stays FP64.
+template <typename R>
+__device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo, double& px, double& py) {
+  typedef Mesh<R> Mh;
+  const R half = (R)0.5, one = (R)1.0;
+  R xf = 0, yf = 0;
+  px = 0.0; py = 0.0;
   const size_t e1 = P.NE + 1;
+  const R epor = (R)P.epor[i], iucp = (R)P.iucp[i];
   for (int s = 0; s < 3; ++s) {
     int code = P.cell_edge[3 * i + s];
     int e = code >> 1;
     int side = code & 1;
     int ia = P.iec[e], ib = P.iec[e1 + e];
     int j1 = P.ienode[e], j2 = P.ienode[e1 + e];
-    double dij = 0.5 * (P.d[j1] + P.d[j2]);
+    R dij = (R)(0.5 * (P.d[j1] + P.d[j2]));
     double elij = 0.5 * (P.el[j1] + P.el[j2]);
     if (P.iswetce[ia] * P.iswetc[ia] == 1 || P.iswetce[ib] * P.iswetc[ib] == 1) {
-      Grad ga = load_grad(P, ia);
-      double xij = P.xijc[e] - P.xc[ia];
-      double yij = P.yijc[e] - P.yc[ia];
-      double uij1 = P.ua[ia] + ga.ux * xij + ga.uy * yij;
-      double vij1 = P.va[ia] + ga.vx * xij + ga.vy * yij;
-      Grad gb = load_grad(P, ib);
-      xij = P.xijc[e] - P.xc[ib];
-      yij = P.yijc[e] - P.yc[ib];
-      double uij2 = P.ua[ib] + gb.ux * xij + gb.uy * yij;
-      double vij2 = P.va[ib] + gb.vx * xij + gb.vy * yij;
-      double uij = 0.5 * (uij1 + uij2);
-      double vij = 0.5 * (vij1 + vij2);
-      double un = -uij * P.dltyc[e] + vij * P.dltxc[e];
-      double viscof1 = P.art[ia] * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + 0.5 * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
-      double viscof2 = P.art[ib] * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + 0.5 * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
-      double viscof = (P.fact * 0.5 * (viscof1 * P.cc_hvc[ia] + viscof2 * P.cc_hvc[ib]) +
-                       P.fm1 * 0.5 * (P.cc_hvc[ia] + P.cc_hvc[ib])) / P.hprnu;
-      double txx = (ga.ux + gb.ux) * viscof;
-      double tyy = (ga.vy + gb.vy) * viscof;
-      double txy = 0.5 * (ga.uy + gb.uy + ga.vx + gb.vx) * viscof;
-      double fxx = dij * (txx * P.dltyc[e] - txy * P.dltxc[e]);
-      double fyy = dij * (txy * P.dltyc[e] - tyy * P.dltxc[e]);
-      double sg = fsign1(un);
-      double xadv = dij * un * ((1.0 - sg) * uij2 + (1.0 + sg) * uij1) * 0.5;
-      double yadv = dij * un * ((1.0 - sg) * vij2 + (1.0 + sg) * vij1) * 0.5;
-      double nb = 1.0 - (double)P.isbc[e];
+      Grad<R> ga = load_grad<R>(P, ia);
+      R xij = Mh::xoa(P, e, ia);
+      R yij = Mh::yoa(P, e, ia);
+      R uij1 = (R)P.ua[ia] + ga.ux * xij + ga.uy * yij;
+      R vij1 = (R)P.va[ia] + ga.vx * xij + ga.vy * yij;
+      Grad<R> gb = load_grad<R>(P, ib);
+      xij = Mh::xob(P, e, ib);
+      yij = Mh::yob(P, e, ib);
+      R uij2 = (R)P.ua[ib] + gb.ux * xij + gb.uy * yij;
+      R vij2 = (R)P.va[ib] + gb.vx * xij + gb.vy * yij;
+      R uij = half * (uij1 + uij2);
+      R vij = half * (vij1 + vij2);
+      const R dltxc = Mh::dltxc(P, e), dltyc = Mh::dltyc(P, e);
+      R un = -uij * dltyc + vij * dltxc;
+      R viscof1 = Mh::art(P, ia) * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + half * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
+      R viscof2 = Mh::art(P, ib) * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + half * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
+      const R cca = Mh::cc_hvc(P, ia), ccb = Mh::cc_hvc(P, ib);
+      R viscof = ((R)P.fact * half * (viscof1 * cca + viscof2 * ccb) + (R)P.fm1 * half * (cca + ccb)) / (R)P.hprnu;
+      R txx = (ga.ux + gb.ux) * viscof;
+      R tyy = (ga.vy + gb.vy) * viscof;
+      R txy = half * (ga.uy + gb.uy + ga.vx + gb.vx) * viscof;
+      R fxx = dij * (txx * dltyc - txy * dltxc);
+      R fyy = dij * (txy * dltyc - tyy * dltxc);
+      R sg = fsign1(un);
+      R xadv = dij * un * ((one - sg) * uij2 + (one + sg) * uij1) * half;
+      R yadv = dij * un * ((one - sg) * vij2 + (one + sg) * vij1) * half;
+      R nb = one - (R)P.isbc[e];
       if (side == 0) {
-        xf = xf + (xadv + fxx * P.epor[i]) * nb * P.iucp[i];
-        yf = yf + (yadv + fyy * P.epor[i]) * nb * P.iucp[i];
+        xf = xf + (xadv + fxx * epor) * nb * iucp;
+        yf = yf + (yadv + fyy * epor) * nb * iucp;
       } else {
-        xf = xf - (xadv + fxx * P.epor[i]) * nb * P.iucp[i];
-        yf = yf - (yadv + fyy * P.epor[i]) * nb * P.iucp[i];
+        xf = xf - (xadv + fxx * epor) * nb * iucp;
+        yf = yf - (yadv + fyy * epor) * nb * iucp;
       }
     }
     if (side == 0) {
@@ -208,9 +225,9 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xf, double& yf, 
       py = py - P.grav_e[i] * P.d1[i] * elij * P.dltxc[e];
     }
   }
-  double w = (double)(P.iswetce[i] * P.iswetc[i]);
-  xf = xf * w;
-  yf = yf * w;
+  R w = (R)(P.iswetce[i] * P.iswetc[i]);
+  xfo = (double)(xf * w);
+  yfo = (double)(yf * w);
 }
 
 // FLUX_OBN (mod_obcs.F:1181-1215) value on one open-boundary cell.
@@ -248,6 +265,7 @@ __device__ inline void bc_solid(const Dev& P, int i, int rj, double& uu, double&
 // Per-cell part of one RK stage.  EC_INT_ADVAVE is the internal-step call of ADVAVE
 // followed by ADX2D -= ADVUA (internal_step.F:387-392).
 // -------------------------------------------------------------------------------------
+template <typename R>
 __global__ void k_ext_cell(const Dev P, int iext, int K, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
@@ -268,7 +286,7 @@ __global__ void k_ext_cell(const Dev P, int iext, int K, int parts) {
   }
   double xf, yf, px, py;
   if (parts & (EC_ADVAVE | EC_INT_ADVAVE)) {
-    advave_cell(P, i, xf, yf, px, py);
+    advave_cell<R>(P, i, xf, yf, px, py);
     if (P.isbce[i] == 2) {
       xf = (xf + fob * P.ua[i]) * P.iucp[i];
       yf = (yf + fob * P.va[i]) * P.iucp[i];
@@ -399,12 +417,53 @@ void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
   k_ext_node<<<nblk(n, 256), 256, 0, s>>>(P, iext, K, parts);
 }
 void launch_ext_prep(const Dev& P, cudaStream_t s) { k_ext_prep<<<nblk(P.N, 256), 256, 0, s>>>(P); }
+
+// FP32 copies of the mesh metrics the precision form's flux kernels read.
+__global__ void k_d2f(const double* __restrict__ src, float* __restrict__ dst, size_t n) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    dst[q] = (float)src[q];
+}
+__global__ void k_edge_offsets_f32(const Dev P) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e > P.NE) return;
+  const size_t e1 = P.NE + 1;
+  float xa = 0.f, ya = 0.f, xb = 0.f, yb = 0.f;
+  if (e >= 1) {
+    int ia = P.iec[e], ib = P.iec[e1 + e];
+    xa = (float)(P.xijc[e] - P.xc[ia]);
+    ya = (float)(P.yijc[e] - P.yc[ia]);
+    xb = (float)(P.xijc[e] - P.xc[ib]);
+    yb = (float)(P.yijc[e] - P.yc[ib]);
+  }
+  P.f.xo[e] = xa;
+  P.f.yo[e] = ya;
+  P.f.xo[e1 + e] = xb;
+  P.f.yo[e1 + e] = yb;
+}
+void launch_make_f32(const Dev& P, cudaStream_t s) {
+  auto cvt = [&](const double* a, float* b, size_t n) { k_d2f<<<296, 256, 0, s>>>(a, b, n); };
+  const size_t n1 = P.N + 1, e1 = P.NE + 1, v1 = P.NCV + 1, vi1 = P.NCV_I + 1;
+  k_edge_offsets_f32<<<nblk(P.NE + 1, 256), 256, 0, s>>>(P);
+  cvt(P.dltxc, P.f.dltxc, e1);
+  cvt(P.dltyc, P.f.dltyc, e1);
+  cvt(P.art, P.f.art, n1);
+  cvt(P.cc_hvc, P.f.cc_hvc, n1);
+  cvt(P.a1u, P.f.a1u, 4 * n1);
+  cvt(P.a2u, P.f.a2u, 4 * n1);
+  cvt(P.dltxe, P.f.dltxe, v1);
+  cvt(P.dltye, P.f.dltye, v1);
+  cvt(P.dltxncve, P.f.dltxncve, 2 * vi1);
+  cvt(P.dltyncve, P.f.dltyncve, 2 * vi1);
+}
 void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);
   k_wet_nodes<<<nblk(P.M, 256), 256, 0, s>>>(P);
 }
 void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
-  k_ext_cell<<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
+  if (P.prec)
+    k_ext_cell<float><<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
+  else
+    k_ext_cell<double><<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
 }
 void launch_ext_update(const Dev& P, cudaStream_t s, int K) {
   int n = P.M > P.N ? P.M : P.N;

@@ -96,17 +96,20 @@ __global__ void k_cell_pre(const Dev P, int parts) {
 }
 
 // Least-squares gradient of U,V on layer k (advection_edge_gcn.F:533-536).
+template <typename R>
 struct G3 {
-  double ux, uy, vx, vy;
+  R ux, uy, vx, vy;
 };
-__device__ inline G3 grad3(const Dev& P, int c, const double* U, const double* V) {
+template <typename R>
+__device__ inline G3<R> grad3(const Dev& P, int c, const double* U, const double* V) {
+  typedef Mesh<R> Mh;
   const size_t n1 = P.N + 1;
   int k1 = P.nbe[c], k2 = P.nbe[n1 + c], k3 = P.nbe[2 * n1 + c];
-  double a1 = P.a1u[c], a2 = P.a1u[n1 + c], a3 = P.a1u[2 * n1 + c], a4 = P.a1u[3 * n1 + c];
-  double b1 = P.a2u[c], b2 = P.a2u[n1 + c], b3 = P.a2u[2 * n1 + c], b4 = P.a2u[3 * n1 + c];
-  double u0 = U[c], u1 = U[k1], u2 = U[k2], u3 = U[k3];
-  double v0 = V[c], v1 = V[k1], v2 = V[k2], v3 = V[k3];
-  G3 g;
+  R a1 = Mh::a1u(P, c), a2 = Mh::a1u(P, n1 + c), a3 = Mh::a1u(P, 2 * n1 + c), a4 = Mh::a1u(P, 3 * n1 + c);
+  R b1 = Mh::a2u(P, c), b2 = Mh::a2u(P, n1 + c), b3 = Mh::a2u(P, 2 * n1 + c), b4 = Mh::a2u(P, 3 * n1 + c);
+  R u0 = (R)U[c], u1 = (R)U[k1], u2 = (R)U[k2], u3 = (R)U[k3];
+  R v0 = (R)V[c], v1 = (R)V[k1], v2 = (R)V[k2], v3 = (R)V[k3];
+  G3<R> g;
   g.ux = a1 * u0 + a2 * u1 + a3 * u2 + a4 * u3;
   g.uy = b1 * u0 + b2 * u1 + b3 * u2 + b4 * u3;
   g.vx = a1 * v0 + a2 * v1 + a3 * v2 + a4 * v3;
@@ -115,75 +118,81 @@ __device__ inline G3 grad3(const Dev& P, int c, const double* U, const double* V
 }
 
 // Horizontal flux of one edge on one layer (advection_edge_gcn.F:449-603 and
-// adv_uv_edge_gcn.F:580-779 share this body).  Returns whether the edge is active
-// (at least one wet side) and its upwind/viscous pieces.
+// adv_uv_edge_gcn.F:580-779 share this body), evaluated in R.
+template <typename R>
 struct EdgeFlux {
-  double xadv, yadv, fxx, fyy, viscof;
+  R xadv, yadv, fxx, fyy, viscof;
 };
 
-__device__ inline G3 load_g3(const Dev& P, int c, int k) {
+template <typename R>
+__device__ inline G3<R> load_g3(const Dev& P, int c, int k) {
   size_t q = C3(P, c, k);
-  G3 g;
-  g.ux = P.g3[0][q];
-  g.uy = P.g3[1][q];
-  g.vx = P.g3[2][q];
-  g.vy = P.g3[3][q];
+  G3<R> g;
+  g.ux = Mesh<R>::g3(P, 0)[q];
+  g.uy = Mesh<R>::g3(P, 1)[q];
+  g.vx = Mesh<R>::g3(P, 2)[q];
+  g.vy = Mesh<R>::g3(P, 3)[q];
   return g;
 }
 
 // Least-squares gradient of U, V of every cell and layer (the COFA1..COFA8 inputs of
 // advection_edge_gcn.F:533-548 and adv_uv_edge_gcn.F:704-719), evaluated once per cell.
+template <typename R>
 __global__ void __launch_bounds__(256) k_grad3(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
   int kb, ke;
   col_range(P, 1, P.KBM1, kb, ke);
   for (int k = kb; k <= ke; ++k) {
-  G3 g = grad3(P, i, P.u + C3(P, 0, k), P.v + C3(P, 0, k));
-  size_t q = C3(P, i, k);
-  P.g3[0][q] = g.ux;
-  P.g3[1][q] = g.uy;
-  P.g3[2][q] = g.vx;
-  P.g3[3][q] = g.vy;
+    G3<R> g = grad3<R>(P, i, P.u + C3(P, 0, k), P.v + C3(P, 0, k));
+    size_t q = C3(P, i, k);
+    Mesh<R>::g3(P, 0)[q] = g.ux;
+    Mesh<R>::g3(P, 1)[q] = g.uy;
+    Mesh<R>::g3(P, 2)[q] = g.vx;
+    Mesh<R>::g3(P, 3)[q] = g.vy;
   }
 }
 
-__device__ inline EdgeFlux edge_flux3(const Dev& P, int e, int ia, int ib, int k, double dij, bool exflux_form) {
+template <typename R>
+__device__ inline EdgeFlux<R> edge_flux3(const Dev& P, int e, int ia, int ib, int k, R dij, bool exflux_form) {
+  typedef Mesh<R> Mh;
+  const R half = (R)0.5, one = (R)1.0;
   const double* U = P.u + C3(P, 0, k);
   const double* V = P.v + C3(P, 0, k);
-  double xija = P.xijc[e] - P.xc[ia], yija = P.yijc[e] - P.yc[ia];
-  double xijb = P.xijc[e] - P.xc[ib], yijb = P.yijc[e] - P.yc[ib];
-  G3 ga = load_g3(P, ia, k);
-  double uij1 = U[ia] + ga.ux * xija + ga.uy * yija;
-  double vij1 = V[ia] + ga.vx * xija + ga.vy * yija;
-  G3 gb = load_g3(P, ib, k);
-  double uij2 = U[ib] + gb.ux * xijb + gb.uy * yijb;
-  double vij2 = V[ib] + gb.vx * xijb + gb.vy * yijb;
-  double uij = 0.5 * (uij1 + uij2);
-  double vij = 0.5 * (vij1 + vij2);
-  double viscof1 = P.art[ia] * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + 0.5 * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
-  double viscof2 = P.art[ib] * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + 0.5 * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
-  double viscof = (P.fact * 0.5 * (viscof1 * P.cc_hvc[ia] + viscof2 * P.cc_hvc[ib]) +
-                   P.fm1 * 0.5 * (P.cc_hvc[ia] + P.cc_hvc[ib])) / P.hprnu;
-  double txx = (ga.ux + gb.ux) * viscof;
-  double tyy = (ga.vy + gb.vy) * viscof;
-  double txy = 0.5 * (ga.uy + gb.uy + ga.vx + gb.vx) * viscof;
-  EdgeFlux f;
-  f.fxx = dij * (txx * P.dltyc[e] - txy * P.dltxc[e]);
-  f.fyy = dij * (txy * P.dltyc[e] - tyy * P.dltxc[e]);
+  R xija = Mh::xoa(P, e, ia), yija = Mh::yoa(P, e, ia);
+  R xijb = Mh::xob(P, e, ib), yijb = Mh::yob(P, e, ib);
+  G3<R> ga = load_g3<R>(P, ia, k);
+  R uij1 = (R)U[ia] + ga.ux * xija + ga.uy * yija;
+  R vij1 = (R)V[ia] + ga.vx * xija + ga.vy * yija;
+  G3<R> gb = load_g3<R>(P, ib, k);
+  R uij2 = (R)U[ib] + gb.ux * xijb + gb.uy * yijb;
+  R vij2 = (R)V[ib] + gb.vx * xijb + gb.vy * yijb;
+  R uij = half * (uij1 + uij2);
+  R vij = half * (vij1 + vij2);
+  R viscof1 = Mh::art(P, ia) * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + half * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
+  R viscof2 = Mh::art(P, ib) * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + half * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
+  const R cca = Mh::cc_hvc(P, ia), ccb = Mh::cc_hvc(P, ib);
+  R viscof = ((R)P.fact * half * (viscof1 * cca + viscof2 * ccb) + (R)P.fm1 * half * (cca + ccb)) / (R)P.hprnu;
+  R txx = (ga.ux + gb.ux) * viscof;
+  R tyy = (ga.vy + gb.vy) * viscof;
+  R txy = half * (ga.uy + gb.uy + ga.vx + gb.vx) * viscof;
+  const R dltxc = Mh::dltxc(P, e), dltyc = Mh::dltyc(P, e);
+  EdgeFlux<R> f;
+  f.fxx = dij * (txx * dltyc - txy * dltxc);
+  f.fyy = dij * (txy * dltyc - tyy * dltxc);
   f.viscof = viscof;
   if (exflux_form) {
     // adv_uv_edge_gcn.F:730, 752-753
-    double exflux = dij * (-uij * P.dltyc[e] + vij * P.dltxc[e]);
-    double sg = fsign1(exflux);
-    f.xadv = exflux * ((1.0 - sg) * uij2 + (1.0 + sg) * uij1) * 0.5;
-    f.yadv = exflux * ((1.0 - sg) * vij2 + (1.0 + sg) * vij1) * 0.5;
+    R exflux = dij * (-uij * dltyc + vij * dltxc);
+    R sg = fsign1(exflux);
+    f.xadv = exflux * ((one - sg) * uij2 + (one + sg) * uij1) * half;
+    f.yadv = exflux * ((one - sg) * vij2 + (one + sg) * vij1) * half;
   } else {
     // advection_edge_gcn.F:559, 576-577
-    double un = vij * P.dltxc[e] - uij * P.dltyc[e];
-    double sg = fsign1(un);
-    f.xadv = dij * un * ((1.0 - sg) * uij2 + (1.0 + sg) * uij1) * 0.5;
-    f.yadv = dij * un * ((1.0 - sg) * vij2 + (1.0 + sg) * vij1) * 0.5;
+    R un = vij * dltxc - uij * dltyc;
+    R sg = fsign1(un);
+    f.xadv = dij * un * ((one - sg) * uij2 + (one + sg) * uij1) * half;
+    f.yadv = dij * un * ((one - sg) * vij2 + (one + sg) * vij1) * half;
   }
   return f;
 }
@@ -211,6 +220,7 @@ __device__ inline void river3(const Dev& P, int i, int k, double& x, double& y) 
 // ADVECTION_EDGE_GCN (advection_edge_gcn.F:397-708): per cell and layer, the cell's three
 // edges in ascending edge number.
 // -------------------------------------------------------------------------------------
+template <typename R>
 __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
@@ -218,25 +228,27 @@ __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
   col_range(P, 1, P.KBM1, kb, ke);
   for (int k = kb; k <= ke; ++k) {
   const size_t e1 = P.NE + 1;
-  double x = 0.0, y = 0.0;
+  const R epor = (R)P.epor[i], three = (R)3.0;
+  R xr = 0, yr = 0;
   for (int s = 0; s < 3; ++s) {
     int code = P.cell_edge[3 * i + s];
     int e = code >> 1, side = code & 1;
     int ia = P.iec[e], ib = P.iec[e1 + e];
     if (!(P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1)) continue;
     int j1 = P.ienode[e], j2 = P.ienode[e1 + e];
-    double dij = 0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]);
-    EdgeFlux f = edge_flux3(P, e, ia, ib, k, dij, false);
-    double isb = (double)P.isbc[e];
-    double tp = (double)(float)(1 - P.isbc[e]) * P.epor[i];
+    R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
+    EdgeFlux<R> f = edge_flux3<R>(P, e, ia, ib, k, dij, false);
+    R isb = (R)P.isbc[e];
+    R tp = (R)((double)(float)(1 - P.isbc[e]) * P.epor[i]);
     if (side == 0) {
-      x = x + f.xadv * tp + (f.fxx + 3.0 * f.fxx * isb) * P.epor[i];
-      y = y + f.yadv * tp + (f.fyy + 3.0 * f.fyy * isb) * P.epor[i];
+      xr = xr + f.xadv * tp + (f.fxx + three * f.fxx * isb) * epor;
+      yr = yr + f.yadv * tp + (f.fyy + three * f.fyy * isb) * epor;
     } else {
-      x = x - f.xadv * tp - (f.fxx + 3.0 * f.fxx * isb) * P.epor[i];
-      y = y - f.yadv * tp - (f.fyy + 3.0 * f.fyy * isb) * P.epor[i];
+      xr = xr - f.xadv * tp - (f.fxx + three * f.fxx * isb) * epor;
+      yr = yr - f.yadv * tp - (f.fyy + three * f.fyy * isb) * epor;
     }
   }
+  double x = (double)xr, y = (double)yr;
   double w = (double)(P.iswetct[i] * P.iswetc[i]);
   x = x * w;
   y = y * w;
@@ -366,11 +378,12 @@ __global__ void k_adjust2(const Dev P) {
 // node's half-edges in ascending order.  Result in the scratch field.
 // -------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_vertvl_flux(const Dev P) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (i > P.M) return;
-  int kb, ke;
-  col_range(P, 1, P.KBM1, kb, ke);
-  for (int k = kb; k <= ke; ++k) {
+  // One thread per (node, layer): the half-edge chain of the 8 layer threads of a node
+  // resolves in parallel, which suits this short gather better than a layer loop.
+  int i = blockIdx.x * 32 + threadIdx.x + 1;
+  int k = blockIdx.y * 8 + threadIdx.y + 1;
+  if (i > P.M || k > P.KBM1) return;
+  {
   double x = 0.0;
   if (P.isonb[i] != 2) {
     for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
@@ -519,6 +532,7 @@ __global__ void __launch_bounds__(256) k_w_viscofh(const Dev P, int do_w, int do
 // internal barotropic pressure gradient from EGF, vertical advection, baroclinic
 // pressure gradient, Coriolis, river momentum and the explicit update to UF/VF.
 // -------------------------------------------------------------------------------------
+template <typename R>
 __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
@@ -526,7 +540,9 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
   col_range(P, 1, P.KBM1, kb, ke);
   for (int k = kb; k <= ke; ++k) {
   const size_t e1 = P.NE + 1;
-  double x = 0.0, y = 0.0, px = 0.0, py = 0.0, vm = 0.0;
+  double px = 0.0, py = 0.0;
+  const R epor = (R)P.epor[i], three = (R)3.0;
+  R xr = 0, yr = 0, vmr = 0;
   const double dz1i = P.dz1[C3(P, i, k)];
   const double gdd = P.grav_e[i] * P.dt1[i] * dz1i;
   for (int s = 0; s < 3; ++s) {
@@ -535,18 +551,18 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
     int ia = P.iec[e], ib = P.iec[e1 + e];
     int j1 = P.ienode[e], j2 = P.ienode[e1 + e];
     double elij = 0.5 * (P.egf[j1] + P.egf[j2]);
-    double dij = 0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]);
+    R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
     if (P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1) {
-      EdgeFlux f = edge_flux3(P, e, ia, ib, k, dij, true);
-      vm = vm + f.viscof;
-      double isb = (double)P.isbc[e];
-      double tp = (double)(float)(1 - P.isbc[e]) * P.epor[i];
+      EdgeFlux<R> f = edge_flux3<R>(P, e, ia, ib, k, dij, true);
+      vmr = vmr + f.viscof;
+      R isb = (R)P.isbc[e];
+      R tp = (R)((double)(float)(1 - P.isbc[e]) * P.epor[i]);
       if (side == 0) {
-        x = x + f.xadv * tp + (f.fxx + 3.0 * f.fxx * isb) * P.epor[i];
-        y = y + f.yadv * tp + (f.fyy + 3.0 * f.fyy * isb) * P.epor[i];
+        xr = xr + f.xadv * tp + (f.fxx + three * f.fxx * isb) * epor;
+        yr = yr + f.yadv * tp + (f.fyy + three * f.fyy * isb) * epor;
       } else {
-        x = x - f.xadv * tp - (f.fxx + 3.0 * f.fxx * isb) * P.epor[i];
-        y = y - f.yadv * tp - (f.fyy + 3.0 * f.fyy * isb) * P.epor[i];
+        xr = xr - f.xadv * tp - (f.fxx + three * f.fxx * isb) * epor;
+        yr = yr - f.yadv * tp - (f.fyy + three * f.fyy * isb) * epor;
       }
     }
     if (side == 0) {
@@ -557,6 +573,7 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
       py = py - gdd * elij * P.dltxc[e];
     }
   }
+  double x = (double)xr, y = (double)yr, vm = (double)vmr;
   bool wet = P.iswetct[i] * P.iswetc[i] == 1;
   double w = (double)(P.iswetct[i] * P.iswetc[i]);
   x = x * w;
@@ -720,10 +737,16 @@ void launch_cell_pre(const Dev& P, cudaStream_t s, int parts) {
   k_cell_pre<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);
 }
 void launch_grad3(const Dev& P, cudaStream_t s) {
-  k_grad3<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  if (P.prec)
+    k_grad3<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  else
+    k_grad3<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_advection3d(const Dev& P, cudaStream_t s) {
-  k_advection3d<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  if (P.prec)
+    k_advection3d<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  else
+    k_advection3d<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_baropg(const Dev& P, cudaStream_t s, int do_baropg, int do_sums) {
   k_baropg<<<nblk(P.N, 128), 128, 0, s>>>(P, do_baropg, do_sums);
@@ -734,7 +757,7 @@ void launch_int_reset(const Dev& P, cudaStream_t s) {
 }
 void launch_adjust2(const Dev& P, cudaStream_t s) { k_adjust2<<<nblk(P.N + 1, 128), 128, 0, s>>>(P); }
 void launch_vertvl_flux(const Dev& P, cudaStream_t s) {
-  k_vertvl_flux<<<col_grid(P, P.M, P.KBM1), P.col_bc, 0, s>>>(P);
+  k_vertvl_flux<<<dim3(nblk(P.M, 32), nblk(P.KBM1, 8)), dim3(32, 8), 0, s>>>(P);
 }
 void launch_vertvl_col(const Dev& P, cudaStream_t s, int parts) {
   k_vertvl_col<<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
@@ -744,7 +767,10 @@ void launch_w_viscofh(const Dev& P, cudaStream_t s, int do_w, int do_visc) {
   k_w_viscofh<<<col_grid(P, n, P.KB), P.col_bc, 0, s>>>(P, do_w, do_visc);
 }
 void launch_adv_uv(const Dev& P, cudaStream_t s) {
-  k_adv_uv<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  if (P.prec)
+    k_adv_uv<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  else
+    k_adv_uv<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_vdif_uv(const Dev& P, cudaStream_t s, int parts) {
   k_vdif_uv<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);

@@ -30,49 +30,51 @@ __device__ inline double TRIEY(const Dev& P, int i, int j) { return P.dltytrie[(
 // which == 1: T1 and S1 on K=1..KBM1 with the wet/dry substitution of adv_t.F:214-376,
 // plus PFPXB/PFPYB and AH_BOTTOM at K=KBM1 (adv_t.F:394-408).
 // -------------------------------------------------------------------------------------
+template <typename R>
 __global__ void __launch_bounds__(256) k_grad(const Dev P, int which) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.M) return;
   int kb, ke;
   col_range(P, which == 0 ? 2 : 1, P.KBM1, kb, ke);
   const int nt = P.ntsn[i];
-  const double art2 = P.art2[i];
+  const R art2 = (R)P.art2[i];
+  const R half = (R)0.5;
   for (int k = kb; k <= ke; ++k) {
     for (int t = 0; t < 2; ++t) {
       const double* Q;
       const double* QM = nullptr;
-      double* const* G;
+      R* const* G;
       if (which == 0) {
         Q = (t == 0 ? P.q2 : P.q2l) + N3(P, 0, k);
-        G = P.gq[t];
+        G = Mesh<R>::gq(P, t);
       } else {
         Q = (t == 0 ? P.t1 : P.s1) + N3(P, 0, k);
         QM = (t == 0 ? P.tmean1 : P.smean1) + N3(P, 0, k);
-        G = P.gt[t];
+        G = Mesh<R>::gt(P, t);
       }
-      const double qmean = F4(1.e-8);
-      double px = 0.0, py = 0.0, pxd = 0.0, pyd = 0.0;
-      double rmin = Q[NBSN(P, i, 1)], rmax = rmin;
+      const R qmean = (R)F4(1.e-8);
+      R px = 0, py = 0, pxd = 0, pyd = 0;
+      R rmin = (R)Q[NBSN(P, i, 1)], rmax = rmin;
       for (int j = 1; j <= nt - 1; ++j) {
         int i1 = NBSN(P, i, j), i2 = NBSN(P, i, j + 1);
         if (j >= 2) {
-          rmin = fmin(rmin, Q[i1]);
-          rmax = fmax(rmax, Q[i1]);
+          rmin = fmin(rmin, (R)Q[i1]);
+          rmax = fmax(rmax, (R)Q[i1]);
         }
-        double ffd, ff1;
+        R ffd, ff1;
         if (which == 0) {
-          ffd = 0.5 * (Q[i1] + Q[i2] - qmean - qmean);
-          ff1 = 0.5 * (Q[i1] + Q[i2]);
+          ffd = half * ((R)Q[i1] + (R)Q[i2] - qmean - qmean);
+          ff1 = half * ((R)Q[i1] + (R)Q[i2]);
         } else {
           int w1 = P.iswetn[i1], w2 = P.iswetn[i2];
           int a = i1, b = i2;
           if (w1 == 0 && w2 == 1) { a = i; b = i2; }
           else if (w1 == 1 && w2 == 0) { a = i1; b = i; }
           else if (w1 == 0 && w2 == 0) { a = i; b = i; }
-          ffd = 0.5 * (Q[a] + Q[b] - QM[a] - QM[b]);
-          ff1 = 0.5 * (Q[a] + Q[b]);
+          ffd = half * ((R)Q[a] + (R)Q[b] - (R)QM[a] - (R)QM[b]);
+          ff1 = half * ((R)Q[a] + (R)Q[b]);
         }
-        double ty = TRIEY(P, i, j), tx = TRIEX(P, i, j);
+        R ty = (R)TRIEY(P, i, j), tx = (R)TRIEX(P, i, j);
         px = px + ff1 * ty;
         py = py + ff1 * tx;
         pxd = pxd + ffd * ty;
@@ -90,8 +92,8 @@ __global__ void __launch_bounds__(256) k_grad(const Dev P, int which) {
       G[4][q] = rmin;
       G[5][q] = rmax;
       if (which == 1 && k == P.KBM1) {
-        if (t == 0) { P.pfpxb_t[i] = px; P.pfpyb_t[i] = py; }
-        else { P.pfpxb_s[i] = px; P.pfpyb_s[i] = py; }
+        if (t == 0) { P.pfpxb_t[i] = (double)px; P.pfpyb_t[i] = (double)py; }
+        else { P.pfpxb_s[i] = (double)px; P.pfpyb_s[i] = (double)py; }
         double ah = (P.fact * P.viscofh[N3(P, i, P.KBM1)] + P.fm1) * P.nn_hvc[i];
         if (t == 0) P.ah_bottom_t[i] = ah;
         else P.ah_bottom_s[i] = ah;
@@ -157,25 +159,27 @@ __device__ inline void fct_level_bounds(const Dev& P, int i, int k, const double
 // and applies the vertical flux, the update and the FCT clamp.
 // MODE 0: Q2 and Q2L on interfaces K=2..KBM1; MODE 1: T and S on layers K=1..KBM1.
 // -------------------------------------------------------------------------------------
+template <typename R>
 struct HeCell {
-  double uq, vq, dtij;
+  R uq, vq, dtij;
   int nd[3];
-  double vf[3], nn[3];
+  R vf[3], nn[3];
 };
 
-template <int MODE>
-__device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell& hc) {
+// Cell data of the half-edge fluxes on layer k, formed in FP64 and rounded to R.
+template <typename R, int MODE>
+__device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell<R>& hc) {
   const size_t n1 = P.N + 1;
   size_t ck = C3(P, c, k);
   if (MODE == 0) {
     size_t ckm = C3(P, c, k - 1);
-    hc.uq = (P.u[ck] * P.dz1[ckm] + P.u[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]);
-    hc.vq = (P.v[ck] * P.dz1[ckm] + P.v[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]);
-    hc.dtij = P.dt1[c] * P.dzz1[ckm];
+    hc.uq = (R)((P.u[ck] * P.dz1[ckm] + P.u[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]));
+    hc.vq = (R)((P.v[ck] * P.dz1[ckm] + P.v[ckm] * P.dz1[ck]) / (P.dz1[ck] + P.dz1[ckm]));
+    hc.dtij = (R)(P.dt1[c] * P.dzz1[ckm]);
   } else {
-    hc.uq = P.u[ck];
-    hc.vq = P.v[ck];
-    hc.dtij = P.dt1[c] * P.dz1[ck];
+    hc.uq = (R)P.u[ck];
+    hc.vq = (R)P.v[ck];
+    hc.dtij = (R)(P.dt1[c] * P.dz1[ck]);
   }
   for (int j = 0; j < 3; ++j) {
     int n = P.nv[j * n1 + c];
@@ -183,63 +187,69 @@ __device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell& hc) {
     size_t q = N3(P, n, k);
     if (MODE == 0) {
       size_t qm = N3(P, n, k - 1);
-      hc.vf[j] = (P.viscofh[q] * P.dz[qm] + P.viscofh[qm] * P.dz[q]) / (P.dz[q] + P.dz[qm]);
+      hc.vf[j] = (R)((P.viscofh[q] * P.dz[qm] + P.viscofh[qm] * P.dz[q]) / (P.dz[q] + P.dz[qm]));
     } else {
-      hc.vf[j] = P.viscofh[q];
+      hc.vf[j] = (R)P.viscofh[q];
     }
-    hc.nn[j] = P.nn_hvc[n];
+    hc.nn[j] = (R)P.nn_hvc[n];
   }
 }
 
 // v[j] for a run-time slot j in 0..2, by selects, so v stays in registers.
-__device__ inline double sel3(const double* v, int j) { return j == 0 ? v[0] : (j == 1 ? v[1] : v[2]); }
+template <typename R>
+__device__ inline R sel3(const R* v, int j) { return j == 0 ? v[0] : (j == 1 ? v[1] : v[2]); }
 __device__ inline int sel3i(const int* v, int j) { return j == 0 ? v[0] : (j == 1 ? v[1] : v[2]); }
 
 // One tracer's node data on layer k: value, ring gradients, ring extrema.
+template <typename R>
 struct TRec {
-  double q, px, py, pxd, pyd, rmin, rmax;
+  R q, px, py, pxd, pyd, rmin, rmax;
 };
-template <int MODE>
-__device__ inline TRec load_trec(const Dev& P, int n, int k, int t) {
+template <typename R, int MODE>
+__device__ inline TRec<R> load_trec(const Dev& P, int n, int k, int t) {
   const double* Q = MODE == 0 ? (t == 0 ? P.q2 : P.q2l) : (t == 0 ? P.t1 : P.s1);
-  double* const* G = MODE == 0 ? P.gq[t] : P.gt[t];
+  R* const* G = MODE == 0 ? Mesh<R>::gq(P, t) : Mesh<R>::gt(P, t);
   const size_t q = N3(P, n, k);
-  return TRec{Q[q], G[0][q], G[1][q], G[2][q], G[3][q], G[4][q], G[5][q]};
+  return TRec<R>{(R)Q[q], G[0][q], G[1][q], G[2][q], G[3][q], G[4][q], G[5][q]};
 }
 
-// EXFLUX of half-edge he for tracer t; a and b are the positions of NIEC(he,1) and
-// NIEC(he,2) among the cell's nodes, ra and rb their records.  xadv receives
-// EXFLUX-FXX-FYY.
-template <int MODE>
-__device__ inline double he_flux(const Dev& P, const HeCell& hc, int he, int a, int b, const TRec& ra,
-                                 const TRec& rb, double* xadv) {
+// EXFLUX of half-edge he for tracer t, in R; a and b are the positions of NIEC(he,1) and
+// NIEC(he,2) among the cell's nodes, ra and rb their data.  xadv receives EXFLUX-FXX-FYY.
+template <typename R, int MODE>
+__device__ inline R he_flux(const Dev& P, const HeCell<R>& hc, int he, int a, int b, const TRec<R>& ra,
+                            const TRec<R>& rb, R* xadv) {
+  typedef Mesh<R> Mh;
+  const R half = (R)0.5, one = (R)1.0;
   const size_t vi1 = P.NCV_I + 1;
-  double un = hc.vq * P.dltxe[he] - hc.uq * P.dltye[he];
-  double fij1 = ra.q + P.dltxncve[he] * ra.px + P.dltyncve[he] * ra.py;
-  double fij2 = rb.q + P.dltxncve[vi1 + he] * rb.px + P.dltyncve[vi1 + he] * rb.py;
-  double q1min = fmin(ra.rmin, ra.q), q1max = fmax(ra.rmax, ra.q);
-  double q2min = fmin(rb.rmin, rb.q), q2max = fmax(rb.rmax, rb.q);
+  const R dltxe = Mh::dltxe(P, he), dltye = Mh::dltye(P, he);
+  R un = hc.vq * dltxe - hc.uq * dltye;
+  R fij1 = ra.q + Mh::dltxncve(P, he) * ra.px + Mh::dltyncve(P, he) * ra.py;
+  R fij2 = rb.q + Mh::dltxncve(P, vi1 + he) * rb.px + Mh::dltyncve(P, vi1 + he) * rb.py;
+  R q1min = fmin(ra.rmin, ra.q), q1max = fmax(ra.rmax, ra.q);
+  R q2min = fmin(rb.rmin, rb.q), q2max = fmax(rb.rmax, rb.q);
   if (fij1 < q1min) fij1 = q1min;
   if (fij1 > q1max) fij1 = q1max;
   if (fij2 < q2min) fij2 = q2min;
   if (fij2 > q2max) fij2 = q2max;
-  const double vfa = sel3(hc.vf, a), vfb = sel3(hc.vf, b), nna = sel3(hc.nn, a), nnb = sel3(hc.nn, b);
-  double viscof = P.fact * 0.5 * (vfa * nna + vfb * nnb) + P.fm1 * 0.5 * (nna + nnb);
-  if (MODE == 0) viscof = viscof / P.hprnu;
-  double txx = 0.5 * (ra.pxd + rb.pxd) * viscof;
-  double tyy = 0.5 * (ra.pyd + rb.pyd) * viscof;
-  double fxx = -hc.dtij * txx * P.dltye[he];
-  double fyy = hc.dtij * tyy * P.dltxe[he];
-  double sg = fsign1(un);
-  double exflux = -un * hc.dtij * ((1.0 + sg) * fij2 + (1.0 - sg) * fij1) * 0.5 + fxx + fyy;
+  const R vfa = sel3(hc.vf, a), vfb = sel3(hc.vf, b), nna = sel3(hc.nn, a), nnb = sel3(hc.nn, b);
+  R viscof = (R)P.fact * half * (vfa * nna + vfb * nnb) + (R)P.fm1 * half * (nna + nnb);
+  if (MODE == 0) viscof = viscof / (R)P.hprnu;
+  R txx = half * (ra.pxd + rb.pxd) * viscof;
+  R tyy = half * (ra.pyd + rb.pyd) * viscof;
+  R fxx = -hc.dtij * txx * dltye;
+  R fyy = hc.dtij * tyy * dltxe;
+  R sg = fsign1(un);
+  R exflux = -un * hc.dtij * ((one + sg) * fij2 + (one - sg) * fij1) * half + fxx + fyy;
   if (xadv) *xadv = exflux - fxx - fyy;
   return exflux;
 }
 
-__device__ inline int pos3(const HeCell& hc, int n) { return n == hc.nd[0] ? 0 : (n == hc.nd[1] ? 1 : 2); }
+template <typename R>
+__device__ inline int pos3(const HeCell<R>& hc, int n) { return n == hc.nd[0] ? 0 : (n == hc.nd[1] ? 1 : 2); }
 
-template <int MODE>
+template <typename R, int MODE>
 __global__ void __launch_bounds__(256) k_he_adv(const Dev P, int parts) {
+  typedef typename Mesh<R>::R2 R2;
   int c = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (c > P.N) return;
   int kb, ke;
@@ -258,46 +268,54 @@ __global__ void __launch_bounds__(256) k_he_adv(const Dev P, int parts) {
     }
   }
   for (int k = kb; k <= ke; ++k) {
-    HeCell hc;
-    he_cell_load<MODE>(P, c, k, hc);
-    double2* EX = P.ex2 + (size_t)(k - 1) * P.ncvs;
+    HeCell<R> hc;
+    he_cell_load<R, MODE>(P, c, k, hc);
+    R2* EX = Mesh<R>::ex2(P) + (size_t)(k - 1) * P.ncvs;
     for (int s = 0; s < 3; ++s) {
       const int na = sel3i(hc.nd, pa[s]), nb = sel3i(hc.nd, pb[s]);
-      double e0 = 0.0, e1 = 0.0;
-      if (do0) e0 = he_flux<MODE>(P, hc, hes[s], pa[s], pb[s], load_trec<MODE>(P, na, k, 0), load_trec<MODE>(P, nb, k, 0), nullptr);
-      if (do1) e1 = he_flux<MODE>(P, hc, hes[s], pa[s], pb[s], load_trec<MODE>(P, na, k, 1), load_trec<MODE>(P, nb, k, 1), nullptr);
-      EX[hes[s]] = make_double2(e0, e1);
+      R e0 = 0, e1 = 0;
+      if (do0)
+        e0 = he_flux<R, MODE>(P, hc, hes[s], pa[s], pb[s], load_trec<R, MODE>(P, na, k, 0),
+                              load_trec<R, MODE>(P, nb, k, 0), nullptr);
+      if (do1)
+        e1 = he_flux<R, MODE>(P, hc, hes[s], pa[s], pb[s], load_trec<R, MODE>(P, na, k, 1),
+                              load_trec<R, MODE>(P, nb, k, 1), nullptr);
+      EX[hes[s]] = mk2(e0, e1);
     }
   }
 }
 
 // XFLUX_ADV of one open-boundary node (adv_t.F:510-511, 572-579): the advective parts of
 // its half-edge fluxes, recomputed with the same arithmetic as phase 1.
+template <typename R>
 __device__ inline double obc_xflux_adv(const Dev& P, int i, int k, int t) {
   const size_t v1 = P.NCV + 1;
-  double xa = 0.0;
+  R xa = 0;
   for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
     int code = P.node_he[q];
     int he = code >> 1;
     int c = P.ntrg[he];
-    HeCell hc;
-    he_cell_load<1>(P, c, k, hc);
+    HeCell<R> hc;
+    he_cell_load<R, 1>(P, c, k, hc);
     const int na = P.niec[he], nb = P.niec[v1 + he];
-    double part;
-    he_flux<1>(P, hc, he, pos3(hc, na), pos3(hc, nb), load_trec<1>(P, na, k, t), load_trec<1>(P, nb, k, t), &part);
+    R part;
+    he_flux<R, 1>(P, hc, he, pos3(hc, na), pos3(hc, nb), load_trec<R, 1>(P, na, k, t),
+                  load_trec<R, 1>(P, nb, k, t), &part);
     xa = (code & 1) ? xa - part : xa + part;
   }
-  return xa;
+  return (double)xa;
 }
 
 // Signed sum of a node's half-edge fluxes on layer k, both tracers, in ascending
 // half-edge order (the order of the reference's scatter into XFLUX).
+template <typename R>
 __device__ inline double2 gather_he(const Dev& P, int q0, int q1, int k) {
-  const double2* EX = P.ex2 + (size_t)(k - 1) * P.ncvs;
-  double x0 = 0.0, x1 = 0.0;
+  typedef typename Mesh<R>::R2 R2;
+  const R2* EX = Mesh<R>::ex2(P) + (size_t)(k - 1) * P.ncvs;
+  R x0 = 0, x1 = 0;
   for (int q = q0; q < q1; ++q) {
     int code = P.node_he[q];
-    double2 e = EX[code >> 1];
+    R2 e = EX[code >> 1];
     if (code & 1) {
       x0 = x0 - e.x;
       x1 = x1 - e.y;
@@ -306,10 +324,11 @@ __device__ inline double2 gather_he(const Dev& P, int q0, int q1, int k) {
       x1 = x1 + e.y;
     }
   }
-  return make_double2(x0, x1);
+  return make_double2((double)x0, (double)x1);
 }
 
 // Phase 2 of ADV_Q(Q2,Q2F)/ADV_Q(Q2L,Q2LF) (adv_q.F:114-401) with FCT_Q2/FCT_Q2L.
+template <typename R>
 __global__ void __launch_bounds__(256) k_gather_q(const Dev P, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.M) return;
@@ -318,7 +337,7 @@ __global__ void __launch_bounds__(256) k_gather_q(const Dev P, int parts) {
   const bool wet = P.iswetn[i] * P.iswetnt[i] == 1;
   const int q0 = P.node_he_ptr[i], q1 = P.node_he_ptr[i + 1];
   for (int k = kb; k <= ke; ++k) {
-  const double2 xs = gather_he(P, q0, q1, k);
+  const double2 xs = gather_he<R>(P, q0, q1, k);
   for (int t = 0; t < 2; ++t) {
     if (!(parts & (t == 0 ? AD_Q2 : AD_Q2L))) continue;
     const double* Q = (t == 0 ? P.q2 : P.q2l);
@@ -340,8 +359,8 @@ __global__ void __launch_bounds__(256) k_gather_q(const Dev P, int parts) {
       qf = Q[q];
     }
     if ((parts & AD_FCT) && !P.riv_skip[i]) {
-      double* const* G = P.gq[t];
-      double qmax = G[5][q], qmin = G[4][q];
+      R* const* G = Mesh<R>::gq(P, t);
+      double qmax = (double)G[5][q], qmin = (double)G[4][q];
       fct_level_bounds(P, i, k, Q, qmax, qmin);
       if (qmin - qf > 0.0) qf = qmin;
       if (qf - qmax > 0.0) qf = qmax;
@@ -565,6 +584,7 @@ __global__ void __launch_bounds__(256) k_turb_update(const Dev P) {
 // Phase 2 of ADV_T / ADV_S (adv_t.F:124-1042, adv_s.F) with FCT_T / FCT_S (fct_t.F:51-104,
 // fct_s.F:50-108) on the same (node, layer) thread.
 // -------------------------------------------------------------------------------------
+template <typename R>
 __global__ void __launch_bounds__(256) k_gather_ts(const Dev P, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.M) return;
@@ -574,13 +594,13 @@ __global__ void __launch_bounds__(256) k_gather_ts(const Dev P, int parts) {
   const int ob = P.node_obc[i];
   const int q0 = P.node_he_ptr[i], q1 = P.node_he_ptr[i + 1];
   for (int k = kb; k <= ke; ++k) {
-  const double2 xs = gather_he(P, q0, q1, k);
+  const double2 xs = gather_he<R>(P, q0, q1, k);
   for (int t = 0; t < 2; ++t) {
     if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
     const double* F1 = (t == 0 ? P.t1 : P.s1);
     double* FF1 = (t == 0 ? P.tf1 : P.sf1);
     double x = t == 0 ? xs.x : xs.y;
-    if (ob > 0) (t == 0 ? P.xflux_obc_t : P.xflux_obc_s)[(size_t)(k - 1) * (P.iobcn + 1) + ob] = obc_xflux_adv(P, i, k, t);
+    if (ob > 0) (t == 0 ? P.xflux_obc_t : P.xflux_obc_s)[(size_t)(k - 1) * (P.iobcn + 1) + ob] = obc_xflux_adv<R>(P, i, k, t);
     size_t q = N3(P, i, k);
     double ff;
     if (wet) {
@@ -607,8 +627,8 @@ __global__ void __launch_bounds__(256) k_gather_ts(const Dev P, int parts) {
     }
     if (parts & AD_FCT) {
       if (!P.riv_skip[i]) {
-        double* const* G = P.gt[t];
-        double fmx = G[5][q], fmn = G[4][q];
+        R* const* G = Mesh<R>::gt(P, t);
+        double fmx = (double)G[5][q], fmn = (double)G[4][q];
         fct_layer_bounds(P, i, k, F1, fmx, fmn);
         if (fmn - ff > 0.0) ff = fmn;
         if (ff - fmx > 0.0) ff = fmx;
@@ -878,11 +898,20 @@ __global__ void k_budget_final(const double* part, int nb, double* out) {
 }
 
 void launch_grad(const Dev& P, cudaStream_t s, int which) {
-  k_grad<<<col_grid(P, P.M, which == 0 ? P.KBM1 - 1 : P.KBM1), P.col_bc, 0, s>>>(P, which);
+  const dim3 g = col_grid(P, P.M, which == 0 ? P.KBM1 - 1 : P.KBM1);
+  if (P.prec)
+    k_grad<float><<<g, P.col_bc, 0, s>>>(P, which);
+  else
+    k_grad<double><<<g, P.col_bc, 0, s>>>(P, which);
 }
 void launch_adv_q(const Dev& P, cudaStream_t s, int parts) {
-  k_he_adv<0><<<col_grid(P, P.N, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
-  k_gather_q<<<col_grid(P, P.M, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
+  if (P.prec) {
+    k_he_adv<float, 0><<<col_grid(P, P.N, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
+    k_gather_q<float><<<col_grid(P, P.M, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
+  } else {
+    k_he_adv<double, 0><<<col_grid(P, P.N, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
+    k_gather_q<double><<<col_grid(P, P.M, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
+  }
 }
 void launch_fct_q(const Dev& P, cudaStream_t s, int parts) {
   dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1 - 1, 8));
@@ -897,8 +926,13 @@ void launch_turb_update(const Dev& P, cudaStream_t s) {
   k_turb_update<<<g, b, 0, s>>>(P);
 }
 void launch_adv_ts(const Dev& P, cudaStream_t s, int parts) {
-  k_he_adv<1><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P, parts);
-  k_gather_ts<<<col_grid(P, P.M, P.KBM1), P.col_bc, 0, s>>>(P, parts);
+  if (P.prec) {
+    k_he_adv<float, 1><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P, parts);
+    k_gather_ts<float><<<col_grid(P, P.M, P.KBM1), P.col_bc, 0, s>>>(P, parts);
+  } else {
+    k_he_adv<double, 1><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P, parts);
+    k_gather_ts<double><<<col_grid(P, P.M, P.KBM1), P.col_bc, 0, s>>>(P, parts);
+  }
 }
 void launch_fct_ts(const Dev& P, cudaStream_t s, int parts) {
   dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));

@@ -203,6 +203,20 @@ class Fvcom(CEngine):
     def shutdown_check(self):
         return int(self.lib.fvg_shutdown_check(self.h))
 
+    PRECISION = {"fp64": 0, "fp32flux": 1}
+
+    def set_precision(self, mode):
+        """'fp64' (plain, bitwise equal to the oracle) or 'fp32flux' (FP32 edge fluxes and
+        advection, FP64 elevation update, column solves, state and budgets)."""
+        m = self.PRECISION[mode] if isinstance(mode, str) else int(mode)
+        self.lib.fvg_set_precision.argtypes = [C.c_void_p, C.c_int32]
+        self._check(self.lib.fvg_set_precision(self.h, m), "set_precision")
+
+    def get_precision(self):
+        self.lib.fvg_get_precision.argtypes = [C.c_void_p]
+        self.lib.fvg_get_precision.restype = C.c_int32
+        return {v: k for k, v in self.PRECISION.items()}[self.lib.fvg_get_precision(self.h)]
+
     def set_tuning(self, key, value):
         self.lib.fvg_set_tuning.argtypes = [C.c_void_p, C.c_char_p, C.c_int32]
         self._check(self.lib.fvg_set_tuning(self.h, key.encode(), int(value)), "set_tuning(%s)" % key)

@@ -1,0 +1,100 @@
+"""Error of the precision form against the plain FP64 path after a simulated period.
+
+Both forms start from the same cold start of the same case and run the same number of
+internal steps on the device.  Reported per output (zeta, u, v, T, S): the maximum and
+RMS absolute difference over the interior entities and layers, and for each form the
+drift of the volume, heat and salt budgets (``fvg_budget``) over the run.
+
+    python -m myfvcomcode_b200.precision_report [--npts 200000] [--hours 24] [--md FILE]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+
+
+def _interior(engine, name):
+    if name == "el":
+        return engine.get("el")[1:]
+    return engine.get3(name)[1:, : engine.KB - 1]
+
+
+def compare(ref, other):
+    out = {}
+    for name, label in (("el", "zeta_m"), ("u", "u_m_s"), ("v", "v_m_s"), ("t1", "T_C"), ("s1", "S_psu")):
+        a, b = _interior(ref, name), _interior(other, name)
+        d = np.abs(a - b)
+        out[label] = {"max": float(d.max()), "rms": float(np.sqrt(np.mean(d * d)))}
+    return out
+
+
+def run(case, steps, modes=("fp64", "fp32flux"), chunk=200):
+    from .engine import Fvcom
+    engines = {}
+    budgets = {}
+    times = {}
+    for m in modes:
+        f = Fvcom(case)
+        f.set_precision(m)
+        b0 = f.budget()
+        t0 = time.perf_counter()
+        done = 0
+        while done < steps:
+            n = min(chunk, steps - done)
+            f.run(n)
+            done += n
+            if f.shutdown_check() != 0:
+                raise RuntimeError("%s: non-finite state after %d steps" % (m, done))
+        f.sync()
+        times[m] = time.perf_counter() - t0
+        b1 = f.budget()
+        budgets[m] = {k: (b1[i] - b0[i]) / b0[i] if b0[i] != 0 else math.nan
+                      for i, k in enumerate(("volume", "heat", "salt"))}
+        engines[m] = f
+    ref = engines[modes[0]]
+    report = {"case": case["name"], "internal_steps": steps,
+              "simulated_hours": steps * case["params"]["DTE"] * case["params"]["ISPLIT"] / 3600.0,
+              "budget_drift": budgets, "wall_s": times, "errors_vs_" + modes[0]: {}}
+    for m in modes[1:]:
+        report["errors_vs_" + modes[0]][m] = compare(ref, engines[m])
+    for f in engines.values():
+        f.close()
+    return report
+
+
+def markdown(rep):
+    lines = ["| output | max abs error | RMS error |", "|---|---|---|"]
+    for m, errs in rep["errors_vs_fp64"].items():
+        for k, v in errs.items():
+            lines.append("| %s (%s) | %.3e | %.3e |" % (k, m, v["max"], v["rms"]))
+    lines.append("")
+    lines.append("| form | volume drift | heat drift | salt drift |")
+    lines.append("|---|---|---|---|")
+    for m, b in rep["budget_drift"].items():
+        lines.append("| %s | %.3e | %.3e | %.3e |" % (m, b["volume"], b["heat"], b["salt"]))
+    return "\n".join(lines) + "\n"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--npts", type=int, default=200000)
+    ap.add_argument("--hours", type=float, default=24.0)
+    ap.add_argument("--md", default=None)
+    args = ap.parse_args()
+    from . import cases
+    case = cases.coastal_mesh(npts=args.npts)
+    dti = case["params"]["DTE"] * case["params"]["ISPLIT"]
+    steps = int(round(args.hours * 3600.0 / dti))
+    rep = run(case, steps)
+    print(json.dumps(rep))
+    if args.md:
+        with open(args.md, "w") as fh:
+            fh.write(markdown(rep))
+
+
+if __name__ == "__main__":
+    main()
