@@ -36,7 +36,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="coastal", choices=["coastal", "channel"])
+    ap.add_argument("--workload", default="coastal", choices=["coastal", "channel", "ensemble"])
+    ap.add_argument("--members-small", type=int, default=32,
+                    help="ensemble: members on the 50k-node 30-layer mesh (all ranks together)")
+    ap.add_argument("--members-large", type=int, default=8,
+                    help="ensemble: members on the 200k-node 40-layer mesh (all ranks together)")
+    ap.add_argument("--closure", default=None,
+                    help="a trained closure (.npz from myfvcomcode_b200.closure) for the learned form")
     ap.add_argument("--npts", type=int, default=200000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -144,33 +150,17 @@ class ClockSampler:
 
 
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-        pg = dist
-    return world, rank, local, pg
+    from myfvcomcode_b200 import dist
+    d = dist.setup()
+    return d.world, d.rank, d.local, (d if d.pg is not None else None)
 
 
 def reduce_max(pg, x, local):
-    if pg is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % local)
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    return x if pg is None else pg.reduce_max(x)
 
 
 def barrier(pg, local):
     if pg is not None:
-        import torch
-        torch.cuda.synchronize(local)
         pg.barrier()
 
 
@@ -194,9 +184,104 @@ def cpu_rate(case, seconds, warm=1, cap=None):
     return rate, max_threads(), steps, dt + t1
 
 
+def run_ensemble(args, world, rank, local, pg):
+    """Batched ensemble: perturbed members of two meshes, each mesh's members as one union
+    model, both models stepped by one CUDA graph per internal step.  Members are sharded
+    over the ranks (no data-path collective)."""
+    import torch
+    from myfvcomcode_b200 import autotune, cases, ensemble
+    from myfvcomcode_b200.engine import Fvcom, Group
+    from myfvcomcode_b200.precision_report import compare
+    torch.cuda.set_device(local)
+    groups = [("50k-k30", cases.coastal_mesh(npts=50000, kb=31), args.members_small, 5),
+              ("200k-k40", cases.coastal_mesh(npts=args.npts, kb=41), args.members_large, 6)]
+    trained = None
+    if args.closure:
+        from myfvcomcode_b200 import closure
+        trained = closure.load(args.closure)
+    models, unions, cfg_members, bases = [], [], [], []
+    cells_layers = 0
+    for name, base, n, seed in groups:
+        specs = ensemble.perturbed_members(base, n, seed=seed)
+        from myfvcomcode_b200.dist import shard
+        mine = shard(specs, rank, world)
+        if not mine:
+            continue
+        u = ensemble.union_case(base, mine)
+        f = Fvcom(u)
+        f.set_precision(args.precision)
+        if trained is not None:
+            closure.attach(f, trained)
+        t = autotune.autotune(u, steps=2, warmup=1, engine=f)
+        autotune.apply(f, t)
+        models.append(f)
+        unions.append((u, mine, base))
+        cells_layers += u["grid"]["N"] * (u["grid"]["KB"] - 1)
+        cfg_members.append({"mesh": name, "members_this_rank": len(mine), "members_total": n,
+                            "tiling": [t["col_threads"], t["col_layers"]]})
+    grp = Group(models)
+    grp.run(args.warmup)
+    barrier(pg, local)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    t_ms = grp.time_steps(args.steps)
+    clocks = sampler.stop()
+    barrier(pg, local)
+    t_ms = reduce_max(pg, t_ms, local)
+    total_cl = cells_layers * world  # every rank holds the same member count up to rounding
+    value = total_cl * args.steps / (t_ms / 1e3)
+    # per-member error of member 0 of each model against its standalone FP64 run
+    errors = []
+    if rank == 0:
+        for f, (u, mine, base) in zip(models, unions):
+            n_done = f.clock()[0]
+            ref = Fvcom(ensemble.member_case(base, mine[0]))
+            ref.run(n_done)
+
+            class _Member:
+                KB = f.KB
+
+                def get(self, nm):
+                    return ensemble.member_slice(u, 0, nm, f)
+
+                def get3(self, nm):
+                    a = self.get(nm)
+                    return a.reshape((a.size // self.KB, self.KB), order="F")
+            err = compare(ref, _Member())
+            errors.append({"mesh": u["name"], "internal_steps": n_done, "errors_vs_fp64_member": err})
+            ref.close()
+    import ctypes as C
+    kps = 0
+    for f in models:
+        f.lib.fvg_kernels_per_step.argtypes = [C.c_void_p]
+        f.lib.fvg_kernels_per_step.restype = C.c_int32
+        kps += int(f.lib.fvg_kernels_per_step(f.h))
+    grp.close()
+    for f in models:
+        f.close()
+    if rank == 0:
+        line = {"metric": "cell-layer updates/s", "value": value, "unit": "cell-layer updates/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32 fluxes, f64 state", "data": "synthetic",
+                "config": {"workload": "ensemble", "members": cfg_members, "precision": args.precision,
+                           "learned_closure": bool(trained is not None),
+                           "launch": "one CUDA graph per internal step holding every model",
+                           "perturbations": "wind x U(0.8,1.2), tide amplitude x U(0.9,1.1), T0 + N(0,0.5)"},
+                "clocks": clocks, "member_errors": errors,
+                "gpu_launches": kps * args.steps}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.close()
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
+    if args.workload == "ensemble" and args.impl != "reference":
+        run_ensemble(args, world, rank, local, pg)
+        return
     case = make_case(args)
     g, p = case["grid"], case["params"]
     cells_layers = g["N"] * (g["KB"] - 1)
@@ -358,7 +443,7 @@ def main():
         print(json.dumps(line), flush=True)
     f.close()
     if pg is not None:
-        pg.destroy_process_group()
+        pg.close()
 
 
 if __name__ == "__main__":

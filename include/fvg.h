@@ -221,11 +221,68 @@ int fvg_use_graph(fvg_handle* h, int32_t on);
 #define FVG_PREC_FP32_FLUX 1
 int fvg_set_precision(fvg_handle* h, int32_t mode);
 int32_t fvg_get_precision(const fvg_handle* h);
+/* Closure samples for training a learned vertical closure.  While dev_buf (device
+   memory, at least 12*M*(KBM1-1) floats) is set, every VDIF_Q writes for each node I and
+   interior level K=2..KBM1, at index (K-2)*M + (I-1) of 12 planes of M*(KBM1-1) floats:
+   BOYGR (N^2), shear S^2, D, sigma Z, u*_surf, u*_bot, Q2, Q2L -- the closure's inputs
+   after VDIF_Q's positivity fixes (vdif_q.F:250-262) -- then its outputs before the
+   time averaging, KN*KAPPA*SM, KN*SM, KN*SH*VPRNU (vdif_q.F:479-491), and 1 for a wet
+   node (0: the node's planes are not meaningful).  dev_buf NULL stops sampling. */
+int fvg_closure_sample(fvg_handle* h, float* dev_buf, int64_t cap);
+/* The learned closure's network: an MLP 8 -> 64 -> 64 -> 3, GELU on the hidden layers,
+   FP32 parameters (W1 64x8, b1, W2 64x64, b2, W3 3x64, b3; fvg_mlp_num_params() floats)
+   trained on the device by the library's own forward/backward kernels (mean-squared
+   error, Adam, deterministic gradient sums).  x, y and out are device pointers to
+   row-major [n][8] inputs, [n][3] targets and [n][3] outputs. */
+typedef struct fvg_mlp fvg_mlp;
+int fvg_mlp_create(uint64_t seed, fvg_mlp** out);
+void fvg_mlp_destroy(fvg_mlp* q);
+const char* fvg_mlp_last_error(const fvg_mlp* q);
+int32_t fvg_mlp_num_params(void);
+int fvg_mlp_get_params(fvg_mlp* q, float* host, int32_t n);
+int fvg_mlp_set_params(fvg_mlp* q, const float* host, int32_t n);
+/* Mean-squared error over the n samples and its gradient (host outputs). */
+int fvg_mlp_loss_grad(fvg_mlp* q, const float* x, const float* y, int32_t n, float* loss, float* grad);
+/* epochs of Adam over shuffled batches; epoch_loss[e] (host, may be NULL) = mean error. */
+int fvg_mlp_train(fvg_mlp* q, const float* x, const float* y, int32_t n, int32_t epochs, int32_t batch,
+                  float lr, uint64_t seed, float* epoch_loss);
+/* FP32 forward pass (the reference of the tensor-core inference). */
+int fvg_mlp_forward(fvg_mlp* q, const float* x, int32_t n, float* out);
+const float* fvg_mlp_device_params(const fvg_mlp* q);
+/* The same network in BF16 on the tensor cores (tcgen05.mma, FP32 accumulate), the
+   kernel the learned closure runs; x standardised inputs [n][8], out [n][3]. */
+int fvg_mlp_forward_bf16(fvg_mlp* q, const float* x, int32_t n, float* out);
+/* Learned vertical closure.  mode 1: VDIF_Q's stability functions and KN of the
+   interior levels are replaced by the network (params: fvg_mlp_num_params() floats, the
+   layout of fvg_mlp_get_params) run in BF16 on the tensor cores, for every column whose
+   inputs all lie inside the training envelope; other columns keep MY2.5.  norm
+   (FVG_CLOSURE_NORM_FLOATS floats): input transform kind[8] (0 identity, 1 log, 2
+   asinh(x/scale)), scale[8], mean[8], std[8], envelope lo[8], hi[8]; output tmean[3],
+   tstd[3], teps (new part = exp(y*tstd + tmean) - teps).  mode 0: MY2.5 everywhere. */
+#define FVG_CLOSURE_NORM_FLOATS 55
+int fvg_set_closure(fvg_handle* h, int32_t mode, const float* params, int32_t nparams, const float* norm,
+                    int32_t nnorm);
+/* Columns that used the network in the last step, and the count of tensor-core waits
+   that ran out (0 unless the device misbehaved; results are then incomplete). */
+int fvg_closure_status(fvg_handle* h, int32_t* columns_on_network, int32_t* wait_timeouts);
 /* Launch shape of the 3-D gather kernels (results do not depend on it):
    "col_threads" = entities (threads) per block, 32..256 in steps of 32 (default 128);
    "col_layers"  = consecutive layers each thread walks, 1..KB (default 8). */
 int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value);
 int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value);
+
+/* Groups (batched ensembles).  Several models -- for example union models of ensemble
+   members on meshes of different size or layer count -- stepped together: one CUDA
+   graph per internal step holds one INTERNAL_STEP of every model, each on its own branch,
+   so the models run concurrently from a single launch.  The handles stay usable on their
+   own; a handle may belong to several groups but must not be stepped by two host threads
+   at once.  fvg_group_time_steps returns the device time of nsteps steps of all models. */
+typedef struct fvg_group fvg_group;
+int fvg_group_create(fvg_handle* const* handles, int32_t n, fvg_group** out);
+int fvg_group_run(fvg_group* g, int32_t nsteps);
+int fvg_group_time_steps(fvg_group* g, int32_t nsteps, double* ms);
+const char* fvg_group_last_error(const fvg_group* g);
+void fvg_group_destroy(fvg_group* g);
 
 /* Measurement.  fvg_time_steps runs nsteps internal steps and returns their device time
    (CUDA events on the handle's stream).  fvg_profile runs nsteps with plain launches and

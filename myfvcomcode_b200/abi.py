@@ -104,7 +104,10 @@ def wind_stress(case):
     if wind is None:
         return None
     N = case["grid"]["N"]
-    if wind["kind"] == "speed":
+    if wind["kind"] == "field":
+        sx = np.array(wind["sx"], dtype=np.float64)
+        sy = np.array(wind["sy"], dtype=np.float64)
+    elif wind["kind"] == "speed":
         sx, sy = simple_drag(np.full(N + 1, wind["u"]), np.full(N + 1, wind["v"]))
     else:
         sx, sy = np.full(N + 1, float(wind["u"])), np.full(N + 1, float(wind["v"]))

@@ -50,6 +50,7 @@ struct fvg_handle {
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph = nullptr;
   bool use_graph = true;
+  int clos_grid = 148;
 };
 
 #define CK(call)                                                                      \
@@ -218,6 +219,7 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   launch_adv_q(P, s, AD_Q2 | AD_Q2L | spc);
   mk.mark(s, G_ADV_Q);
   launch_vdif_q(P, s, 1);
+  if (P.closure) launch_closure(P, s, P.clos_err, h->clos_grid);
   mk.mark(s, G_VDIF_Q);
   int ts = (p.temperature_active ? AD_T : 0) | (p.salinity_active ? AD_S : 0);
   if (ts) {
@@ -655,6 +657,32 @@ int fvg_set_ramp(fvg_handle* h, double ramp) {
 // mode 0: graph replay (or plain launches when graphs are off); mode 1: plain launches
 // with events between kernel groups, accumulated into group_ms; total_ms gets the device
 // time of all steps measured with events on the handle's stream.
+// Schedule rows of the next c internal steps (RAMP, tidal phase arguments) and the device
+// slot counter, on the handle's stream; the stream must be idle.
+static int prep_chunk(fvg_handle* h, int c) {
+  const int len = h->P.sl.len;
+  int32_t iint = h->iint;
+  double t = h->ext_time;
+  for (int s = 0; s < c; ++s) {
+    fill_sched_row(h, h->h_sched + (size_t)s * len, iint + 1, t);
+    iint += 1;
+    for (int iext = 1; iext <= h->prm.isplit; ++iext) t = t + h->prm.dte;
+  }
+  CK(cudaMemcpyAsync(h->d_sched, h->h_sched, (size_t)c * len * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  h->h_ctl[0] = -1;
+  CK(cudaMemcpyAsync(h->P.ctl, h->h_ctl, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  return FVG_OK;
+}
+
+// Advance the host clock by c internal steps exactly as the reference accumulates ExtTime.
+static void finish_chunk(fvg_handle* h, int c) {
+  for (int s = 0; s < c; ++s) {
+    h->iint += 1;
+    for (int iext = 1; iext <= h->prm.isplit; ++iext) h->ext_time = h->ext_time + h->prm.dte;
+  }
+  h->ramp = h->prm.iramp != 0 ? std::tanh((double)h->iint / (double)h->prm.iramp) : 1.0;
+}
+
 static int run_steps(fvg_handle* h, int32_t nsteps, int mode, double* group_ms, double* total_ms) {
   if (!h || nsteps < 0) return FVG_ERR_ARG;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -663,21 +691,11 @@ static int run_steps(fvg_handle* h, int32_t nsteps, int mode, double* group_ms, 
     CK(cudaEventCreate(&t1));
   }
   double total = 0.0;
-  const int len = h->P.sl.len;
   int done = 0;
   while (done < nsteps) {
     int c = std::min(h->sched_cap, nsteps - done);
     CK(cudaStreamSynchronize(h->stream));
-    int32_t iint = h->iint;
-    double t = h->ext_time;
-    for (int s = 0; s < c; ++s) {
-      fill_sched_row(h, h->h_sched + (size_t)s * len, iint + 1, t);
-      iint += 1;
-      for (int iext = 1; iext <= h->prm.isplit; ++iext) t = t + h->prm.dte;
-    }
-    CK(cudaMemcpyAsync(h->d_sched, h->h_sched, (size_t)c * len * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    h->h_ctl[0] = -1;
-    CK(cudaMemcpyAsync(h->P.ctl, h->h_ctl, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    { int rc = prep_chunk(h, c); if (rc) return rc; }
     if (total_ms) CK(cudaEventRecord(t0, h->stream));
     std::vector<cudaEvent_t> ev;
     std::vector<int> grp;
@@ -717,12 +735,7 @@ static int run_steps(fvg_handle* h, int32_t nsteps, int mode, double* group_ms, 
       }
       for (auto e : ev) cudaEventDestroy(e);
     }
-    // advance the host clock exactly as the reference accumulates ExtTime
-    for (int s = 0; s < c; ++s) {
-      h->iint += 1;
-      for (int iext = 1; iext <= h->prm.isplit; ++iext) h->ext_time = h->ext_time + h->prm.dte;
-    }
-    h->ramp = h->prm.iramp != 0 ? std::tanh((double)h->iint / (double)h->prm.iramp) : 1.0;
+    finish_chunk(h, c);
     done += c;
   }
   CK(cudaStreamSynchronize(h->stream));
@@ -752,6 +765,7 @@ int32_t fvg_kernels_per_step(const fvg_handle* h) {
   n += p.isplit * 4 * (3 + (p.wetting_drying_on ? 2 : 0)); // RK stages
   n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv
   n += 4;                                                  // grad_q, adv_q (2 phases), vdif_q
+  if (h->P.closure) n += 2;                                // learned closure, shallow columns
   if (p.temperature_active || p.salinity_active)           // grad_ts, adv_ts (2 phases), vdif_ts,
     n += 5 + (h->P.iobcn > 0 ? 1 : 0);                     // bcond_ts (rivers, open boundary)
   n += 1;                                                  // final
@@ -822,6 +836,99 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
 }
 
 int32_t fvg_get_precision(const fvg_handle* h) { return h ? h->P.prec : -1; }
+
+int fvg_set_closure(fvg_handle* h, int32_t mode, const float* params, int32_t nparams, const float* norm,
+                    int32_t nnorm) {
+  if (!h) return FVG_ERR_ARG;
+  Dev& P = h->P;
+  CK(cudaStreamSynchronize(h->stream));
+  auto regraph = [&]() {
+    if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  };
+  if (mode == 0) { P.closure = 0; regraph(); return FVG_OK; }
+  if (mode != 1 || !params || nparams != fvg_mlp_num_params() || !norm || nnorm != FVG_CLOSURE_NORM_FLOATS) {
+    h->err = "fvg_set_closure: bad mode, parameter or scaling vector";
+    return FVG_ERR_ARG;
+  }
+  if (P.KBM1 < 2) { h->err = "fvg_set_closure: no interior levels"; return FVG_ERR_ARG; }
+  const size_t S = (size_t)P.M * (P.KBM1 - 1);
+  int rc;
+  if (!P.clos_feat) {
+    if (closure_setup_attrs()) { h->err = "cannot configure the closure kernel"; return FVG_ERR_CUDA; }
+    if ((rc = dalloc(h, &P.clos_feat, (size_t)CLOS_IN * S))) return rc;
+    if ((rc = dalloc(h, &P.clos_plain, 3 * S))) return rc;
+    if ((rc = dalloc(h, &P.clos_env, (size_t)P.M + 1))) return rc;
+    if ((rc = dalloc(h, &P.clos_err, 1))) return rc;
+    float* b = nullptr;
+    if ((rc = dalloc(h, &b, 144))) return rc;
+    P.clos_b = b;
+    uint8_t* w = nullptr;
+    if ((rc = dalloc(h, &w, closure_weight_image_bytes()))) return rc;
+    P.clos_w = w;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    h->clos_grid = 2 * nsm;
+  }
+  std::vector<uint8_t> img;
+  std::vector<float> bias;
+  closure_weight_image(params, img, bias);
+  CK(cudaMemcpy((void*)P.clos_w, img.data(), img.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy((void*)P.clos_b, bias.data(), bias.size() * sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMemset(P.clos_err, 0, sizeof(int)));
+  ClosNorm nm{};
+  for (int f = 0; f < 8; ++f) {
+    nm.kind[f] = (int)norm[f];
+    nm.scale[f] = norm[8 + f];
+    nm.mean[f] = norm[16 + f];
+    nm.std[f] = norm[24 + f];
+    nm.lo[f] = norm[32 + f];
+    nm.hi[f] = norm[40 + f];
+  }
+  for (int c = 0; c < 3; ++c) {
+    nm.tmean[c] = norm[48 + c];
+    nm.tstd[c] = norm[51 + c];
+  }
+  nm.teps = norm[54];
+  P.clos_norm = nm;
+  P.closure = 1;
+  regraph();
+  return FVG_OK;
+}
+
+int fvg_closure_status(fvg_handle* h, int32_t* columns_on_network, int32_t* wait_timeouts) {
+  if (!h) return FVG_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  if (columns_on_network) {
+    *columns_on_network = 0;
+    if (h->P.clos_env) {
+      std::vector<int> env(h->P.M + 1);
+      CK(cudaMemcpy(env.data(), h->P.clos_env, env.size() * sizeof(int), cudaMemcpyDeviceToHost));
+      int c = 0;
+      for (int i = 1; i <= h->P.M; ++i) c += env[i] != 0;
+      *columns_on_network = c;
+    }
+  }
+  if (wait_timeouts) {
+    *wait_timeouts = 0;
+    if (h->P.clos_err) CK(cudaMemcpy(wait_timeouts, h->P.clos_err, sizeof(int), cudaMemcpyDeviceToHost));
+  }
+  return FVG_OK;
+}
+
+int fvg_closure_sample(fvg_handle* h, float* dev_buf, int64_t cap) {
+  if (!h) return FVG_ERR_ARG;
+  const int64_t need = (int64_t)CLOS_PLANES * h->P.M * (h->P.KBM1 - 1);
+  if (dev_buf && cap < need) { h->err = "closure sample buffer too small"; return FVG_ERR_ARG; }
+  CK(cudaStreamSynchronize(h->stream));
+  if (dev_buf != h->P.clos_samp) {
+    h->P.clos_samp = dev_buf;
+    if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  }
+  return FVG_OK;
+}
 
 int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value) {
   if (!h || !key) return FVG_ERR_ARG;
@@ -948,7 +1055,10 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
       launch_adv_q(P, s, (arg == 0 ? AD_Q2 : AD_Q2L) | spc);
       break;
     case FVG_R_FCT_Q: launch_fct_q(P, s, arg == 0 ? AD_Q2 : AD_Q2L); break;
-    case FVG_R_VDIF_Q: launch_vdif_q(P, s, 0); break;
+    case FVG_R_VDIF_Q:
+      launch_vdif_q(P, s, 0);
+      if (P.closure) launch_closure(P, s, P.clos_err, h->clos_grid);
+      break;
     case FVG_R_TURB_UPDATE: launch_turb_update(P, s); break;
     case FVG_R_ADV_TS:
       launch_grad(P, s, 1);
@@ -980,6 +1090,136 @@ int fvg_shutdown_check(fvg_handle* h) {
   for (int i = 1; i <= h->P.N; ++i) s = s + d1[i];
   if (!std::isfinite(s)) { h->err = "non-finite depth (SHUTDOWN_CHECK)"; return FVG_ERR_NAN; }
   return FVG_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Groups: several models stepped by one CUDA graph per internal step.
+// ---------------------------------------------------------------------------------------
+}  // extern "C"
+
+struct fvg_group {
+  std::vector<fvg_handle*> hs;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<cudaEvent_t> ev;  // fork event + one join event per model
+  std::string err;
+};
+
+static void group_free(fvg_group* g) {
+  if (!g) return;
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  if (g->gexec) cudaGraphExecDestroy(g->gexec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  for (auto e : g->ev) cudaEventDestroy(e);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+#define GK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      g->err = std::string(#call) + ": " + cudaGetErrorString(e_);                     \
+      return FVG_ERR_CUDA;                                                             \
+    }                                                                                  \
+  } while (0)
+
+static int group_capture(fvg_group* g) {
+  GK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+  GK(cudaEventRecord(g->ev[0], g->stream));
+  for (size_t q = 0; q < g->hs.size(); ++q) {
+    fvg_handle* h = g->hs[q];
+    GK(cudaStreamWaitEvent(h->stream, g->ev[0], 0));
+    enqueue_internal_step(h, h->stream);
+    GK(cudaEventRecord(g->ev[q + 1], h->stream));
+    GK(cudaStreamWaitEvent(g->stream, g->ev[q + 1], 0));
+  }
+  cudaError_t e = cudaStreamEndCapture(g->stream, &g->graph);
+  if (e != cudaSuccess) { g->err = std::string("group capture: ") + cudaGetErrorString(e); return FVG_ERR_CUDA; }
+  GK(cudaGraphInstantiate(&g->gexec, g->graph, 0));
+  return FVG_OK;
+}
+
+static int group_steps(fvg_group* g, int32_t nsteps, double* ms) {
+  if (nsteps < 0) return FVG_ERR_ARG;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (ms) {
+    GK(cudaEventCreate(&t0));
+    GK(cudaEventCreate(&t1));
+  }
+  double total = 0.0;
+  int cap = g->hs[0]->sched_cap;
+  for (fvg_handle* h : g->hs) cap = std::min(cap, h->sched_cap);
+  int done = 0;
+  while (done < nsteps) {
+    const int c = std::min(cap, nsteps - done);
+    GK(cudaStreamSynchronize(g->stream));
+    for (fvg_handle* h : g->hs) {
+      GK(cudaStreamSynchronize(h->stream));
+      int rc = prep_chunk(h, c);
+      if (rc) { g->err = h->err; return rc; }
+      GK(cudaStreamSynchronize(h->stream));
+    }
+    if (!g->gexec) {
+      int rc = group_capture(g);
+      if (rc) return rc;
+    }
+    if (ms) GK(cudaEventRecord(t0, g->stream));
+    for (int s = 0; s < c; ++s) GK(cudaGraphLaunch(g->gexec, g->stream));
+    if (ms) {
+      GK(cudaEventRecord(t1, g->stream));
+      GK(cudaEventSynchronize(t1));
+      float f = 0.f;
+      GK(cudaEventElapsedTime(&f, t0, t1));
+      total += f;
+    }
+    GK(cudaStreamSynchronize(g->stream));
+    for (fvg_handle* h : g->hs) finish_chunk(h, c);
+    done += c;
+  }
+  if (ms) {
+    *ms = total;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+  }
+  return FVG_OK;
+}
+
+extern "C" {
+
+int fvg_group_create(fvg_handle* const* hs, int32_t n, fvg_group** out) {
+  if (!hs || !out || n < 1) return FVG_ERR_ARG;
+  *out = nullptr;
+  int dev0 = -1;
+  for (int32_t q = 0; q < n; ++q) {
+    if (!hs[q]) return FVG_ERR_ARG;
+    for (int32_t r = 0; r < q; ++r)
+      if (hs[r] == hs[q]) return FVG_ERR_ARG;
+  }
+  (void)dev0;
+  fvg_group* g = new fvg_group();
+  g->hs.assign(hs, hs + n);
+  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) { group_free(g); return FVG_ERR_CUDA; }
+  g->ev.resize((size_t)n + 1, nullptr);
+  for (auto& e : g->ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) { group_free(g); return FVG_ERR_CUDA; }
+  *out = g;
+  return FVG_OK;
+}
+
+void fvg_group_destroy(fvg_group* g) { group_free(g); }
+
+const char* fvg_group_last_error(const fvg_group* g) { return g ? g->err.c_str() : "null group"; }
+
+int fvg_group_run(fvg_group* g, int32_t nsteps) {
+  if (!g) return FVG_ERR_ARG;
+  return group_steps(g, nsteps, nullptr);
+}
+
+int fvg_group_time_steps(fvg_group* g, int32_t nsteps, double* ms) {
+  if (!g || !ms) return FVG_ERR_ARG;
+  return group_steps(g, nsteps, ms);
 }
 
 int fvg_budget(fvg_handle* h, double out[3]) {

@@ -19,6 +19,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "../../include/fvg.h"
 
 namespace fvg {
@@ -44,6 +46,17 @@ struct F32 {
   float2* ex2;
   float *xo, *yo, *dltxc, *dltyc, *art, *cc_hvc, *a1u, *a2u;
   float *dltxe, *dltye, *dltxncve, *dltyncve;
+};
+
+// Input and output scaling of the learned closure's network, and the training envelope.
+// Input f: kind 0 identity, 1 log(x), 2 asinh(x/scale); then (t - mean)/std.  Output c:
+// new part = exp(y*tstd + tmean) - teps.  A column uses the network only when every
+// interior level's raw inputs lie in [lo, hi] (0.5 and 99.5 percentiles of the training
+// samples).
+struct ClosNorm {
+  int kind[8];
+  float scale[8], mean[8], std[8], lo[8], hi[8];
+  float tmean[3], tstd[3], teps;
 };
 
 // Device pointers and sizes, passed by value to kernels.
@@ -132,6 +145,23 @@ struct Dev {
   // FCT) in FP32 arithmetic over FP32 scratch and FP32 copies of their mesh metrics.
   int prec;
   F32 f;
+  // Closure samples (fvg_closure_sample): when set, VDIF_Q writes for every node and
+  // interior level K=2..KBM1 at index (K-2)*M + (I-1) of each plane of CLOS_PLANES:
+  // N^2 (BOYGR), S^2, D, sigma Z, u*_surf, u*_bot, Q2, Q2L, the new parts KN*KAPPA*SM,
+  // KN*SM, KN*SH*VPRNU that MY2.5 averages into KQ, KM, KH, and 1 for a wet node.
+  float* clos_samp;
+  // Learned closure (fvg_set_closure): 0 = MY2.5; 1 = the network with MY2.5 as the
+  // per-column fallback.  clos_feat: [8][M*(KBM1-1)] inputs, clos_plain: [3][...] MY2.5's
+  // new parts (FP64), clos_env: per node 1 = wet and inside the envelope; clos_w: the BF16
+  // weight image, clos_b: biases (64 + 64 + 16).
+  int closure;
+  ClosNorm clos_norm;
+  const void* clos_w;
+  const float* clos_b;
+  float* clos_feat;
+  double* clos_plain;
+  int* clos_env;
+  int* clos_err;
   // Column tiling of the 3-D gather kernels: col_bc threads (entities) per block, each
   // walking col_lc consecutive layers, so the entity's index chain (cell -> edge ->
   // neighbour) is resolved from cache after the first layer.  Results do not depend on it.
@@ -149,6 +179,8 @@ __device__ inline void col_range(const Dev& P, int k0, int klast, int& kb, int& 
   if (ke > klast) ke = klast;
 }
 
+
+constexpr int CLOS_IN = 8, CLOS_OUT = 3, CLOS_PLANES = CLOS_IN + CLOS_OUT + 1;
 
 // index helpers
 __host__ __device__ inline size_t N3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ms + i; }
@@ -222,6 +254,13 @@ void launch_ext_update(const Dev& P, cudaStream_t s, int K);
 void launch_begin_step(const Dev& P, cudaStream_t s);
 void launch_ext_prep(const Dev& P, cudaStream_t s);
 void launch_make_f32(const Dev& P, cudaStream_t s);
+void launch_closure(const Dev& P, cudaStream_t s, int* err, int grid);
+size_t closure_smem_bytes();
+size_t closure_weight_image_bytes();
+int closure_setup_attrs();
+void launch_mlp_tc_forward(const void* wimg, const float* bias, const float* x, int n, float* out, int* err, int grid,
+                           cudaStream_t s);
+void closure_weight_image(const float* params, std::vector<uint8_t>& img, std::vector<float>& bias);
 void launch_set_qdis(const Dev& P, cudaStream_t s);
 
 // ---------------- 3-D momentum (k_mom3d.cu) ----------------

@@ -1,0 +1,361 @@
+// k_closure.cu - the learned vertical closure: BF16 inference of the MLP 8 -> 64 -> 64 -> 3
+// on the 5th-generation tensor cores (tcgen05.mma, accumulators in tensor memory), fused
+// with the closure's update of KQ, KM, KH.
+//
+// VDIF_Q in learned mode (P.closure == 1) stores, for every node and interior level, the
+// eight network inputs and MY2.5's own new parts KN*KAPPA*SM, KN*SM, KN*SH*VPRNU
+// (clos_feat, the planes of fvg_closure_sample), and per column whether the node is wet
+// and all its inputs lie inside the training envelope (clos_env).  It leaves KQ, KM, KH
+// of the interior levels to k_closure_mlp, which for each (node, level) row takes the
+// network's prediction where the column is inside the envelope and MY2.5's value where it
+// is not (the per-column fallback), then averages with the old value as MY2.5 does:
+// K = 0.5*(new + K_old) (vdif_q.F:489-491).
+//
+// Tile scheme: a CTA of 128 threads owns tiles of 128 rows; thread t owns row t of the
+// tile and TMEM lane t.  For each layer the threads write their row's BF16 activations
+// into shared memory in the canonical no-swizzle K-major layout (core matrices of 8 rows
+// x 16 bytes; core (row group g, k group c) at g*SBO + c*128 bytes), one elected thread
+// issues tcgen05.mma (M=128, N=64 or 16, K=16 per instruction, FP32 accumulate) and
+// commits to an mbarrier, and every thread reads its row back with tcgen05.ld, adds the
+// bias and applies GELU.  Weights are staged once per CTA in the same layout.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "fvg_model.h"
+
+namespace fvg {
+
+namespace {
+
+constexpr int ROWS = 128;          // rows per tile = MMA M = threads per CTA
+constexpr int K1 = 16;             // layer-1 K (8 inputs padded with zeros)
+constexpr int HID = 64;            // hidden width = MMA N of layers 1 and 2
+constexpr int NOUT = 16;           // layer-3 N (3 outputs padded)
+constexpr int CORE = 128;          // bytes of one core matrix (8 rows x 16 bytes)
+// shared-memory image (bytes)
+constexpr int S_W1 = 0;                           // 64 x 16 bf16, SBO 256
+constexpr int S_W2 = S_W1 + HID * K1 * 2;         // 64 x 64 bf16, SBO 1024
+constexpr int S_W3 = S_W2 + HID * HID * 2;        // 16 x 64 bf16, SBO 1024
+constexpr int S_A1 = S_W3 + NOUT * HID * 2;         // 128 x 16 bf16, SBO 256
+constexpr int S_A2 = S_A1 + ROWS * K1 * 2;        // 128 x 64 bf16, SBO 1024
+constexpr int S_END = S_A2 + ROWS * HID * 2;
+constexpr int W_IMAGE = S_A1;                     // bytes of the weight image
+// TMEM columns: D1 [0,64), D2 [64,128), D3 [0,16) (D1 is read out before layer 3 runs);
+// 128 allocated, so four CTAs fit in an SM's 512 columns.
+constexpr uint32_t TMEM_COLS = 128;
+constexpr long kSpin = 1 << 22;  // bound of every mbarrier wait
+
+__device__ inline uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: no swizzle, K-major, version 1.
+__device__ inline uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version
+  return d;                 // base offset 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+  return (1u << 4)                     // D format FP32
+         | (1u << 7)                   // A format BF16
+         | (1u << 10)                  // B format BF16
+         | ((uint32_t)(n >> 3) << 17)  // N / 8
+         | ((uint32_t)(m >> 4) << 24);  // M / 16
+}
+
+__device__ inline void mma_bf16(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t idesc, bool accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.u32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
+      "l"(a), "l"(b), "r"(idesc), "r"((uint32_t)accumulate));
+}
+
+__device__ inline void mma_commit(uint64_t* mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+
+// Bounded wait for the mbarrier phase with the given parity; false if it ran out.
+__device__ inline bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+  const uint32_t a = smem_u32(mbar);
+  for (long it = 0; it < kSpin; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ inline void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ inline void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ inline void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane.
+__device__ inline void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ inline float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+
+__device__ inline uint32_t pack_bf16(float a, float b) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// Row r (0..127) of an activation tile with K columns (multiple of 8): 8 values per
+// 16-byte store at core (r/8, c) row r%8.
+__device__ inline void store_row(uint8_t* tile, int sbo, int r, const float* v, int k) {
+  for (int c = 0; c < k / 8; ++c) {
+    uint4 q;
+    q.x = pack_bf16(v[8 * c + 0], v[8 * c + 1]);
+    q.y = pack_bf16(v[8 * c + 2], v[8 * c + 3]);
+    q.z = pack_bf16(v[8 * c + 4], v[8 * c + 5]);
+    q.w = pack_bf16(v[8 * c + 6], v[8 * c + 7]);
+    *reinterpret_cast<uint4*>(tile + (r / 8) * sbo + c * CORE + (r % 8) * 16) = q;
+  }
+}
+
+// Network input transform of feature f: 0 identity, 1 log(x), 2 asinh(x / s).
+__device__ inline float feat_transform(const ClosNorm& nm, int f, float x) {
+  float t = x;
+  const int kind = nm.kind[f];
+  if (kind == 1) t = logf(fmaxf(x, 1e-30f));
+  else if (kind == 2) t = asinhf(x / nm.scale[f]);
+  return (t - nm.mean[f]) / nm.std[f];
+}
+
+}  // namespace
+
+// The tile pipeline shared by the closure and the standalone forward pass.  load(r, v)
+// fills the 8 standardised inputs of row r; store(r, o) receives the 3 network outputs
+// (bias included).  err receives 1 if a wait ran out (results then incomplete).
+template <class Load, class Store>
+__device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nrows, Load load, Store store, int* err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  const int t = threadIdx.x, warp = t >> 5;
+  const int ntiles = (nrows + ROWS - 1) / ROWS;
+  // stage the weight image (bf16, core-matrix layout) and allocate TMEM
+  for (int q = t; q < W_IMAGE / 16; q += ROWS) reinterpret_cast<uint4*>(sm)[q] = reinterpret_cast<const uint4*>(wimg)[q];
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  fence_async_smem();
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tm = tmem_base;
+  const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+  const uint32_t s0 = smem_u32(sm);
+  uint32_t phase = 0;
+  const float* b1 = bias;
+  const float* b2 = bias + HID;
+  const float* b3 = bias + 2 * HID;
+
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r = tile * ROWS + t;
+    const bool live = r < nrows;
+    float v[HID];
+    for (int f = 0; f < K1; ++f) v[f] = 0.f;
+    if (live) load(r, v);
+    store_row(sm + S_A1, 256, t, v, K1);
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    for (int layer = 0; layer < 3; ++layer) {
+      if (t == 0) {
+        fence_after();
+        if (layer == 0) {
+          mma_bf16(tm + 0, sdesc(s0 + S_A1, CORE, 256), sdesc(s0 + S_W1, CORE, 256), idesc_bf16(ROWS, HID), false);
+        } else {
+          const uint32_t dcol = layer == 1 ? 64u : 0u;
+          const uint32_t bw = layer == 1 ? S_W2 : S_W3;
+          const uint32_t idesc = idesc_bf16(ROWS, layer == 1 ? HID : NOUT);
+          for (int s = 0; s < HID / 16; ++s)
+            mma_bf16(tm + dcol, sdesc(s0 + S_A2 + s * 2 * CORE, CORE, 1024), sdesc(s0 + bw + s * 2 * CORE, CORE, 1024),
+                     idesc, s > 0);
+        }
+        mma_commit(&mbar);
+      }
+      const bool ok = mbar_wait(&mbar, phase & 1);
+      phase += 1;
+      if (!ok) {
+        atomicExch(&abort_flag, 1);
+        atomicExch(err, 1);
+      }
+      __syncthreads();
+      if (abort_flag) break;
+      fence_after();
+      if (layer < 2) {
+        const uint32_t dcol = layer == 0 ? 0u : 64u;
+        const float* bb = layer == 0 ? b1 : b2;
+        for (int c = 0; c < HID / 16; ++c) tmem_ld16(tm + lane_off + dcol + 16 * c, v + 16 * c);
+        for (int j = 0; j < HID; ++j) v[j] = gelu(v[j] + bb[j]);
+        store_row(sm + S_A2, 1024, t, v, HID);
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+      } else {
+        float o[16];
+        tmem_ld16(tm + lane_off + 0, o);
+        fence_before();
+        if (live) {
+          for (int c = 0; c < 3; ++c) o[c] += b3[c];
+          store(r, o);
+        }
+        __syncthreads();
+      }
+    }
+    if (abort_flag) break;
+  }
+  // give the tensor memory back (every issued MMA has completed or the wait ran out)
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(TMEM_COLS));
+  }
+}
+
+// The closure step: rows are (level K, node I) with r = (K-2)*M + (I-1).
+__global__ void __launch_bounds__(ROWS, 1) k_closure_mlp(const Dev P, int* err) {
+  const int nrows = P.M * (P.KBM1 - 1);
+  const size_t S = (size_t)nrows;
+  const ClosNorm& nm = P.clos_norm;
+  auto load = [&](int r, float* v) {
+    for (int f = 0; f < CLOS_IN; ++f) v[f] = feat_transform(nm, f, P.clos_feat[(size_t)f * S + r]);
+  };
+  auto store = [&](int r, const float* o) {
+    const int k = r / P.M + 2, i = r % P.M + 1;
+    const size_t q = N3(P, i, k);
+    const bool use_net = P.clos_env[i] != 0;
+    double nw[3];
+    for (int c = 0; c < 3; ++c) {
+      if (use_net) {
+        float y = o[c] * nm.tstd[c] + nm.tmean[c];
+        nw[c] = (double)expf(y) - (double)nm.teps;
+        if (nw[c] < 0.0) nw[c] = 0.0;
+      } else {
+        nw[c] = P.clos_plain[(size_t)c * S + r];  // MY2.5, FP64
+      }
+    }
+    P.kq[q] = 0.5 * (nw[0] + P.kq[q]);
+    P.km[q] = 0.5 * (nw[1] + P.km[q]);
+    P.kh[q] = 0.5 * (nw[2] + P.kh[q]);
+  };
+  mlp_tc_tiles(P.clos_w, P.clos_b, nrows, load, store, err);
+}
+
+// Standalone BF16 forward pass on standardised inputs x [n][8] -> out [n][3].
+__global__ void __launch_bounds__(ROWS, 1) k_mlp_tc_forward(const void* wimg, const float* bias, const float* x,
+                                                            int n, float* out, int* err) {
+  auto load = [&](int r, float* v) {
+    for (int f = 0; f < CLOS_IN; ++f) v[f] = x[(size_t)r * CLOS_IN + f];
+  };
+  auto store = [&](int r, const float* o) {
+    for (int c = 0; c < 3; ++c) out[(size_t)r * 3 + c] = o[c];
+  };
+  mlp_tc_tiles(wimg, bias, n, load, store, err);
+}
+
+// VDIF_Q's averaging of shallow columns (vdif_q.F:494-512) after the learned update.
+__global__ void k_closure_shallow(const Dev P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M || P.h[i] > P.static_ssh_adj) return;
+  const int KBM1 = P.KBM1;
+  double kqt = 0.0, kmt = 0.0, kht = 0.0;
+  for (int k = 2; k <= KBM1; ++k) { kqt = kqt + P.kq[N3(P, i, k)]; kmt = kmt + P.km[N3(P, i, k)]; kht = kht + P.kh[N3(P, i, k)]; }
+  kqt = kqt / (double)(KBM1 - 1);
+  kmt = kmt / (double)(KBM1 - 1);
+  kht = kht / (double)(KBM1 - 1);
+  for (int k = 2; k <= KBM1; ++k) { P.kq[N3(P, i, k)] = kqt; P.km[N3(P, i, k)] = kmt; P.kh[N3(P, i, k)] = kht; }
+}
+
+size_t closure_smem_bytes() { return (size_t)S_END; }
+size_t closure_weight_image_bytes() { return (size_t)W_IMAGE; }
+
+void launch_closure(const Dev& P, cudaStream_t s, int* err, int grid) {
+  k_closure_mlp<<<grid, ROWS, S_END, s>>>(P, err);
+  k_closure_shallow<<<(P.M + 127) / 128, 128, 0, s>>>(P);
+}
+
+int closure_setup_attrs() {
+  if (cudaFuncSetAttribute(k_closure_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S_END) != cudaSuccess)
+    return 1;
+  if (cudaFuncSetAttribute(k_mlp_tc_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S_END) != cudaSuccess)
+    return 1;
+  return 0;
+}
+
+void launch_mlp_tc_forward(const void* wimg, const float* bias, const float* x, int n, float* out, int* err, int grid,
+                           cudaStream_t s) {
+  k_mlp_tc_forward<<<grid, ROWS, S_END, s>>>(wimg, bias, x, n, out, err);
+}
+
+// Round to nearest even BF16: the IEEE binary32 bits with the low 16 discarded, rounding
+// half to even on the discarded part.
+static uint16_t bf16_rne(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)(u >> 16 | ((u & 0xFFFF) ? 0x40 : 0));
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+// Element (n, k) of a K-major matrix in core matrices of 8 rows x 8 elements, core (g, c)
+// at g*sbo + c*128 bytes.
+static void put_core(std::vector<uint8_t>& img, size_t base, int sbo, int n, int k, uint16_t v) {
+  size_t off = base + (size_t)(n / 8) * sbo + (size_t)(k / 8) * 128 + (size_t)(n % 8) * 16 + (size_t)(k % 8) * 2;
+  img[off] = (uint8_t)(v & 0xFF);
+  img[off + 1] = (uint8_t)(v >> 8);
+}
+
+void closure_weight_image(const float* params, std::vector<uint8_t>& img, std::vector<float>& bias) {
+  const float* W1 = params;
+  const float* B1 = W1 + 64 * 8;
+  const float* W2 = B1 + 64;
+  const float* B2 = W2 + 64 * 64;
+  const float* W3 = B2 + 64;
+  const float* B3 = W3 + 3 * 64;
+  img.assign(W_IMAGE, 0);
+  for (int n = 0; n < 64; ++n)
+    for (int k = 0; k < 8; ++k) put_core(img, S_W1, 256, n, k, bf16_rne(W1[n * 8 + k]));
+  for (int n = 0; n < 64; ++n)
+    for (int k = 0; k < 64; ++k) put_core(img, S_W2, 1024, n, k, bf16_rne(W2[n * 64 + k]));
+  for (int n = 0; n < 3; ++n)
+    for (int k = 0; k < 64; ++k) put_core(img, S_W3, 1024, n, k, bf16_rne(W3[n * 64 + k]));
+  bias.assign(2 * HID + NOUT, 0.f);
+  for (int j = 0; j < 64; ++j) { bias[j] = B1[j]; bias[64 + j] = B2[j]; }
+  for (int j = 0; j < 3; ++j) bias[128 + j] = B3[j];
+}
+
+}  // namespace fvg

@@ -451,6 +451,11 @@ __global__ void __launch_bounds__(128) k_vdif_q(const Dev P, int copy_back) {
   wub = wub / fn;
   wvb = wvb / fn;
   Q2F[n3(KB)] = sqrt(wub * wub + wvb * wvb) * P.const1;
+  // closure samples: plane f of level k at clos_samp + f*ss + (k-2)*M + (i-1)
+  float* const cs = P.clos_samp;
+  bool in_env = wet;
+  const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
+  auto samp = [&](int f, int k, double v) { cs[(size_t)f * ss + (size_t)(k - 2) * P.M + (i - 1)] = (float)v; };
   for (int k = 1; k <= KB; ++k) {
     Q2[n3(k)] = fabs(Q2[n3(k)] + SMALL);
     Q2L[n3(k)] = fabs(Q2L[n3(k)]);
@@ -478,6 +483,28 @@ __global__ void __launch_bounds__(128) k_vdif_q(const Dev P, int copy_back) {
       double uk, vk;
       ring_mean(k, uk, vk);
       double den = P.dzz[n3(k - 1)] * d;
+      if (P.closure) {
+        // the network's inputs and the envelope test of this level
+        const float fv[CLOS_IN] = {(float)boygr[k],
+                                   (float)(((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den)),
+                                   (float)d, (float)P.z[n3(k)], (float)sqrt(utau2),
+                                   (float)sqrt(sqrt(wub * wub + wvb * wvb)), (float)Q2[n3(k)], (float)Q2L[n3(k)]};
+        const size_t r = (size_t)(k - 2) * P.M + (i - 1);
+        for (int f = 0; f < CLOS_IN; ++f) {
+          P.clos_feat[(size_t)f * ss + r] = fv[f];
+          if (!(fv[f] >= P.clos_norm.lo[f] && fv[f] <= P.clos_norm.hi[f])) in_env = false;
+        }
+      }
+      if (cs) {
+        samp(0, k, boygr[k]);
+        samp(1, k, ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den));
+        samp(2, k, d);
+        samp(3, k, P.z[n3(k)]);
+        samp(4, k, sqrt(utau2));
+        samp(5, k, sqrt(sqrt(wub * wub + wvb * wvb)));
+        samp(6, k, Q2[n3(k)]);
+        samp(7, k, Q2L[n3(k)]);
+      }
       prod[k] = prod[k] + P.km[n3(k)] * SEF * ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den);
       prod[k] = prod[k] + P.kh[n3(k)] * boygr[k];
       ukm1 = uk;
@@ -548,11 +575,26 @@ __global__ void __launch_bounds__(128) k_vdif_q(const Dev P, int copy_back) {
     double sm = (coef3 + sh * COEF4 * gh[k]) / (1. - COEF5 * gh[k]);
     double kn = L[n3(k)] * sqrt(Q2[n3(k)]);
     size_t q = n3(k);
+    if (cs && k >= 2 && k <= KBM1) {
+      samp(8, k, kn * KAPPA * sm);
+      samp(9, k, kn * sm);
+      samp(10, k, kn * sh * P.vprnu);
+      samp(11, k, wet ? 1.0 : 0.0);
+    }
+    if (P.closure && k >= 2 && k <= KBM1) {
+      // interior levels are finished by the network kernel (k_closure_mlp)
+      const size_t r = (size_t)(k - 2) * P.M + (i - 1);
+      P.clos_plain[r] = kn * KAPPA * sm;
+      P.clos_plain[ss + r] = kn * sm;
+      P.clos_plain[2 * ss + r] = kn * sh * P.vprnu;
+      continue;
+    }
     P.kq[q] = 0.5 * (kn * KAPPA * sm + P.kq[q]);
     P.km[q] = 0.5 * (kn * sm + P.km[q]);
     P.kh[q] = 0.5 * (kn * sh * P.vprnu + P.kh[q]);
   }
-  if (P.h[i] <= P.static_ssh_adj) {
+  if (P.closure) P.clos_env[i] = in_env ? 1 : 0;
+  if (!P.closure && P.h[i] <= P.static_ssh_adj) {
     double kqt = 0.0, kmt = 0.0, kht = 0.0;
     for (int k = 2; k <= KBM1; ++k) { kqt = kqt + P.kq[n3(k)]; kmt = kmt + P.km[n3(k)]; kht = kht + P.kh[n3(k)]; }
     kqt = kqt / (double)(KBM1 - 1);

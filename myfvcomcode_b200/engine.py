@@ -233,3 +233,117 @@ class Fvcom(CEngine):
         self.lib.fvg_time_steps.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]
         self._check(self.lib.fvg_time_steps(self.h, int(n), C.byref(ms)), "time_steps")
         return ms.value
+
+
+class Group:
+    """Several Fvcom models stepped together by one CUDA graph per internal step."""
+
+    def __init__(self, models):
+        self.models = list(models)
+        self.lib = self.models[0].lib
+        arr = (C.c_void_p * len(self.models))(*[m.h for m in self.models])
+        g = C.c_void_p()
+        self.lib.fvg_group_create.argtypes = [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]
+        rc = self.lib.fvg_group_create(arr, len(self.models), C.byref(g))
+        if rc != 0:
+            raise FvgError("fvg_group_create failed with status %d" % rc)
+        self.g = g
+
+    def _check(self, rc, what):
+        if rc != 0:
+            self.lib.fvg_group_last_error.argtypes = [C.c_void_p]
+            self.lib.fvg_group_last_error.restype = C.c_char_p
+            raise FvgError("%s failed with status %d %s" % (what, rc, self.lib.fvg_group_last_error(self.g).decode()))
+
+    def run(self, n):
+        self.lib.fvg_group_run.argtypes = [C.c_void_p, C.c_int32]
+        self._check(self.lib.fvg_group_run(self.g, int(n)), "fvg_group_run")
+
+    def time_steps(self, n):
+        ms = C.c_double()
+        self.lib.fvg_group_time_steps.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]
+        self._check(self.lib.fvg_group_time_steps(self.g, int(n), C.byref(ms)), "fvg_group_time_steps")
+        return ms.value
+
+    def close(self):
+        if getattr(self, "g", None):
+            self.lib.fvg_group_destroy.argtypes = [C.c_void_p]
+            self.lib.fvg_group_destroy(self.g)
+            self.g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mlp:
+    """The learned closure's network (fvg_mlp_*): parameters on the device, trained by the
+    library's CUDA kernels.  Data arguments are device pointers (ints) to float32 arrays."""
+
+    def __init__(self, seed=0, lib_path=None):
+        self.lib = load_library(lib_path)
+        L = self.lib
+        L.fvg_mlp_create.argtypes = [C.c_uint64, C.POINTER(C.c_void_p)]
+        L.fvg_mlp_destroy.argtypes = [C.c_void_p]
+        L.fvg_mlp_last_error.argtypes = [C.c_void_p]
+        L.fvg_mlp_last_error.restype = C.c_char_p
+        L.fvg_mlp_num_params.restype = C.c_int32
+        fp = C.POINTER(C.c_float)
+        L.fvg_mlp_get_params.argtypes = [C.c_void_p, fp, C.c_int32]
+        L.fvg_mlp_set_params.argtypes = [C.c_void_p, fp, C.c_int32]
+        L.fvg_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, fp, fp]
+        L.fvg_mlp_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                    C.c_float, C.c_uint64, fp]
+        L.fvg_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+        L.fvg_mlp_device_params.argtypes = [C.c_void_p]
+        L.fvg_mlp_device_params.restype = C.c_void_p
+        h = C.c_void_p()
+        rc = L.fvg_mlp_create(int(seed), C.byref(h))
+        if rc != 0:
+            raise FvgError("fvg_mlp_create failed with status %d" % rc)
+        self.h = h
+        self.npar = int(L.fvg_mlp_num_params())
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise FvgError("%s failed with status %d %s" % (what, rc, self.lib.fvg_mlp_last_error(self.h).decode()))
+
+    def params(self):
+        out = np.zeros(self.npar, dtype=np.float32)
+        self._check(self.lib.fvg_mlp_get_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), self.npar),
+                    "fvg_mlp_get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(self.lib.fvg_mlp_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), self.npar),
+                    "fvg_mlp_set_params")
+
+    def loss_grad(self, x_ptr, y_ptr, n):
+        loss = C.c_float()
+        g = np.zeros(self.npar, dtype=np.float32)
+        self._check(self.lib.fvg_mlp_loss_grad(self.h, x_ptr, y_ptr, int(n), C.byref(loss),
+                                               g.ctypes.data_as(C.POINTER(C.c_float))), "fvg_mlp_loss_grad")
+        return loss.value, g
+
+    def train(self, x_ptr, y_ptr, n, epochs, batch, lr, seed=0):
+        hist = np.zeros(epochs, dtype=np.float32)
+        self._check(self.lib.fvg_mlp_train(self.h, x_ptr, y_ptr, int(n), int(epochs), int(batch), float(lr),
+                                           int(seed), hist.ctypes.data_as(C.POINTER(C.c_float))), "fvg_mlp_train")
+        return hist
+
+    def forward(self, x_ptr, n, out_ptr):
+        self._check(self.lib.fvg_mlp_forward(self.h, x_ptr, int(n), out_ptr), "fvg_mlp_forward")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fvg_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -101,6 +101,9 @@ def coldstart(case):
         ss, sb = init["s"]
         t1[1:, :KBM1] = tt + (tb - tt) * (-zz[1:, :KBM1])
         s1[1:, :KBM1] = ss + (sb - ss) * (-zz[1:, :KBM1])
+    if init.get("t_offset") is not None:
+        # ensemble perturbation of the initial temperature, per node (0:M)
+        t1[1:, :KBM1] += np.asarray(init["t_offset"], dtype=np.float64)[1:, None]
     rho1 = dens2(s1, t1)
     rho1[:, KB - 1] = 0.0
     rho1[0, :] = 0.0
