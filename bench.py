@@ -364,7 +364,7 @@ def main():
         if f.clock()[0] == n_done:
             plain["error_of_chosen_form"] = dict(compare(fp, f), internal_steps=n_done)
         fp.close()
-        day = os.path.join(ROOT, "profiles", "precision_error_coastal200k_k40_1day.json")
+        day = os.path.join(ROOT, "myfvcomcode_b200", "data", "precision_error_coastal200k_k40_1day.json")
         if os.path.exists(day):
             with open(day) as fh:
                 plain["error_after_1_day"] = json.load(fh).get("errors_vs_fp64")

@@ -200,6 +200,14 @@ int fvg_get_clock(const fvg_handle* h, int32_t* iint, double* ext_time);
 
 /* One INTERNAL_STEP for IINT+1 (fvcom.F:848-852), ISPLIT external steps included. */
 int fvg_internal_step(fvg_handle* h);
+/* One EXTERNAL_STEP (external_step.F:29) of external step IEXT (1..ISPLIT) of the current
+   internal step: the 4 Runge-Kutta stages with their boundary conditions, as
+   INTERNAL_STEP calls it at internal_step.F:499 (fvg_internal_step runs all ISPLIT). */
+int fvg_external_step(fvg_handle* h, int32_t iext);
+/* New forcing for the following steps (UPDATE_TIDE/UPDATE_RIVERS/UPDATE_WIND,
+   mod_force.F:14341, :11229, :13415): tidal constituents (same NTIDE as at creation),
+   river discharge/T/S and surface stress; NULL members are left unchanged. */
+int fvg_set_forcing(fvg_handle* h, const fvg_forcing* f);
 /* n consecutive internal steps; replayed from a captured CUDA graph after the first. */
 int fvg_run(fvg_handle* h, int32_t nsteps);
 /* One reference routine (enum fvg_routine) on the current state, for parity checks. */

@@ -37,15 +37,31 @@ def channel_seed_case(seed, base_kw=None):
     return c
 
 
-def generate(n_target=5_000_000, seeds=8, spinup=360, every=5, base_kw=None):
-    """(X [n,8], Y [n,3]) float32 samples of MY2.5 from the seeded channel runs."""
+def coastal_seed_case(seed, npts=50000, kb=41):
+    """The coastal mesh (default 50k nodes, 40 layers) with a seeded wind and tidal phase."""
+    from . import cases
+    rng = np.random.default_rng(2000 + seed)
+    speed = rng.uniform(0.0, 12.0)
+    head = rng.uniform(0.0, 2 * np.pi)
+    phase = rng.uniform(0.0, 360.0)
+    c = cases.coastal_mesh(npts=npts, kb=kb, wind_speed=speed)
+    c["forcing"]["tide"]["phai"] = c["forcing"]["tide"]["phai"] + phase
+    c["forcing"]["wind"] = {"kind": "speed", "u": speed * np.cos(head), "v": speed * np.sin(head)}
+    c["name"] = c["name"] + "-seed%d" % seed
+    return c
+
+
+def generate(n_target=5_000_000, seeds=8, spinup=360, every=5, base_kw=None, source="channel"):
+    """(X [n,8], Y [n,3]) float32 samples of MY2.5 from seeded runs of the estuary channel
+    (``source`` "channel", the training set of the closure as specified) or of the 50k-node
+    coastal mesh ("coastal")."""
     import ctypes as C
     import torch
     from .engine import Fvcom
     per_seed = int(np.ceil(n_target / seeds))
     xs, ys = [], []
     for sd in range(seeds):
-        case = channel_seed_case(sd, base_kw)
+        case = channel_seed_case(sd, base_kw) if source == "channel" else coastal_seed_case(sd)
         f = Fvcom(case)
         M, K = f.M, f.KB - 1
         S = M * (K - 1)
@@ -243,10 +259,11 @@ def main():
     ap.add_argument("--out", default=None, help="write the trained network (.npz)")
     ap.add_argument("--eval-npts", type=int, default=200000)
     ap.add_argument("--eval-steps", type=int, default=200)
+    ap.add_argument("--source", default="channel", choices=["channel", "coastal"])
     args = ap.parse_args()
     from . import cases
     t0 = time.time()
-    X, Y = generate(args.samples)
+    X, Y = generate(args.samples, source=args.source)
     t1 = time.time()
     rng = np.random.default_rng(0)
     perm = rng.permutation(X.shape[0])
@@ -258,7 +275,7 @@ def main():
     pred = predict(trained, X[hold][inside_h])
     ref = Y[hold][inside_h]
     rel = np.abs(pred - ref) / (np.abs(ref) + 1e-7)
-    report = {"samples": int(X.shape[0]), "generate_s": t1 - t0, "train_s": t2 - t1,
+    report = {"source": args.source, "samples": int(X.shape[0]), "generate_s": t1 - t0, "train_s": t2 - t1,
               "history": [float(h) for h in trained["history"]],
               "holdout": {"inside_envelope": float(inside_h.mean()),
                           "median_rel_err": [float(v) for v in np.median(rel, axis=0)],

@@ -791,6 +791,41 @@ int fvg_use_graph(fvg_handle* h, int32_t on) {
   return FVG_OK;
 }
 
+int fvg_external_step(fvg_handle* h, int32_t iext) {
+  if (!h || iext < 1 || iext > h->prm.isplit) return FVG_ERR_ARG;
+  return fvg_run_routine(h, FVG_R_EXTERNAL_STEP, iext);
+}
+
+int fvg_set_forcing(fvg_handle* h, const fvg_forcing* f) {
+  if (!h || !f) return FVG_ERR_ARG;
+  Dev& P = h->P;
+  if (f->ntide != h->ntide) { h->err = "fvg_set_forcing: ntide differs from fvg_create"; return FVG_ERR_ARG; }
+  const bool wind = f->wstress_x && f->wstress_y;
+  if (wind && !P.have_wind) { h->err = "fvg_set_forcing: the model was created without wind stress"; return FVG_ERR_UNSUPPORTED; }
+  CK(cudaStreamSynchronize(h->stream));
+  const size_t o1 = (size_t)P.iobcn + 1, q1 = (size_t)P.numqbc + 1, n1 = (size_t)P.N + 1;
+  const size_t nt = h->ntide;
+  if (nt) {
+    std::vector<double> apt(o1 * nt), ph(o1 * nt), em(o1, 0.0);
+    for (size_t q = 0; q < o1 * nt; ++q) { apt[q] = f->apt[q]; ph[q] = f->phai[q] * kPI2 / 360.0; }
+    for (size_t q = 0; q < o1; ++q) em[q] = f->emean ? f->emean[q] : 0.0;
+    for (size_t j = 0; j < nt; ++j) h->period[j] = f->period[j];
+    CK(cudaMemcpy((void*)P.apt, apt.data(), apt.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)P.phai_rad, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)P.emean, em.data(), em.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (P.numqbc > 0) {
+    if (f->qdis) CK(cudaMemcpy((void*)P.qdis0, f->qdis, q1 * sizeof(double), cudaMemcpyHostToDevice));
+    if (f->tdis) CK(cudaMemcpy((void*)P.tdis, f->tdis, q1 * sizeof(double), cudaMemcpyHostToDevice));
+    if (f->sdis) CK(cudaMemcpy((void*)P.sdis, f->sdis, q1 * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (wind) {
+    CK(cudaMemcpy((void*)P.wsx, f->wstress_x, n1 * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)P.wsy, f->wstress_y, n1 * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  return FVG_OK;
+}
+
 int fvg_set_precision(fvg_handle* h, int32_t mode) {
   if (!h) return FVG_ERR_ARG;
   if (mode != FVG_PREC_FP64 && mode != FVG_PREC_FP32_FLUX) { h->err = "unknown precision mode"; return FVG_ERR_ARG; }
@@ -869,7 +904,7 @@ int fvg_set_closure(fvg_handle* h, int32_t mode, const float* params, int32_t np
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    h->clos_grid = 2 * nsm;
+    h->clos_grid = 4 * nsm;
   }
   std::vector<uint8_t> img;
   std::vector<float> bias;

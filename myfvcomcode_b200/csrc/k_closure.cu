@@ -149,8 +149,9 @@ __device__ inline float feat_transform(const ClosNorm& nm, int f, float x) {
 // The tile pipeline shared by the closure and the standalone forward pass.  load(r, v)
 // fills the 8 standardised inputs of row r; store(r, o) receives the 3 network outputs
 // (bias included).  err receives 1 if a wait ran out (results then incomplete).
-template <class Load, class Store>
-__device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nrows, Load load, Store store, int* err) {
+template <class Load, class Store, class Need>
+__device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nrows, Load load, Store store, Need need,
+                                    int* err) {
   extern __shared__ __align__(1024) uint8_t sm[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_base;
@@ -184,6 +185,12 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int r = tile * ROWS + t;
     const bool live = r < nrows;
+    // a tile none of whose rows uses the network skips the tensor cores
+    if (!__syncthreads_or(live && need(r))) {
+      float o[16] = {};
+      if (live) store(r, o);
+      continue;
+    }
     float v[HID];
     for (int f = 0; f < K1; ++f) v[f] = 0.f;
     if (live) load(r, v);
@@ -272,7 +279,8 @@ __global__ void __launch_bounds__(ROWS, 1) k_closure_mlp(const Dev P, int* err) 
     P.km[q] = 0.5 * (nw[1] + P.km[q]);
     P.kh[q] = 0.5 * (nw[2] + P.kh[q]);
   };
-  mlp_tc_tiles(P.clos_w, P.clos_b, nrows, load, store, err);
+  auto need = [&](int r) { return P.clos_env[r % P.M + 1] != 0; };
+  mlp_tc_tiles(P.clos_w, P.clos_b, nrows, load, store, need, err);
 }
 
 // Standalone BF16 forward pass on standardised inputs x [n][8] -> out [n][3].
@@ -284,7 +292,8 @@ __global__ void __launch_bounds__(ROWS, 1) k_mlp_tc_forward(const void* wimg, co
   auto store = [&](int r, const float* o) {
     for (int c = 0; c < 3; ++c) out[(size_t)r * 3 + c] = o[c];
   };
-  mlp_tc_tiles(wimg, bias, n, load, store, err);
+  auto need = [](int) { return true; };
+  mlp_tc_tiles(wimg, bias, n, load, store, need, err);
 }
 
 // VDIF_Q's averaging of shallow columns (vdif_q.F:494-512) after the learned update.

@@ -173,3 +173,33 @@ def test_autotuner_returns_a_timed_shape(small_channel):
     r = autotune.autotune(small_channel, cands=[(64, 1), (128, 5)], steps=2, warmup=1)
     assert (r["col_threads"], r["col_layers"]) in [(64, 1), (128, 5)]
     assert len(r["table"]) == 2 and all(t[0] > 0 for t in r["table"])
+
+
+def test_set_forcing_and_external_step(small_coastal):
+    import ctypes as C
+    from myfvcomcode_b200 import abi
+    from myfvcomcode_b200.engine import Fvcom
+    a, b, c = Fvcom(small_coastal), Fvcom(small_coastal), Fvcom(small_coastal)
+    _, _, fs, keep = abi.make_structs(small_coastal)
+    b.lib.fvg_set_forcing.argtypes = [C.c_void_p, C.c_void_p]
+    assert b.lib.fvg_set_forcing(b.h, C.byref(fs)) == 0  # the same forcing: no change
+    ws = abi.wind_stress(small_coastal)
+    sx = np.ascontiguousarray(ws[0] * 2.0)
+    sy = np.ascontiguousarray(ws[1] * 2.0)
+    fs2 = abi.FvgForcing()
+    C.pointer(fs2)[0] = fs
+    fs2.wstress_x = sx.ctypes.data_as(C.POINTER(C.c_double))
+    fs2.wstress_y = sy.ctypes.data_as(C.POINTER(C.c_double))
+    assert c.lib.fvg_set_forcing(c.h, C.byref(fs2)) == 0
+    for m in (a, b, c):
+        m.run(3)
+    assert np.array_equal(a.get("el"), b.get("el")) and np.array_equal(a.get("u"), b.get("u"))
+    assert not np.array_equal(a.get("u"), c.get("u"))
+    # one EXTERNAL_STEP through its own entry point equals the routine call
+    d, e = Fvcom(small_coastal), Fvcom(small_coastal)
+    d.lib.fvg_external_step.argtypes = [C.c_void_p, C.c_int32]
+    assert d.lib.fvg_external_step(d.h, 1) == 0
+    e.routine("EXTERNAL_STEP", 1)
+    for n in ("el", "ua", "va", "elf"):
+        assert np.array_equal(d.get(n), e.get(n)), n
+    assert d.lib.fvg_external_step(d.h, 0) == 1
