@@ -395,6 +395,34 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
       for (int s = 0; s < 3; ++s) ce[3 * i + s] = cl[i][s];
     }
     UPI(cell_edge, ce.data(), ce.size());
+    // Slot table of the edge loops: slot s of cell i at s*(N+1) + i, the edges in the
+    // order of cell_edge.  code = edge*4 + ISBC*2 + side; offsets XIJC-XC of both ends.
+    {
+      const size_t S3 = 3 * n1;
+      std::vector<int> cc(S3, 0), ca(S3, 0), cb(S3, 0), cj1(S3, 0), cj2(S3, 0);
+      std::vector<double> xa(S3, 0.0), ya(S3, 0.0), xb(S3, 0.0), yb(S3, 0.0), dx(S3, 0.0), dy(S3, 0.0);
+      for (size_t i = 1; i < n1; ++i)
+        for (int sl = 0; sl < 3; ++sl) {
+          const int code = cl[i][sl], e = code >> 1, side = code & 1;
+          const size_t q = (size_t)sl * n1 + i;
+          const int ia = m->iec[e], ib = m->iec[e1 + e];
+          cc[q] = e * 4 + (m->isbc[e] != 0 ? 2 : 0) + side;
+          ca[q] = ia;
+          cb[q] = ib;
+          cj1[q] = m->ienode[e];
+          cj2[q] = m->ienode[e1 + e];
+          xa[q] = m->xijc[e] - m->xc[ia];
+          ya[q] = m->yijc[e] - m->yc[ia];
+          xb[q] = m->xijc[e] - m->xc[ib];
+          yb[q] = m->yijc[e] - m->yc[ib];
+          dx[q] = m->dltxc[e];
+          dy[q] = m->dltyc[e];
+        }
+      UPI(ce_code, cc.data(), S3); UPI(ce_ia, ca.data(), S3); UPI(ce_ib, cb.data(), S3);
+      UPI(ce_j1, cj1.data(), S3); UPI(ce_j2, cj2.data(), S3);
+      UPD(ce_xoa, xa.data(), S3); UPD(ce_yoa, ya.data(), S3); UPD(ce_xob, xb.data(), S3);
+      UPD(ce_yob, yb.data(), S3); UPD(ce_dx, dx.data(), S3); UPD(ce_dy, dy.data(), S3);
+    }
     std::vector<std::vector<int>> ch(n1);
     for (int he = 1; he <= m->ncv; ++he) ch[m->ntrg[he]].push_back(he);
     std::vector<int> chv(3 * n1, 0);
@@ -551,6 +579,9 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
       if ((rc = dalloc(h, &P.gt[t][g], ms * KB))) return fail(rc);
     }
   if ((rc = dalloc(h, &P.budget, 3 + 3 * 148))) return fail(rc);
+  for (double** pp : {&P.vq_prod, &P.vq_gh, &P.vq_dtef, &P.vq_dtefl})
+    if ((rc = dalloc(h, pp, ms * KB))) return fail(rc);
+  if ((rc = dalloc(h, &P.vq_ut, ms))) return fail(rc);
   P.ncvs = (int)pad32(m->ncv + 1);
   for (int q = 0; q < 4; ++q) {
     if ((rc = dalloc(h, &P.g2d[q], n1))) return fail(rc);
@@ -764,8 +795,8 @@ int32_t fvg_kernels_per_step(const fvg_handle* h) {
   int n = 1 + 1 + 2 + 2 + 2;                                // begin, cell_pre, grad3+adv3d, baropg+prep, int advave+reset
   n += p.isplit * 4 * (3 + (p.wetting_drying_on ? 2 : 0)); // RK stages
   n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv
-  n += 4;                                                  // grad_q, adv_q (2 phases), vdif_q
-  if (h->P.closure) n += 2;                                // learned closure, shallow columns
+  n += 7;                                                  // grad_q, adv_q (2 phases), vdif_q (4 passes)
+  if (h->P.closure) n += 1;                                // learned closure
   if (p.temperature_active || p.salinity_active)           // grad_ts, adv_ts (2 phases), vdif_ts,
     n += 5 + (h->P.iobcn > 0 ? 1 : 0);                     // bcond_ts (rivers, open boundary)
   n += 1;                                                  // final
@@ -859,6 +890,8 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     if ((rc = dalloc(h, &f.dltye, v1))) return fail(rc);
     if ((rc = dalloc(h, &f.dltxncve, 2 * vi1))) return fail(rc);
     if ((rc = dalloc(h, &f.dltyncve, 2 * vi1))) return fail(rc);
+    for (float** pp : {&f.ce_xoa, &f.ce_yoa, &f.ce_xob, &f.ce_yob, &f.ce_dx, &f.ce_dy})
+      if ((rc = dalloc(h, pp, 3 * n1))) return fail(rc);
     launch_make_f32(P, h->stream);
     CK(cudaGetLastError());
   }

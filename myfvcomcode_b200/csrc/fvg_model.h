@@ -46,6 +46,7 @@ struct F32 {
   float2* ex2;
   float *xo, *yo, *dltxc, *dltyc, *art, *cc_hvc, *a1u, *a2u;
   float *dltxe, *dltye, *dltxncve, *dltyncve;
+  float *ce_xoa, *ce_yoa, *ce_xob, *ce_yob, *ce_dx, *ce_dy;
 };
 
 // Input and output scaling of the learned closure's network, and the training envelope.
@@ -93,6 +94,11 @@ struct Dev {
   // ----- gather lists -----
   const int *node_he_ptr, *node_he;   // node -> half-edges (id*2 + side), ascending id
   const int *cell_edge;               // cell -> its 3 edges (id*2 + side), ascending id
+  // Slot table of the cell edge loops, slot s of cell i at s*(N+1) + i (edges in the order
+  // of cell_edge): code = edge*4 + ISBC*2 + side, the two cells, the two nodes, the edge
+  // offsets XIJC-XC / YIJC-YC of both cells, DLTXC, DLTYC.  Read coalesced by cell.
+  const int *ce_code, *ce_ia, *ce_ib, *ce_j1, *ce_j2;
+  const double *ce_xoa, *ce_yoa, *ce_xob, *ce_yob, *ce_dx, *ce_dy;
   const int *cell_he;                 // cell -> its 3 control-volume half-edges (NTRG(he) == cell)
   // ----- open boundary -----
   const int *i_obc_n, *next_obc, *node_obc;  // node_obc[node] = OBC index (0 = none)
@@ -135,6 +141,8 @@ struct Dev {
   double *gq[2][6];  // ADV_Q of Q2 / Q2L: PQPX, PQPY, PQPXD, PQPYD, ring min, ring max
   double *gt[2][6];  // ADV_T / ADV_S: the same six per tracer
   double* budget;                            // 3 doubles
+  // VDIF_Q between its passes: PROD, GH, DTEF, the q2l DTEF (node 3-D) and UTAU2 (node)
+  double *vq_prod, *vq_gh, *vq_dtef, *vq_dtefl, *vq_ut;
   double2* ex2;                              // half-edge fluxes of both advected tracers (ncvs x KB)
   double* g2d[4];                            // least-squares gradient of UA, VA per cell (COFA1/2/5/6)
   double* exf2d;                             // EXTEL_EDGE flux of each half-edge (NCV+1)
@@ -196,6 +204,12 @@ template <> struct Mesh<double> {
   __device__ static double yoa(const Dev& P, int e, int ia) { return P.yijc[e] - P.yc[ia]; }
   __device__ static double xob(const Dev& P, int e, int ib) { return P.xijc[e] - P.xc[ib]; }
   __device__ static double yob(const Dev& P, int e, int ib) { return P.yijc[e] - P.yc[ib]; }
+  __device__ static double s_xoa(const Dev& P, size_t q) { return P.ce_xoa[q]; }
+  __device__ static double s_yoa(const Dev& P, size_t q) { return P.ce_yoa[q]; }
+  __device__ static double s_xob(const Dev& P, size_t q) { return P.ce_xob[q]; }
+  __device__ static double s_yob(const Dev& P, size_t q) { return P.ce_yob[q]; }
+  __device__ static double s_dx(const Dev& P, size_t q) { return P.ce_dx[q]; }
+  __device__ static double s_dy(const Dev& P, size_t q) { return P.ce_dy[q]; }
   __device__ static double dltxc(const Dev& P, int e) { return P.dltxc[e]; }
   __device__ static double dltyc(const Dev& P, int e) { return P.dltyc[e]; }
   __device__ static double art(const Dev& P, int c) { return P.art[c]; }
@@ -218,6 +232,12 @@ template <> struct Mesh<float> {
   __device__ static float yoa(const Dev& P, int e, int) { return P.f.yo[e]; }
   __device__ static float xob(const Dev& P, int e, int) { return P.f.xo[(size_t)P.NE + 1 + e]; }
   __device__ static float yob(const Dev& P, int e, int) { return P.f.yo[(size_t)P.NE + 1 + e]; }
+  __device__ static float s_xoa(const Dev& P, size_t q) { return P.f.ce_xoa[q]; }
+  __device__ static float s_yoa(const Dev& P, size_t q) { return P.f.ce_yoa[q]; }
+  __device__ static float s_xob(const Dev& P, size_t q) { return P.f.ce_xob[q]; }
+  __device__ static float s_yob(const Dev& P, size_t q) { return P.f.ce_yob[q]; }
+  __device__ static float s_dx(const Dev& P, size_t q) { return P.f.ce_dx[q]; }
+  __device__ static float s_dy(const Dev& P, size_t q) { return P.f.ce_dy[q]; }
   __device__ static float dltxc(const Dev& P, int e) { return P.f.dltxc[e]; }
   __device__ static float dltyc(const Dev& P, int e) { return P.f.dltyc[e]; }
   __device__ static float art(const Dev& P, int c) { return P.f.art[c]; }
@@ -255,6 +275,7 @@ void launch_begin_step(const Dev& P, cudaStream_t s);
 void launch_ext_prep(const Dev& P, cudaStream_t s);
 void launch_make_f32(const Dev& P, cudaStream_t s);
 void launch_closure(const Dev& P, cudaStream_t s, int* err, int grid);
+void launch_vdif_q_shallow(const Dev& P, cudaStream_t s);
 size_t closure_smem_bytes();
 size_t closure_weight_image_bytes();
 int closure_setup_attrs();

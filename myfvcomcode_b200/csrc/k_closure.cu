@@ -115,7 +115,16 @@ __device__ inline void tmem_ld16(uint32_t taddr, float* v) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ inline float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU, tanh form, with the hardware tanh approximation (the network is trained with the
+// same form; the approximation error is far below the BF16 rounding of the activations).
+__device__ inline float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ inline float gelu(float z) {
+  return 0.5f * z * (1.0f + tanh_fast(0.79788456080286536f * (z + 0.044715f * z * z * z)));
+}
 
 __device__ inline uint32_t pack_bf16(float a, float b) {
   __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -124,8 +133,10 @@ __device__ inline uint32_t pack_bf16(float a, float b) {
 
 // Row r (0..127) of an activation tile with K columns (multiple of 8): 8 values per
 // 16-byte store at core (r/8, c) row r%8.
-__device__ inline void store_row(uint8_t* tile, int sbo, int r, const float* v, int k) {
-  for (int c = 0; c < k / 8; ++c) {
+template <int K>
+__device__ inline void store_row(uint8_t* tile, int sbo, int r, const float* v) {
+#pragma unroll
+  for (int c = 0; c < K / 8; ++c) {
     uint4 q;
     q.x = pack_bf16(v[8 * c + 0], v[8 * c + 1]);
     q.y = pack_bf16(v[8 * c + 2], v[8 * c + 3]);
@@ -192,9 +203,10 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
       continue;
     }
     float v[HID];
+#pragma unroll
     for (int f = 0; f < K1; ++f) v[f] = 0.f;
     if (live) load(r, v);
-    store_row(sm + S_A1, 256, t, v, K1);
+    store_row<K1>(sm + S_A1, 256, t, v);
     fence_async_smem();
     fence_before();
     __syncthreads();
@@ -225,9 +237,11 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
       if (layer < 2) {
         const uint32_t dcol = layer == 0 ? 0u : 64u;
         const float* bb = layer == 0 ? b1 : b2;
+#pragma unroll
         for (int c = 0; c < HID / 16; ++c) tmem_ld16(tm + lane_off + dcol + 16 * c, v + 16 * c);
+#pragma unroll
         for (int j = 0; j < HID; ++j) v[j] = gelu(v[j] + bb[j]);
-        store_row(sm + S_A2, 1024, t, v, HID);
+        store_row<HID>(sm + S_A2, 1024, t, v);
         fence_async_smem();
         fence_before();
         __syncthreads();
@@ -259,6 +273,7 @@ __global__ void __launch_bounds__(ROWS, 1) k_closure_mlp(const Dev P, int* err) 
   const size_t S = (size_t)nrows;
   const ClosNorm& nm = P.clos_norm;
   auto load = [&](int r, float* v) {
+#pragma unroll
     for (int f = 0; f < CLOS_IN; ++f) v[f] = feat_transform(nm, f, P.clos_feat[(size_t)f * S + r]);
   };
   auto store = [&](int r, const float* o) {
@@ -287,6 +302,7 @@ __global__ void __launch_bounds__(ROWS, 1) k_closure_mlp(const Dev P, int* err) 
 __global__ void __launch_bounds__(ROWS, 1) k_mlp_tc_forward(const void* wimg, const float* bias, const float* x,
                                                             int n, float* out, int* err) {
   auto load = [&](int r, float* v) {
+#pragma unroll
     for (int f = 0; f < CLOS_IN; ++f) v[f] = x[(size_t)r * CLOS_IN + f];
   };
   auto store = [&](int r, const float* o) {
@@ -296,7 +312,8 @@ __global__ void __launch_bounds__(ROWS, 1) k_mlp_tc_forward(const void* wimg, co
   mlp_tc_tiles(wimg, bias, n, load, store, need, err);
 }
 
-// VDIF_Q's averaging of shallow columns (vdif_q.F:494-512) after the learned update.
+// VDIF_Q's averaging of shallow columns (vdif_q.F:494-512), after the per-level update of
+// KQ, KM, KH (MY2.5 or the network).
 __global__ void k_closure_shallow(const Dev P) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.M || P.h[i] > P.static_ssh_adj) return;
@@ -311,6 +328,10 @@ __global__ void k_closure_shallow(const Dev P) {
 
 size_t closure_smem_bytes() { return (size_t)S_END; }
 size_t closure_weight_image_bytes() { return (size_t)W_IMAGE; }
+
+void launch_vdif_q_shallow(const Dev& P, cudaStream_t s) {
+  k_closure_shallow<<<(P.M + 127) / 128, 128, 0, s>>>(P);
+}
 
 void launch_closure(const Dev& P, cudaStream_t s, int* err, int grid) {
   k_closure_mlp<<<grid, ROWS, S_END, s>>>(P, err);

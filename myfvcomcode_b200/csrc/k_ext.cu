@@ -87,16 +87,18 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   // cell part: least-squares gradient of the current UA, VA for ADVAVE of this stage
   if ((parts & EN_GRAD) && i <= P.N) store_grad(P, i);
   if (i > P.M) return;
-  if (parts & EN_COPY_ELRK) P.elrk[i] = P.el[i];
-  const double alpha = dAlphaRK[K];
-  int ob = P.node_obc[i];
+  double x = 0.0;
   if (parts & EN_EXTEL) {
-    double x = 0.0;
     for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
       int e = P.node_he[q];
       double exflux = P.exf2d[e >> 1];
       x = (e & 1) ? x + exflux : x - exflux;
     }
+  }
+  if (parts & EN_COPY_ELRK) P.elrk[i] = P.el[i];
+  const double alpha = dAlphaRK[K];
+  int ob = P.node_obc[i];
+  if (parts & EN_EXTEL) {
     if (ob > 0) {
       P.xflux_obcn[ob] = x;
       x = 0.0;
@@ -163,38 +165,39 @@ __global__ void k_wet_nodes(const Dev P) {
   P.elf[i] = fmax(e, -P.h[i] + P.min_depth);
 }
 
-// ADVAVE_EDGE_GCN for one cell (advave_edge_gcn.F:115-1003, LIMITED_NO branch).  The
-// edge fluxes are evaluated in R; the surface-slope pressure gradient PSTX/PSTY stays FP64.
+// ADVAVE_EDGE_GCN for one cell (advave_edge_gcn.F:115-1003, LIMITED_NO branch), over the
+// cell's slot table.  The edge fluxes are evaluated in R; the surface-slope pressure
+// gradient PSTX/PSTY stays FP64.
 template <typename R>
 __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo, double& px, double& py) {
   typedef Mesh<R> Mh;
   const R half = (R)0.5, one = (R)1.0;
   R xf = 0, yf = 0;
   px = 0.0; py = 0.0;
-  const size_t e1 = P.NE + 1;
+  const size_t n1 = P.N + 1;
   const R epor = (R)P.epor[i], iucp = (R)P.iucp[i];
   for (int s = 0; s < 3; ++s) {
-    int code = P.cell_edge[3 * i + s];
-    int e = code >> 1;
-    int side = code & 1;
-    int ia = P.iec[e], ib = P.iec[e1 + e];
-    int j1 = P.ienode[e], j2 = P.ienode[e1 + e];
+    const size_t q = (size_t)s * n1 + i;
+    const int code = P.ce_code[q];
+    const int side = code & 1;
+    const int ia = P.ce_ia[q], ib = P.ce_ib[q];
+    const int j1 = P.ce_j1[q], j2 = P.ce_j2[q];
     R dij = (R)(0.5 * (P.d[j1] + P.d[j2]));
     double elij = 0.5 * (P.el[j1] + P.el[j2]);
     if (P.iswetce[ia] * P.iswetc[ia] == 1 || P.iswetce[ib] * P.iswetc[ib] == 1) {
       Grad<R> ga = load_grad<R>(P, ia);
-      R xij = Mh::xoa(P, e, ia);
-      R yij = Mh::yoa(P, e, ia);
+      R xij = Mh::s_xoa(P, q);
+      R yij = Mh::s_yoa(P, q);
       R uij1 = (R)P.ua[ia] + ga.ux * xij + ga.uy * yij;
       R vij1 = (R)P.va[ia] + ga.vx * xij + ga.vy * yij;
       Grad<R> gb = load_grad<R>(P, ib);
-      xij = Mh::xob(P, e, ib);
-      yij = Mh::yob(P, e, ib);
+      xij = Mh::s_xob(P, q);
+      yij = Mh::s_yob(P, q);
       R uij2 = (R)P.ua[ib] + gb.ux * xij + gb.uy * yij;
       R vij2 = (R)P.va[ib] + gb.vx * xij + gb.vy * yij;
       R uij = half * (uij1 + uij2);
       R vij = half * (vij1 + vij2);
-      const R dltxc = Mh::dltxc(P, e), dltyc = Mh::dltyc(P, e);
+      const R dltxc = Mh::s_dx(P, q), dltyc = Mh::s_dy(P, q);
       R un = -uij * dltyc + vij * dltxc;
       R viscof1 = Mh::art(P, ia) * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + half * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
       R viscof2 = Mh::art(P, ib) * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + half * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
@@ -208,7 +211,7 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
       R sg = fsign1(un);
       R xadv = dij * un * ((one - sg) * uij2 + (one + sg) * uij1) * half;
       R yadv = dij * un * ((one - sg) * vij2 + (one + sg) * vij1) * half;
-      R nb = one - (R)P.isbc[e];
+      R nb = one - (R)((code >> 1) & 1);
       if (side == 0) {
         xf = xf + (xadv + fxx * epor) * nb * iucp;
         yf = yf + (yadv + fyy * epor) * nb * iucp;
@@ -217,12 +220,13 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
         yf = yf - (yadv + fyy * epor) * nb * iucp;
       }
     }
+    const double edx = P.ce_dx[q], edy = P.ce_dy[q];
     if (side == 0) {
-      px = px - P.grav_e[i] * P.d1[i] * elij * P.dltyc[e];
-      py = py + P.grav_e[i] * P.d1[i] * elij * P.dltxc[e];
+      px = px - P.grav_e[i] * P.d1[i] * elij * edy;
+      py = py + P.grav_e[i] * P.d1[i] * elij * edx;
     } else {
-      px = px + P.grav_e[i] * P.d1[i] * elij * P.dltyc[e];
-      py = py - P.grav_e[i] * P.d1[i] * elij * P.dltxc[e];
+      px = px + P.grav_e[i] * P.d1[i] * elij * edy;
+      py = py - P.grav_e[i] * P.d1[i] * elij * edx;
     }
   }
   R w = (R)(P.iswetce[i] * P.iswetc[i]);
@@ -454,6 +458,12 @@ void launch_make_f32(const Dev& P, cudaStream_t s) {
   cvt(P.dltye, P.f.dltye, v1);
   cvt(P.dltxncve, P.f.dltxncve, 2 * vi1);
   cvt(P.dltyncve, P.f.dltyncve, 2 * vi1);
+  cvt(P.ce_xoa, P.f.ce_xoa, 3 * n1);
+  cvt(P.ce_yoa, P.f.ce_yoa, 3 * n1);
+  cvt(P.ce_xob, P.f.ce_xob, 3 * n1);
+  cvt(P.ce_yob, P.f.ce_yob, 3 * n1);
+  cvt(P.ce_dx, P.f.ce_dx, 3 * n1);
+  cvt(P.ce_dy, P.f.ce_dy, 3 * n1);
 }
 void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);

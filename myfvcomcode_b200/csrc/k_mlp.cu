@@ -1,5 +1,5 @@
 // k_mlp.cu - the network of the learned vertical closure: an MLP 8 -> 64 -> 64 -> 3 with
-// GELU on the two hidden layers, trained in FP32 by the kernels in this file (mean-squared
+// GELU (tanh form) on the two hidden layers, trained in FP32 by the kernels in this file (mean-squared
 // error, Adam).  Inference in BF16 on the tensor cores is in k_closure.cu; the FP32
 // forward pass here is its reference.
 //
@@ -32,9 +32,13 @@ constexpr int OW1 = 0, OB1 = OW1 + MH * MI, OW2 = OB1 + MH, OB2 = OW2 + MH * MH,
 constexpr int T = 64;        // samples per block
 constexpr int TS = T + 1;    // padded stride of the activation planes
 
-__device__ inline float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 z (1 + tanh(c (z + 0.044715 z^3))), c = sqrt(2/pi), and its
+// derivative.
+constexpr float kGc = 0.79788456080286536f, kGa = 0.044715f;
+__device__ inline float gelu(float z) { return 0.5f * z * (1.0f + tanhf(kGc * (z + kGa * z * z * z))); }
 __device__ inline float gelu_d(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  const float t = tanhf(kGc * (z + kGa * z * z * z));
+  return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGc * (1.0f + 3.0f * kGa * z * z);
 }
 
 // Shared-memory layout of k_mlp_fwd_bwd (floats).

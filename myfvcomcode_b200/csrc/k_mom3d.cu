@@ -153,14 +153,15 @@ __global__ void __launch_bounds__(256) k_grad3(const Dev P) {
   }
 }
 
+// q: the edge's slot in the cell slot table (offsets and DLTXC/DLTYC of the edge).
 template <typename R>
-__device__ inline EdgeFlux<R> edge_flux3(const Dev& P, int e, int ia, int ib, int k, R dij, bool exflux_form) {
+__device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib, int k, R dij, bool exflux_form) {
   typedef Mesh<R> Mh;
   const R half = (R)0.5, one = (R)1.0;
   const double* U = P.u + C3(P, 0, k);
   const double* V = P.v + C3(P, 0, k);
-  R xija = Mh::xoa(P, e, ia), yija = Mh::yoa(P, e, ia);
-  R xijb = Mh::xob(P, e, ib), yijb = Mh::yob(P, e, ib);
+  R xija = Mh::s_xoa(P, q), yija = Mh::s_yoa(P, q);
+  R xijb = Mh::s_xob(P, q), yijb = Mh::s_yob(P, q);
   G3<R> ga = load_g3<R>(P, ia, k);
   R uij1 = (R)U[ia] + ga.ux * xija + ga.uy * yija;
   R vij1 = (R)V[ia] + ga.vx * xija + ga.vy * yija;
@@ -176,7 +177,7 @@ __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, int e, int ia, int ib, in
   R txx = (ga.ux + gb.ux) * viscof;
   R tyy = (ga.vy + gb.vy) * viscof;
   R txy = half * (ga.uy + gb.uy + ga.vx + gb.vx) * viscof;
-  const R dltxc = Mh::dltxc(P, e), dltyc = Mh::dltyc(P, e);
+  const R dltxc = Mh::s_dx(P, q), dltyc = Mh::s_dy(P, q);
   EdgeFlux<R> f;
   f.fxx = dij * (txx * dltyc - txy * dltxc);
   f.fyy = dij * (txy * dltyc - tyy * dltxc);
@@ -227,19 +228,19 @@ __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
   int kb, ke;
   col_range(P, 1, P.KBM1, kb, ke);
   for (int k = kb; k <= ke; ++k) {
-  const size_t e1 = P.NE + 1;
+  const size_t n1 = P.N + 1;
   const R epor = (R)P.epor[i], three = (R)3.0;
   R xr = 0, yr = 0;
   for (int s = 0; s < 3; ++s) {
-    int code = P.cell_edge[3 * i + s];
-    int e = code >> 1, side = code & 1;
-    int ia = P.iec[e], ib = P.iec[e1 + e];
+    const size_t q = (size_t)s * n1 + i;
+    const int code = P.ce_code[q], side = code & 1, isbc = (code >> 1) & 1;
+    const int ia = P.ce_ia[q], ib = P.ce_ib[q];
     if (!(P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1)) continue;
-    int j1 = P.ienode[e], j2 = P.ienode[e1 + e];
+    const int j1 = P.ce_j1[q], j2 = P.ce_j2[q];
     R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
-    EdgeFlux<R> f = edge_flux3<R>(P, e, ia, ib, k, dij, false);
-    R isb = (R)P.isbc[e];
-    R tp = (R)((double)(float)(1 - P.isbc[e]) * P.epor[i]);
+    EdgeFlux<R> f = edge_flux3<R>(P, q, ia, ib, k, dij, false);
+    R isb = (R)isbc;
+    R tp = (R)((double)(float)(1 - isbc) * P.epor[i]);
     if (side == 0) {
       xr = xr + f.xadv * tp + (f.fxx + three * f.fxx * isb) * epor;
       yr = yr + f.yadv * tp + (f.fyy + three * f.fyy * isb) * epor;
@@ -386,13 +387,24 @@ __global__ void __launch_bounds__(256) k_vertvl_flux(const Dev P) {
   {
   double x = 0.0;
   if (P.isonb[i] != 2) {
-    for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
-      int e = P.node_he[q];
-      int he = e >> 1;
-      int c = P.ntrg[he];
-      double dij = P.dt1[c] * P.dz1[C3(P, c, k)];
-      double exflux = dij * (-P.u[C3(P, c, k)] * P.dltye[he] + P.v[C3(P, c, k)] * P.dltxe[he]);
-      x = (e & 1) ? x + exflux : x - exflux;
+    // EXFLUX of one half-edge; the entries are fetched two at a time and added in order
+    auto flux = [&](int he) {
+      const int c = P.ntrg[he];
+      const double dij = P.dt1[c] * P.dz1[C3(P, c, k)];
+      return dij * (-P.u[C3(P, c, k)] * P.dltye[he] + P.v[C3(P, c, k)] * P.dltxe[he]);
+    };
+    const int q1 = P.node_he_ptr[i + 1];
+    int q = P.node_he_ptr[i];
+    for (; q + 2 <= q1; q += 2) {
+      const int e0 = P.node_he[q], e1 = P.node_he[q + 1];
+      const double f0 = flux(e0 >> 1), f1 = flux(e1 >> 1);
+      x = (e0 & 1) ? x + f0 : x - f0;
+      x = (e1 & 1) ? x + f1 : x - f1;
+    }
+    for (; q < q1; ++q) {
+      const int e = P.node_he[q];
+      const double f = flux(e >> 1);
+      x = (e & 1) ? x + f : x - f;
     }
   }
   for (int q = P.node_riv_ptr[i]; q < P.node_riv_ptr[i + 1]; ++q) {
@@ -539,24 +551,24 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
   int kb, ke;
   col_range(P, 1, P.KBM1, kb, ke);
   for (int k = kb; k <= ke; ++k) {
-  const size_t e1 = P.NE + 1;
+  const size_t n1 = P.N + 1;
   double px = 0.0, py = 0.0;
   const R epor = (R)P.epor[i], three = (R)3.0;
   R xr = 0, yr = 0, vmr = 0;
   const double dz1i = P.dz1[C3(P, i, k)];
   const double gdd = P.grav_e[i] * P.dt1[i] * dz1i;
   for (int s = 0; s < 3; ++s) {
-    int code = P.cell_edge[3 * i + s];
-    int e = code >> 1, side = code & 1;
-    int ia = P.iec[e], ib = P.iec[e1 + e];
-    int j1 = P.ienode[e], j2 = P.ienode[e1 + e];
+    const size_t q = (size_t)s * n1 + i;
+    const int code = P.ce_code[q], side = code & 1, isbc = (code >> 1) & 1;
+    const int ia = P.ce_ia[q], ib = P.ce_ib[q];
+    const int j1 = P.ce_j1[q], j2 = P.ce_j2[q];
     double elij = 0.5 * (P.egf[j1] + P.egf[j2]);
     R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
     if (P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1) {
-      EdgeFlux<R> f = edge_flux3<R>(P, e, ia, ib, k, dij, true);
+      EdgeFlux<R> f = edge_flux3<R>(P, q, ia, ib, k, dij, true);
       vmr = vmr + f.viscof;
-      R isb = (R)P.isbc[e];
-      R tp = (R)((double)(float)(1 - P.isbc[e]) * P.epor[i]);
+      R isb = (R)isbc;
+      R tp = (R)((double)(float)(1 - isbc) * P.epor[i]);
       if (side == 0) {
         xr = xr + f.xadv * tp + (f.fxx + three * f.fxx * isb) * epor;
         yr = yr + f.yadv * tp + (f.fyy + three * f.fyy * isb) * epor;
@@ -565,12 +577,13 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
         yr = yr - f.yadv * tp - (f.fyy + three * f.fyy * isb) * epor;
       }
     }
+    const double edx = P.ce_dx[q], edy = P.ce_dy[q];
     if (side == 0) {
-      px = px - gdd * elij * P.dltyc[e];
-      py = py + gdd * elij * P.dltxc[e];
+      px = px - gdd * elij * edy;
+      py = py + gdd * elij * edx;
     } else {
-      px = px + gdd * elij * P.dltyc[e];
-      py = py - gdd * elij * P.dltxc[e];
+      px = px + gdd * elij * edy;
+      py = py - gdd * elij * edx;
     }
   }
   double x = (double)xr, y = (double)yr, vm = (double)vmr;

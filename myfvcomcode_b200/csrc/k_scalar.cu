@@ -308,14 +308,13 @@ __device__ inline double obc_xflux_adv(const Dev& P, int i, int k, int t) {
 
 // Signed sum of a node's half-edge fluxes on layer k, both tracers, in ascending
 // half-edge order (the order of the reference's scatter into XFLUX).
+// The loads are issued four entries at a time (codes, then fluxes) and added in order.
 template <typename R>
 __device__ inline double2 gather_he(const Dev& P, int q0, int q1, int k) {
   typedef typename Mesh<R>::R2 R2;
   const R2* EX = Mesh<R>::ex2(P) + (size_t)(k - 1) * P.ncvs;
   R x0 = 0, x1 = 0;
-  for (int q = q0; q < q1; ++q) {
-    int code = P.node_he[q];
-    R2 e = EX[code >> 1];
+  auto add = [&](int code, R2 e) {
     if (code & 1) {
       x0 = x0 - e.x;
       x1 = x1 - e.y;
@@ -323,6 +322,19 @@ __device__ inline double2 gather_he(const Dev& P, int q0, int q1, int k) {
       x0 = x0 + e.x;
       x1 = x1 + e.y;
     }
+  };
+  int q = q0;
+  for (; q + 4 <= q1; q += 4) {
+    const int c0 = P.node_he[q], c1 = P.node_he[q + 1], c2 = P.node_he[q + 2], c3 = P.node_he[q + 3];
+    const R2 e0 = EX[c0 >> 1], e1 = EX[c1 >> 1], e2 = EX[c2 >> 1], e3 = EX[c3 >> 1];
+    add(c0, e0);
+    add(c1, e1);
+    add(c2, e2);
+    add(c3, e3);
+  }
+  for (; q < q1; ++q) {
+    const int c = P.node_he[q];
+    add(c, EX[c >> 1]);
   }
   return make_double2((double)x0, (double)x1);
 }
@@ -398,51 +410,38 @@ __global__ void __launch_bounds__(256) k_fct_q(const Dev P, int parts) {
 // VDIF_Q, MY2.5 (vdif_q.F:119-513), one thread per node column.  With copy_back the
 // end-of-closure shift Q2=Q2F, Q2L=Q2LF (internal_step.F:1034-1035) follows.
 // -------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_vdif_q(const Dev P, int copy_back) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (i > P.M) return;
-  const double A1 = 0.92, B1 = 16.6, A2 = 0.74, B2 = 10.1, C1 = 0.08;
-  const double E1 = 1.80, E2 = 1.33, SEF = 1.00, KAPPA = 0.40;
-  const double SMALL = 1.e-8, GH_MAX = .0233, GH_MIN = -.281;
-  const double SURFL = 2.e+5, GHC = -6.0;
-  const double COEF4 = 18.0 * A1 * A1 + 9.0 * A1 * A2;
-  const double COEF5 = 9.0 * A1 * A2;
-  const int KB = P.KB, KBM1 = P.KBM1;
-  const double DTI = P.dti;
-  const double d = P.d[i];
-  const bool wet = P.iswetn[i] == 1;
-  double boygr[kMaxKBs], prod[kMaxKBs], gh[kMaxKBs], dtef[kMaxKBs], vh[kMaxKBs], vhp[kMaxKBs];
-  for (int k = 0; k <= KB; ++k) { boygr[k] = 0.0; prod[k] = 0.0; gh[k] = 0.0; dtef[k] = 0.0; vh[k] = 0.0; vhp[k] = 0.0; }
-  double* Q2 = P.q2;
-  double* Q2L = P.q2l;
-  double* Q2F = P.q2f;
-  double* Q2LF = P.q2lf;
-  double* L = P.l;
-  auto n3 = [&](int k) { return N3(P, i, k); };
-  for (int k = 2; k <= KBM1; ++k)
-    if (Q2F[n3(k)] <= SMALL || Q2LF[n3(k)] <= SMALL) { Q2F[n3(k)] = SMALL; Q2LF[n3(k)] = SMALL; }
-  auto Acoef = [&](int k) {
-    return wet ? -0.5 * DTI * (P.kq[n3(k + 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k)] * d * d) : 0.0;
-  };
-  auto Ccoef = [&](int k) {
-    return wet ? -0.5 * DTI * (P.kq[n3(k - 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k - 1)] * d * d) : 0.0;
-  };
-  // Surface and bottom boundary values (vdif_q.F:172-246).
+// VDIF_Q in three passes.  The reference's column loop (one node at a time) has only two
+// truly sequential parts, the tridiagonal sweeps of the q2 and q2l equations; everything
+// else is per level.  k_vdif_q_levels forms, per (node, level), every input of the sweeps
+// (the positivity fixes, BOYGR, the shear production PROD, the length scale L and its
+// limits, GH, DTEF and the q2l wall-function DTEF); k_vdif_q_sweep runs the two sweeps per
+// column; k_vdif_q_coef applies the stability functions per (node, level).  Each value is
+// computed with the reference's expression, so the result is bitwise that of the column
+// loop.
+namespace vq {
+constexpr double A1 = 0.92, B1 = 16.6, A2 = 0.74, B2 = 10.1, C1 = 0.08;
+constexpr double E1 = 1.80, E2 = 1.33, SEF = 1.00, KAPPA = 0.40;
+constexpr double SMALL = 1.e-8, GH_MAX = .0233, GH_MIN = -.281;
+constexpr double SURFL = 2.e+5, GHC = -6.0;
+}  // namespace vq
+
+// Surface stress magnitude UTAU2 and bottom stress magnitude of node i (vdif_q.F:172-246),
+// the NBVE means in ring order.
+__device__ inline void vq_stress(const Dev& P, int i, double& utau2, double& wub, double& wvb) {
   const size_t m1 = P.M + 1;
   const int nt = P.ntve[i];
-  double wus = 0.0, wvs = 0.0, wub = 0.0, wvb = 0.0;
+  double wus = 0.0, wvs = 0.0;
+  wub = 0.0;
+  wvb = 0.0;
   for (int j = 1; j <= nt; ++j) {
     int c = P.nbve[(size_t)(j - 1) * m1 + i];
     wus = wus + P.wusurf[c];
     wvs = wvs + P.wvsurf[c];
   }
-  double fn = (double)(float)nt;
+  const double fn = (double)(float)nt;
   wus = wus / fn;
   wvs = wvs / fn;
-  double utau2 = sqrt(wus * wus + wvs * wvs);
-  vhp[1] = P.vhp1c * utau2;
-  vh[1] = 0.0;
-  double l0 = SURFL * utau2 / P.grav_n[i];
+  utau2 = sqrt(wus * wus + wvs * wvs);
   for (int j = 1; j <= nt; ++j) {
     int c = P.nbve[(size_t)(j - 1) * m1 + i];
     wub = wub + P.wubot[c];
@@ -450,160 +449,231 @@ __global__ void __launch_bounds__(128) k_vdif_q(const Dev P, int copy_back) {
   }
   wub = wub / fn;
   wvb = wvb / fn;
-  Q2F[n3(KB)] = sqrt(wub * wub + wvb * wvb) * P.const1;
-  // closure samples: plane f of level k at clos_samp + f*ss + (k-2)*M + (i-1)
+}
+
+__global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
+  using namespace vq;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  int kb, ke;
+  col_range(P, 1, P.KB, kb, ke);
+  const int KB = P.KB, KBM1 = P.KBM1;
+  const double d = P.d[i];
+  const bool wet = P.iswetn[i] == 1;
+  double* Q2 = P.q2;
+  double* Q2L = P.q2l;
+  double* L = P.l;
+  auto n3 = [&](int k) { return N3(P, i, k); };
+  double utau2, wub, wvb;
+  vq_stress(P, i, utau2, wub, wvb);
+  const double l0 = SURFL * utau2 / P.grav_n[i];
+  if (kb == 1) P.vq_ut[i] = utau2;
+  if (ke == KB) P.q2f[n3(KB)] = sqrt(wub * wub + wvb * wvb) * P.const1;
   float* const cs = P.clos_samp;
-  bool in_env = wet;
   const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
   auto samp = [&](int f, int k, double v) { cs[(size_t)f * ss + (size_t)(k - 2) * P.M + (i - 1)] = (float)v; };
-  for (int k = 1; k <= KB; ++k) {
-    Q2[n3(k)] = fabs(Q2[n3(k)] + SMALL);
-    Q2L[n3(k)] = fabs(Q2L[n3(k)]);
-  }
-  if (wet) {
-    for (int k = 2; k <= KBM1; ++k) {
-      boygr[k] = P.grav_n[i] * (P.rho1[n3(k - 1)] - P.rho1[n3(k)]) / (P.dzz[n3(k - 1)] * d);
-      prod[k] = P.km[n3(k)] * 0.0 * pow(.5 * (-boygr[k] + fabs(boygr[k])), 1.5);
+  // ring means of U, V on the level above the first interior level of the chunk
+  const size_t m1 = P.M + 1;
+  const int nt = P.ntve[i];
+  const double fn = (double)(float)nt;
+  auto ring_mean = [&](int k, double& um, double& vm) {
+    double su = 0.0, sv = 0.0;
+    for (int j = 1; j <= nt; ++j) {
+      int c = P.nbve[(size_t)(j - 1) * m1 + i];
+      su = su + P.u[C3(P, c, k)];
+      sv = sv + P.v[C3(P, c, k)];
     }
-    // Ring means of U and V on layer k; the layer k-1 means of the reference's loop are
-    // the same sums in the same order, carried from the previous iteration.
-    auto ring_mean = [&](int k, double& um, double& vm) {
-      double su = 0.0, sv = 0.0;
-      for (int j = 1; j <= nt; ++j) {
-        int c = P.nbve[(size_t)(j - 1) * m1 + i];
-        su = su + P.u[C3(P, c, k)];
-        sv = sv + P.v[C3(P, c, k)];
-      }
-      um = su / fn;
-      vm = sv / fn;
-    };
-    double ukm1, vkm1;
-    ring_mean(1, ukm1, vkm1);
-    for (int k = 2; k <= KBM1; ++k) {
-      double uk, vk;
-      ring_mean(k, uk, vk);
-      double den = P.dzz[n3(k - 1)] * d;
-      if (P.closure) {
-        // the network's inputs and the envelope test of this level
-        const float fv[CLOS_IN] = {(float)boygr[k],
-                                   (float)(((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den)),
-                                   (float)d, (float)P.z[n3(k)], (float)sqrt(utau2),
-                                   (float)sqrt(sqrt(wub * wub + wvb * wvb)), (float)Q2[n3(k)], (float)Q2L[n3(k)]};
-        const size_t r = (size_t)(k - 2) * P.M + (i - 1);
-        for (int f = 0; f < CLOS_IN; ++f) {
-          P.clos_feat[(size_t)f * ss + r] = fv[f];
-          if (!(fv[f] >= P.clos_norm.lo[f] && fv[f] <= P.clos_norm.hi[f])) in_env = false;
-        }
-      }
-      if (cs) {
-        samp(0, k, boygr[k]);
-        samp(1, k, ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den));
-        samp(2, k, d);
-        samp(3, k, P.z[n3(k)]);
-        samp(4, k, sqrt(utau2));
-        samp(5, k, sqrt(sqrt(wub * wub + wvb * wvb)));
-        samp(6, k, Q2[n3(k)]);
-        samp(7, k, Q2L[n3(k)]);
-      }
-      prod[k] = prod[k] + P.km[n3(k)] * SEF * ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den);
-      prod[k] = prod[k] + P.kh[n3(k)] * boygr[k];
-      ukm1 = uk;
-      vkm1 = vk;
-    }
-  }
-  for (int k = 2; k <= KBM1; ++k) L[n3(k)] = Q2L[n3(k)] / Q2[n3(k)];
-  for (int k = 2; k <= KBM1; ++k) {
-    if (P.z[n3(k)] > -0.5) L[n3(k)] = fmax(L[n3(k)], KAPPA * l0);
-    if (boygr[k] < 0.0) {
-      double lmax = sqrt(fabs(GH_MIN) * Q2[n3(k)] / (-boygr[k] + SMALL));
-      L[n3(k)] = fmin(L[n3(k)], lmax);
-      Q2L[n3(k)] = Q2[n3(k)] * L[n3(k)];
-    }
-  }
-  for (int k = 1; k <= KBM1; ++k) gh[k] = (L[n3(k)] * L[n3(k)] / Q2[n3(k)]) * boygr[k];
-  for (int k = 1; k <= KB; ++k) gh[k] = fmin(gh[k], GH_MAX);
-  L[n3(1)] = KAPPA * l0;
-  L[n3(KB)] = 0.0;
-  gh[1] = 0.0;
-  gh[KB] = 0.0;
-  // STF (vdif_q.F:358-367) is recomputed from GH where it is needed.
-  auto stf_of = [&](int k) {
-    double s = 1.0;
-    if (gh[k] < 0.0) s = 1.0 - F4(0.9) * pow(gh[k] / GHC, 1.5);
-    if (gh[k] < GHC) s = F4(0.1);
-    return s;
+    um = su / fn;
+    vm = sv / fn;
   };
-  for (int k = 1; k <= KB; ++k) dtef[k] = sqrt(Q2[n3(k)]) / (B1 * L[n3(k)] + SMALL) * stf_of(k);
-  // q2 equation (vdif_q.F:372-391)
-  for (int k = 2; k <= KBM1; ++k) {
-    double a = Acoef(k), c = Ccoef(k);
-    double p = 1. / (a + c * (1. - vh[k - 1]) - (2. * DTI * dtef[k] + 1.));
-    vh[k] = a * p;
-    vhp[k] = (-2. * DTI * prod[k] + c * vhp[k - 1] - Q2F[n3(k)]) * p;
-  }
-  if (wet)
-    for (int k = 1; k <= KBM1; ++k) {
-      int ki = KB - k;
-      Q2F[n3(ki)] = vh[ki] * Q2F[n3(ki + 1)] + vhp[ki];
+  double ukm1 = 0.0, vkm1 = 0.0;
+  if (wet && kb <= KBM1) ring_mean(kb >= 2 ? kb - 1 : 1, ukm1, vkm1);
+  for (int k = kb; k <= ke; ++k) {
+    const size_t q = n3(k);
+    // positivity of the previous Q2F/Q2LF (vdif_q.F:144-149)
+    if (k >= 2 && k <= KBM1 && (P.q2f[q] <= SMALL || P.q2lf[q] <= SMALL)) {
+      P.q2f[q] = SMALL;
+      P.q2lf[q] = SMALL;
     }
-  // q2l equation (vdif_q.F:398-431)
+    const double q2 = fabs(Q2[q] + SMALL);
+    double q2l = fabs(Q2L[q]);
+    Q2[q] = q2;
+    double boygr = 0.0, prod = 0.0, lk;
+    if (k >= 2 && k <= KBM1) {
+      if (wet) {
+        boygr = P.grav_n[i] * (P.rho1[n3(k - 1)] - P.rho1[q]) / (P.dzz[n3(k - 1)] * d);
+        prod = P.km[q] * 0.0 * pow(.5 * (-boygr + fabs(boygr)), 1.5);
+        double uk, vk;
+        ring_mean(k, uk, vk);
+        const double den = P.dzz[n3(k - 1)] * d;
+        const double shear2 = ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den);
+        if (P.closure) {
+          const float fv[CLOS_IN] = {(float)boygr, (float)shear2, (float)d, (float)P.z[q], (float)sqrt(utau2),
+                                     (float)sqrt(sqrt(wub * wub + wvb * wvb)), (float)q2, (float)q2l};
+          const size_t r = (size_t)(k - 2) * P.M + (i - 1);
+          for (int f = 0; f < CLOS_IN; ++f) P.clos_feat[(size_t)f * ss + r] = fv[f];
+        }
+        if (cs) {
+          samp(0, k, boygr);
+          samp(1, k, shear2);
+          samp(2, k, d);
+          samp(3, k, P.z[q]);
+          samp(4, k, sqrt(utau2));
+          samp(5, k, sqrt(sqrt(wub * wub + wvb * wvb)));
+          samp(6, k, q2);
+          samp(7, k, q2l);
+        }
+        prod = prod + P.km[q] * SEF * ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den);
+        prod = prod + P.kh[q] * boygr;
+        ukm1 = uk;
+        vkm1 = vk;
+      }
+      // length scale and its limits (vdif_q.F:300-331)
+      lk = q2l / q2;
+      if (P.z[q] > -0.5) lk = fmax(lk, KAPPA * l0);
+      if (boygr < 0.0) {
+        double lmax = sqrt(fabs(GH_MIN) * q2 / (-boygr + SMALL));
+        lk = fmin(lk, lmax);
+        q2l = q2 * lk;
+      }
+    } else {
+      lk = k == 1 ? KAPPA * l0 : 0.0;
+    }
+    Q2L[q] = q2l;
+    L[q] = lk;
+    double gh = 0.0;
+    if (k >= 2 && k <= KBM1) gh = fmin((lk * lk / q2) * boygr, GH_MAX);
+    double stf = 1.0;
+    if (gh < 0.0) stf = 1.0 - F4(0.9) * pow(gh / GHC, 1.5);
+    if (gh < GHC) stf = F4(0.1);
+    const double dtef = sqrt(q2) / (B1 * lk + SMALL) * stf;
+    P.vq_prod[q] = prod;
+    P.vq_gh[q] = gh;
+    P.vq_dtef[q] = dtef;
+    if (wet && k >= 2 && k <= KBM1) {
+      const double x = (1. / fabs(P.z[q] - P.z[n3(1)]) + 1. / fabs(P.z[q] - P.z[n3(KB)])) * lk / (d * KAPPA);
+      P.vq_dtefl[q] = dtef * (1. + E2 * (x * x));
+    }
+  }
+}
+
+// The q2 and q2l tridiagonal sweeps of one column (vdif_q.F:372-431), and the column's
+// envelope flag of the learned closure.
+__global__ void __launch_bounds__(128) k_vdif_q_sweep(const Dev P) {
+  using namespace vq;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  const int KB = P.KB, KBM1 = P.KBM1;
+  const double DTI = P.dti;
+  const double d = P.d[i];
+  const bool wet = P.iswetn[i] == 1;
+  auto n3 = [&](int k) { return N3(P, i, k); };
+  if (P.closure) {
+    bool in_env = wet;
+    const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
+    for (int k = 2; k <= KBM1 && in_env; ++k) {
+      const size_t r = (size_t)(k - 2) * P.M + (i - 1);
+      for (int f = 0; f < CLOS_IN; ++f) {
+        const float v = P.clos_feat[(size_t)f * ss + r];
+        if (!(v >= P.clos_norm.lo[f] && v <= P.clos_norm.hi[f])) in_env = false;
+      }
+    }
+    P.clos_env[i] = in_env ? 1 : 0;
+  }
+  if (!wet) return;
+  double vh[kMaxKBs], vhp[kMaxKBs];
+  auto Acoef = [&](int k) {
+    return -0.5 * DTI * (P.kq[n3(k + 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k)] * d * d);
+  };
+  auto Ccoef = [&](int k) {
+    return -0.5 * DTI * (P.kq[n3(k - 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k - 1)] * d * d);
+  };
+  double* Q2F = P.q2f;
+  double* Q2LF = P.q2lf;
+  vh[1] = 0.0;
+  vhp[1] = P.vhp1c * P.vq_ut[i];
+  for (int k = 2; k <= KBM1; ++k) {
+    const double a = Acoef(k), c = Ccoef(k);
+    const double p = 1. / (a + c * (1. - vh[k - 1]) - (2. * DTI * P.vq_dtef[n3(k)] + 1.));
+    vh[k] = a * p;
+    vhp[k] = (-2. * DTI * P.vq_prod[n3(k)] + c * vhp[k - 1] - Q2F[n3(k)]) * p;
+  }
+  for (int k = 1; k <= KBM1; ++k) {
+    int ki = KB - k;
+    Q2F[n3(ki)] = vh[ki] * Q2F[n3(ki + 1)] + vhp[ki];
+  }
   vh[1] = 0.0;
   vhp[1] = 0.0;
-  if (wet) {
-    for (int k = 2; k <= KBM1; ++k) {
-      double x = (1. / fabs(P.z[n3(k)] - P.z[n3(1)]) + 1. / fabs(P.z[n3(k)] - P.z[n3(KB)])) * L[n3(k)] / (d * KAPPA);
-      dtef[k] = dtef[k] * (1. + E2 * (x * x));
-      double a = Acoef(k), c = Ccoef(k);
-      double p = 1. / (a + c * (1. - vh[k - 1]) - (DTI * dtef[k] + 1.));
-      vh[k] = a * p;
-      vhp[k] = (DTI * (-prod[k] * L[n3(k)] * E1) + c * vhp[k - 1] - Q2LF[n3(k)]) * p;
-    }
-    for (int k = 1; k <= KBM1; ++k) {
-      int ki = KB - k;
-      Q2LF[n3(ki)] = vh[ki] * Q2LF[n3(ki + 1)] + vhp[ki];
-    }
+  for (int k = 2; k <= KBM1; ++k) {
+    const double a = Acoef(k), c = Ccoef(k);
+    const double p = 1. / (a + c * (1. - vh[k - 1]) - (DTI * P.vq_dtefl[n3(k)] + 1.));
+    vh[k] = a * p;
+    vhp[k] = (DTI * (-P.vq_prod[n3(k)] * P.l[n3(k)] * E1) + c * vhp[k - 1] - Q2LF[n3(k)]) * p;
   }
-  for (int k = 2; k <= KBM1; ++k)
-    if (Q2F[n3(k)] <= SMALL || Q2LF[n3(k)] <= SMALL) { Q2F[n3(k)] = SMALL; Q2LF[n3(k)] = SMALL; }
-  // Stability functions and mixing coefficients (vdif_q.F:470-491)
-  for (int k = 1; k <= KB; ++k) {
-    double stf = stf_of(k);
+  for (int k = 1; k <= KBM1; ++k) {
+    int ki = KB - k;
+    Q2LF[n3(ki)] = vh[ki] * Q2LF[n3(ki + 1)] + vhp[ki];
+  }
+}
+
+// Positivity of the new Q2F/Q2LF, the stability functions and KQ, KM, KH
+// (vdif_q.F:443-491), per (node, level); then Q2 = Q2F, Q2L = Q2LF.
+__global__ void __launch_bounds__(256) k_vdif_q_coef(const Dev P, int copy_back) {
+  using namespace vq;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  int kb, ke;
+  col_range(P, 1, P.KB, kb, ke);
+  const int KBM1 = P.KBM1;
+  const double COEF4 = 18.0 * A1 * A1 + 9.0 * A1 * A2;
+  const double COEF5 = 9.0 * A1 * A2;
+  const bool wet = P.iswetn[i] == 1;
+  float* const cs = P.clos_samp;
+  const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
+  auto samp = [&](int f, int k, double v) { cs[(size_t)f * ss + (size_t)(k - 2) * P.M + (i - 1)] = (float)v; };
+  for (int k = kb; k <= ke; ++k) {
+    const size_t q = N3(P, i, k);
+    if (k >= 2 && k <= KBM1 && (P.q2f[q] <= SMALL || P.q2lf[q] <= SMALL)) {
+      P.q2f[q] = SMALL;
+      P.q2lf[q] = SMALL;
+    }
+    const double gh = P.vq_gh[q];
+    double stf = 1.0;
+    if (gh < 0.0) stf = 1.0 - F4(0.9) * pow(gh / GHC, 1.5);
+    if (gh < GHC) stf = F4(0.1);
     double coef1 = A2 * (1.0 - 6.0 * A1 / B1 * stf);
     double coef2 = 3.0 * A2 * B2 / stf + 18.0 * A1 * A2;
     double coef3 = A1 * (1.0 - 3.0 * C1 - 6.0 * A1 / B1 * stf);
-    double sh = coef1 / (1.0 - coef2 * gh[k]);
-    double sm = (coef3 + sh * COEF4 * gh[k]) / (1. - COEF5 * gh[k]);
-    double kn = L[n3(k)] * sqrt(Q2[n3(k)]);
-    size_t q = n3(k);
-    if (cs && k >= 2 && k <= KBM1) {
-      samp(8, k, kn * KAPPA * sm);
-      samp(9, k, kn * sm);
-      samp(10, k, kn * sh * P.vprnu);
-      samp(11, k, wet ? 1.0 : 0.0);
+    double sh = coef1 / (1.0 - coef2 * gh);
+    double sm = (coef3 + sh * COEF4 * gh) / (1. - COEF5 * gh);
+    double kn = P.l[q] * sqrt(P.q2[q]);
+    bool interior_by_network = false;
+    if (k >= 2 && k <= KBM1) {
+      if (cs) {
+        samp(8, k, kn * KAPPA * sm);
+        samp(9, k, kn * sm);
+        samp(10, k, kn * sh * P.vprnu);
+        samp(11, k, wet ? 1.0 : 0.0);
+      }
+      if (P.closure) {
+        // interior levels are finished by the network kernel (k_closure_mlp)
+        const size_t r = (size_t)(k - 2) * P.M + (i - 1);
+        P.clos_plain[r] = kn * KAPPA * sm;
+        P.clos_plain[ss + r] = kn * sm;
+        P.clos_plain[2 * ss + r] = kn * sh * P.vprnu;
+        interior_by_network = true;
+      }
     }
-    if (P.closure && k >= 2 && k <= KBM1) {
-      // interior levels are finished by the network kernel (k_closure_mlp)
-      const size_t r = (size_t)(k - 2) * P.M + (i - 1);
-      P.clos_plain[r] = kn * KAPPA * sm;
-      P.clos_plain[ss + r] = kn * sm;
-      P.clos_plain[2 * ss + r] = kn * sh * P.vprnu;
-      continue;
+    if (!interior_by_network) {
+      P.kq[q] = 0.5 * (kn * KAPPA * sm + P.kq[q]);
+      P.km[q] = 0.5 * (kn * sm + P.km[q]);
+      P.kh[q] = 0.5 * (kn * sh * P.vprnu + P.kh[q]);
     }
-    P.kq[q] = 0.5 * (kn * KAPPA * sm + P.kq[q]);
-    P.km[q] = 0.5 * (kn * sm + P.km[q]);
-    P.kh[q] = 0.5 * (kn * sh * P.vprnu + P.kh[q]);
+    if (copy_back) {
+      P.q2[q] = P.q2f[q];
+      P.q2l[q] = P.q2lf[q];
+    }
   }
-  if (P.closure) P.clos_env[i] = in_env ? 1 : 0;
-  if (!P.closure && P.h[i] <= P.static_ssh_adj) {
-    double kqt = 0.0, kmt = 0.0, kht = 0.0;
-    for (int k = 2; k <= KBM1; ++k) { kqt = kqt + P.kq[n3(k)]; kmt = kmt + P.km[n3(k)]; kht = kht + P.kh[n3(k)]; }
-    kqt = kqt / (double)(KBM1 - 1);
-    kmt = kmt / (double)(KBM1 - 1);
-    kht = kht / (double)(KBM1 - 1);
-    for (int k = 2; k <= KBM1; ++k) { P.kq[n3(k)] = kqt; P.km[n3(k)] = kmt; P.kh[n3(k)] = kht; }
-  }
-  if (copy_back)
-    for (int k = 1; k <= KB; ++k) { Q2[n3(k)] = Q2F[n3(k)]; Q2L[n3(k)] = Q2LF[n3(k)]; }
 }
 
 // Q2=Q2F, Q2L=Q2LF on every node and level; N2E3D(KM,KM1) (internal_step.F:1034-1053).
@@ -960,7 +1030,10 @@ void launch_fct_q(const Dev& P, cudaStream_t s, int parts) {
   k_fct_q<<<g, b, 0, s>>>(P, parts);
 }
 void launch_vdif_q(const Dev& P, cudaStream_t s, int copy_back) {
-  k_vdif_q<<<nblk(P.M, 128), 128, 0, s>>>(P, copy_back);
+  k_vdif_q_levels<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P);
+  k_vdif_q_sweep<<<nblk(P.M, 128), 128, 0, s>>>(P);
+  k_vdif_q_coef<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P, copy_back);
+  if (!P.closure) launch_vdif_q_shallow(P, s);
 }
 void launch_turb_update(const Dev& P, cudaStream_t s) {
   int n = (P.M > P.N ? P.M : P.N) + 1;

@@ -13,7 +13,6 @@ MI, MH, MO = 8, 64, 3
 SIZES = [("W1", (MH, MI)), ("b1", (MH,)), ("W2", (MH, MH)), ("b2", (MH,)), ("W3", (MO, MH)), ("b3", (MO,))]
 NPAR = sum(int(np.prod(s)) for _, s in SIZES)
 
-_erf = np.vectorize(math.erf)
 
 
 def unpack(p):
@@ -25,12 +24,18 @@ def unpack(p):
     return out
 
 
+GC = math.sqrt(2.0 / math.pi)
+GA = 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU in its tanh form, as the kernels use it."""
+    return 0.5 * z * (1.0 + np.tanh(GC * (z + GA * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(GC * (z + GA * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GC * (1.0 + 3.0 * GA * z * z)
 
 
 def forward(p, x):
