@@ -872,11 +872,7 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
       if ((rc = dalloc(h, &f.g2d[q], n1))) return fail(rc);
       if ((rc = dalloc(h, &f.g3[q], ns * KB))) return fail(rc);
     }
-    for (int t = 0; t < 2; ++t)
-      for (int g = 0; g < 6; ++g) {
-        if ((rc = dalloc(h, &f.gq[t][g], ms * KB))) return fail(rc);
-        if ((rc = dalloc(h, &f.gt[t][g], ms * KB))) return fail(rc);
-      }
+    if ((rc = dalloc(h, &f.npk, ms * KB * 16))) return fail(rc);
     if ((rc = dalloc(h, (float**)&f.ex2, (size_t)P.ncvs * KB * 2))) return fail(rc);
     if ((rc = dalloc(h, &f.xo, 2 * e1))) return fail(rc);
     if ((rc = dalloc(h, &f.yo, 2 * e1))) return fail(rc);

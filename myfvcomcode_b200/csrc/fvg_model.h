@@ -42,7 +42,7 @@ struct SchedLayout {
 // same for y.
 struct F32 {
   float *g2d[4], *g3[4];
-  float *gq[2][6], *gt[2][6];
+  float* npk;  // node records of the ring gradients, 16 floats per (node, layer)
   float2* ex2;
   float *xo, *yo, *dltxc, *dltyc, *art, *cc_hvc, *a1u, *a2u;
   float *dltxe, *dltye, *dltxncve, *dltyncve;
@@ -222,8 +222,6 @@ template <> struct Mesh<double> {
   __device__ static double dltyncve(const Dev& P, size_t q) { return P.dltyncve[q]; }
   __device__ static double* g2d(const Dev& P, int q) { return P.g2d[q]; }
   __device__ static double* g3(const Dev& P, int q) { return P.g3[q]; }
-  __device__ static double* const* gq(const Dev& P, int t) { return P.gq[t]; }
-  __device__ static double* const* gt(const Dev& P, int t) { return P.gt[t]; }
   __device__ static double2* ex2(const Dev& P) { return P.ex2; }
 };
 template <> struct Mesh<float> {
@@ -250,8 +248,6 @@ template <> struct Mesh<float> {
   __device__ static float dltyncve(const Dev& P, size_t q) { return P.f.dltyncve[q]; }
   __device__ static float* g2d(const Dev& P, int q) { return P.f.g2d[q]; }
   __device__ static float* g3(const Dev& P, int q) { return P.f.g3[q]; }
-  __device__ static float* const* gq(const Dev& P, int t) { return P.f.gq[t]; }
-  __device__ static float* const* gt(const Dev& P, int t) { return P.f.gt[t]; }
   __device__ static float2* ex2(const Dev& P) { return P.f.ex2; }
 };
 __device__ inline double2 mk2(double a, double b) { return make_double2(a, b); }

@@ -25,6 +25,70 @@ __device__ inline int NBSN(const Dev& P, int i, int j) { return P.nbsn[(size_t)(
 __device__ inline double TRIEX(const Dev& P, int i, int j) { return P.dltxtrie[(size_t)(j - 1) * (P.M + 1) + i]; }
 __device__ inline double TRIEY(const Dev& P, int i, int j) { return P.dltytrie[(size_t)(j - 1) * (P.M + 1) + i]; }
 
+// One tracer's node data on layer k: value, ring gradients, ring extrema.
+template <typename R>
+struct TRec {
+  R q, px, py, pxd, pyd, rmin, rmax;
+};
+
+// Storage of the ring gradients and extrema by arithmetic type.  FP64: six arrays per
+// tracer (P.gq, P.gt).  FP32: one 32-byte record per tracer and (node, layer) in P.f.npk,
+// record r = (K-1)*ms + I holding {value, PX, PY, PXD, PYD, min, max, 0} for tracer t at
+// floats 16r + 8t, read and written as two float4.
+template <typename R> struct NodeRec;
+template <> struct NodeRec<double> {
+  __device__ static void store(const Dev& P, int mode, int t, size_t q, double, double px, double py, double pxd,
+                               double pyd, double mn, double mx) {
+    double* const* G = mode == 0 ? P.gq[t] : P.gt[t];
+    G[0][q] = px;
+    G[1][q] = py;
+    G[2][q] = pxd;
+    G[3][q] = pyd;
+    G[4][q] = mn;
+    G[5][q] = mx;
+  }
+  __device__ static TRec<double> load(const Dev& P, int mode, int t, size_t q, double qv) {
+    double* const* G = mode == 0 ? P.gq[t] : P.gt[t];
+    return TRec<double>{qv, G[0][q], G[1][q], G[2][q], G[3][q], G[4][q], G[5][q]};
+  }
+  __device__ static void minmax(const Dev& P, int mode, int t, size_t q, double& mn, double& mx) {
+    double* const* G = mode == 0 ? P.gq[t] : P.gt[t];
+    mn = G[4][q];
+    mx = G[5][q];
+  }
+};
+template <> struct NodeRec<float> {
+  __device__ static float4* rec(const Dev& P, int t, size_t q) {
+    return reinterpret_cast<float4*>(P.f.npk + 16 * q + 8 * t);
+  }
+  __device__ static void store(const Dev& P, int, int t, size_t q, float qv, float px, float py, float pxd,
+                               float pyd, float mn, float mx) {
+    float4* r = rec(P, t, q);
+    r[0] = make_float4(qv, px, py, pxd);
+    r[1] = make_float4(pyd, mn, mx, 0.f);
+  }
+  __device__ static TRec<float> load(const Dev& P, int, int t, size_t q, double) {
+    const float4* r = rec(P, t, q);
+    const float4 a = r[0], b = r[1];
+    return TRec<float>{a.x, a.y, a.z, a.w, b.x, b.y, b.z};
+  }
+  __device__ static void minmax(const Dev& P, int, int t, size_t q, double& mn, double& mx) {
+    const float4 b = rec(P, t, q)[1];
+    mn = (double)b.y;
+    mx = (double)b.z;
+  }
+};
+
+template <typename R, int MODE>
+__device__ inline TRec<R> load_trec(const Dev& P, int n, int k, int t) {
+  const size_t q = N3(P, n, k);
+  if (sizeof(R) == 8) {
+    const double* Q = MODE == 0 ? (t == 0 ? P.q2 : P.q2l) : (t == 0 ? P.t1 : P.s1);
+    return NodeRec<R>::load(P, MODE, t, q, Q[q]);
+  }
+  return NodeRec<R>::load(P, MODE, t, q, 0.0);
+}
+
 // -------------------------------------------------------------------------------------
 // Ring gradients and extrema.  which == 0: Q2 and Q2L on K=2..KBM1 (adv_q.F:161-235);
 // which == 1: T1 and S1 on K=1..KBM1 with the wet/dry substitution of adv_t.F:214-376,
@@ -43,14 +107,11 @@ __global__ void __launch_bounds__(256) k_grad(const Dev P, int which) {
     for (int t = 0; t < 2; ++t) {
       const double* Q;
       const double* QM = nullptr;
-      R* const* G;
       if (which == 0) {
         Q = (t == 0 ? P.q2 : P.q2l) + N3(P, 0, k);
-        G = Mesh<R>::gq(P, t);
       } else {
         Q = (t == 0 ? P.t1 : P.s1) + N3(P, 0, k);
         QM = (t == 0 ? P.tmean1 : P.smean1) + N3(P, 0, k);
-        G = Mesh<R>::gt(P, t);
       }
       const R qmean = (R)F4(1.e-8);
       R px = 0, py = 0, pxd = 0, pyd = 0;
@@ -85,12 +146,7 @@ __global__ void __launch_bounds__(256) k_grad(const Dev P, int which) {
       pxd = pxd / art2;
       pyd = pyd / art2;
       size_t q = N3(P, i, k);
-      G[0][q] = px;
-      G[1][q] = py;
-      G[2][q] = pxd;
-      G[3][q] = pyd;
-      G[4][q] = rmin;
-      G[5][q] = rmax;
+      NodeRec<R>::store(P, which, t, q, (R)Q[i], px, py, pxd, pyd, rmin, rmax);
       if (which == 1 && k == P.KBM1) {
         if (t == 0) { P.pfpxb_t[i] = (double)px; P.pfpyb_t[i] = (double)py; }
         else { P.pfpxb_s[i] = (double)px; P.pfpyb_s[i] = (double)py; }
@@ -199,19 +255,6 @@ __device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell<R>& hc) {
 template <typename R>
 __device__ inline R sel3(const R* v, int j) { return j == 0 ? v[0] : (j == 1 ? v[1] : v[2]); }
 __device__ inline int sel3i(const int* v, int j) { return j == 0 ? v[0] : (j == 1 ? v[1] : v[2]); }
-
-// One tracer's node data on layer k: value, ring gradients, ring extrema.
-template <typename R>
-struct TRec {
-  R q, px, py, pxd, pyd, rmin, rmax;
-};
-template <typename R, int MODE>
-__device__ inline TRec<R> load_trec(const Dev& P, int n, int k, int t) {
-  const double* Q = MODE == 0 ? (t == 0 ? P.q2 : P.q2l) : (t == 0 ? P.t1 : P.s1);
-  R* const* G = MODE == 0 ? Mesh<R>::gq(P, t) : Mesh<R>::gt(P, t);
-  const size_t q = N3(P, n, k);
-  return TRec<R>{(R)Q[q], G[0][q], G[1][q], G[2][q], G[3][q], G[4][q], G[5][q]};
-}
 
 // EXFLUX of half-edge he for tracer t, in R; a and b are the positions of NIEC(he,1) and
 // NIEC(he,2) among the cell's nodes, ra and rb their data.  xadv receives EXFLUX-FXX-FYY.
@@ -371,8 +414,8 @@ __global__ void __launch_bounds__(256) k_gather_q(const Dev P, int parts) {
       qf = Q[q];
     }
     if ((parts & AD_FCT) && !P.riv_skip[i]) {
-      R* const* G = Mesh<R>::gq(P, t);
-      double qmax = (double)G[5][q], qmin = (double)G[4][q];
+      double qmin, qmax;
+      NodeRec<R>::minmax(P, 0, t, q, qmin, qmax);
       fct_level_bounds(P, i, k, Q, qmax, qmin);
       if (qmin - qf > 0.0) qf = qmin;
       if (qf - qmax > 0.0) qf = qmax;
@@ -739,8 +782,8 @@ __global__ void __launch_bounds__(256) k_gather_ts(const Dev P, int parts) {
     }
     if (parts & AD_FCT) {
       if (!P.riv_skip[i]) {
-        R* const* G = Mesh<R>::gt(P, t);
-        double fmx = (double)G[5][q], fmn = (double)G[4][q];
+        double fmn, fmx;
+        NodeRec<R>::minmax(P, 1, t, q, fmn, fmx);
         fct_layer_bounds(P, i, k, F1, fmx, fmn);
         if (fmn - ff > 0.0) ff = fmn;
         if (ff - fmx > 0.0) ff = fmx;
