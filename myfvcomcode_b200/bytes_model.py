@@ -45,10 +45,15 @@ def ledger(grid, isplit, wet_dry, precision="fp64"):
     pg_extra = 0 if X == D else NE * 2 * D  # FP64 DLTXC/DLTYC of the surface-slope term
     g = {}
     # ---- external mode, per RK stage ----
-    g["ext_node"] = (M * (I + I + 3 * D) + halfedge_csr + NCV * (I + 2 * D) + N * 3 * D, st)
+    # The update after each stage (external_step.F:333-436) runs inside the next stage's
+    # kernels: its node part (ELF read, H read, EL, D, DTFA written) at the head of
+    # k_ext_node, its cell part (H1 read, EL1, D1 and the three half-edge continuity
+    # fluxes written, CELL_HE read) at the tail of k_ext_cell; one closing launch
+    # (k_ext_finish) does the last stage's node part and the UA/VA copies.
+    g["ext_node"] = (M * (I + I + 3 * D) + halfedge_csr + NCV * (I + 2 * D) + N * 3 * D + M * 5 * D, st)
     g["ext_cell"] = (N * (cell_lsq // N + 22 * D + 4 * X + 6 * I) + N * 8 * D + edge_geo + pg_extra
-                     + M * 4 * D, st)
-    g["ext_update"] = (M * (6 * D + I) + N * (10 * D + (2 * I if wet_dry else 0)), st)
+                     + M * 4 * D + N * (6 * D + 3 * I), st)
+    g["ext_update"] = (M * (6 * D + I) + N * (10 * D + (2 * I if wet_dry else 0)), 1)
     if wet_dry:
         g["wet_judge"] = (N * (3 * I + I + D) + M * (4 * D + 2 * I) + I * ntve, st)
     # ---- 3-D, once per internal step ----

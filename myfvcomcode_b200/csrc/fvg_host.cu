@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "fvg_model.h"
@@ -185,22 +186,36 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   launch_ext_cell(P, s, 1, 1, EC_INT_ADVAVE);
   launch_int_reset(P, s);
   mk.mark(s, G_INT_ADVAVE);
+  // The ISPLIT x 4 Runge-Kutta stages.  Instead of copying UAF to UA and ISWETC to
+  // ISWETCE after each stage (external_step.F:333-436), the stage reads and writes swapped
+  // arrays: stage n+1's UA is stage n's UAF, its ISWETCE stage n's ISWETC.  The update's
+  // cell part ends the cell kernel, its node part starts the next stage's node kernel,
+  // and k_ext_finish closes the last stage (an even number of stages leaves the arrays in
+  // their own roles).
+  int stage = 0;
   for (int iext = 1; iext <= p.isplit; ++iext) {
-    for (int K = 1; K <= 4; ++K) {
-      launch_ext_node(P, s, iext, K, EN_EXTEL | EN_BC | EN_GRAD | (K == 1 ? EN_COPY_ELRK : 0));
+    for (int K = 1; K <= 4; ++K, ++stage) {
+      Dev Q = P;
+      if (stage & 1) {
+        std::swap(Q.ua, Q.uaf);
+        std::swap(Q.va, Q.vaf);
+        std::swap(Q.iswetce, Q.iswetc);
+      }
+      const int prev = stage > 0 ? (EN_FINISH_PREV | ((K == 1 ? 4 : K - 1) << 8)) : 0;
+      launch_ext_node(Q, s, iext, K, EN_EXTEL | EN_BC | EN_GRAD | (K == 1 ? EN_COPY_ELRK : 0) | prev);
       mk.mark(s, G_EXT_NODE);
       if (p.wetting_drying_on) {
-        launch_wet_judge(P, s);
+        launch_wet_judge(Q, s);
         mk.mark(s, G_WET);
       }
-      launch_ext_cell(P, s, iext, K,
+      launch_ext_cell(Q, s, iext, K,
                       (p.wetting_drying_on ? 0 : EC_N2E) | EC_FLUXOBN | EC_ADVAVE | EC_EXTUV | EC_BC2 |
-                          (K == 1 ? EC_COPY_RK : 0));
+                          (K == 1 ? EC_COPY_RK : 0) | EC_FINISH);
       mk.mark(s, G_EXT_CELL);
-      launch_ext_update(P, s, K);
-      mk.mark(s, G_EXT_UPD);
     }
   }
+  launch_ext_finish(P, s, 4);
+  mk.mark(s, G_EXT_UPD);
   launch_adjust2(P, s);
   mk.mark(s, G_ADJ2);
   launch_vertvl_flux(P, s);
@@ -793,7 +808,7 @@ int32_t fvg_kernels_per_step(const fvg_handle* h) {
   if (!h) return -1;
   const fvg_params& p = h->prm;
   int n = 1 + 1 + 2 + 2 + 2;                                // begin, cell_pre, grad3+adv3d, baropg+prep, int advave+reset
-  n += p.isplit * 4 * (3 + (p.wetting_drying_on ? 2 : 0)); // RK stages
+  n += p.isplit * 4 * (2 + (p.wetting_drying_on ? 2 : 0)) + 1; // RK stages, closing update
   n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv
   n += 7;                                                  // grad_q, adv_q (2 phases), vdif_q (4 passes)
   if (h->P.closure) n += 1;                                // learned closure

@@ -82,11 +82,47 @@ __device__ inline void store_exf(const Dev& P, int c) {
 // (external_step.F:262-266).  One thread per node; the node's control-volume half-edges
 // are gathered in ascending half-edge number, the order of the reference's scatter.
 // -------------------------------------------------------------------------------------
+// Node part of the update after stage K (external_step.F:333-436): EL = ELF, D, DTFA, and
+// the K == 3 and K == 4 sums.
+__device__ inline void ext_update_node(const Dev& P, int i, int K) {
+  double e = P.elf[i];
+  P.el[i] = e;
+  double dd = P.h[i] + e;
+  P.d[i] = dd;
+  P.dtfa[i] = dd;
+  if (K == 3) P.egf[i] = P.egf[i] + e / (double)P.isplit;
+  if (K == 4) {
+    int ob = P.node_obc[i];
+    if (ob > 0) {
+      double tmp = -(P.elf[i] - P.elrk[i]) * P.art1[i] / P.dte - P.xflux_obcn[ob];
+      P.uard_obcn[ob] = P.uard_obcn[ob] + tmp / (double)(float)P.isplit;
+    }
+  }
+}
+
+// Cell part of the update after stage K with the new UA, VA: EL1, D1, the K == 3 sums and
+// the half-edge continuity fluxes of the next stage.
+__device__ inline void ext_update_cell(const Dev& P, int i, int K, double u, double v) {
+  double e1 = P.elf1[i];
+  P.el1[i] = e1;
+  double dd1 = P.h1[i] + e1;
+  P.d1[i] = dd1;
+  if (K == 3) {
+    P.uard[i] = P.uard[i] + u * dd1;
+    P.vard[i] = P.vard[i] + v * dd1;
+  }
+  for (int s = 0; s < 3; ++s) {
+    int he = P.cell_he[3 * i + s];
+    P.exf2d[he] = dd1 * (-u * P.dltye[he] + v * P.dltxe[he]);
+  }
+}
+
 __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   // cell part: least-squares gradient of the current UA, VA for ADVAVE of this stage
   if ((parts & EN_GRAD) && i <= P.N) store_grad(P, i);
   if (i > P.M) return;
+  if (parts & EN_FINISH_PREV) ext_update_node(P, i, (parts >> 8) & 7);
   double x = 0.0;
   if (parts & EN_EXTEL) {
     for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
@@ -354,6 +390,7 @@ __global__ void k_ext_cell(const Dev P, int iext, int K, int parts) {
     }
     P.uaf[i] = uaf;
     P.vaf[i] = vaf;
+    if (parts & EC_FINISH) ext_update_cell(P, i, K, uaf, vaf);
   }
 }
 
@@ -363,40 +400,27 @@ __global__ void k_ext_cell(const Dev P, int iext, int K, int parts) {
 // -------------------------------------------------------------------------------------
 __global__ void k_ext_update(const Dev P, int K) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (i <= P.M) {
-    double e = P.elf[i];
-    P.el[i] = e;
-    double dd = P.h[i] + e;
-    P.d[i] = dd;
-    P.dtfa[i] = dd;
-    if (K == 3) P.egf[i] = P.egf[i] + e / (double)P.isplit;
-    if (K == 4) {
-      int ob = P.node_obc[i];
-      if (ob > 0) {
-        double tmp = -(P.elf[i] - P.elrk[i]) * P.art1[i] / P.dte - P.xflux_obcn[ob];
-        P.uard_obcn[ob] = P.uard_obcn[ob] + tmp / (double)(float)P.isplit;
-      }
-    }
-  }
+  if (i <= P.M) ext_update_node(P, i, K);
   if (i <= P.N) {
-    double e1 = P.elf1[i];
-    P.el1[i] = e1;
-    double dd1 = P.h1[i] + e1;
-    P.d1[i] = dd1;
     double u = P.uaf[i], v = P.vaf[i];
     P.ua[i] = u;
     P.va[i] = v;
-    if (K == 3) {
-      P.uard[i] = P.uard[i] + u * dd1;
-      P.vard[i] = P.vard[i] + v * dd1;
-    }
     if (P.wetting_drying_on) P.iswetce[i] = P.iswetc[i];
-    store_exf(P, i);
+    ext_update_cell(P, i, K, u, v);
   }
 }
 
-// Gradients and half-edge continuity fluxes of the current UA, VA, D1 for every cell
-// (start of the external mode, and before single-routine calls).
+// After the last stage of a fused external loop: the node part of its update, and UAF,
+// VAF, ISWETC made equal to UA, VA, ISWETCE as the copying update leaves them.
+__global__ void k_ext_finish(const Dev P, int K) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i <= P.M) ext_update_node(P, i, K);
+  if (i <= P.N) {
+    P.uaf[i] = P.ua[i];
+    P.vaf[i] = P.va[i];
+    P.iswetc[i] = P.iswetce[i];
+  }
+}
 __global__ void k_ext_prep(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
@@ -478,6 +502,10 @@ void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
 void launch_ext_update(const Dev& P, cudaStream_t s, int K) {
   int n = P.M > P.N ? P.M : P.N;
   k_ext_update<<<nblk(n, 256), 256, 0, s>>>(P, K);
+}
+void launch_ext_finish(const Dev& P, cudaStream_t s, int K) {
+  int n = P.M > P.N ? P.M : P.N;
+  k_ext_finish<<<nblk(n, 256), 256, 0, s>>>(P, K);
 }
 void launch_begin_step(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 1); }
 void launch_set_qdis(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 0); }
