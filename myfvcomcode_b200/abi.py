@@ -178,6 +178,21 @@ def make_structs(case):
     ps.river_location = {"node": 0, "edge": 1}[g["RIVER_LOC"]]
     ps.tide_ref_time = p.get("TIDE_REF_TIME", 0.0)
 
+    fs = forcing_struct(case, b)
+    return ms, ps, fs, b
+
+
+def forcing_struct(case, b=None):
+    """An fvg_forcing struct for ``case["forcing"]``: the tide, river discharge with its
+    temperature and salinity, and the wind stress (``wind_stress``).  ``b`` (a Bundle)
+    keeps the arrays the struct points to alive; pass ``None`` to get a new one back as
+    the struct's ``_keep`` attribute."""
+    g = case["grid"]
+    fc = case["forcing"]
+    nob, nq = g["IOBCN"], g["NUMQBC"]
+    own = b is None
+    if own:
+        b = Bundle()
     fs = FvgForcing()
     tide = fc.get("tide")
     if tide is not None and nob > 0:
@@ -197,4 +212,6 @@ def make_structs(case):
     ws = wind_stress(case)
     if ws is not None:
         fs.wstress_x, fs.wstress_y = b.d(ws[0]), b.d(ws[1])
-    return ms, ps, fs, b
+    if own:
+        fs._keep = b
+    return fs

@@ -143,6 +143,17 @@ class CEngine:
     def internal_step(self):
         self._check(self._f("internal_step")(self.h), "internal_step")
 
+    def set_forcing(self, forcing):
+        """Replace the boundary forcing between internal steps (fvg_set_forcing):
+        ``forcing`` has the keys of ``case["forcing"]`` (tide, qdis, tdis, sdis, wind);
+        the tide must keep its number of constituents, and wind needs a model created
+        with wind."""
+        fs = abi.forcing_struct(dict(self.case, forcing=forcing))
+        f = self._f("set_forcing")
+        f.argtypes = [C.c_void_p, C.c_void_p]
+        f.restype = C.c_int
+        self._check(f(self.h, C.byref(fs)), "set_forcing")
+
     def run(self, n):
         self._check(self._f("run")(self.h, int(n)), "run")
 

@@ -75,14 +75,15 @@ class Grid:
 
 def build_grid(vx_in, vy_in, nv_cw, h_in, kb, obc_nodes=(), obc_types=(),
                cor_lat=None, sponge=(), horcon=0.2, z0b=0.001,
-               rivers=None, river_location="node", static_ssh_adj=0.0):
+               rivers=None, river_location="node", static_ssh_adj=0.0, p_sigma=1.0):
     """Build every mesh array the mode-split step reads.
 
     vx_in, vy_in, h_in: node coordinates (m) and depth (m), length M (0-based input).
     nv_cw: (N, 3) 1-based node numbers of each cell in FVCOM's internal clockwise order
       (the order READ_COLDSTART_GRID produces after its node 2/3 swap,
       FVCOM_source/mod_input.F:3739-3741).
-    kb: number of sigma levels (uniform sigma, FVCOM_source/mod_setup.F:848-877).
+    kb: number of sigma levels; p_sigma: the power of GEOMETRIC sigma levels, 1.0 for
+      UNIFORM (SIGMA_GEOMETRIC, FVCOM_source/mod_setup.F:848-877).
     obc_nodes/obc_types: 1-based open-boundary nodes and their TYPE_OBC (1..10).
     cor_lat: per-node latitude in degrees used for the Coriolis parameter.
     sponge: iterable of (node, radius, coefficient) as in the *_spg.dat file.
@@ -121,7 +122,8 @@ def build_grid(vx_in, vy_in, nv_cw, h_in, kb, obc_nodes=(), obc_types=(),
     _edge_len(g)
     _depth_gradient(g)
     _obc_setup(g, list(obc_nodes), list(obc_types))
-    _sigma(g, kb)
+    _sigma(g, kb, p_sigma)
+    g["P_SIGMA"] = float(p_sigma)
     _constants(g, cor_lat, sponge, horcon, z0b)
     _rivers(g, rivers or [], river_location)
     return g
@@ -615,12 +617,25 @@ def _obc_setup(g, obc_nodes, obc_types):
 # the cell versions of SET_WATER_DEPTH (mod_setup.F:848-877, 1009-1047;
 # mod_startup.F:1460-1491).
 # --------------------------------------------------------------------------------------
-def _sigma(g, kb):
+def _sigma(g, kb, p_sigma=1.0):
     M, N = g["M"], g["N"]
     nv = g["NV"]
     # ZTMP(K) = -((K-1)/FLOAT(KB-1))**P_SIGMA: the quotient is a default-real (single
     # precision) division because FLOAT returns default real; **1.0 leaves it unchanged.
-    ztmp = np.array([-float(np.float32(k - 1) / np.float32(kb - 1)) for k in range(1, kb + 1)])
+    if p_sigma == 1.0:
+        ztmp = np.array([-float(np.float32(k - 1) / np.float32(kb - 1)) for k in range(1, kb + 1)])
+    else:
+        # Geometric levels symmetric about mid-depth (mod_setup.F:854-860): the same
+        # single-precision quotient, raised to the FP64 power and halved.
+        if kb % 2 == 0:
+            raise ValueError("GEOMETRIC sigma with a power other than 1 needs an odd KB (mod_setup.F:805)")
+        half = (kb + 1) // 2
+        p = float(p_sigma)
+        ztmp = np.zeros(kb)
+        for k in range(1, half + 1):
+            ztmp[k - 1] = -(float(np.float32(k - 1) / np.float32(half - 1)) ** p) / 2.0
+        for k in range(half + 1, kb + 1):
+            ztmp[k - 1] = (float(np.float32(kb - k) / np.float32(half - 1)) ** p) / 2.0 - 1.0
     z = np.zeros((M + 1, kb))
     z[1:, :] = ztmp[None, :]
     z1 = np.zeros((N + 1, kb))
@@ -675,7 +690,7 @@ def _constants(g, cor_lat, sponge, horcon, z0b):
     nn_hvc = np.full(M + 1, float(horcon)); nn_hvc[0] = 0.0
     cc_z0b = np.full(N + 1, float(z0b)); cc_z0b[0] = 0.0
     g.a.update(COR=cor, GRAV_N=grav_n, GRAV_E=grav_e, CC_SPONGE=sp, CC_HVC=cc_hvc,
-               NN_HVC=nn_hvc, CC_Z0B=cc_z0b)
+               NN_HVC=nn_hvc, CC_Z0B=cc_z0b, LAT=lat, SPONGE_LIST=[tuple(x) for x in sponge])
 
 
 # --------------------------------------------------------------------------------------

@@ -1848,6 +1848,32 @@ struct Oracle {
   void reg(const char* name, std::vector<double>& v) { fields[name] = Field{v.data(), nullptr, (int64_t)v.size()}; }
   void regi(const char* name, std::vector<int32_t>& v) { fields[name] = Field{nullptr, v.data(), (int64_t)v.size()}; }
 
+  // The boundary forcing between internal steps (the caller's UPDATE_RIVERS / UPDATE_WIND
+  // of BCOND_GCN(8), bcond_gcn.F:626-676, done on the host): the same rules as
+  // fvg_set_forcing.  NULL river or wind arrays leave those values unchanged.
+  int set_forcing(const fvg_forcing* f) {
+    if (!f || f->ntide != NTIDE) return FVG_ERR_ARG;
+    const bool wind = f->wstress_x && f->wstress_y;
+    if (wind && !have_wind) return FVG_ERR_UNSUPPORTED;
+    const size_t o1 = IOBCN + 1, q1 = NUMQBC + 1, n1 = N1;
+    if (NTIDE > 0) {
+      cp(t_period, f->period, (size_t)NTIDE);
+      cp(t_apt, f->apt, o1 * NTIDE);
+      cp(t_phai, f->phai, o1 * NTIDE);
+      if (f->emean) cp(t_emean, f->emean, o1); else t_emean.assign(o1, 0.0);
+    }
+    if (NUMQBC > 0) {
+      if (f->qdis) cp(qdis0, f->qdis, q1);
+      if (f->tdis) cp(tdis, f->tdis, q1);
+      if (f->sdis) cp(sdis, f->sdis, q1);
+    }
+    if (wind) {
+      cp(wsx, f->wstress_x, n1);
+      cp(wsy, f->wstress_y, n1);
+    }
+    return FVG_OK;
+  }
+
   int init(const fvg_mesh* m, const fvg_params* p, const fvg_forcing* f) {
     M = m->m; N = m->n; KB = m->kb; KBM1 = KB - 1; KBM2 = KB - 2;
     NE = m->ne; NCV = m->ncv; NCV_I = m->ncv_i; M1 = M + 1; N1 = N + 1;
@@ -2013,6 +2039,7 @@ int orc_run(orc* h, int32_t n) {
   for (int i = 0; i < n; ++i) reinterpret_cast<Oracle*>(h)->internal_step();
   return FVG_OK;
 }
+int orc_set_forcing(orc* h, const fvg_forcing* f) { return reinterpret_cast<Oracle*>(h)->set_forcing(f); }
 int orc_run_routine(orc* h, int32_t r, int32_t arg) { return reinterpret_cast<Oracle*>(h)->run_routine(r, arg); }
 int orc_set_threads(int32_t n) {
 #ifdef _OPENMP
