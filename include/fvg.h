@@ -119,6 +119,13 @@ typedef struct fvg_params {
   int32_t river_ts_setting;   /* 0 'specified' */
   int32_t river_location;     /* 0 'node', 1 'edge' */
   double tide_ref_time;       /* SpecTime: the zero of the tidal phase, seconds */
+  /* HEATING_ON with HEATING_TYPE 'flux' (vdif_ts.F:118-150, cntrl_prmtrs.F:144-160):
+     the surface net heat flux and the short-wave radiation absorbed over depth as
+     RHEAT*exp(z/ZETA1) + (1-RHEAT)*exp(z/ZETA2).  0 for no surface heating. */
+  int32_t heating_on;
+  double rheat;               /* HEATING_LONGWAVE_PERCTAGE */
+  double zeta1;               /* HEATING_LONGWAVE_LENGTHSCALE, m */
+  double zeta2;               /* HEATING_SHORTWAVE_LENGTHSCALE, m */
 } fvg_params;
 
 /* Boundary forcing that is constant in time for the supported cases. */
@@ -135,6 +142,10 @@ typedef struct fvg_forcing {
   /* surface wind stress before RAMP*0.001 scaling (UPDATE_WIND / ASIMPLE_DRAG);
      NULL for no wind.  (0:N) */
   const double *wstress_x, *wstress_y;
+  /* surface heating in W/m^2 before RAMP (UPDATE_HEAT, mod_force.F:12427; positive warms
+     the ocean): short-wave radiation and net heat flux per node (0:M).  Read only when
+     heating_on; NULL is taken as zero. */
+  const double *swrad, *wtsurf;
 } fvg_forcing;
 
 typedef struct fvg_handle fvg_handle;

@@ -59,6 +59,7 @@ class FvgParams(C.Structure):
         ("salinity_active", C.c_int32), ("obc_elevation_forcing_on", C.c_int32),
         ("obc_ts_type", C.c_int32), ("river_ts_setting", C.c_int32),
         ("river_location", C.c_int32), ("tide_ref_time", C.c_double),
+        ("heating_on", C.c_int32), ("rheat", C.c_double), ("zeta1", C.c_double), ("zeta2", C.c_double),
     ]
 
 
@@ -67,6 +68,7 @@ class FvgForcing(C.Structure):
         ("ntide", C.c_int32), ("period", _d), ("apt", _d), ("phai", _d), ("emean", _d),
         ("qdis", _d), ("tdis", _d), ("sdis", _d),
         ("wstress_x", _d), ("wstress_y", _d),
+        ("swrad", _d), ("wtsurf", _d),
     ]
 
 
@@ -114,6 +116,21 @@ def wind_stress(case):
     sx[0] = 0.0
     sy[0] = 0.0
     return sx, sy
+
+
+def heat_flux(case):
+    """(short-wave, net heat flux) in W/m^2 per node (0:M) before RAMP, or None.
+    ``case["forcing"]["heat"]`` holds ``swrad`` and ``wtsurf`` as scalars or (0:M) arrays."""
+    heat = case["forcing"].get("heat")
+    if heat is None:
+        return None
+    M = case["grid"]["M"]
+    out = []
+    for key in ("swrad", "wtsurf"):
+        a = np.broadcast_to(np.asarray(heat[key], dtype=np.float64), (M + 1,)).copy()
+        a[0] = 0.0
+        out.append(a)
+    return tuple(out)
 
 
 def make_structs(case):
@@ -177,6 +194,10 @@ def make_structs(case):
     ps.river_ts_setting = {"specified": 0, "calculated": 1}[p["RIVER_TS_SETTING"]]
     ps.river_location = {"node": 0, "edge": 1}[g["RIVER_LOC"]]
     ps.tide_ref_time = p.get("TIDE_REF_TIME", 0.0)
+    ps.heating_on = int(bool(p.get("HEATING_ON", False)))
+    ps.rheat = p.get("HEATING_LONGWAVE_PERCTAGE", 0.78)
+    ps.zeta1 = p.get("HEATING_LONGWAVE_LENGTHSCALE", 1.4)
+    ps.zeta2 = p.get("HEATING_SHORTWAVE_LENGTHSCALE", 6.3)
 
     fs = forcing_struct(case, b)
     return ms, ps, fs, b
@@ -212,6 +233,9 @@ def forcing_struct(case, b=None):
     ws = wind_stress(case)
     if ws is not None:
         fs.wstress_x, fs.wstress_y = b.d(ws[0]), b.d(ws[1])
+    hf = heat_flux(case)
+    if hf is not None:
+        fs.swrad, fs.wtsurf = b.d(hf[0]), b.d(hf[1])
     if own:
         fs._keep = b
     return fs

@@ -271,6 +271,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   if (prm->vertical_mixing != 0 || prm->river_ts_setting != 0) return FVG_ERR_UNSUPPORTED;
   if (prm->obc_ts_type < 1 || prm->obc_ts_type > 3) return FVG_ERR_UNSUPPORTED;
   if (f && f->ntide > kMaxTide) return FVG_ERR_UNSUPPORTED;
+  if (prm->heating_on && !(prm->rheat >= 0.0 && prm->zeta1 > 0.0 && prm->zeta2 > 0.0)) return FVG_ERR_ARG;
   fvg_handle* h = new fvg_handle();
   h->prm = *prm;
   Dev& P = h->P;
@@ -301,6 +302,8 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   P.ntide = h->ntide;
   P.obc_elev_on = prm->obc_elevation_forcing_on && h->ntide > 0;
   P.have_wind = f && f->wstress_x && f->wstress_y;
+  P.heating_on = prm->heating_on != 0;
+  P.rheat = prm->rheat; P.zeta1 = prm->zeta1; P.zeta2 = prm->zeta2;
   P.sl.isplit = prm->isplit;
   P.sl.ntide = h->ntide;
   P.sl.len = 1 + prm->isplit + prm->isplit * 4 * h->ntide;
@@ -543,6 +546,8 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   }
   UPD(wsx, P.have_wind ? f->wstress_x : nullptr, n1);
   UPD(wsy, P.have_wind ? f->wstress_y : nullptr, n1);
+  UPD(swrad_w, P.heating_on && f ? f->swrad : nullptr, m1);
+  UPD(wtsurf_w, P.heating_on && f ? f->wtsurf : nullptr, m1);
 
   // ---- state ----
   auto reg = [&](const char* name, double** p, size_t rows, int layers, size_t stride) -> int {
@@ -587,6 +592,8 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   // surface stress before the RAMP*0.001 scaling: a per-step forcing input
   h->fields["wstress_x"] = FieldDesc{(void*)P.wsx, (int64_t)n1, 1, (int64_t)n1, false};
   h->fields["wstress_y"] = FieldDesc{(void*)P.wsy, (int64_t)n1, 1, (int64_t)n1, false};
+  h->fields["swrad_watts"] = FieldDesc{(void*)P.swrad_w, (int64_t)m1, 1, (int64_t)m1, false};
+  h->fields["wtsurf_watts"] = FieldDesc{(void*)P.wtsurf_w, (int64_t)m1, 1, (int64_t)m1, false};
   if ((rc = dalloc(h, &P.scr_xflux, ms * KB))) return fail(rc);
   for (int t = 0; t < 2; ++t)
     for (int g = 0; g < 6; ++g) {
@@ -868,6 +875,11 @@ int fvg_set_forcing(fvg_handle* h, const fvg_forcing* f) {
   if (wind) {
     CK(cudaMemcpy((void*)P.wsx, f->wstress_x, n1 * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy((void*)P.wsy, f->wstress_y, n1 * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (P.heating_on) {
+    const size_t m1 = (size_t)P.M + 1;
+    if (f->swrad) CK(cudaMemcpy((void*)P.swrad_w, f->swrad, m1 * sizeof(double), cudaMemcpyHostToDevice));
+    if (f->wtsurf) CK(cudaMemcpy((void*)P.wtsurf_w, f->wtsurf, m1 * sizeof(double), cudaMemcpyHostToDevice));
   }
   return FVG_OK;
 }
@@ -1270,13 +1282,11 @@ extern "C" {
 int fvg_group_create(fvg_handle* const* hs, int32_t n, fvg_group** out) {
   if (!hs || !out || n < 1) return FVG_ERR_ARG;
   *out = nullptr;
-  int dev0 = -1;
   for (int32_t q = 0; q < n; ++q) {
     if (!hs[q]) return FVG_ERR_ARG;
     for (int32_t r = 0; r < q; ++r)
       if (hs[r] == hs[q]) return FVG_ERR_ARG;
   }
-  (void)dev0;
   fvg_group* g = new fvg_group();
   g->hs.assign(hs, hs + n);
   if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) { group_free(g); return FVG_ERR_CUDA; }

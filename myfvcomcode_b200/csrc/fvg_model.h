@@ -70,6 +70,8 @@ struct Dev {
   double fact, fm1;
   double const1, vhp1c;  // 16.6**0.6666667 and (15.8*100)**0.6666667 (vdif_q.F:172,227)
   int wetting_drying_on, river_location, obc_ts_type, obc_elev_on, have_wind;
+  int heating_on;
+  double rheat, zeta1, zeta2;
   SchedLayout sl;
   const double* sched;  // schedule table
   int* ctl;             // ctl[0] = current schedule slot; ctl[1] = error word
@@ -116,6 +118,7 @@ struct Dev {
   const int *cell_bcriv;                      // first river whose inflow cell this is (BCOND_GCN 2/3/5)
   // ----- forcing -----
   const double *wsx, *wsy;
+  const double *swrad_w, *wtsurf_w;  // surface heating, W/m^2 before RAMP (0:M)
 
   // ----- state, node 2-D -----
   double *el, *elf, *elrk, *et, *d, *dt, *dtfa, *egf, *wubot_n, *wvbot_n, *taubm_n;
@@ -193,6 +196,8 @@ constexpr int CLOS_IN = 8, CLOS_OUT = 3, CLOS_PLANES = CLOS_IN + CLOS_OUT + 1;
 // index helpers
 __host__ __device__ inline size_t N3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ms + i; }
 __host__ __device__ inline size_t C3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ns + i; }
+// RAMP of the current internal step, from its schedule row.
+__device__ inline double ramp_int(const Dev& P) { return P.sched[(size_t)P.ctl[0] * P.sl.len]; }
 
 // Mesh metrics and scratch of the edge-flux kernels by arithmetic type R.  The FP64
 // instantiation reads the FP64 arrays and forms the edge offsets as the reference does;

@@ -18,7 +18,6 @@ __device__ __constant__ double dAlpha3[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
 
 static inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
-__device__ inline double ramp_int(const Dev& P) { return P.sched[(size_t)P.ctl[0] * P.sl.len]; }
 
 // River clamp / tangential projection (bcond_gcn.F:345-405, 443-499, 552-608).
 __device__ inline void bc_solid3(const Dev& P, int i, double& uu, double& vv) {

@@ -823,8 +823,12 @@ __global__ void __launch_bounds__(256) k_fct_ts(const Dev P, int parts) {
 }
 
 // -------------------------------------------------------------------------------------
-// VDIF_TS(1,TF1) and VDIF_TS(2,SF1) (vdif_ts.F:78-337) with heating off (the surface
-// heat and short-wave terms are zero), one thread per node column.
+// VDIF_TS(1,TF1) and VDIF_TS(2,SF1) (vdif_ts.F:78-337), one thread per node column.
+// With surface heating (HEATING_TYPE 'flux', vdif_ts.F:118-150) the temperature column
+// takes the net heat flux WTSURF, held at zero while cooling water at or below -2 C,
+// and the short-wave flux RAD(K) = SWRAD*(RHEAT*EXP(Z*D/ZETA1) + (1-RHEAT)*EXP(Z*D/ZETA2))
+// absorbed between levels; WTSURF and SWRAD are the forcing in W/m^2 times RAMP over
+// -SPCP*ROSEA (BCOND_GCN(8), bcond_gcn.F:683-694).  Without heating every term is zero.
 // -------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_vdif_ts(const Dev P, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -841,16 +845,36 @@ __global__ void __launch_bounds__(128) k_vdif_ts(const Dev P, int parts) {
     if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
     double* F = (t == 0 ? P.tf1 : P.sf1);
     double vhf[kMaxKBs], vhpf[kMaxKBs];
-    const double rad = 0.0, wfsurf = 0.0, swradf = 0.0, sasurf = 0.0;
+    const double sasurf = 0.0;
+    double wfsurf = 0.0, swradf = 0.0;
+    const bool heat = t == 0 && P.heating_on;
+    if (heat) {
+      const double spro = 4.2174E3 * 1.023E3;
+      const double ramp = ramp_int(P);
+      wfsurf = -(P.wtsurf_w[i] * ramp) / spro;
+      swradf = -(P.swrad_w[i] * ramp) / spro;
+      const double wftmp1 = -2.0, wftmp2 = wfsurf;
+      const double wftmp3 = 0.5 * (1.0 + fsign1(wftmp1 - F[n3(1)]));
+      wfsurf = wftmp2 - wftmp3 * 0.5 * (wftmp2 + fabs(wftmp2));
+    }
+    // RAD at level k; zero without heating
+    auto RAD = [&](int k) {
+      if (!heat) return 0.0;
+      const double zdep = P.z[n3(k)] * d;
+      return swradf * (P.rheat * exp(zdep / P.zeta1) + (1 - P.rheat) * exp(zdep / P.zeta2));
+    };
+    double rad_k = RAD(1), rad_k1 = RAD(2);
     double af1 = AF(1);
     vhf[1] = af1 / (af1 - 1.);
-    vhpf[1] = -DTI * (sasurf + wfsurf - swradf + rad - rad) / (-P.dz[n3(1)] * d) - F[n3(1)];
+    vhpf[1] = -DTI * (sasurf + wfsurf - swradf + rad_k - rad_k1) / (-P.dz[n3(1)] * d) - F[n3(1)];
     vhpf[1] = vhpf[1] / (af1 - 1.);
     for (int k = 2; k <= KBM2; ++k) {
+      rad_k = rad_k1;
+      rad_k1 = RAD(k + 1);
       double af = AF(k), cf = CF(k);
       double p = 1. / (af + cf * (1. - vhf[k - 1]) - 1.);
       vhf[k] = af * p;
-      vhpf[k] = (cf * vhpf[k - 1] - F[n3(k)] + DTI * (rad - rad) / (d * P.dz[n3(k)])) * p;
+      vhpf[k] = (cf * vhpf[k - 1] - F[n3(k)] + DTI * (rad_k - rad_k1) / (d * P.dz[n3(k)])) * p;
     }
     if (P.isonb[i] != 2 && update) {
       double pfx = t == 0 ? P.pfpxb_t[i] : P.pfpxb_s[i];
@@ -867,7 +891,8 @@ __global__ void __launch_bounds__(128) k_vdif_ts(const Dev P, int parts) {
         tmp = -tmp;
       }
       double cfb = CF(KBM1);
-      double ff = (cfb * vhpf[KBM2] - F[n3(KBM1)] - GW + DTI * (rad - rad - tmp) / (d * P.dz[n3(KBM1)])) /
+      const double rad_b = RAD(KBM1), rad_kb = RAD(KB);
+      double ff = (cfb * vhpf[KBM2] - F[n3(KBM1)] - GW + DTI * (rad_b - rad_kb - tmp) / (d * P.dz[n3(KBM1)])) /
                   (cfb * (1. - vhf[KBM2]) - 1.);
       F[n3(KBM1)] = ff;
       for (int k = 2; k <= KBM1; ++k) {

@@ -18,7 +18,7 @@ import copy
 
 import numpy as np
 
-from .abi import wind_stress
+from .abi import heat_flux, wind_stress
 
 # Row dimension and value kind of every grid array that depends on the mesh.
 # row: "node" (M+1), "cell" (N+1), "edge" (NE+1), "he" (NCV+1), "hei" (NCV_I+1),
@@ -143,6 +143,10 @@ def union_case(base, specs):
         f["wind"] = {"kind": "field", "sx": np.concatenate(sx), "sy": np.concatenate(sy)}
     else:
         f["wind"] = None
+    hf = heat_flux(base)
+    if hf is not None:
+        f["heat"] = {"swrad": np.concatenate([hf[0][:1]] + [hf[0][1:]] * nm),
+                     "wtsurf": np.concatenate([hf[1][:1]] + [hf[1][1:]] * nm)}
     init = dict(base["init"])
     M = g["M"]
     toff = np.zeros(M * nm + 1)

