@@ -126,6 +126,11 @@ typedef struct fvg_params {
   double rheat;               /* HEATING_LONGWAVE_PERCTAGE */
   double zeta1;               /* HEATING_LONGWAVE_LENGTHSCALE, m */
   double zeta2;               /* HEATING_SHORTWAVE_LENGTHSCALE, m */
+  /* Face-value limiter of the momentum advection (ADVAVE, ADVECTION, ADV_UV), FVCOM's
+     compile-time choice: 0 LIMITED_NO; 1 LIMITED_1 (the slope limiter UALFA/VALFA and the
+     clamp of both face values into the range of the two cells); 2 the slope limiter alone
+     (advave_edge_gcn.F:128-330, advection_edge_gcn.F:107-335, adv_uv_edge_gcn.F:138-400). */
+  int32_t limiter;
 } fvg_params;
 
 /* Boundary forcing that is constant in time for the supported cases. */

@@ -60,6 +60,7 @@ class FvgParams(C.Structure):
         ("obc_ts_type", C.c_int32), ("river_ts_setting", C.c_int32),
         ("river_location", C.c_int32), ("tide_ref_time", C.c_double),
         ("heating_on", C.c_int32), ("rheat", C.c_double), ("zeta1", C.c_double), ("zeta2", C.c_double),
+        ("limiter", C.c_int32),
     ]
 
 
@@ -198,6 +199,7 @@ def make_structs(case):
     ps.rheat = p.get("HEATING_LONGWAVE_PERCTAGE", 0.78)
     ps.zeta1 = p.get("HEATING_LONGWAVE_LENGTHSCALE", 1.4)
     ps.zeta2 = p.get("HEATING_SHORTWAVE_LENGTHSCALE", 6.3)
+    ps.limiter = {"LIMITED_NO": 0, "LIMITED_1": 1, "LIMITED_2": 2}.get(p.get("LIMITER", "LIMITED_NO"), -1)
 
     fs = forcing_struct(case, b)
     return ms, ps, fs, b

@@ -182,6 +182,7 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   mk.mark(s, G_ADV3D);
   launch_baropg(P, s, !p.barotropic, 1);
   launch_ext_prep(P, s);
+  if (P.limiter) launch_alfa2(P, s);
   mk.mark(s, G_BAROPG);
   launch_ext_cell(P, s, 1, 1, EC_INT_ADVAVE);
   launch_int_reset(P, s);
@@ -208,6 +209,7 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
         launch_wet_judge(Q, s);
         mk.mark(s, G_WET);
       }
+      if (P.limiter) launch_alfa2(Q, s);
       launch_ext_cell(Q, s, iext, K,
                       (p.wetting_drying_on ? 0 : EC_N2E) | EC_FLUXOBN | EC_ADVAVE | EC_EXTUV | EC_BC2 |
                           (K == 1 ? EC_COPY_RK : 0) | EC_FINISH);
@@ -272,6 +274,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   if (prm->obc_ts_type < 1 || prm->obc_ts_type > 3) return FVG_ERR_UNSUPPORTED;
   if (f && f->ntide > kMaxTide) return FVG_ERR_UNSUPPORTED;
   if (prm->heating_on && !(prm->rheat >= 0.0 && prm->zeta1 > 0.0 && prm->zeta2 > 0.0)) return FVG_ERR_ARG;
+  if (prm->limiter < 0 || prm->limiter > 2) return FVG_ERR_ARG;
   fvg_handle* h = new fvg_handle();
   h->prm = *prm;
   Dev& P = h->P;
@@ -303,6 +306,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   P.obc_elev_on = prm->obc_elevation_forcing_on && h->ntide > 0;
   P.have_wind = f && f->wstress_x && f->wstress_y;
   P.heating_on = prm->heating_on != 0;
+  P.limiter = prm->limiter;
   P.rheat = prm->rheat; P.zeta1 = prm->zeta1; P.zeta2 = prm->zeta2;
   P.sl.isplit = prm->isplit;
   P.sl.ntide = h->ntide;
@@ -608,6 +612,13 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   for (int q = 0; q < 4; ++q) {
     if ((rc = dalloc(h, &P.g2d[q], n1))) return fail(rc);
   }
+  if (P.limiter) {
+    std::vector<double> ones(std::max(n1, (size_t)P.ns * KB), 1.0);
+    for (int q = 0; q < 2; ++q) {
+      if ((rc = upload(h, &P.alfa2[q], ones.data(), n1))) return fail(rc);
+      if ((rc = upload(h, &P.alfa3[q], ones.data(), (size_t)P.ns * KB))) return fail(rc);
+    }
+  }
   if ((rc = dalloc(h, &P.exf2d, v1))) return fail(rc);
   for (int q = 0; q < 4; ++q)
     if ((rc = dalloc(h, &P.g3[q], ns * KB))) return fail(rc);
@@ -816,6 +827,7 @@ int32_t fvg_kernels_per_step(const fvg_handle* h) {
   const fvg_params& p = h->prm;
   int n = 1 + 1 + 2 + 2 + 2;                                // begin, cell_pre, grad3+adv3d, baropg+prep, int advave+reset
   n += p.isplit * 4 * (2 + (p.wetting_drying_on ? 2 : 0)) + 1; // RK stages, closing update
+  if (p.limiter) n += p.isplit * 4 + 1 + 2;                  // slope limiters: stages, ADVAVE, 3-D
   n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv
   n += 7;                                                  // grad_q, adv_q (2 phases), vdif_q (4 passes)
   if (h->P.closure) n += 1;                                // learned closure
@@ -898,6 +910,15 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     for (int q = 0; q < 4; ++q) {
       if ((rc = dalloc(h, &f.g2d[q], n1))) return fail(rc);
       if ((rc = dalloc(h, &f.g3[q], ns * KB))) return fail(rc);
+    }
+    if (P.limiter) {
+      std::vector<float> ones(std::max(n1, ns * KB), 1.0f);
+      for (int q = 0; q < 2; ++q) {
+        if ((rc = dalloc(h, &f.alfa2[q], n1))) return fail(rc);
+        if ((rc = dalloc(h, &f.alfa3[q], ns * KB))) return fail(rc);
+        CK(cudaMemcpy(f.alfa2[q], ones.data(), n1 * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(f.alfa3[q], ones.data(), ns * KB * sizeof(float), cudaMemcpyHostToDevice));
+      }
     }
     if ((rc = dalloc(h, &f.npk, ms * KB * 16))) return fail(rc);
     if ((rc = dalloc(h, (float**)&f.ex2, (size_t)P.ncvs * KB * 2))) return fail(rc);
@@ -1089,6 +1110,7 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
     case FVG_R_FLUX_OBN: launch_ext_cell(P, s, 1, arg, EC_FLUXOBN); break;
     case FVG_R_ADVAVE:
       launch_ext_prep(P, s);
+      if (P.limiter) launch_alfa2(P, s);
       launch_ext_cell(P, s, 1, 1, EC_ADVAVE);
       break;
     case FVG_R_EXTUV_EDGE: launch_ext_cell(P, s, 1, arg, EC_EXTUV); break;
@@ -1099,6 +1121,7 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
       for (int K = 1; K <= 4; ++K) {
         launch_ext_node(P, s, iext, K, EN_EXTEL | EN_BC | EN_GRAD | (K == 1 ? EN_COPY_ELRK : 0));
         if (p.wetting_drying_on) launch_wet_judge(P, s);
+        if (P.limiter) launch_alfa2(P, s);
         launch_ext_cell(P, s, iext, K,
                         (p.wetting_drying_on ? 0 : EC_N2E) | EC_FLUXOBN | EC_ADVAVE | EC_EXTUV | EC_BC2 |
                             (K == 1 ? EC_COPY_RK : 0));
@@ -1125,6 +1148,7 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
     case FVG_R_INT_PRE_EXT:
       launch_baropg(P, s, 0, 1);
       launch_ext_prep(P, s);
+      if (P.limiter) launch_alfa2(P, s);
       launch_ext_cell(P, s, 1, 1, EC_INT_ADVAVE);
       launch_int_reset(P, s);
       break;

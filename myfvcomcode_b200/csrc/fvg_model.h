@@ -42,6 +42,7 @@ struct SchedLayout {
 // same for y.
 struct F32 {
   float *g2d[4], *g3[4];
+  float *alfa2[2], *alfa3[2];  // slope limiters UALFA, VALFA (see Dev)
   float* npk;  // node records of the ring gradients, 16 floats per (node, layer)
   float2* ex2;
   float *xo, *yo, *dltxc, *dltyc, *art, *cc_hvc, *a1u, *a2u;
@@ -72,6 +73,7 @@ struct Dev {
   int wetting_drying_on, river_location, obc_ts_type, obc_elev_on, have_wind;
   int heating_on;
   double rheat, zeta1, zeta2;
+  int limiter;  // 0 LIMITED_NO, 1 LIMITED_1, 2 the slope limiter alone
   SchedLayout sl;
   const double* sched;  // schedule table
   int* ctl;             // ctl[0] = current schedule slot; ctl[1] = error word
@@ -148,6 +150,9 @@ struct Dev {
   double *vq_prod, *vq_gh, *vq_dtef, *vq_dtefl, *vq_ut;
   double2* ex2;                              // half-edge fluxes of both advected tracers (ncvs x KB)
   double* g2d[4];                            // least-squares gradient of UA, VA per cell (COFA1/2/5/6)
+  // Slope limiters of the limited schemes, UALFA and VALFA: per cell of the 2-D mode
+  // (N+1) and per cell and layer of the 3-D mode (ns x KB); index 0 holds 1.
+  double *alfa2[2], *alfa3[2];
   double* exf2d;                             // EXTEL_EDGE flux of each half-edge (NCV+1)
   double* g3[4];                             // least-squares gradient of U, V per cell and layer (ns x KB)
   int ncvs;                                  // layer stride of ex (>= NCV+1)
@@ -226,6 +231,8 @@ template <> struct Mesh<double> {
   __device__ static double dltxncve(const Dev& P, size_t q) { return P.dltxncve[q]; }
   __device__ static double dltyncve(const Dev& P, size_t q) { return P.dltyncve[q]; }
   __device__ static double* g2d(const Dev& P, int q) { return P.g2d[q]; }
+  __device__ static double* alfa2(const Dev& P, int q) { return P.alfa2[q]; }
+  __device__ static double* alfa3(const Dev& P, int q) { return P.alfa3[q]; }
   __device__ static double* g3(const Dev& P, int q) { return P.g3[q]; }
   __device__ static double2* ex2(const Dev& P) { return P.ex2; }
 };
@@ -252,9 +259,33 @@ template <> struct Mesh<float> {
   __device__ static float dltxncve(const Dev& P, size_t q) { return P.f.dltxncve[q]; }
   __device__ static float dltyncve(const Dev& P, size_t q) { return P.f.dltyncve[q]; }
   __device__ static float* g2d(const Dev& P, int q) { return P.f.g2d[q]; }
+  __device__ static float* alfa2(const Dev& P, int q) { return P.f.alfa2[q]; }
+  __device__ static float* alfa3(const Dev& P, int q) { return P.f.alfa3[q]; }
   __device__ static float* g3(const Dev& P, int q) { return P.f.g3[q]; }
   __device__ static float2* ex2(const Dev& P) { return P.f.ex2; }
 };
+// Limited schemes (advave_edge_gcn.F:226-229, 300-303, 340-357): the slope limiter of one
+// cell and edge, min(ALFA, min(1, |U(IA)-U(IB)| / |U'+EPSILON|)), EPSILON of the form's type.
+template <typename R>
+__device__ inline void lim_alfa(R num, R ext, R& a) {
+  R t = num / fabs(ext + (R)(sizeof(R) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07));
+  if (t > (R)1) t = (R)1;
+  a = t < a ? t : a;
+}
+// Face values U + ALFA*U' of both cells; under LIMITED_1 both revert to the cell values
+// when either leaves their range.
+template <typename R>
+__device__ inline void lim_faces(int limiter, R ua, R ub, R ea, R eb, R alfa_a, R alfa_b, R& f1, R& f2) {
+  f1 = ua + alfa_a * ea;
+  f2 = ub + alfa_b * eb;
+  if (limiter == 1) {
+    R hi = ua > ub ? ua : ub, lo = ua < ub ? ua : ub;
+    if (f1 > hi || f1 < lo || f2 > hi || f2 < lo) {
+      f1 = ua;
+      f2 = ub;
+    }
+  }
+}
 __device__ inline double2 mk2(double a, double b) { return make_double2(a, b); }
 __device__ inline float2 mk2(float a, float b) { return make_float2(a, b); }
 
@@ -277,6 +308,7 @@ void launch_ext_finish(const Dev& P, cudaStream_t s, int K);
 void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts);
 void launch_wet_judge(const Dev& P, cudaStream_t s);
 void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts);
+void launch_alfa2(const Dev& P, cudaStream_t s);
 void launch_ext_update(const Dev& P, cudaStream_t s, int K);
 void launch_begin_step(const Dev& P, cudaStream_t s);
 void launch_ext_prep(const Dev& P, cudaStream_t s);

@@ -117,6 +117,31 @@ __device__ inline void ext_update_cell(const Dev& P, int i, int K, double u, dou
   }
 }
 
+// Slope limiters UALFA, VALFA of each cell for the limited ADVAVE (advave_edge_gcn.F:141-318):
+// the cell's three edges with a wet side, in any order (a minimum), from the cell's own
+// gradient and the two cells' UA, VA.  After WET_JUDGE, before the stage's ADVAVE.
+template <typename R>
+__global__ void k_alfa2(const Dev P) {
+  typedef Mesh<R> Mh;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (c > P.N) return;
+  const size_t n1 = P.N + 1;
+  const Grad<R> g = load_grad<R>(P, c);
+  R au = (R)1, av = (R)1;
+  for (int s = 0; s < 3; ++s) {
+    const size_t q = (size_t)s * n1 + c;
+    const int ia = P.ce_ia[q], ib = P.ce_ib[q];
+    if (!(P.iswetce[ia] * P.iswetc[ia] == 1 || P.iswetce[ib] * P.iswetc[ib] == 1)) continue;
+    const bool a_side = (P.ce_code[q] & 1) == 0;
+    const R x = a_side ? Mh::s_xoa(P, q) : Mh::s_xob(P, q);
+    const R y = a_side ? Mh::s_yoa(P, q) : Mh::s_yob(P, q);
+    lim_alfa<R>(fabs((R)P.ua[ia] - (R)P.ua[ib]), g.ux * x + g.uy * y, au);
+    lim_alfa<R>(fabs((R)P.va[ia] - (R)P.va[ib]), g.vx * x + g.vy * y, av);
+  }
+  Mh::alfa2(P, 0)[c] = au;
+  Mh::alfa2(P, 1)[c] = av;
+}
+
 __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   // cell part: least-squares gradient of the current UA, VA for ADVAVE of this stage
@@ -222,15 +247,21 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
     double elij = 0.5 * (P.el[j1] + P.el[j2]);
     if (P.iswetce[ia] * P.iswetc[ia] == 1 || P.iswetce[ib] * P.iswetc[ib] == 1) {
       Grad<R> ga = load_grad<R>(P, ia);
-      R xij = Mh::s_xoa(P, q);
-      R yij = Mh::s_yoa(P, q);
-      R uij1 = (R)P.ua[ia] + ga.ux * xij + ga.uy * yij;
-      R vij1 = (R)P.va[ia] + ga.vx * xij + ga.vy * yij;
       Grad<R> gb = load_grad<R>(P, ib);
-      xij = Mh::s_xob(P, q);
-      yij = Mh::s_yob(P, q);
-      R uij2 = (R)P.ua[ib] + gb.ux * xij + gb.uy * yij;
-      R vij2 = (R)P.va[ib] + gb.vx * xij + gb.vy * yij;
+      const R xija = Mh::s_xoa(P, q), yija = Mh::s_yoa(P, q);
+      const R xijb = Mh::s_xob(P, q), yijb = Mh::s_yob(P, q);
+      R uij1, vij1, uij2, vij2;
+      if (P.limiter == 0) {
+        uij1 = (R)P.ua[ia] + ga.ux * xija + ga.uy * yija;
+        vij1 = (R)P.va[ia] + ga.vx * xija + ga.vy * yija;
+        uij2 = (R)P.ua[ib] + gb.ux * xijb + gb.uy * yijb;
+        vij2 = (R)P.va[ib] + gb.vx * xijb + gb.vy * yijb;
+      } else {
+        lim_faces<R>(P.limiter, (R)P.ua[ia], (R)P.ua[ib], ga.ux * xija + ga.uy * yija, gb.ux * xijb + gb.uy * yijb,
+                     Mh::alfa2(P, 0)[ia], Mh::alfa2(P, 0)[ib], uij1, uij2);
+        lim_faces<R>(P.limiter, (R)P.va[ia], (R)P.va[ib], ga.vx * xija + ga.vy * yija, gb.vx * xijb + gb.vy * yijb,
+                     Mh::alfa2(P, 1)[ia], Mh::alfa2(P, 1)[ib], vij1, vij2);
+      }
       R uij = half * (uij1 + uij2);
       R vij = half * (vij1 + vij2);
       const R dltxc = Mh::s_dx(P, q), dltyc = Mh::s_dy(P, q);
@@ -445,6 +476,12 @@ void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
   k_ext_node<<<nblk(n, 256), 256, 0, s>>>(P, iext, K, parts);
 }
 void launch_ext_prep(const Dev& P, cudaStream_t s) { k_ext_prep<<<nblk(P.N, 256), 256, 0, s>>>(P); }
+void launch_alfa2(const Dev& P, cudaStream_t s) {
+  if (P.prec)
+    k_alfa2<float><<<nblk(P.N, 128), 128, 0, s>>>(P);
+  else
+    k_alfa2<double><<<nblk(P.N, 128), 128, 0, s>>>(P);
+}
 
 // FP32 copies of the mesh metrics the precision form's flux kernels read.
 __global__ void k_d2f(const double* __restrict__ src, float* __restrict__ dst, size_t n) {

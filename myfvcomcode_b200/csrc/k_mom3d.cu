@@ -152,6 +152,37 @@ __global__ void __launch_bounds__(256) k_grad3(const Dev P) {
   }
 }
 
+// Slope limiters UALFA, VALFA of each cell and layer for the limited ADVECTION and ADV_UV
+// (advection_edge_gcn.F:118-259, adv_uv_edge_gcn.F:152-330): the cell's three edges with a
+// wet side on the layer, from the cell's own gradient and the two cells' U, V.
+template <typename R>
+__global__ void __launch_bounds__(256) k_alfa3(const Dev P) {
+  typedef Mesh<R> Mh;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (c > P.N) return;
+  const size_t n1 = P.N + 1;
+  int kb, ke;
+  col_range(P, 1, P.KBM1, kb, ke);
+  for (int k = kb; k <= ke; ++k) {
+    const double* U = P.u + C3(P, 0, k);
+    const double* V = P.v + C3(P, 0, k);
+    const G3<R> g = load_g3<R>(P, c, k);
+    R au = (R)1, av = (R)1;
+    for (int s = 0; s < 3; ++s) {
+      const size_t q = (size_t)s * n1 + c;
+      const int ia = P.ce_ia[q], ib = P.ce_ib[q];
+      if (!(P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1)) continue;
+      const bool a_side = (P.ce_code[q] & 1) == 0;
+      const R x = a_side ? Mh::s_xoa(P, q) : Mh::s_xob(P, q);
+      const R y = a_side ? Mh::s_yoa(P, q) : Mh::s_yob(P, q);
+      lim_alfa<R>(fabs((R)U[ia] - (R)U[ib]), g.ux * x + g.uy * y, au);
+      lim_alfa<R>(fabs((R)V[ia] - (R)V[ib]), g.vx * x + g.vy * y, av);
+    }
+    Mh::alfa3(P, 0)[C3(P, c, k)] = au;
+    Mh::alfa3(P, 1)[C3(P, c, k)] = av;
+  }
+}
+
 // q: the edge's slot in the cell slot table (offsets and DLTXC/DLTYC of the edge).
 template <typename R>
 __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib, int k, R dij, bool exflux_form) {
@@ -162,11 +193,20 @@ __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib,
   R xija = Mh::s_xoa(P, q), yija = Mh::s_yoa(P, q);
   R xijb = Mh::s_xob(P, q), yijb = Mh::s_yob(P, q);
   G3<R> ga = load_g3<R>(P, ia, k);
-  R uij1 = (R)U[ia] + ga.ux * xija + ga.uy * yija;
-  R vij1 = (R)V[ia] + ga.vx * xija + ga.vy * yija;
   G3<R> gb = load_g3<R>(P, ib, k);
-  R uij2 = (R)U[ib] + gb.ux * xijb + gb.uy * yijb;
-  R vij2 = (R)V[ib] + gb.vx * xijb + gb.vy * yijb;
+  R uij1, vij1, uij2, vij2;
+  if (P.limiter == 0) {
+    uij1 = (R)U[ia] + ga.ux * xija + ga.uy * yija;
+    vij1 = (R)V[ia] + ga.vx * xija + ga.vy * yija;
+    uij2 = (R)U[ib] + gb.ux * xijb + gb.uy * yijb;
+    vij2 = (R)V[ib] + gb.vx * xijb + gb.vy * yijb;
+  } else {
+    const size_t qa = C3(P, ia, k), qb = C3(P, ib, k);
+    lim_faces<R>(P.limiter, (R)U[ia], (R)U[ib], ga.ux * xija + ga.uy * yija, gb.ux * xijb + gb.uy * yijb,
+                 Mh::alfa3(P, 0)[qa], Mh::alfa3(P, 0)[qb], uij1, uij2);
+    lim_faces<R>(P.limiter, (R)V[ia], (R)V[ib], ga.vx * xija + ga.vy * yija, gb.vx * xijb + gb.vy * yijb,
+                 Mh::alfa3(P, 1)[qa], Mh::alfa3(P, 1)[qb], vij1, vij2);
+  }
   R uij = half * (uij1 + uij2);
   R vij = half * (vij1 + vij2);
   R viscof1 = Mh::art(P, ia) * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + half * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
@@ -754,7 +794,14 @@ void launch_grad3(const Dev& P, cudaStream_t s) {
   else
     k_grad3<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
+static void launch_alfa3(const Dev& P, cudaStream_t s) {
+  if (P.prec)
+    k_alfa3<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  else
+    k_alfa3<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+}
 void launch_advection3d(const Dev& P, cudaStream_t s) {
+  if (P.limiter) launch_alfa3(P, s);
   if (P.prec)
     k_advection3d<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
   else
@@ -779,6 +826,7 @@ void launch_w_viscofh(const Dev& P, cudaStream_t s, int do_w, int do_visc) {
   k_w_viscofh<<<col_grid(P, n, P.KB), P.col_bc, 0, s>>>(P, do_w, do_visc);
 }
 void launch_adv_uv(const Dev& P, cudaStream_t s) {
+  if (P.limiter) launch_alfa3(P, s);
   if (P.prec)
     k_adv_uv<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
   else

@@ -43,6 +43,7 @@ MODULE FVG_BIND
     REAL(C_DOUBLE) :: TIDE_REF_TIME
     INTEGER(C_INT32_T) :: HEATING_ON
     REAL(C_DOUBLE) :: RHEAT, ZETA1, ZETA2
+    INTEGER(C_INT32_T) :: LIMITER        ! 0 LIMITED_NO, 1 LIMITED_1, 2 slope limiter alone
   END TYPE FVG_PARAMS_T
 
   TYPE, BIND(C) :: FVG_FORCING_T

@@ -577,7 +577,9 @@ def _s(v, default=""):
 class FvcomRun:
     """An FVCOM case read from its run namelist (``<case>_run.nml``) and input files."""
 
-    def __init__(self, nml_path, input_dir=None):
+    def __init__(self, nml_path, input_dir=None, limiter="LIMITED_NO"):
+        """``limiter``: FVCOM's compile-time choice of the momentum advection limiter,
+        LIMITED_NO, LIMITED_1 or LIMITED_2 (the run namelist does not carry it)."""
         self.nml_path = os.path.abspath(nml_path)
         nml = read_namelist(nml_path)
         self.nml = nml
@@ -630,6 +632,7 @@ class FvcomRun:
             SALINITY_ACTIVE=_b(ph.get("SALINITY_ACTIVE"), True),
             OBC_TS_TYPE=int(obc.get("OBC_TS_TYPE", 3)),
             RIVER_TS_SETTING=_s(rt.get("RIVER_TS_SETTING"), "specified").lower(),
+            LIMITER=limiter,
         )
 
         gc = group(nml, "NML_GRID_COORDINATES")

@@ -291,10 +291,65 @@ struct Oracle {
   // =====================================================================================
   // ADVAVE_EDGE_GCN(XFLUX,YFLUX), LIMITED_NO branch (advave_edge_gcn.F:32-1145)
   // =====================================================================================
+  // Phase one of the limited schemes (advave_edge_gcn.F:141-318, advection_edge_gcn.F:
+  // 118-259, adv_uv_edge_gcn.F:152-330): per cell the smallest, over its wet edges, of
+  // |U(IA)-U(IB)| / |U'+EPSILON|, at most 1, where U' = COFA1*XIJ + COFA2*YIJ is the
+  // cell's gradient extrapolation to the edge.  wet(c) is the routine's wet flag product.
+  template <class Wet>
+  void limiter_alfa(const double* U, const double* V, Wet wet, std::vector<double>& ualfa,
+                    std::vector<double>& valfa) const {
+    const double eps = 2.220446049250313e-16;  // EPSILON of the reference's REAL(SP) = REAL(DP)
+    ualfa.assign(N1, 1.0);
+    valfa.assign(N1, 1.0);
+    auto lim = [&](double num, double ext, double& a) {
+      double t = num / std::fabs(ext + eps);
+      if (t > 1) t = 1.0;
+      a = t < a ? t : a;
+    };
+    for (int i = 1; i <= NE; ++i) {
+      int ia = IEC(i, 1), ib = IEC(i, 2);
+      if (!(wet(ia) || wet(ib))) continue;
+      for (int side = 0; side < 2; ++side) {
+        int c = side == 0 ? ia : ib;
+        int k1 = NBE(c, 1), k2 = NBE(c, 2), k3 = NBE(c, 3);
+        double cofa1 = A1U(c, 1) * U[c] + A1U(c, 2) * U[k1] + A1U(c, 3) * U[k2] + A1U(c, 4) * U[k3];
+        double cofa2 = A2U(c, 1) * U[c] + A2U(c, 2) * U[k1] + A2U(c, 3) * U[k2] + A2U(c, 4) * U[k3];
+        double cofa5 = A1U(c, 1) * V[c] + A1U(c, 2) * V[k1] + A1U(c, 3) * V[k2] + A1U(c, 4) * V[k3];
+        double cofa6 = A2U(c, 1) * V[c] + A2U(c, 2) * V[k1] + A2U(c, 3) * V[k2] + A2U(c, 4) * V[k3];
+        double xij = xijc[i] - xc[c], yij = yijc[i] - yc[c];
+        lim(std::fabs(U[ia] - U[ib]), cofa1 * xij + cofa2 * yij, ualfa[c]);
+        lim(std::fabs(V[ia] - V[ib]), cofa5 * xij + cofa6 * yij, valfa[c]);
+      }
+    }
+  }
+  // Face values of one edge: unlimited, U + COFA1*XIJ + COFA2*YIJ; limited, U + ALFA*(COFA1*
+  // XIJ + COFA2*YIJ), and under LIMITED_1 both faces reset to the cell values when either
+  // leaves their range.
+  void face_values(double ua_, double ub_, double ca1, double ca2, double xa, double ya, double cb1,
+                   double cb2, double xb, double yb, double alfa_a, double alfa_b, double& f1,
+                   double& f2) const {
+    if (P.limiter == 0) {
+      f1 = ua_ + ca1 * xa + ca2 * ya;
+      f2 = ub_ + cb1 * xb + cb2 * yb;
+      return;
+    }
+    f1 = ua_ + alfa_a * (ca1 * xa + ca2 * ya);
+    f2 = ub_ + alfa_b * (cb1 * xb + cb2 * yb);
+    if (P.limiter == 1) {
+      double hi = std::max(ua_, ub_), lo = std::min(ua_, ub_);
+      if (f1 > hi || f1 < lo || f2 > hi || f2 < lo) {
+        f1 = ua_;
+        f2 = ub_;
+      }
+    }
+  }
+
   void advave(std::vector<double>& xflux, std::vector<double>& yflux) {
     double fact = P.horizontal_mixing == 0 ? 1.0 : 0.0;
     double fm1 = P.horizontal_mixing == 0 ? 0.0 : 1.0;
     for (int i = 0; i <= N; ++i) { xflux[i] = 0.0; yflux[i] = 0.0; pstx[i] = 0.0; psty[i] = 0.0; }
+    std::vector<double> ualfa, valfa;
+    if (P.limiter) limiter_alfa(ua.data(), va.data(), [&](int c) { return iswetce[c] * iswetc[c] == 1; }, ualfa, valfa);
     for (int i = 1; i <= NE; ++i) {
       int ia = IEC(i, 1), ib = IEC(i, 2);
       int j1 = IENODE(i, 1), j2 = IENODE(i, 2);
@@ -306,19 +361,21 @@ struct Oracle {
         double cofa2 = A2U(ia, 1) * ua[ia] + A2U(ia, 2) * ua[k1] + A2U(ia, 3) * ua[k2] + A2U(ia, 4) * ua[k3];
         double cofa5 = A1U(ia, 1) * va[ia] + A1U(ia, 2) * va[k1] + A1U(ia, 3) * va[k2] + A1U(ia, 4) * va[k3];
         double cofa6 = A2U(ia, 1) * va[ia] + A2U(ia, 2) * va[k1] + A2U(ia, 3) * va[k2] + A2U(ia, 4) * va[k3];
-        double xij = xijc[i] - xc[ia];
-        double yij = yijc[i] - yc[ia];
-        double uij1 = ua[ia] + cofa1 * xij + cofa2 * yij;
-        double vij1 = va[ia] + cofa5 * xij + cofa6 * yij;
+        double xija = xijc[i] - xc[ia];
+        double yija = yijc[i] - yc[ia];
         k1 = NBE(ib, 1); k2 = NBE(ib, 2); k3 = NBE(ib, 3);
         double cofa3 = A1U(ib, 1) * ua[ib] + A1U(ib, 2) * ua[k1] + A1U(ib, 3) * ua[k2] + A1U(ib, 4) * ua[k3];
         double cofa4 = A2U(ib, 1) * ua[ib] + A2U(ib, 2) * ua[k1] + A2U(ib, 3) * ua[k2] + A2U(ib, 4) * ua[k3];
         double cofa7 = A1U(ib, 1) * va[ib] + A1U(ib, 2) * va[k1] + A1U(ib, 3) * va[k2] + A1U(ib, 4) * va[k3];
         double cofa8 = A2U(ib, 1) * va[ib] + A2U(ib, 2) * va[k1] + A2U(ib, 3) * va[k2] + A2U(ib, 4) * va[k3];
-        xij = xijc[i] - xc[ib];
-        yij = yijc[i] - yc[ib];
-        double uij2 = ua[ib] + cofa3 * xij + cofa4 * yij;
-        double vij2 = va[ib] + cofa7 * xij + cofa8 * yij;
+        double xijb = xijc[i] - xc[ib];
+        double yijb = yijc[i] - yc[ib];
+        const bool L = P.limiter != 0;
+        double uij1, uij2, vij1, vij2;
+        face_values(ua[ia], ua[ib], cofa1, cofa2, xija, yija, cofa3, cofa4, xijb, yijb, L ? ualfa[ia] : 1.0,
+                    L ? ualfa[ib] : 1.0, uij1, uij2);
+        face_values(va[ia], va[ib], cofa5, cofa6, xija, yija, cofa7, cofa8, xijb, yijb, L ? valfa[ia] : 1.0,
+                    L ? valfa[ib] : 1.0, vij1, vij2);
         double uij = 0.5 * (uij1 + uij2);
         double vij = 0.5 * (vij1 + vij2);
         double un = -uij * dltyc[i] + vij * dltxc[i];
@@ -625,6 +682,10 @@ struct Oracle {
     std::fill(advy.begin(), advy.end(), 0.0);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int k = 1; k <= KBM1; ++k) {
+      std::vector<double> ualfa, valfa;
+      if (P.limiter)
+        limiter_alfa(&u[c3(0, k)], &v[c3(0, k)], [&](int c) { return iswetct[c] * iswetc[c] == 1; }, ualfa, valfa);
+      const bool L = P.limiter != 0;
       for (int i = 1; i <= NE; ++i) {
         int ia = IEC(i, 1), ib = IEC(i, 2);
         if (!(iswetct[ia] * iswetc[ia] == 1 || iswetct[ib] * iswetc[ib] == 1)) continue;
@@ -639,14 +700,15 @@ struct Oracle {
         double cofa2 = A2U(ia, 1) * U_[ia] + A2U(ia, 2) * U_[k1] + A2U(ia, 3) * U_[k2] + A2U(ia, 4) * U_[k3];
         double cofa5 = A1U(ia, 1) * V_[ia] + A1U(ia, 2) * V_[k1] + A1U(ia, 3) * V_[k2] + A1U(ia, 4) * V_[k3];
         double cofa6 = A2U(ia, 1) * V_[ia] + A2U(ia, 2) * V_[k1] + A2U(ia, 3) * V_[k2] + A2U(ia, 4) * V_[k3];
-        double uij1 = U_[ia] + cofa1 * xija + cofa2 * yija;
-        double vij1 = V_[ia] + cofa5 * xija + cofa6 * yija;
         double cofa3 = A1U(ib, 1) * U_[ib] + A1U(ib, 2) * U_[k4] + A1U(ib, 3) * U_[k5] + A1U(ib, 4) * U_[k6];
         double cofa4 = A2U(ib, 1) * U_[ib] + A2U(ib, 2) * U_[k4] + A2U(ib, 3) * U_[k5] + A2U(ib, 4) * U_[k6];
         double cofa7 = A1U(ib, 1) * V_[ib] + A1U(ib, 2) * V_[k4] + A1U(ib, 3) * V_[k5] + A1U(ib, 4) * V_[k6];
         double cofa8 = A2U(ib, 1) * V_[ib] + A2U(ib, 2) * V_[k4] + A2U(ib, 3) * V_[k5] + A2U(ib, 4) * V_[k6];
-        double uij2 = U_[ib] + cofa3 * xijb + cofa4 * yijb;
-        double vij2 = V_[ib] + cofa7 * xijb + cofa8 * yijb;
+        double uij1, uij2, vij1, vij2;
+        face_values(U_[ia], U_[ib], cofa1, cofa2, xija, yija, cofa3, cofa4, xijb, yijb, L ? ualfa[ia] : 1.0,
+                    L ? ualfa[ib] : 1.0, uij1, uij2);
+        face_values(V_[ia], V_[ib], cofa5, cofa6, xija, yija, cofa7, cofa8, xijb, yijb, L ? valfa[ia] : 1.0,
+                    L ? valfa[ib] : 1.0, vij1, vij2);
         double uij = 0.5 * (uij1 + uij2);
         double vij = 0.5 * (vij1 + vij2);
         double un = vij * dltxc[i] - uij * dltyc[i];
@@ -933,6 +995,9 @@ struct Oracle {
       const double *U_ = &u[c3(0, k)], *V_ = &v[c3(0, k)];
       double *X = &xflux[c3(0, k)], *Y = &yflux[c3(0, k)];
       double *PX = &pstx_tm[c3(0, k)], *PY = &psty_tm[c3(0, k)], *VM = &viscofm[c3(0, k)];
+      std::vector<double> ualfa, valfa;
+      if (P.limiter) limiter_alfa(U_, V_, [&](int c) { return iswetct[c] * iswetc[c] == 1; }, ualfa, valfa);
+      const bool L = P.limiter != 0;
       for (int i = 1; i <= NE; ++i) {
         int ia = IEC(i, 1), ib = IEC(i, 2);
         int j1 = IENODE(i, 1), j2 = IENODE(i, 2);
@@ -947,14 +1012,15 @@ struct Oracle {
           double cofa2 = A2U(ia, 1) * U_[ia] + A2U(ia, 2) * U_[k1] + A2U(ia, 3) * U_[k2] + A2U(ia, 4) * U_[k3];
           double cofa5 = A1U(ia, 1) * V_[ia] + A1U(ia, 2) * V_[k1] + A1U(ia, 3) * V_[k2] + A1U(ia, 4) * V_[k3];
           double cofa6 = A2U(ia, 1) * V_[ia] + A2U(ia, 2) * V_[k1] + A2U(ia, 3) * V_[k2] + A2U(ia, 4) * V_[k3];
-          double uij1 = U_[ia] + cofa1 * xija + cofa2 * yija;
-          double vij1 = V_[ia] + cofa5 * xija + cofa6 * yija;
           double cofa3 = A1U(ib, 1) * U_[ib] + A1U(ib, 2) * U_[k4] + A1U(ib, 3) * U_[k5] + A1U(ib, 4) * U_[k6];
           double cofa4 = A2U(ib, 1) * U_[ib] + A2U(ib, 2) * U_[k4] + A2U(ib, 3) * U_[k5] + A2U(ib, 4) * U_[k6];
           double cofa7 = A1U(ib, 1) * V_[ib] + A1U(ib, 2) * V_[k4] + A1U(ib, 3) * V_[k5] + A1U(ib, 4) * V_[k6];
           double cofa8 = A2U(ib, 1) * V_[ib] + A2U(ib, 2) * V_[k4] + A2U(ib, 3) * V_[k5] + A2U(ib, 4) * V_[k6];
-          double uij2 = U_[ib] + cofa3 * xijb + cofa4 * yijb;
-          double vij2 = V_[ib] + cofa7 * xijb + cofa8 * yijb;
+          double uij1, uij2, vij1, vij2;
+          face_values(U_[ia], U_[ib], cofa1, cofa2, xija, yija, cofa3, cofa4, xijb, yijb, L ? ualfa[ia] : 1.0,
+                      L ? ualfa[ib] : 1.0, uij1, uij2);
+          face_values(V_[ia], V_[ib], cofa5, cofa6, xija, yija, cofa7, cofa8, xijb, yijb, L ? valfa[ia] : 1.0,
+                      L ? valfa[ib] : 1.0, vij1, vij2);
           double uij = 0.5 * (uij1 + uij2);
           double vij = 0.5 * (vij1 + vij2);
           double exflux = dij * (-uij * dltyc[i] + vij * dltxc[i]);
@@ -1957,6 +2023,7 @@ struct Oracle {
     cp(wsx, have_wind ? f->wstress_x : nullptr, n1);
     cp(wsy, have_wind ? f->wstress_y : nullptr, n1);
     if (P.heating_on && !(P.rheat >= 0.0 && P.zeta1 > 0.0 && P.zeta2 > 0.0)) return FVG_ERR_ARG;
+    if (P.limiter < 0 || P.limiter > 2) return FVG_ERR_ARG;
     cp(swrad_w, P.heating_on && f ? f->swrad : nullptr, m1);
     cp(wtsurf_w, P.heating_on && f ? f->wtsurf : nullptr, m1);
     swrad.assign(m1, 0.0);

@@ -32,6 +32,15 @@ def copy_state(src, dst):
     dst.set_ramp(src.ramp())
 
 
+def copy_oracle_state(src, dst):
+    """Copy every state field between two oracles (their own field names)."""
+    for n in ALL + list(MAPPED):
+        dst.set(n, src.get(n))
+    i, t = src.clock()
+    dst.set_clock(i, t)
+    dst.set_ramp(src.ramp())
+
+
 def gpu_name(name, tracer=1):
     if name in MAPPED:
         return MAPPED[name][tracer - 1]

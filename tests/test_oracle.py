@@ -119,3 +119,37 @@ def test_routines_compose_internal_step(small_channel):
         b.routine(r, arg)
     for n in ("el", "ua", "u", "v", "t1", "s1", "q2", "q2l", "km", "kh", "rho1", "wts", "ww"):
         assert np.array_equal(a.get(n), b.get(n)), n
+
+
+def test_limited_schemes_properties(small_coastal):
+    """The limited momentum advection: for a uniform flow the gradients vanish away from
+    the boundary (the ghost cell holds zero velocity), so on cells two rings inside it the
+    three schemes agree to rounding; for the evolved flow they differ, and the LIMITED_1
+    clamp changes the fluxes beyond the slope limiter alone."""
+    import numpy as np
+    from oracle.oracle import Oracle
+    from tests import parity
+    base = Oracle(small_coastal)
+    base.run(8)
+    out = {}
+    for lim in ("LIMITED_NO", "LIMITED_1", "LIMITED_2"):
+        case = dict(small_coastal, params=dict(small_coastal["params"], LIMITER=lim))
+        o = Oracle(case)
+        parity.copy_oracle_state(base, o)
+        o.routine("ADVAVE", 0)
+        evolved = o.get("advua").copy()
+        n1 = o.size("ua")
+        o.set("ua", np.r_[0.0, np.full(n1 - 1, 0.3)])
+        o.set("va", np.r_[0.0, np.full(n1 - 1, -0.1)])
+        o.routine("ADVAVE", 0)
+        out[lim] = (o.get("advua").copy(), evolved)
+    nbe = np.asarray(small_coastal["grid"]["NBE"])
+    inner = np.all(nbe > 0, axis=1)
+    inner[0] = False
+    inner2 = inner & np.all(inner[nbe], axis=1)
+    scale = np.abs(out["LIMITED_NO"][0][inner2]).max()
+    for lim in ("LIMITED_1", "LIMITED_2"):
+        d = np.abs(out["LIMITED_NO"][0] - out[lim][0])[inner2].max()
+        assert d <= 1e-12 * scale, (lim, d, scale)
+    assert not np.array_equal(out["LIMITED_NO"][1], out["LIMITED_2"][1])
+    assert not np.array_equal(out["LIMITED_1"][1], out["LIMITED_2"][1])
