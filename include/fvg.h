@@ -131,6 +131,9 @@ typedef struct fvg_params {
      clamp of both face values into the range of the two cells); 2 the slope limiter alone
      (advave_edge_gcn.F:128-330, advection_edge_gcn.F:107-335, adv_uv_edge_gcn.F:138-400). */
   int32_t limiter;
+  /* BAROCLINIC_PRESSURE_GRADIENT: 0 'sigma levels' (BAROPG), 1 'z coordinates'
+     (PHY_BAROPG, phy_baropg.F:37-151: 600 z levels of HMAX/600) */
+  int32_t baropg_z;
 } fvg_params;
 
 /* Boundary forcing that is constant in time for the supported cases. */

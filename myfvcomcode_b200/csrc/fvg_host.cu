@@ -180,7 +180,12 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   launch_grad3(P, s);
   launch_advection3d(P, s);
   mk.mark(s, G_ADV3D);
-  launch_baropg(P, s, !p.barotropic, 1);
+  if (!p.barotropic && P.baropg_z) {
+    launch_phy_baropg(P, s);
+    launch_baropg(P, s, 0, 1);
+  } else {
+    launch_baropg(P, s, !p.barotropic, 1);
+  }
   launch_ext_prep(P, s);
   if (P.limiter) launch_alfa2(P, s);
   mk.mark(s, G_BAROPG);
@@ -222,7 +227,7 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   mk.mark(s, G_ADJ2);
   launch_vertvl_flux(P, s);
   mk.mark(s, G_VV_FLUX);
-  launch_vertvl_col(P, s, VC_WTS | VC_WD2 | (p.barotropic ? 0 : VC_RHO_ROUNDTRIP) | VC_BOT_NODE);
+  launch_vertvl_col(P, s, VC_WTS | VC_WD2 | (p.barotropic || P.baropg_z ? 0 : VC_RHO_ROUNDTRIP) | VC_BOT_NODE);
   mk.mark(s, G_VV_COL);
   launch_w_viscofh(P, s, 1, 1);
   mk.mark(s, G_W_VISC);
@@ -307,6 +312,12 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   P.have_wind = f && f->wstress_x && f->wstress_y;
   P.heating_on = prm->heating_on != 0;
   P.limiter = prm->limiter;
+  P.baropg_z = prm->baropg_z != 0;
+  {
+    double hmax = m->h[1];
+    for (int i = 2; i <= M; ++i) hmax = std::max(hmax, m->h[i]);
+    P.deltz = hmax / (double)(float)600;
+  }
   P.rheat = prm->rheat; P.zeta1 = prm->zeta1; P.zeta2 = prm->zeta2;
   P.sl.isplit = prm->isplit;
   P.sl.ntide = h->ntide;
@@ -612,6 +623,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   for (int q = 0; q < 4; ++q) {
     if ((rc = dalloc(h, &P.g2d[q], n1))) return fail(rc);
   }
+  if (P.baropg_z && (rc = dalloc(h, &P.rhoz, (size_t)P.ms * 600))) return fail(rc);
   if (P.limiter) {
     std::vector<double> ones(std::max(n1, (size_t)P.ns * KB), 1.0);
     for (int q = 0; q < 2; ++q) {
@@ -828,6 +840,7 @@ int32_t fvg_kernels_per_step(const fvg_handle* h) {
   int n = 1 + 1 + 2 + 2 + 2;                                // begin, cell_pre, grad3+adv3d, baropg+prep, int advave+reset
   n += p.isplit * 4 * (2 + (p.wetting_drying_on ? 2 : 0)) + 1; // RK stages, closing update
   if (p.limiter) n += p.isplit * 4 + 1 + 2;                  // slope limiters: stages, ADVAVE, 3-D
+  if (p.baropg_z && !p.barotropic) n += 2;                   // PHY_BAROPG's two kernels
   n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv
   n += 7;                                                  // grad_q, adv_q (2 phases), vdif_q (4 passes)
   if (h->P.closure) n += 1;                                // learned closure
@@ -1142,8 +1155,12 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
       launch_advection3d(P, s);
       break;
     case FVG_R_BAROPG:
-      launch_baropg(P, s, 1, 0);
-      launch_vertvl_col(P, s, VC_RHO_ROUNDTRIP);
+      if (P.baropg_z) {
+        launch_phy_baropg(P, s);
+      } else {
+        launch_baropg(P, s, 1, 0);
+        launch_vertvl_col(P, s, VC_RHO_ROUNDTRIP);
+      }
       break;
     case FVG_R_INT_PRE_EXT:
       launch_baropg(P, s, 0, 1);

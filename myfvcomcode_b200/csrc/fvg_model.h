@@ -74,6 +74,9 @@ struct Dev {
   int heating_on;
   double rheat, zeta1, zeta2;
   int limiter;  // 0 LIMITED_NO, 1 LIMITED_1, 2 the slope limiter alone
+  int baropg_z;   // BAROCLINIC_PRESSURE_GRADIENT 'z coordinates' (PHY_BAROPG)
+  double deltz;   // its z spacing HMAX/600
+  double* rhoz;   // RHO1 interpolated to the 600 z levels, [(k-1)*ms + node]
   SchedLayout sl;
   const double* sched;  // schedule table
   int* ctl;             // ctl[0] = current schedule slot; ctl[1] = error word
@@ -329,6 +332,7 @@ void launch_cell_pre(const Dev& P, cudaStream_t s, int parts);
 void launch_grad3(const Dev& P, cudaStream_t s);
 void launch_advection3d(const Dev& P, cudaStream_t s);
 void launch_baropg(const Dev& P, cudaStream_t s, int do_baropg, int do_sums);
+void launch_phy_baropg(const Dev& P, cudaStream_t s);
 void launch_int_reset(const Dev& P, cudaStream_t s);
 void launch_adjust2(const Dev& P, cudaStream_t s);
 void launch_vertvl_flux(const Dev& P, cudaStream_t s);

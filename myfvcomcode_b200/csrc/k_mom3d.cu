@@ -807,6 +807,140 @@ void launch_advection3d(const Dev& P, cudaStream_t s) {
   else
     k_advection3d<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
+// -------------------------------------------------------------------------------------
+// PHY_BAROPG (phy_baropg.F:37-151), BAROCLINIC_PRESSURE_GRADIENT = 'z coordinates'.
+// SINTER_EXTRP_DOWN (sinter.F) takes, for each target Y, the last interval J of the
+// descending abscissae with X(J+1) <= Y <= X(J); both kernels walk targets and abscissae
+// together, which finds the same interval: the largest J with X(J) >= Y.
+// -------------------------------------------------------------------------------------
+constexpr int kZLevels = 600;
+
+__device__ inline double phy_z(const Dev& P, int k) { return (0.5 - (double)(float)k) * P.deltz; }
+
+// RHO1 of each node column interpolated (extrapolated below) to the 600 z levels.
+__global__ void __launch_bounds__(128) k_phy_rhoz(const Dev P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.M) return;
+  const int M1 = P.KBM1;
+  double X[kMaxKB], A[kMaxKB];
+  for (int k = 1; k <= M1; ++k) {
+    X[k - 1] = P.zz[N3(P, i, k)] * P.dt[i] + P.et[i];
+    A[k - 1] = P.rho1[N3(P, i, k)];
+  }
+  int j = 0;
+  for (int t = 1; t <= kZLevels; ++t) {
+    const double Y = phy_z(P, t);
+    double b = 0.0;
+    if (Y > X[0]) b = A[0];
+    if (Y < X[M1 - 1]) b = A[M1 - 1] + (A[M1 - 2] - A[M1 - 1]) * (Y - X[M1 - 1]) / (X[M1 - 2] - X[M1 - 1]);
+    while (j + 1 <= M1 - 2 && X[j + 1] >= Y) ++j;
+    if (Y <= X[j] && Y >= X[j + 1]) b = A[j] - (A[j] - A[j + 1]) * (X[j] - Y) / (X[j] - X[j + 1]);
+    P.rhoz[(size_t)(t - 1) * P.ms + i] = b;
+  }
+}
+
+// Per cell: the pressure integrals of the three edges down the z levels where all three
+// nodes are deeper, their gradient PBXZ, PBYZ per level, and those interpolated back to the
+// cell's sigma depths while the levels are walked.
+__global__ void __launch_bounds__(128) k_phy_baropg(const Dev P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  const size_t n1 = P.N + 1;
+  const int j1 = P.nv[i], j2 = P.nv[n1 + i], j3 = P.nv[2 * n1 + i];
+  const int KBM1 = P.KBM1;
+  const double deltz = P.deltz, art = P.art[i], dt1 = P.dt1[i], ramp = ramp_int(P);
+  const double h1 = P.h[j1], h2 = P.h[j2], h3 = P.h[j3];
+  // NTMP: the levels K = 1.. where no node is shallower than K*DELTZ (a leading run)
+  int ntmp = 0;
+  while (ntmp < kZLevels) {
+    const double tmp = (double)(float)(ntmp + 1) * deltz;
+    if (h1 < tmp || h2 < tmp || h3 < tmp) break;
+    ++ntmp;
+  }
+  auto emit = [&](int k, double bx, double by) {
+    const size_t q = C3(P, i, k);
+    const double dz1 = P.dz1[q];
+    P.drhox[q] = -bx * dt1 * dz1 * art * ramp;
+    P.drhoy[q] = -by * dt1 * dz1 * art * ramp;
+  };
+  auto target = [&](int k) {
+    return (P.zz[N3(P, j1, k)] * P.dt[j1] + P.et[j1] + (P.zz[N3(P, j2, k)] * P.dt[j2] + P.et[j2]) +
+            (P.zz[N3(P, j3, k)] * P.dt[j3] + P.et[j3])) / 3.;
+  };
+  if (ntmp <= 1) {
+    double bx = 0.0, by = 0.0;
+    if (ntmp == 1) {
+      const double g1 = 0.5 * (P.grav_n[j2] + P.grav_n[j3]);
+      const double g2 = 0.5 * (P.grav_n[j3] + P.grav_n[j1]);
+      const double g3 = 0.5 * (P.grav_n[j1] + P.grav_n[j2]);
+      const double r1 = P.rhoz[j1], r2 = P.rhoz[j2], r3 = P.rhoz[j3];
+      const double pb1 = 0.0 + g1 * (0.5 * (r2 + r3)) * deltz;
+      const double pb2 = 0.0 + g2 * (0.5 * (r3 + r1)) * deltz;
+      const double pb3 = 0.0 + g3 * (0.5 * (r1 + r2)) * deltz;
+      const double ax1 = (P.vy[j3] - P.vy[j2]) * deltz, ay1 = (P.vx[j2] - P.vx[j3]) * deltz;
+      const double ax2 = (P.vy[j1] - P.vy[j3]) * deltz, ay2 = (P.vx[j3] - P.vx[j1]) * deltz;
+      const double ax3 = (P.vy[j2] - P.vy[j1]) * deltz, ay3 = (P.vx[j1] - P.vx[j2]) * deltz;
+      bx = (ax1 * pb1 + ax2 * pb2 + ax3 * pb3) / art / deltz;
+      by = (ay1 * pb1 + ay2 * pb2 + ay3 * pb3) / art / deltz;
+    }
+    for (int k = 1; k <= KBM1; ++k) emit(k, bx, by);
+    return;
+  }
+  const double g1 = 0.5 * (P.grav_n[j2] + P.grav_n[j3]);
+  const double g2 = 0.5 * (P.grav_n[j3] + P.grav_n[j1]);
+  const double g3 = 0.5 * (P.grav_n[j1] + P.grav_n[j2]);
+  const double ax1 = (P.vy[j3] - P.vy[j2]) * deltz, ay1 = (P.vx[j2] - P.vx[j3]) * deltz;
+  const double ax2 = (P.vy[j1] - P.vy[j3]) * deltz, ay2 = (P.vx[j3] - P.vx[j1]) * deltz;
+  const double ax3 = (P.vy[j2] - P.vy[j1]) * deltz, ay3 = (P.vx[j1] - P.vx[j2]) * deltz;
+  double pb1 = 0.0, pb2 = 0.0, pb3 = 0.0;
+  double xprev = 0.0, xcur = 0.0, yprev = 0.0, ycur = 0.0;  // PBXZ, PBYZ at levels K-1, K
+  double x0 = 0.0, y0 = 0.0;                                 // at level 1
+  int t = 1;
+  double Y = target(1);
+  for (int K = 1; K <= ntmp; ++K) {
+    const double* rz = P.rhoz + (size_t)(K - 1) * P.ms;
+    const double r1 = rz[j1], r2 = rz[j2], r3 = rz[j3];
+    pb1 = pb1 + g1 * (0.5 * (r2 + r3)) * deltz;
+    pb2 = pb2 + g2 * (0.5 * (r3 + r1)) * deltz;
+    pb3 = pb3 + g3 * (0.5 * (r1 + r2)) * deltz;
+    xprev = xcur;
+    yprev = ycur;
+    xcur = (ax1 * pb1 + ax2 * pb2 + ax3 * pb3) / art / deltz;
+    ycur = (ay1 * pb1 + ay2 * pb2 + ay3 * pb3) / art / deltz;
+    if (K == 1) {
+      x0 = xcur;
+      y0 = ycur;
+      continue;
+    }
+    // interval j = K-2 (0-based) spans levels K-1, K: every pending target whose last
+    // interval with X(J) >= Y is this one
+    const double Xj = phy_z(P, K - 1), Xj1 = phy_z(P, K);
+    while (t <= KBM1) {
+      if (Y > phy_z(P, 1)) {
+        emit(t, x0, y0);
+      } else {
+        if (Xj1 >= Y && K < ntmp) break;  // a later interval still has X(J) >= Y
+        double bx, by;
+        if (Y >= Xj1) {
+          bx = xprev - (xprev - xcur) * (Xj - Y) / (Xj - Xj1);
+          by = yprev - (yprev - ycur) * (Xj - Y) / (Xj - Xj1);
+        } else {  // below the last level: extrapolation from the last two
+          bx = xcur + (xprev - xcur) * (Y - Xj1) / (Xj - Xj1);
+          by = ycur + (yprev - ycur) * (Y - Xj1) / (Xj - Xj1);
+        }
+        emit(t, bx, by);
+      }
+      ++t;
+      if (t <= KBM1) Y = target(t);
+    }
+  }
+}
+
+void launch_phy_baropg(const Dev& P, cudaStream_t s) {
+  k_phy_rhoz<<<nblk(P.M, 128), 128, 0, s>>>(P);
+  k_phy_baropg<<<nblk(P.N, 128), 128, 0, s>>>(P);
+}
+
 void launch_baropg(const Dev& P, cudaStream_t s, int do_baropg, int do_sums) {
   k_baropg<<<nblk(P.N, 128), 128, 0, s>>>(P, do_baropg, do_sums);
 }

@@ -44,6 +44,7 @@ MODULE FVG_BIND
     INTEGER(C_INT32_T) :: HEATING_ON
     REAL(C_DOUBLE) :: RHEAT, ZETA1, ZETA2
     INTEGER(C_INT32_T) :: LIMITER        ! 0 LIMITED_NO, 1 LIMITED_1, 2 slope limiter alone
+    INTEGER(C_INT32_T) :: BAROPG_Z       ! 1: BAROCLINIC_PRESSURE_GRADIENT = 'z coordinates'
   END TYPE FVG_PARAMS_T
 
   TYPE, BIND(C) :: FVG_FORCING_T

@@ -613,8 +613,8 @@ class FvcomRun:
         if _s(ph.get("BOTTOM_ROUGHNESS_KIND"), "constant").lower() != "constant":
             raise ValueError("BOTTOM_ROUGHNESS_KIND other than 'constant' is not on the supported path")
         bpg = _s(ph.get("BAROCLINIC_PRESSURE_GRADIENT"), "sigma levels").lower()
-        if bpg != "sigma levels":
-            raise ValueError("BAROCLINIC_PRESSURE_GRADIENT '%s' is not on the supported path" % bpg)
+        if bpg not in ("sigma levels", "z coordinates"):
+            raise ValueError("BAROCLINIC_PRESSURE_GRADIENT '%s' is not 'sigma levels' or 'z coordinates'" % bpg)
         rt = group(nml, "NML_RIVER_TYPE")
         obc = group(nml, "NML_OPEN_BOUNDARY_CONTROL")
         params = default_params(
@@ -632,7 +632,7 @@ class FvcomRun:
             SALINITY_ACTIVE=_b(ph.get("SALINITY_ACTIVE"), True),
             OBC_TS_TYPE=int(obc.get("OBC_TS_TYPE", 3)),
             RIVER_TS_SETTING=_s(rt.get("RIVER_TS_SETTING"), "specified").lower(),
-            LIMITER=limiter,
+            LIMITER=limiter, BAROCLINIC_PRESSURE_GRADIENT=bpg,
         )
 
         gc = group(nml, "NML_GRID_COORDINATES")
@@ -975,7 +975,7 @@ def write_run(case, directory, name="case", days=1.0, river_series=None, wind_se
         " BOTTOM_ROUGHNESS_MINIMUM = %s," % _fmt(p["CBCMIN"]),
         " SCALAR_POSITIVITY_CONTROL = %s," % L(p["SCALAR_POSITIVITY_CONTROL"]),
         " BAROTROPIC = %s," % L(p["BAROTROPIC"]),
-        " BAROCLINIC_PRESSURE_GRADIENT = 'sigma levels',",
+        " BAROCLINIC_PRESSURE_GRADIENT = '%s'," % p.get("BAROCLINIC_PRESSURE_GRADIENT", "sigma levels"),
         " TEMPERATURE_ACTIVE = %s," % L(p["TEMPERATURE_ACTIVE"]),
         " SALINITY_ACTIVE = %s," % L(p["SALINITY_ACTIVE"]),
         " WETTING_DRYING_ON = %s," % L(p["WETTING_DRYING_ON"]), " /",

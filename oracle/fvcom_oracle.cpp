@@ -781,6 +781,92 @@ struct Oracle {
   // =====================================================================================
   // BAROPG, sigma levels (baropg.F:33-166)
   // =====================================================================================
+  // SINTER_EXTRP_DOWN (sinter.F): B(I) from A over the descending abscissae X(1..M1): A(1)
+  // above X(1), linear extrapolation of the last two below X(M1), else linear
+  // interpolation in the last interval J (of all J = 1..M1-1) with X(J+1) <= Y <= X(J).
+  static void sinter_extrp_down(const double* X, const double* A, const double* Y, double* B, int M1, int N1) {
+    for (int i = 0; i < N1; ++i) {
+      if (Y[i] > X[0]) B[i] = A[0];
+      if (Y[i] < X[M1 - 1]) B[i] = A[M1 - 1] + (A[M1 - 2] - A[M1 - 1]) * (Y[i] - X[M1 - 1]) / (X[M1 - 2] - X[M1 - 1]);
+    }
+    for (int i = 0; i < N1; ++i)
+      for (int j = 0; j < M1 - 1; ++j)
+        if (Y[i] <= X[j] && Y[i] >= X[j + 1]) B[i] = A[j] - (A[j] - A[j + 1]) * (X[j] - Y[i]) / (X[j] - X[j + 1]);
+  }
+
+  // PHY_BAROPG (phy_baropg.F:37-151): the baroclinic pressure gradient on 600 z levels of
+  // HMAX/600, with RHO1 interpolated down each node column, integrated per cell edge and
+  // interpolated back to the cell's sigma depths.
+  void phy_baropg() {
+    const int KBBM1 = 600;
+    double hmax = h[1];
+    for (int i = 2; i <= M; ++i) hmax = std::max(hmax, h[i]);
+    const double deltz = hmax / (double)(float)KBBM1;
+    std::vector<double> phy_z(KBBM1), rhoz((size_t)(M + 1) * KBBM1), sig_z((size_t)(M + 1) * KBM1);
+    for (int k = 1; k <= KBBM1; ++k) phy_z[k - 1] = (0.5 - (double)(float)k) * deltz;
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i <= M; ++i) {
+      std::vector<double> sz(KBM1), rs(KBM1);
+      for (int k = 1; k <= KBM1; ++k) {
+        sig_z[(size_t)i * KBM1 + k - 1] = zz[n3(i, k)] * dt[i] + et[i];
+        sz[k - 1] = sig_z[(size_t)i * KBM1 + k - 1];
+        rs[k - 1] = rho1[n3(i, k)];
+      }
+      sinter_extrp_down(sz.data(), rs.data(), phy_z.data(), &rhoz[(size_t)i * KBBM1], KBM1, KBBM1);
+    }
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i <= N; ++i) {
+      int j1 = NV(i, 1), j2 = NV(i, 2), j3 = NV(i, 3);
+      std::vector<double> pb1(KBBM1 + 1), pb2(KBBM1 + 1), pb3(KBBM1 + 1), pbxz(KBBM1), pbyz(KBBM1);
+      std::vector<double> sz(KBM1), pbxs(KBM1), pbys(KBM1);
+      int ntmp = 0;
+      pb1[0] = pb2[0] = pb3[0] = 0.0;
+      const double* r1 = &rhoz[(size_t)j1 * KBBM1];
+      const double* r2 = &rhoz[(size_t)j2 * KBBM1];
+      const double* r3 = &rhoz[(size_t)j3 * KBBM1];
+      for (int k = 1; k <= KBBM1; ++k) {
+        double tmp = (double)(float)k * deltz;
+        if (h[j1] < tmp || h[j2] < tmp || h[j3] < tmp) {
+          pb1[k] = pb2[k] = pb3[k] = 0.0;
+        } else {
+          double rz1 = 0.5 * (r2[k - 1] + r3[k - 1]);
+          double rz2 = 0.5 * (r3[k - 1] + r1[k - 1]);
+          double rz3 = 0.5 * (r1[k - 1] + r2[k - 1]);
+          double g1 = 0.5 * (grav_n[j2] + grav_n[j3]);
+          double g2 = 0.5 * (grav_n[j3] + grav_n[j1]);
+          double g3 = 0.5 * (grav_n[j1] + grav_n[j2]);
+          pb1[k] = pb1[k - 1] + g1 * rz1 * deltz;
+          pb2[k] = pb2[k - 1] + g2 * rz2 * deltz;
+          pb3[k] = pb3[k - 1] + g3 * rz3 * deltz;
+          ntmp = ntmp + 1;
+        }
+      }
+      double ax1 = (vy[j3] - vy[j2]) * deltz, ay1 = (vx[j2] - vx[j3]) * deltz;
+      double ax2 = (vy[j1] - vy[j3]) * deltz, ay2 = (vx[j3] - vx[j1]) * deltz;
+      double ax3 = (vy[j2] - vy[j1]) * deltz, ay3 = (vx[j1] - vx[j2]) * deltz;
+      for (int k = 1; k <= KBBM1; ++k) {
+        double px = ax1 * pb1[k] + ax2 * pb2[k] + ax3 * pb3[k];
+        double py = ay1 * pb1[k] + ay2 * pb2[k] + ay3 * pb3[k];
+        pbxz[k - 1] = px / art[i] / deltz;
+        pbyz[k - 1] = py / art[i] / deltz;
+      }
+      for (int k = 1; k <= KBM1; ++k)
+        sz[k - 1] = (sig_z[(size_t)j1 * KBM1 + k - 1] + sig_z[(size_t)j2 * KBM1 + k - 1] + sig_z[(size_t)j3 * KBM1 + k - 1]) / 3.;
+      if (ntmp == 0) {
+        for (int k = 0; k < KBM1; ++k) pbxs[k] = pbys[k] = 0.0;
+      } else if (ntmp == 1) {
+        for (int k = 0; k < KBM1; ++k) { pbxs[k] = pbxz[0]; pbys[k] = pbyz[0]; }
+      } else {
+        sinter_extrp_down(phy_z.data(), pbxz.data(), sz.data(), pbxs.data(), ntmp, KBM1);
+        sinter_extrp_down(phy_z.data(), pbyz.data(), sz.data(), pbys.data(), ntmp, KBM1);
+      }
+      for (int k = 1; k <= KBM1; ++k) {
+        drhox[c3(i, k)] = -pbxs[k - 1] * dt1[i] * dz1[c3(i, k)] * art[i] * RAMP;
+        drhoy[c3(i, k)] = -pbys[k - 1] * dt1[i] * dz1[c3(i, k)] * art[i] * RAMP;
+      }
+    }
+  }
+
   void baropg() {
     for (int k = 1; k <= KBM1; ++k)
       for (int i = 0; i <= M; ++i) rho1[n3(i, k)] = rho1[n3(i, k)] - rmean1[n3(i, k)];
@@ -1844,7 +1930,10 @@ struct Oracle {
     bcond8();
     bottom_roughness();
     advection3d();
-    if (!P.barotropic) baropg();
+    if (!P.barotropic) {
+      if (P.baropg_z) phy_baropg();
+      else baropg();
+    }
     int_pre_ext();
     for (int iext = 1; iext <= P.isplit; ++iext) {
       ExtTime = ExtTime + P.dte;
@@ -1903,7 +1992,10 @@ struct Oracle {
       case FVG_R_BCOND_UV3D_SOLID: bcond_uv3d(u, v); break;
       case FVG_R_BROUGH: bottom_roughness(); break;
       case FVG_R_ADVECTION3D: advection3d(); break;
-      case FVG_R_BAROPG: baropg(); break;
+      case FVG_R_BAROPG:
+        if (P.baropg_z) phy_baropg();
+        else baropg();
+        break;
       case FVG_R_INT_PRE_EXT: int_pre_ext(); break;
       case FVG_R_VERTVL: vertvl(); break;
       case FVG_R_VISCOFH: viscof_h(); break;

@@ -153,3 +153,43 @@ def test_limited_schemes_properties(small_coastal):
         assert d <= 1e-12 * scale, (lim, d, scale)
     assert not np.array_equal(out["LIMITED_NO"][1], out["LIMITED_2"][1])
     assert not np.array_equal(out["LIMITED_1"][1], out["LIMITED_2"][1])
+
+
+def test_z_level_pressure_gradient_on_flat_bottom():
+    """PHY_BAROPG (z levels) against BAROPG (sigma levels) where both discretise the same
+    integral: flat bottom, flat surface, density linear in x.  PHY_BAROPG integrates each
+    z level down to its lower edge K*DELTZ but places the value at the level centre
+    (K-1/2)*DELTZ, so it exceeds BAROPG by the pressure gradient of half a level,
+    g*(drho/dx)*DELTZ/2 * DT1*DZ1*ART, at every depth: that offset holds to 1e-6 of the
+    gradient.  A horizontally uniform density gives a gradient 1e-12 of that."""
+    import numpy as np
+    from myfvcomcode_b200 import cases
+    from myfvcomcode_b200.grid import build_grid
+    from oracle.oracle import Oracle
+    base = cases.estuary_channel(nx=16, ny=4, kb=11, lx=3200.0, ly=800.0, river=False, sponge=False)
+    g0 = base["grid"]
+    M = g0["M"]
+    g = build_grid(g0["VX"][1:] + g0["VXMIN"], g0["VY"][1:] + g0["VYMIN"], g0["NV"][1:], np.full(M, 12.0), 11,
+                   obc_nodes=list(g0["I_OBC_N"][1:]), obc_types=list(g0["TYPE_OBC"][1:]), cor_lat=30.0)
+    out = {}
+    for name in ("sigma levels", "z coordinates"):
+        case = dict(base, grid=g, params=dict(base["params"], BAROCLINIC_PRESSURE_GRADIENT=name))
+        o = Oracle(case)
+        o.set_ramp(1.0)
+        kb = g["KB"]
+        rho = np.zeros((M + 1, kb))
+        rho[1:, : kb - 1] = (1e-4 * g["VX"][1:])[:, None]
+        o.set("rho1", rho)
+        o.set("rmean1", np.zeros_like(rho))
+        o.routine("BAROPG", 0)
+        out[name] = o.get3("drhox")[1:, : kb - 1].copy()
+        rho[1:, : kb - 1] = 0.7
+        o.set("rho1", rho)
+        o.routine("BAROPG", 0)
+        out[name + " uniform"] = o.get3("drhox")[1:, : kb - 1].copy()
+    scale = np.abs(out["sigma levels"]).max()
+    assert scale > 0
+    deltz = 12.0 / 600.0
+    half_level = 0.5 * 9.81 * 1e-4 * deltz * 12.0 * g["DZ1"][1:, : g["KB"] - 1] * g["ART"][1:, None]
+    assert np.abs(out["z coordinates"] - out["sigma levels"] - half_level).max() <= 1e-6 * scale
+    assert np.abs(out["z coordinates uniform"]).max() <= 1e-12 * scale

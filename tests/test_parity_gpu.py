@@ -242,3 +242,25 @@ def test_limited_schemes_match_oracle(case_name, limiter, request):
     b.set_precision("fp32flux")
     b.run(5)
     assert np.isfinite(b.get("u")).all() and np.isfinite(b.get("el")).all()
+
+
+@pytest.mark.parametrize("case_name", ["small_channel", "small_coastal"])
+def test_z_level_pressure_gradient_matches_oracle(case_name, request):
+    """BAROCLINIC_PRESSURE_GRADIENT = 'z coordinates' (PHY_BAROPG): the routine bit for
+    bit from the same state, and 20 whole steps to 1e-10."""
+    from myfvcomcode_b200.engine import Fvcom
+    from oracle.oracle import Oracle
+    base = request.getfixturevalue(case_name)
+    case = dict(base, params=dict(base["params"], BAROCLINIC_PRESSURE_GRADIENT="z coordinates"))
+    ora, gpu = Oracle(case), Fvcom(case)
+    ora.run(4)
+    parity.copy_state(ora, gpu)
+    gpu.routine("BAROPG", 0)
+    ora.routine("BAROPG", 0)
+    bad = parity.compare(gpu, ora, ["drhox", "drhoy", "rho1"])
+    assert not bad, bad
+    a, b = Oracle(case), Fvcom(case)
+    a.run(20)
+    b.run(20)
+    bad = parity.compare(b, a, ["el", "ua", "va", "u", "v", "t1", "s1", "rho1"], rtol=1e-10)
+    assert not bad, bad
