@@ -103,53 +103,75 @@ __global__ void __launch_bounds__(256) k_grad(const Dev P, int which) {
   const int nt = P.ntsn[i];
   const R art2 = (R)P.art2[i];
   const R half = (R)0.5;
+  const R qmean = (R)F4(1.e-8);
+  // One walk of the ring per layer serves both tracers: the ring node, its wet flag and
+  // the ring-edge metrics are loaded once, and each neighbour's values are carried to
+  // the next ring edge.  Per tracer the arithmetic is the reference's, term by term.
   for (int k = kb; k <= ke; ++k) {
+    const double* Q[2];
+    const double* QM[2] = {nullptr, nullptr};
+    if (which == 0) {
+      Q[0] = P.q2 + N3(P, 0, k);
+      Q[1] = P.q2l + N3(P, 0, k);
+    } else {
+      Q[0] = P.t1 + N3(P, 0, k);
+      Q[1] = P.s1 + N3(P, 0, k);
+      QM[0] = P.tmean1 + N3(P, 0, k);
+      QM[1] = P.smean1 + N3(P, 0, k);
+    }
+    R qi[2], qmi[2] = {0, 0}, q1[2], qm1[2] = {0, 0};
+    R px[2] = {0, 0}, py[2] = {0, 0}, pxd[2] = {0, 0}, pyd[2] = {0, 0}, rmin[2], rmax[2];
+    int i1 = NBSN(P, i, 1);
+    int w1 = which == 0 ? 1 : P.iswetn[i1];
     for (int t = 0; t < 2; ++t) {
-      const double* Q;
-      const double* QM = nullptr;
-      if (which == 0) {
-        Q = (t == 0 ? P.q2 : P.q2l) + N3(P, 0, k);
-      } else {
-        Q = (t == 0 ? P.t1 : P.s1) + N3(P, 0, k);
-        QM = (t == 0 ? P.tmean1 : P.smean1) + N3(P, 0, k);
+      qi[t] = (R)Q[t][i];
+      q1[t] = (R)Q[t][i1];
+      if (which != 0) {
+        qmi[t] = (R)QM[t][i];
+        qm1[t] = (R)QM[t][i1];
       }
-      const R qmean = (R)F4(1.e-8);
-      R px = 0, py = 0, pxd = 0, pyd = 0;
-      R rmin = (R)Q[NBSN(P, i, 1)], rmax = rmin;
-      for (int j = 1; j <= nt - 1; ++j) {
-        int i1 = NBSN(P, i, j), i2 = NBSN(P, i, j + 1);
+      rmin[t] = q1[t];
+      rmax[t] = q1[t];
+    }
+    for (int j = 1; j <= nt - 1; ++j) {
+      const int i2 = NBSN(P, i, j + 1);
+      const int w2 = which == 0 ? 1 : P.iswetn[i2];
+      const R ty = (R)TRIEY(P, i, j), tx = (R)TRIEX(P, i, j);
+      for (int t = 0; t < 2; ++t) {
+        const R q2 = (R)Q[t][i2];
         if (j >= 2) {
-          rmin = fmin(rmin, (R)Q[i1]);
-          rmax = fmax(rmax, (R)Q[i1]);
+          rmin[t] = fmin(rmin[t], q1[t]);
+          rmax[t] = fmax(rmax[t], q1[t]);
         }
         R ffd, ff1;
         if (which == 0) {
-          ffd = half * ((R)Q[i1] + (R)Q[i2] - qmean - qmean);
-          ff1 = half * ((R)Q[i1] + (R)Q[i2]);
+          ffd = half * (q1[t] + q2 - qmean - qmean);
+          ff1 = half * (q1[t] + q2);
         } else {
-          int w1 = P.iswetn[i1], w2 = P.iswetn[i2];
-          int a = i1, b = i2;
-          if (w1 == 0 && w2 == 1) { a = i; b = i2; }
-          else if (w1 == 1 && w2 == 0) { a = i1; b = i; }
-          else if (w1 == 0 && w2 == 0) { a = i; b = i; }
-          ffd = half * ((R)Q[a] + (R)Q[b] - (R)QM[a] - (R)QM[b]);
-          ff1 = half * ((R)Q[a] + (R)Q[b]);
+          const R qm2 = (R)QM[t][i2];
+          R qa = q1[t], qb = q2, qma = qm1[t], qmb = qm2;
+          if (w1 == 0 && w2 == 1) { qa = qi[t]; qma = qmi[t]; }
+          else if (w1 == 1 && w2 == 0) { qb = qi[t]; qmb = qmi[t]; }
+          else if (w1 == 0 && w2 == 0) { qa = qi[t]; qb = qi[t]; qma = qmi[t]; qmb = qmi[t]; }
+          ffd = half * (qa + qb - qma - qmb);
+          ff1 = half * (qa + qb);
+          qm1[t] = qm2;
         }
-        R ty = (R)TRIEY(P, i, j), tx = (R)TRIEX(P, i, j);
-        px = px + ff1 * ty;
-        py = py + ff1 * tx;
-        pxd = pxd + ffd * ty;
-        pyd = pyd + ffd * tx;
+        px[t] = px[t] + ff1 * ty;
+        py[t] = py[t] + ff1 * tx;
+        pxd[t] = pxd[t] + ffd * ty;
+        pyd[t] = pyd[t] + ffd * tx;
+        q1[t] = q2;
       }
-      px = px / art2;
-      py = py / art2;
-      pxd = pxd / art2;
-      pyd = pyd / art2;
-      size_t q = N3(P, i, k);
-      NodeRec<R>::store(P, which, t, q, (R)Q[i], px, py, pxd, pyd, rmin, rmax);
+      w1 = w2;
+    }
+    const size_t q = N3(P, i, k);
+    for (int t = 0; t < 2; ++t) {
+      const R gx = px[t] / art2, gy = py[t] / art2, gxd = pxd[t] / art2, gyd = pyd[t] / art2;
+      NodeRec<R>::store(P, which, t, q, qi[t], gx, gy, gxd, gyd, rmin[t], rmax[t]);
       if (which == 1 && k == P.KBM1) {
-        if (t == 0) { P.pfpxb_t[i] = (double)px; P.pfpyb_t[i] = (double)py; }
-        else { P.pfpxb_s[i] = (double)px; P.pfpyb_s[i] = (double)py; }
+        if (t == 0) { P.pfpxb_t[i] = (double)gx; P.pfpyb_t[i] = (double)gy; }
+        else { P.pfpxb_s[i] = (double)gx; P.pfpyb_s[i] = (double)gy; }
         double ah = (P.fact * P.viscofh[N3(P, i, P.KBM1)] + P.fm1) * P.nn_hvc[i];
         if (t == 0) P.ah_bottom_t[i] = ah;
         else P.ah_bottom_s[i] = ah;
