@@ -197,7 +197,9 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   // arrays: stage n+1's UA is stage n's UAF, its ISWETCE stage n's ISWETC.  The update's
   // cell part ends the cell kernel, its node part starts the next stage's node kernel,
   // and k_ext_finish closes the last stage (an even number of stages leaves the arrays in
-  // their own roles).
+  // their own roles).  With wetting and drying, WET_JUDGE's node part (ISWETN, the ELF
+  // clamp) moves the same way to the head of the next node kernel; FLUX_OBN, the one
+  // reader of ELF in between, applies the clamp itself.
   int stage = 0;
   for (int iext = 1; iext <= p.isplit; ++iext) {
     for (int K = 1; K <= 4; ++K, ++stage) {
@@ -207,11 +209,12 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
         std::swap(Q.va, Q.vaf);
         std::swap(Q.iswetce, Q.iswetc);
       }
-      const int prev = stage > 0 ? (EN_FINISH_PREV | ((K == 1 ? 4 : K - 1) << 8)) : 0;
+      const int prev =
+          stage > 0 ? (EN_FINISH_PREV | (p.wetting_drying_on ? EN_WET_PREV : 0) | ((K == 1 ? 4 : K - 1) << 8)) : 0;
       launch_ext_node(Q, s, iext, K, EN_EXTEL | EN_BC | EN_GRAD | (K == 1 ? EN_COPY_ELRK : 0) | prev);
       mk.mark(s, G_EXT_NODE);
       if (p.wetting_drying_on) {
-        launch_wet_judge(Q, s);
+        launch_wet_cells(Q, s);  // its node part opens the next stage's node kernel
         mk.mark(s, G_WET);
       }
       if (P.limiter) launch_alfa2(Q, s);
@@ -221,7 +224,7 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
       mk.mark(s, G_EXT_CELL);
     }
   }
-  launch_ext_finish(P, s, 4);
+  launch_ext_finish(P, s, 4, p.wetting_drying_on);
   mk.mark(s, G_EXT_UPD);
   launch_adjust2(P, s);
   mk.mark(s, G_ADJ2);
@@ -838,7 +841,7 @@ int32_t fvg_kernels_per_step(const fvg_handle* h) {
   if (!h) return -1;
   const fvg_params& p = h->prm;
   int n = 1 + 1 + 2 + 2 + 2;                                // begin, cell_pre, grad3+adv3d, baropg+prep, int advave+reset
-  n += p.isplit * 4 * (2 + (p.wetting_drying_on ? 2 : 0)) + 1; // RK stages, closing update
+  n += p.isplit * 4 * (2 + (p.wetting_drying_on ? 1 : 0)) + 1; // RK stages, closing update
   if (p.limiter) n += p.isplit * 4 + 1 + 2;                  // slope limiters: stages, ADVAVE, 3-D
   if (p.baropg_z && !p.barotropic) n += 2;                   // PHY_BAROPG's two kernels
   n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv

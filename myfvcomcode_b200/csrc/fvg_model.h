@@ -301,15 +301,18 @@ extern const double kAlphaRK[5];
 // ---------------- external mode (k_ext.cu) ----------------
 // EN_FINISH_PREV: first finish the node part of the previous stage's update (EL = ELF,
 // D, DTFA, the stage sums), that stage's K in bits 8-10 of parts.
-enum ExtNodeParts { EN_EXTEL = 1, EN_BC = 2, EN_COPY_ELRK = 4, EN_GRAD = 8, EN_FINISH_PREV = 16 };
+// EN_WET_PREV: before that, the node part of the previous stage's WET_JUDGE (ISWETN and the
+// ELF clamp, mod_wd.F:222-284) from that stage's cell flags, then in ISWETCE.
+enum ExtNodeParts { EN_EXTEL = 1, EN_BC = 2, EN_COPY_ELRK = 4, EN_GRAD = 8, EN_FINISH_PREV = 16, EN_WET_PREV = 32 };
 // EC_FINISH: end with the cell part of the stage's update (EL1, D1, the stage sums, the
 // next stage's continuity fluxes from the new UAF, VAF), UA/VA being swapped with
 // UAF/VAF between stages instead of copied.
 enum ExtCellParts { EC_N2E = 1, EC_FLUXOBN = 2, EC_ADVAVE = 4, EC_EXTUV = 8, EC_BC2 = 16, EC_COPY_RK = 32,
                     EC_INT_ADVAVE = 64, EC_FINISH = 128 };
-void launch_ext_finish(const Dev& P, cudaStream_t s, int K);
+void launch_ext_finish(const Dev& P, cudaStream_t s, int K, int wet_prev);
 void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts);
 void launch_wet_judge(const Dev& P, cudaStream_t s);
+void launch_wet_cells(const Dev& P, cudaStream_t s);
 void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts);
 void launch_alfa2(const Dev& P, cudaStream_t s);
 void launch_ext_update(const Dev& P, cudaStream_t s, int K);

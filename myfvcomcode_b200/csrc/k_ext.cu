@@ -81,6 +81,17 @@ __device__ inline void store_exf(const Dev& P, int c) {
 // (mod_obcs.F:509-617) with the Runge-Kutta blend of the specified-elevation nodes
 // (external_step.F:262-266).  One thread per node; the node's control-volume half-edges
 // are gathered in ascending half-edge number, the order of the reference's scatter.
+// Node part of WET_JUDGE for node i from the cell flags cwet of the same judgement.
+__device__ inline void wet_node(const Dev& P, int i, const int* cwet) {
+  double e = P.elf[i];
+  int wet = ((P.h[i] + e - P.min_depth) < 1.0e-5) ? 0 : 1;
+  int s = 0;
+  for (int j = 1; j <= P.ntve[i]; ++j) s += cwet[P.nbve[(size_t)(j - 1) * (P.M + 1) + i]];
+  if (s == 0) wet = 0;
+  P.iswetn[i] = wet;
+  P.elf[i] = fmax(e, -P.h[i] + P.min_depth);
+}
+
 // -------------------------------------------------------------------------------------
 // Node part of the update after stage K (external_step.F:333-436): EL = ELF, D, DTFA, and
 // the K == 3 and K == 4 sums.
@@ -147,6 +158,8 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   // cell part: least-squares gradient of the current UA, VA for ADVAVE of this stage
   if ((parts & EN_GRAD) && i <= P.N) store_grad(P, i);
   if (i > P.M) return;
+  // the previous stage's node judgement, its cell flags now in ISWETCE (roles swapped)
+  if (parts & EN_WET_PREV) wet_node(P, i, P.iswetce);
   if (parts & EN_FINISH_PREV) ext_update_node(P, i, (parts >> 8) & 7);
   double x = 0.0;
   if (parts & EN_EXTEL) {
@@ -217,19 +230,13 @@ __global__ void k_wet_cells(const Dev P) {
 __global__ void k_wet_nodes(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.M) return;
-  double e = P.elf[i];
-  int wet = ((P.h[i] + e - P.min_depth) < 1.0e-5) ? 0 : 1;
-  int s = 0;
-  for (int j = 1; j <= P.ntve[i]; ++j) s += P.iswetc[P.nbve[(size_t)(j - 1) * (P.M + 1) + i]];
-  if (s == 0) wet = 0;
-  P.iswetn[i] = wet;
-  P.elf[i] = fmax(e, -P.h[i] + P.min_depth);
+  wet_node(P, i, P.iswetc);
 }
 
 // ADVAVE_EDGE_GCN for one cell (advave_edge_gcn.F:115-1003, LIMITED_NO branch), over the
 // cell's slot table.  The edge fluxes are evaluated in R; the surface-slope pressure
 // gradient PSTX/PSTY stays FP64.
-template <typename R>
+template <typename R, bool LIM>
 __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo, double& px, double& py) {
   typedef Mesh<R> Mh;
   const R half = (R)0.5, one = (R)1.0;
@@ -237,6 +244,12 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
   px = 0.0; py = 0.0;
   const size_t n1 = P.N + 1;
   const R epor = (R)P.epor[i], iucp = (R)P.iucp[i];
+  // The cell's own side of its three edges is loaded once; per edge only the other
+  // cell's gradient, UA, VA, ART, CC_HVC and wet flags are gathered.
+  const Grad<R> gi = load_grad<R>(P, i);
+  const R ui = (R)P.ua[i], vi = (R)P.va[i], arti = Mh::art(P, i), cci = Mh::cc_hvc(P, i);
+  const int weti = P.iswetce[i] * P.iswetc[i];
+  const double ged1 = P.grav_e[i] * P.d1[i];
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;
     const int code = P.ce_code[q];
@@ -245,18 +258,40 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
     const int j1 = P.ce_j1[q], j2 = P.ce_j2[q];
     R dij = (R)(0.5 * (P.d[j1] + P.d[j2]));
     double elij = 0.5 * (P.el[j1] + P.el[j2]);
-    if (P.iswetce[ia] * P.iswetc[ia] == 1 || P.iswetce[ib] * P.iswetc[ib] == 1) {
-      Grad<R> ga = load_grad<R>(P, ia);
-      Grad<R> gb = load_grad<R>(P, ib);
-      const R xija = Mh::s_xoa(P, q), yija = Mh::s_yoa(P, q);
-      const R xijb = Mh::s_xob(P, q), yijb = Mh::s_yob(P, q);
+    const int o = side == 0 ? ib : ia;  // the other cell of the edge
+    if (weti == 1 || P.iswetce[o] * P.iswetc[o] == 1) {
       R uij1, vij1, uij2, vij2;
-      if (P.limiter == 0) {
-        uij1 = (R)P.ua[ia] + ga.ux * xija + ga.uy * yija;
-        vij1 = (R)P.va[ia] + ga.vx * xija + ga.vy * yija;
-        uij2 = (R)P.ua[ib] + gb.ux * xijb + gb.uy * yijb;
-        vij2 = (R)P.va[ib] + gb.vx * xijb + gb.vy * yijb;
+      Grad<R> ga, gb;
+      R arta, artb, cca, ccb;
+      if constexpr (!LIM) {
+        const Grad<R> go = load_grad<R>(P, o);
+        const R uo = (R)P.ua[o], vo = (R)P.va[o];
+        ga = side == 0 ? gi : go;
+        gb = side == 0 ? go : gi;
+        const R uia = side == 0 ? ui : uo, via = side == 0 ? vi : vo;
+        const R uib = side == 0 ? uo : ui, vib = side == 0 ? vo : vi;
+        R xij = Mh::s_xoa(P, q);
+        R yij = Mh::s_yoa(P, q);
+        uij1 = uia + ga.ux * xij + ga.uy * yij;
+        vij1 = via + ga.vx * xij + ga.vy * yij;
+        xij = Mh::s_xob(P, q);
+        yij = Mh::s_yob(P, q);
+        uij2 = uib + gb.ux * xij + gb.uy * yij;
+        vij2 = vib + gb.vx * xij + gb.vy * yij;
+        const R arto = Mh::art(P, o), cco = Mh::cc_hvc(P, o);
+        arta = side == 0 ? arti : arto;
+        artb = side == 0 ? arto : arti;
+        cca = side == 0 ? cci : cco;
+        ccb = side == 0 ? cco : cci;
       } else {
+        arta = Mh::art(P, ia);
+        artb = Mh::art(P, ib);
+        cca = Mh::cc_hvc(P, ia);
+        ccb = Mh::cc_hvc(P, ib);
+        ga = load_grad<R>(P, ia);
+        gb = load_grad<R>(P, ib);
+        const R xija = Mh::s_xoa(P, q), yija = Mh::s_yoa(P, q);
+        const R xijb = Mh::s_xob(P, q), yijb = Mh::s_yob(P, q);
         lim_faces<R>(P.limiter, (R)P.ua[ia], (R)P.ua[ib], ga.ux * xija + ga.uy * yija, gb.ux * xijb + gb.uy * yijb,
                      Mh::alfa2(P, 0)[ia], Mh::alfa2(P, 0)[ib], uij1, uij2);
         lim_faces<R>(P.limiter, (R)P.va[ia], (R)P.va[ib], ga.vx * xija + ga.vy * yija, gb.vx * xijb + gb.vy * yijb,
@@ -266,9 +301,8 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
       R vij = half * (vij1 + vij2);
       const R dltxc = Mh::s_dx(P, q), dltyc = Mh::s_dy(P, q);
       R un = -uij * dltyc + vij * dltxc;
-      R viscof1 = Mh::art(P, ia) * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + half * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
-      R viscof2 = Mh::art(P, ib) * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + half * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
-      const R cca = Mh::cc_hvc(P, ia), ccb = Mh::cc_hvc(P, ib);
+      R viscof1 = arta * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + half * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
+      R viscof2 = artb * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + half * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
       R viscof = ((R)P.fact * half * (viscof1 * cca + viscof2 * ccb) + (R)P.fm1 * half * (cca + ccb)) / (R)P.hprnu;
       R txx = (ga.ux + gb.ux) * viscof;
       R tyy = (ga.vy + gb.vy) * viscof;
@@ -289,14 +323,14 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
     }
     const double edx = P.ce_dx[q], edy = P.ce_dy[q];
     if (side == 0) {
-      px = px - P.grav_e[i] * P.d1[i] * elij * edy;
-      py = py + P.grav_e[i] * P.d1[i] * elij * edx;
+      px = px - ged1 * elij * edy;
+      py = py + ged1 * elij * edx;
     } else {
-      px = px + P.grav_e[i] * P.d1[i] * elij * edy;
-      py = py - P.grav_e[i] * P.d1[i] * elij * edx;
+      px = px + ged1 * elij * edy;
+      py = py - ged1 * elij * edx;
     }
   }
-  R w = (R)(P.iswetce[i] * P.iswetc[i]);
+  R w = (R)weti;
   xfo = (double)(xf * w);
   yfo = (double)(yf * w);
 }
@@ -308,7 +342,10 @@ __device__ inline double fluxobn_cell(const Dev& P, int i, int K) {
     int code = P.cell_obc[q];
     int ob = code >> 1, slot = code & 1;
     int j = P.i_obc_n[ob];
-    double flux = -(P.elf[j] - P.elrk[j]) * P.art1[j] / (dAlphaRK[K] * P.dte) - P.xflux_obcn[ob];
+    // ELF as WET_JUDGE leaves it (its node part may still be pending in a fused loop;
+    // the clamp is idempotent)
+    double ej = P.wetting_drying_on ? fmax(P.elf[j], -P.h[j] + P.min_depth) : P.elf[j];
+    double flux = -(ej - P.elrk[j]) * P.art1[j] / (dAlphaRK[K] * P.dte) - P.xflux_obcn[ob];
     f = f + P.fluxf_obc[(size_t)slot * (P.iobcn + 1) + ob] * flux;
   }
   return f;
@@ -336,8 +373,8 @@ __device__ inline void bc_solid(const Dev& P, int i, int rj, double& uu, double&
 // Per-cell part of one RK stage.  EC_INT_ADVAVE is the internal-step call of ADVAVE
 // followed by ADX2D -= ADVUA (internal_step.F:387-392).
 // -------------------------------------------------------------------------------------
-template <typename R>
-__global__ void k_ext_cell(const Dev P, int iext, int K, int parts) {
+template <typename R, bool LIM>
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 4) k_ext_cell(const Dev P, int iext, int K, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
   const size_t n1 = P.N + 1;
@@ -357,7 +394,7 @@ __global__ void k_ext_cell(const Dev P, int iext, int K, int parts) {
   }
   double xf, yf, px, py;
   if (parts & (EC_ADVAVE | EC_INT_ADVAVE)) {
-    advave_cell<R>(P, i, xf, yf, px, py);
+    advave_cell<R, LIM>(P, i, xf, yf, px, py);
     if (P.isbce[i] == 2) {
       xf = (xf + fob * P.ua[i]) * P.iucp[i];
       yf = (yf + fob * P.va[i]) * P.iucp[i];
@@ -443,9 +480,12 @@ __global__ void k_ext_update(const Dev P, int K) {
 
 // After the last stage of a fused external loop: the node part of its update, and UAF,
 // VAF, ISWETC made equal to UA, VA, ISWETCE as the copying update leaves them.
-__global__ void k_ext_finish(const Dev P, int K) {
+__global__ void k_ext_finish(const Dev P, int K, int wet_prev) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (i <= P.M) ext_update_node(P, i, K);
+  if (i <= P.M) {
+    if (wet_prev) wet_node(P, i, P.iswetce);
+    ext_update_node(P, i, K);
+  }
   if (i <= P.N) {
     P.uaf[i] = P.ua[i];
     P.vaf[i] = P.va[i];
@@ -530,19 +570,20 @@ void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);
   k_wet_nodes<<<nblk(P.M, 256), 256, 0, s>>>(P);
 }
+void launch_wet_cells(const Dev& P, cudaStream_t s) { k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P); }
 void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
   if (P.prec)
-    k_ext_cell<float><<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
+    (P.limiter ? k_ext_cell<float, true> : k_ext_cell<float, false>)<<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
   else
-    k_ext_cell<double><<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
+    (P.limiter ? k_ext_cell<double, true> : k_ext_cell<double, false>)<<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
 }
 void launch_ext_update(const Dev& P, cudaStream_t s, int K) {
   int n = P.M > P.N ? P.M : P.N;
   k_ext_update<<<nblk(n, 256), 256, 0, s>>>(P, K);
 }
-void launch_ext_finish(const Dev& P, cudaStream_t s, int K) {
+void launch_ext_finish(const Dev& P, cudaStream_t s, int K, int wet_prev) {
   int n = P.M > P.N ? P.M : P.N;
-  k_ext_finish<<<nblk(n, 256), 256, 0, s>>>(P, K);
+  k_ext_finish<<<nblk(n, 256), 256, 0, s>>>(P, K, wet_prev);
 }
 void launch_begin_step(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 1); }
 void launch_set_qdis(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 0); }

@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(256) k_alfa3(const Dev P) {
 }
 
 // q: the edge's slot in the cell slot table (offsets and DLTXC/DLTYC of the edge).
-template <typename R>
+template <typename R, bool LIM>
 __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib, int k, R dij, bool exflux_form) {
   typedef Mesh<R> Mh;
   const R half = (R)0.5, one = (R)1.0;
@@ -192,15 +192,18 @@ __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib,
   const double* V = P.v + C3(P, 0, k);
   R xija = Mh::s_xoa(P, q), yija = Mh::s_yoa(P, q);
   R xijb = Mh::s_xob(P, q), yijb = Mh::s_yob(P, q);
-  G3<R> ga = load_g3<R>(P, ia, k);
-  G3<R> gb = load_g3<R>(P, ib, k);
+  G3<R> ga, gb;
   R uij1, vij1, uij2, vij2;
-  if (P.limiter == 0) {
+  if constexpr (!LIM) {
+    ga = load_g3<R>(P, ia, k);
     uij1 = (R)U[ia] + ga.ux * xija + ga.uy * yija;
     vij1 = (R)V[ia] + ga.vx * xija + ga.vy * yija;
+    gb = load_g3<R>(P, ib, k);
     uij2 = (R)U[ib] + gb.ux * xijb + gb.uy * yijb;
     vij2 = (R)V[ib] + gb.vx * xijb + gb.vy * yijb;
   } else {
+    ga = load_g3<R>(P, ia, k);
+    gb = load_g3<R>(P, ib, k);
     const size_t qa = C3(P, ia, k), qb = C3(P, ib, k);
     lim_faces<R>(P.limiter, (R)U[ia], (R)U[ib], ga.ux * xija + ga.uy * yija, gb.ux * xijb + gb.uy * yijb,
                  Mh::alfa3(P, 0)[qa], Mh::alfa3(P, 0)[qb], uij1, uij2);
@@ -260,7 +263,7 @@ __device__ inline void river3(const Dev& P, int i, int k, double& x, double& y) 
 // ADVECTION_EDGE_GCN (advection_edge_gcn.F:397-708): per cell and layer, the cell's three
 // edges in ascending edge number.
 // -------------------------------------------------------------------------------------
-template <typename R>
+template <typename R, bool LIM>
 __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
     if (!(P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1)) continue;
     const int j1 = P.ce_j1[q], j2 = P.ce_j2[q];
     R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
-    EdgeFlux<R> f = edge_flux3<R>(P, q, ia, ib, k, dij, false);
+    EdgeFlux<R> f = edge_flux3<R, LIM>(P, q, ia, ib, k, dij, false);
     R isb = (R)isbc;
     R tp = (R)((double)(float)(1 - isbc) * P.epor[i]);
     if (side == 0) {
@@ -323,40 +326,61 @@ __global__ void k_baropg(const Dev P, int do_baropg, int do_sums) {
       dij[j] = 0.5 * (P.dt[nvv[J1]] + P.dt[nvv[J2]]);
     }
     double rprev[4] = {0, 0, 0, 0}, d1p[4] = {0, 0, 0, 0};
-    double d2 = 0.0, rhoc_prev = 0.0;
+    double d2 = 0.0, rhoc_prev = 0.0, zprev = 0.0;
     double dt1 = P.dt1[i], ge = P.grav_e[i];
-    for (int k = 1; k <= KBM1; ++k) {
-      double rij[4];
-      for (int j = 1; j <= 3; ++j) {
-        int J1 = j + 1 - ((j + 1) / 4) * 3, J2 = j + 2 - ((j + 2) / 4) * 3;
-        size_t q1 = N3(P, nvv[J1], k), q2 = N3(P, nvv[J2], k);
-        rij[j] = 0.5 * ((P.rho1[q1] - P.rmean1[q1]) + (P.rho1[q2] - P.rmean1[q2]));
-      }
-      double rhoc = P.rho[C3(P, i, k)] - P.rmean[C3(P, i, k)];
-      if (k == 1) {
-        for (int j = 1; j <= 3; ++j) d1p[j] = rij[j] * (-P.zz1[C3(P, i, 1)]);
-        d2 = 0.0;
-      } else {
-        double zkm = P.zz1[C3(P, i, k - 1)], zk = P.zz1[C3(P, i, k)];
-        for (int j = 1; j <= 3; ++j) d1p[j] = 0.5 * (rprev[j] + rij[j]) * (zkm - zk) + d1p[j];
-        d2 = d2 + 0.5 * (zkm + zk) * (rhoc - rhoc_prev);
-      }
-      double drhox = 0.0, drhoy = 0.0;
-      if (active) {
+    // Layers in batches of kB: every input of a batch is loaded before its vertical
+    // integrals run, so the loads of a batch are in flight together.
+    constexpr int kB = 4;
+    for (int k0 = 1; k0 <= KBM1; k0 += kB) {
+      double dn[kB][4], rhoc[kB], zz[kB], dz[kB];
+#pragma unroll
+      for (int b = 0; b < kB; ++b) {
+        const int k = k0 + b;
+        if (k > KBM1) break;
         for (int j = 1; j <= 3; ++j) {
-          double drho1 = dyv[j] * d1p[j] * dt1;
-          double drho2 = dyv[j] * dij[j] * d2;
-          drhox = drhox + drho1 + drho2;
-          drho1 = dx[j] * d1p[j] * dt1;
-          drho2 = dx[j] * dij[j] * d2;
-          drhoy = drhoy + drho1 + drho2;
+          const size_t q = N3(P, nvv[j], k);
+          dn[b][j] = P.rho1[q] - P.rmean1[q];
         }
+        const size_t c = C3(P, i, k);
+        rhoc[b] = P.rho[c] - P.rmean[c];
+        zz[b] = P.zz1[c];
+        dz[b] = P.dz1[c];
       }
-      double dz1 = P.dz1[C3(P, i, k)];
-      P.drhox[C3(P, i, k)] = drhox * dt1 * dz1 * ge * ramp;
-      P.drhoy[C3(P, i, k)] = drhoy * dt1 * dz1 * ge * ramp;
-      for (int j = 1; j <= 3; ++j) rprev[j] = rij[j];
-      rhoc_prev = rhoc;
+#pragma unroll
+      for (int b = 0; b < kB; ++b) {
+        const int k = k0 + b;
+        if (k > KBM1) break;
+        double rij[4];
+        for (int j = 1; j <= 3; ++j) {
+          int J1 = j + 1 - ((j + 1) / 4) * 3, J2 = j + 2 - ((j + 2) / 4) * 3;
+          rij[j] = 0.5 * (dn[b][J1] + dn[b][J2]);
+        }
+        if (k == 1) {
+          for (int j = 1; j <= 3; ++j) d1p[j] = rij[j] * (-zz[b]);
+          d2 = 0.0;
+        } else {
+          const double zkm = zprev, zk = zz[b];
+          for (int j = 1; j <= 3; ++j) d1p[j] = 0.5 * (rprev[j] + rij[j]) * (zkm - zk) + d1p[j];
+          d2 = d2 + 0.5 * (zkm + zk) * (rhoc[b] - rhoc_prev);
+        }
+        double drhox = 0.0, drhoy = 0.0;
+        if (active) {
+          for (int j = 1; j <= 3; ++j) {
+            double drho1 = dyv[j] * d1p[j] * dt1;
+            double drho2 = dyv[j] * dij[j] * d2;
+            drhox = drhox + drho1 + drho2;
+            drho1 = dx[j] * d1p[j] * dt1;
+            drho2 = dx[j] * dij[j] * d2;
+            drhoy = drhoy + drho1 + drho2;
+          }
+        }
+        const size_t c = C3(P, i, k);
+        P.drhox[c] = drhox * dt1 * dz[b] * ge * ramp;
+        P.drhoy[c] = drhoy * dt1 * dz[b] * ge * ramp;
+        for (int j = 1; j <= 3; ++j) rprev[j] = rij[j];
+        rhoc_prev = rhoc[b];
+        zprev = zz[b];
+      }
     }
     for (int k = 1; k <= P.KB; ++k) {
       size_t q = C3(P, i, k);
@@ -583,7 +607,7 @@ __global__ void __launch_bounds__(256) k_w_viscofh(const Dev P, int do_w, int do
 // internal barotropic pressure gradient from EGF, vertical advection, baroclinic
 // pressure gradient, Coriolis, river momentum and the explicit update to UF/VF.
 // -------------------------------------------------------------------------------------
-template <typename R>
+template <typename R, bool LIM>
 __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
@@ -604,7 +628,7 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
     double elij = 0.5 * (P.egf[j1] + P.egf[j2]);
     R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
     if (P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1) {
-      EdgeFlux<R> f = edge_flux3<R>(P, q, ia, ib, k, dij, true);
+      EdgeFlux<R> f = edge_flux3<R, LIM>(P, q, ia, ib, k, dij, true);
       vmr = vmr + f.viscof;
       R isb = (R)isbc;
       R tp = (R)((double)(float)(1 - isbc) * P.epor[i]);
@@ -803,9 +827,9 @@ static void launch_alfa3(const Dev& P, cudaStream_t s) {
 void launch_advection3d(const Dev& P, cudaStream_t s) {
   if (P.limiter) launch_alfa3(P, s);
   if (P.prec)
-    k_advection3d<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+    (P.limiter ? k_advection3d<float, true> : k_advection3d<float, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
   else
-    k_advection3d<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+    (P.limiter ? k_advection3d<double, true> : k_advection3d<double, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 // -------------------------------------------------------------------------------------
 // PHY_BAROPG (phy_baropg.F:37-151), BAROCLINIC_PRESSURE_GRADIENT = 'z coordinates'.
@@ -962,9 +986,9 @@ void launch_w_viscofh(const Dev& P, cudaStream_t s, int do_w, int do_visc) {
 void launch_adv_uv(const Dev& P, cudaStream_t s) {
   if (P.limiter) launch_alfa3(P, s);
   if (P.prec)
-    k_adv_uv<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+    (P.limiter ? k_adv_uv<float, true> : k_adv_uv<float, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
   else
-    k_adv_uv<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+    (P.limiter ? k_adv_uv<double, true> : k_adv_uv<double, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_vdif_uv(const Dev& P, cudaStream_t s, int parts) {
   k_vdif_uv<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);

@@ -850,8 +850,10 @@ __global__ void __launch_bounds__(256) k_fct_ts(const Dev P, int parts) {
 // takes the net heat flux WTSURF, held at zero while cooling water at or below -2 C,
 // and the short-wave flux RAD(K) = SWRAD*(RHEAT*EXP(Z*D/ZETA1) + (1-RHEAT)*EXP(Z*D/ZETA2))
 // absorbed between levels; WTSURF and SWRAD are the forcing in W/m^2 times RAMP over
-// -SPCP*ROSEA (BCOND_GCN(8), bcond_gcn.F:683-694).  Without heating every term is zero.
+// -SPCP*ROSEA (BCOND_GCN(8), bcond_gcn.F:683-694).  Without heating every term is zero
+// and the kernel is instantiated without them (HEAT = false).
 // -------------------------------------------------------------------------------------
+template <bool HEAT>
 __global__ void __launch_bounds__(128) k_vdif_ts(const Dev P, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.M || P.iswetn[i] != 1) return;
@@ -869,7 +871,7 @@ __global__ void __launch_bounds__(128) k_vdif_ts(const Dev P, int parts) {
     double vhf[kMaxKBs], vhpf[kMaxKBs];
     const double sasurf = 0.0;
     double wfsurf = 0.0, swradf = 0.0;
-    const bool heat = t == 0 && P.heating_on;
+    const bool heat = HEAT && t == 0;
     if (heat) {
       const double spro = 4.2174E3 * 1.023E3;
       const double ramp = ramp_int(P);
@@ -1144,7 +1146,10 @@ void launch_fct_ts(const Dev& P, cudaStream_t s, int parts) {
   k_fct_ts<<<g, b, 0, s>>>(P, parts);
 }
 void launch_vdif_ts(const Dev& P, cudaStream_t s, int parts) {
-  k_vdif_ts<<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
+  if (P.heating_on)
+    k_vdif_ts<true><<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
+  else
+    k_vdif_ts<false><<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
 }
 void launch_bcond_ts(const Dev& P, cudaStream_t s, int parts) {
   k_bcond_ts_riv<<<1, 128, 0, s>>>(P);
