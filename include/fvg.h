@@ -134,6 +134,11 @@ typedef struct fvg_params {
   /* BAROCLINIC_PRESSURE_GRADIENT: 0 'sigma levels' (BAROPG), 1 'z coordinates'
      (PHY_BAROPG, phy_baropg.F:37-151: 600 z levels of HMAX/600) */
   int32_t baropg_z;
+  /* Solid-boundary treatment of the momentum advection: 0 GCN (no ghost cell); 1 GCY,
+     ghost cells (ghostuv.F, advave_edge_gcy.F, advection_edge_gcy.F, adv_uv_edge_gcy.F,
+     bcond_gcy.F).  The GCY1/GCY2 choice of ghost point lives in the mesh's A1U/A2U
+     (SHAPE_COEF_GCY). */
+  int32_t ghost_cells;
 } fvg_params;
 
 /* Boundary forcing that is constant in time for the supported cases. */

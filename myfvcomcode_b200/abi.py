@@ -60,7 +60,7 @@ class FvgParams(C.Structure):
         ("obc_ts_type", C.c_int32), ("river_ts_setting", C.c_int32),
         ("river_location", C.c_int32), ("tide_ref_time", C.c_double),
         ("heating_on", C.c_int32), ("rheat", C.c_double), ("zeta1", C.c_double), ("zeta2", C.c_double),
-        ("limiter", C.c_int32), ("baropg_z", C.c_int32),
+        ("limiter", C.c_int32), ("baropg_z", C.c_int32), ("ghost_cells", C.c_int32),
     ]
 
 
@@ -202,6 +202,7 @@ def make_structs(case):
     ps.limiter = {"LIMITED_NO": 0, "LIMITED_1": 1, "LIMITED_2": 2}.get(p.get("LIMITER", "LIMITED_NO"), -1)
     ps.baropg_z = {"sigma levels": 0, "z coordinates": 1}.get(
         p.get("BAROCLINIC_PRESSURE_GRADIENT", "sigma levels"), -1)
+    ps.ghost_cells = 0 if g.a.get("GHOST_CELLS", "GCN") == "GCN" else 1
 
     fs = forcing_struct(case, b)
     return ms, ps, fs, b

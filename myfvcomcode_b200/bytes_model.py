@@ -50,12 +50,16 @@ def ledger(grid, isplit, wet_dry, precision="fp64"):
     # k_ext_node, its cell part (H1 read, EL1, D1 and the three half-edge continuity
     # fluxes written, CELL_HE read) at the tail of k_ext_cell; one closing launch
     # (k_ext_finish) does the last stage's node part and the UA/VA copies.
-    g["ext_node"] = (M * (I + I + 3 * D) + halfedge_csr + NCV * (I + 2 * D) + N * 3 * D + M * 5 * D, st)
+    # With wetting and drying WET_JUDGE's node part (ELF read and written, H read, ISWETN
+    # written, the NBVE ring of cell flags) also runs at the head of k_ext_node; its cell
+    # part (the three nodes' ELF and H, ISWETC and ELF1 written) keeps its own kernel.
+    wet_node = (M * (3 * D + 2 * I) + I * ntve) if wet_dry else 0
+    g["ext_node"] = (M * (I + I + 3 * D) + halfedge_csr + NCV * (I + 2 * D) + N * 3 * D + M * 5 * D + wet_node, st)
     g["ext_cell"] = (N * (cell_lsq // N + 22 * D + 4 * X + 6 * I) + N * 8 * D + edge_geo + pg_extra
                      + M * 4 * D + N * (6 * D + 3 * I), st)
     g["ext_update"] = (M * (6 * D + I) + N * (10 * D + (2 * I if wet_dry else 0)), 1)
     if wet_dry:
-        g["wet_judge"] = (N * (3 * I + I + D) + M * (4 * D + 2 * I) + I * ntve, st)
+        g["wet_judge"] = (N * (3 * I + I + D) + M * D, st)
     # ---- 3-D, once per internal step ----
     g["cell_pre"] = (N * K * 4 * D + N * K * D + N * 12 * D, 1)              # U,V rw; DZ1; 2-D
     g["advection3d"] = (N * K * 2 * D + N * K * 2 * X + M * K * D + cell_lsq + N * 6 * D + N * 4 * X

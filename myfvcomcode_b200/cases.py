@@ -8,7 +8,8 @@ shapes, sizes and forcing the workloads call for:
   tide of 1.0 m on the 21 seaward nodes, one 100 m^3/s fresh river at the head,
   T = 15 C / S = 30 initially, MY2.5, DTE = 2 s, ISPLIT = 10, no wetting and drying,
   a sponge layer (radius 6 km, coefficient 0.01) at the open boundary.
-  ``nx``/``ny``/``kb`` shrink it for quick tests.
+  ``nx``/``ny``/``kb`` shrink it for quick tests.  ``ghost_cells`` (both cases) selects
+  FVCOM's solid-boundary treatment: "GCN", "GCY1" or "GCY2".
 * ``coastal_mesh``: the large coastal mesh, a Delaunay triangulation of jittered lattice
   points in a 200 km x 100 km box (200,000 points by default), bathymetry
   5 m + 195 m x a smoothed Gaussian random field (correlation length 10 km) with a
@@ -76,7 +77,7 @@ def default_params(**kw):
 
 
 def estuary_channel(nx=100, ny=20, kb=11, lx=20000.0, ly=4000.0, river_q=100.0,
-                    river_location="node", lat=30.0, river=True, sponge=True, **pkw):
+                    river_location="node", lat=30.0, river=True, sponge=True, ghost_cells="GCN", **pkw):
     # The lower seaward corner quad is split along its other diagonal so that no cell
     # has one open and one solid side (tge.F:563-580 rejects such cells).
     vx, vy, tri, nid = _structured(nx, ny, lx, ly, flip={(nx - 1, 0)})
@@ -97,7 +98,7 @@ def estuary_channel(nx=100, ny=20, kb=11, lx=20000.0, ly=4000.0, river_q=100.0,
     spg = [(obc[len(obc) // 2], 0.3 * lx, 0.01)] if sponge else ()
     g = build_grid(vx, vy, nv, h, kb, obc_nodes=obc, obc_types=[1] * len(obc),
                    cor_lat=lat, sponge=spg, horcon=0.2, z0b=0.001,
-                   rivers=rivers, river_location=river_location)
+                   rivers=rivers, river_location=river_location, ghost_cells=ghost_cells)
     n_obc = len(obc)
     tide = dict(period=np.array([M2_PERIOD]), apt=np.full((n_obc, 1), 1.0),
                 phai=np.zeros((n_obc, 1)), emean=np.zeros(n_obc))
@@ -133,7 +134,7 @@ def _bilinear(f, res, x, y):
 
 
 def coastal_mesh(npts=200000, kb=41, lx=200000.0, ly=100000.0, seed=1234, lat=40.0,
-                 wind_speed=10.0, dte=2.0, blend=6000.0, sponge=(10000.0, 0.01), **pkw):
+                 wind_speed=10.0, dte=2.0, blend=6000.0, sponge=(10000.0, 0.01), ghost_cells="GCN", **pkw):
     """Jittered-lattice Delaunay coastal mesh; ``npts`` sets the approximate node count.
 
     ``sponge`` = (radius m, coefficient) of a sponge layer centred on every open-boundary
@@ -188,7 +189,7 @@ def coastal_mesh(npts=200000, kb=41, lx=200000.0, ly=100000.0, seed=1234, lat=40
         spg = [(n, radius, coef) for n in obc]
     g = build_grid(vx, vy, nv, h, kb, obc_nodes=obc, obc_types=[1] * len(obc),
                    cor_lat=lat, sponge=spg, horcon=0.2, z0b=0.001, rivers=[],
-                   river_location="node")
+                   river_location="node", ghost_cells=ghost_cells)
     n_obc = len(obc)
     ph = rng.uniform(0.0, 360.0, 2)
     tide = dict(period=np.array([M2_PERIOD, S2_PERIOD]),

@@ -283,6 +283,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   if (f && f->ntide > kMaxTide) return FVG_ERR_UNSUPPORTED;
   if (prm->heating_on && !(prm->rheat >= 0.0 && prm->zeta1 > 0.0 && prm->zeta2 > 0.0)) return FVG_ERR_ARG;
   if (prm->limiter < 0 || prm->limiter > 2) return FVG_ERR_ARG;
+  if (prm->ghost_cells < 0 || prm->ghost_cells > 1) return FVG_ERR_ARG;
   fvg_handle* h = new fvg_handle();
   h->prm = *prm;
   Dev& P = h->P;
@@ -316,6 +317,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   P.heating_on = prm->heating_on != 0;
   P.limiter = prm->limiter;
   P.baropg_z = prm->baropg_z != 0;
+  P.gcy = prm->ghost_cells != 0;
   {
     double hmax = m->h[1];
     for (int i = 2; i <= M; ++i) hmax = std::max(hmax, m->h[i]);
@@ -627,6 +629,20 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
     if ((rc = dalloc(h, &P.g2d[q], n1))) return fail(rc);
   }
   if (P.baropg_z && (rc = dalloc(h, &P.rhoz, (size_t)P.ms * 600))) return fail(rc);
+  if (P.gcy) {
+    // GHOSTUV2/3's ATAN2, COS, SIN of the edge opposite node j, once on the host
+    std::vector<double> gc(3 * n1, 1.0), gs(3 * n1, 0.0);
+    for (size_t i = 1; i < n1; ++i)
+      for (int j = 1; j <= 3; ++j) {
+        const int J1 = j + 1 - ((j + 1) / 4) * 3, J2 = j + 2 - ((j + 2) / 4) * 3;
+        const int na = m->nv[(size_t)(J1 - 1) * n1 + i], nb = m->nv[(size_t)(J2 - 1) * n1 + i];
+        const double a = std::atan2(m->vy[na] - m->vy[nb], m->vx[na] - m->vx[nb]);
+        gc[(size_t)(j - 1) * n1 + i] = std::cos(a);
+        gs[(size_t)(j - 1) * n1 + i] = std::sin(a);
+      }
+    UPD(gh_cos, gc.data(), 3 * n1);
+    UPD(gh_sin, gs.data(), 3 * n1);
+  }
   if (P.limiter) {
     std::vector<double> ones(std::max(n1, (size_t)P.ns * KB), 1.0);
     for (int q = 0; q < 2; ++q) {

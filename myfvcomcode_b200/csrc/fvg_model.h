@@ -75,6 +75,8 @@ struct Dev {
   double rheat, zeta1, zeta2;
   int limiter;  // 0 LIMITED_NO, 1 LIMITED_1, 2 the slope limiter alone
   int baropg_z;   // BAROCLINIC_PRESSURE_GRADIENT 'z coordinates' (PHY_BAROPG)
+  int gcy;        // ghost cells on the solid boundary (GCY); 0: GCN
+  const double *gh_cos, *gh_sin;  // GCY: cos, sin of the edge opposite node j, [(j-1)*(N+1)+c]
   double deltz;   // its z spacing HMAX/600
   double* rhoz;   // RHO1 interpolated to the 600 z levels, [(k-1)*ms + node]
   SchedLayout sl;
@@ -204,6 +206,25 @@ constexpr int CLOS_IN = 8, CLOS_OUT = 3, CLOS_PLANES = CLOS_IN + CLOS_OUT + 1;
 // index helpers
 __host__ __device__ inline size_t N3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ms + i; }
 __host__ __device__ inline size_t C3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ns + i; }
+// Velocity of neighbour j (1..3, cell index k) of cell c for the least-squares gradient
+// under GCY where the neighbour is missing (k == 0): GHOSTUV2/GHOSTUV3 (ghostuv.F:32-223),
+// the cell's velocity projected on the boundary edge opposite node j, or on an
+// open-boundary cell the cell's own velocity.  The angle's cos and sin come from the host.
+__device__ inline void ghost_uv(const Dev& P, const double* U, const double* V, int c, int j, double& uk,
+                                double& vk) {
+  if (P.isbce[c] != 2) {
+    const size_t q = (size_t)(j - 1) * (P.N + 1) + c;
+    const double ca = P.gh_cos[q], sa = P.gh_sin[q];
+    const double utmp = U[c] * ca + V[c] * sa;
+    const double vtmp = 0.0;
+    uk = utmp * ca - vtmp * sa;
+    vk = utmp * sa + vtmp * ca;
+  } else {
+    uk = U[c];
+    vk = V[c];
+  }
+}
+
 // RAMP of the current internal step, from its schedule row.
 __device__ inline double ramp_int(const Dev& P) { return P.sched[(size_t)P.ctl[0] * P.sl.len]; }
 

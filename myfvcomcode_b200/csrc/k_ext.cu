@@ -36,6 +36,12 @@ __device__ inline Grad<R> cell_grad(const Dev& P, int c, const double* U, const 
   R b1 = Mh::a2u(P, c), b2 = Mh::a2u(P, n1 + c), b3 = Mh::a2u(P, 2 * n1 + c), b4 = Mh::a2u(P, 3 * n1 + c);
   R u0 = (R)U[c], u1 = (R)U[k1], u2 = (R)U[k2], u3 = (R)U[k3];
   R v0 = (R)V[c], v1 = (R)V[k1], v2 = (R)V[k2], v3 = (R)V[k3];
+  if (P.gcy && (k1 == 0 || k2 == 0 || k3 == 0)) {
+    double gu, gv;
+    if (k1 == 0) { ghost_uv(P, U, V, c, 1, gu, gv); u1 = (R)gu; v1 = (R)gv; }
+    if (k2 == 0) { ghost_uv(P, U, V, c, 2, gu, gv); u2 = (R)gu; v2 = (R)gv; }
+    if (k3 == 0) { ghost_uv(P, U, V, c, 3, gu, gv); u3 = (R)gu; v3 = (R)gv; }
+  }
   Grad<R> g;
   g.ux = a1 * u0 + a2 * u1 + a3 * u2 + a4 * u3;
   g.uy = b1 * u0 + b2 * u1 + b3 * u2 + b4 * u3;
@@ -155,9 +161,13 @@ __global__ void k_alfa2(const Dev P) {
 
 __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  // cell part: least-squares gradient of the current UA, VA for ADVAVE of this stage
-  if ((parts & EN_GRAD) && i <= P.N) store_grad(P, i);
-  if (i > P.M) return;
+  // threads 1..M take the nodes, threads M+1..M+N the cells' least-squares gradients of
+  // the current UA, VA for ADVAVE of this stage (one job per thread)
+  if (i > P.M) {
+    const int c = i - P.M;
+    if ((parts & EN_GRAD) && c <= P.N) store_grad(P, c);
+    return;
+  }
   // the previous stage's node judgement, its cell flags now in ISWETCE (roles swapped)
   if (parts & EN_WET_PREV) wet_node(P, i, P.iswetce);
   if (parts & EN_FINISH_PREV) ext_update_node(P, i, (parts >> 8) & 7);
@@ -245,7 +255,7 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
   const size_t n1 = P.N + 1;
   const R epor = (R)P.epor[i], iucp = (R)P.iucp[i];
   // The cell's own side of its three edges is loaded once; per edge only the other
-  // cell's gradient, UA, VA, ART, CC_HVC and wet flags are gathered.
+  // cell's gradient, UA, VA, ART, CC_HVC and wet flags are gathered (FP32 form).
   const Grad<R> gi = load_grad<R>(P, i);
   const R ui = (R)P.ua[i], vi = (R)P.va[i], arti = Mh::art(P, i), cci = Mh::cc_hvc(P, i);
   const int weti = P.iswetce[i] * P.iswetc[i];
@@ -263,7 +273,23 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
       R uij1, vij1, uij2, vij2;
       Grad<R> ga, gb;
       R arta, artb, cca, ccb;
-      if constexpr (!LIM) {
+      if constexpr (!LIM && sizeof(R) == 8) {
+        // FP64: per-edge loads of both sides keep the kernel at 108 registers
+        ga = load_grad<R>(P, ia);
+        R xij = Mh::s_xoa(P, q);
+        R yij = Mh::s_yoa(P, q);
+        uij1 = (R)P.ua[ia] + ga.ux * xij + ga.uy * yij;
+        vij1 = (R)P.va[ia] + ga.vx * xij + ga.vy * yij;
+        gb = load_grad<R>(P, ib);
+        xij = Mh::s_xob(P, q);
+        yij = Mh::s_yob(P, q);
+        uij2 = (R)P.ua[ib] + gb.ux * xij + gb.uy * yij;
+        vij2 = (R)P.va[ib] + gb.vx * xij + gb.vy * yij;
+        arta = Mh::art(P, ia);
+        artb = Mh::art(P, ib);
+        cca = Mh::cc_hvc(P, ia);
+        ccb = Mh::cc_hvc(P, ib);
+      } else if constexpr (!LIM) {
         const Grad<R> go = load_grad<R>(P, o);
         const R uo = (R)P.ua[o], vo = (R)P.va[o];
         ga = side == 0 ? gi : go;
@@ -374,7 +400,7 @@ __device__ inline void bc_solid(const Dev& P, int i, int rj, double& uu, double&
 // followed by ADX2D -= ADVUA (internal_step.F:387-392).
 // -------------------------------------------------------------------------------------
 template <typename R, bool LIM>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 4) k_ext_cell(const Dev P, int iext, int K, int parts) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_ext_cell(const Dev P, int iext, int K, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
   const size_t n1 = P.N + 1;
@@ -396,8 +422,13 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 4) k_ext_cell(const 
   if (parts & (EC_ADVAVE | EC_INT_ADVAVE)) {
     advave_cell<R, LIM>(P, i, xf, yf, px, py);
     if (P.isbce[i] == 2) {
-      xf = (xf + fob * P.ua[i]) * P.iucp[i];
-      yf = (yf + fob * P.va[i]) * P.iucp[i];
+      if (P.gcy) {  // advave_edge_gcy.F
+        xf = xf + fob * P.ua[i] * P.iucp[i];
+        yf = yf + fob * P.va[i] * P.iucp[i];
+      } else {
+        xf = (xf + fob * P.ua[i]) * P.iucp[i];
+        yf = (yf + fob * P.va[i]) * P.iucp[i];
+      }
     }
     for (int q = P.cell_riv_ptr[i]; q < P.cell_riv_ptr[i + 1]; ++q) {
       int k = P.cell_riv[q] >> 1;
@@ -453,8 +484,9 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 4) k_ext_cell(const 
     if (parts & EC_BC2) {
       // BCOND_GCN(2,K) (bcond_gcn.F:325-406)
       int b = P.isbce[i];
-      if (b == 3) { uaf = 0.0; vaf = 0.0; }
-      if (b == 1) bc_solid(P, i, P.cell_bcriv[i], uaf, vaf);
+      // GCY (bcond_gcy.F): the river clamp only, no tangential projection or corner zero
+      if (b == 3 && !P.gcy) { uaf = 0.0; vaf = 0.0; }
+      if (b == 1 && (!P.gcy || P.cell_bcriv[i] > 0)) bc_solid(P, i, P.cell_bcriv[i], uaf, vaf);
     }
     P.uaf[i] = uaf;
     P.vaf[i] = vaf;
@@ -512,7 +544,7 @@ __global__ void k_begin_step(const Dev P, int advance) {
 static inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
 void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
-  int n = (parts & EN_GRAD) ? (P.M > P.N ? P.M : P.N) : P.M;
+  int n = (parts & EN_GRAD) ? P.M + P.N : P.M;
   k_ext_node<<<nblk(n, 256), 256, 0, s>>>(P, iext, K, parts);
 }
 void launch_ext_prep(const Dev& P, cudaStream_t s) { k_ext_prep<<<nblk(P.N, 256), 256, 0, s>>>(P); }

@@ -29,7 +29,7 @@ __device__ inline void bc_solid3(const Dev& P, int i, double& uu, double& vv) {
     untmp = fmax(untmp, 0.0);
     uu = untmp * ca - vntmp * sa;
     vv = untmp * sa + vntmp * ca;
-  } else {
+  } else if (!P.gcy) {  // GCY (bcond_gcy.F) keeps the river clamp only
     double sa = P.sin_alpha[i], ca = P.cos_alpha[i];
     double ui = uu * (sa * sa) - vv * sa * ca;
     double vi = -uu * sa * ca + vv * (ca * ca);
@@ -63,8 +63,11 @@ __global__ void k_cell_pre(const Dev P, int parts) {
       for (int k = 1; k <= KBM1; ++k) {
         size_t q = C3(P, i, k);
         double uu = P.u[q], vv = P.v[q];
-        if (b == 3) { uu = 0.0; vv = 0.0; }
-        else bc_solid3(P, i, uu, vv);
+        if (b == 3) {
+          if (!P.gcy) { uu = 0.0; vv = 0.0; }
+        } else {
+          bc_solid3(P, i, uu, vv);
+        }
         P.u[q] = uu;
         P.v[q] = vv;
       }
@@ -108,6 +111,12 @@ __device__ inline G3<R> grad3(const Dev& P, int c, const double* U, const double
   R b1 = Mh::a2u(P, c), b2 = Mh::a2u(P, n1 + c), b3 = Mh::a2u(P, 2 * n1 + c), b4 = Mh::a2u(P, 3 * n1 + c);
   R u0 = (R)U[c], u1 = (R)U[k1], u2 = (R)U[k2], u3 = (R)U[k3];
   R v0 = (R)V[c], v1 = (R)V[k1], v2 = (R)V[k2], v3 = (R)V[k3];
+  if (P.gcy && (k1 == 0 || k2 == 0 || k3 == 0)) {
+    double gu, gv;
+    if (k1 == 0) { ghost_uv(P, U, V, c, 1, gu, gv); u1 = (R)gu; v1 = (R)gv; }
+    if (k2 == 0) { ghost_uv(P, U, V, c, 2, gu, gv); u2 = (R)gu; v2 = (R)gv; }
+    if (k3 == 0) { ghost_uv(P, U, V, c, 3, gu, gv); u3 = (R)gu; v3 = (R)gv; }
+  }
   G3<R> g;
   g.ux = a1 * u0 + a2 * u1 + a3 * u2 + a4 * u3;
   g.uy = b1 * u0 + b2 * u1 + b3 * u2 + b4 * u3;
@@ -283,12 +292,15 @@ __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
     EdgeFlux<R> f = edge_flux3<R, LIM>(P, q, ia, ib, k, dij, false);
     R isb = (R)isbc;
     R tp = (R)((double)(float)(1 - isbc) * P.epor[i]);
+    // viscous part: GCN (fxx + 3 fxx ISBC) EPOR; GCY (advection_edge_gcy.F) fxx TPA
+    const R vfx = P.gcy ? f.fxx * tp : (f.fxx + three * f.fxx * isb) * epor;
+    const R vfy = P.gcy ? f.fyy * tp : (f.fyy + three * f.fyy * isb) * epor;
     if (side == 0) {
-      xr = xr + f.xadv * tp + (f.fxx + three * f.fxx * isb) * epor;
-      yr = yr + f.yadv * tp + (f.fyy + three * f.fyy * isb) * epor;
+      xr = xr + f.xadv * tp + vfx;
+      yr = yr + f.yadv * tp + vfy;
     } else {
-      xr = xr - f.xadv * tp - (f.fxx + three * f.fxx * isb) * epor;
-      yr = yr - f.yadv * tp - (f.fyy + three * f.fyy * isb) * epor;
+      xr = xr - f.xadv * tp - vfx;
+      yr = yr - f.yadv * tp - vfy;
     }
   }
   double x = (double)xr, y = (double)yr;
@@ -632,12 +644,14 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
       vmr = vmr + f.viscof;
       R isb = (R)isbc;
       R tp = (R)((double)(float)(1 - isbc) * P.epor[i]);
+      const R vfx = P.gcy ? f.fxx * tp : (f.fxx + three * f.fxx * isb) * epor;  // GCY: adv_uv_edge_gcy.F
+      const R vfy = P.gcy ? f.fyy * tp : (f.fyy + three * f.fyy * isb) * epor;
       if (side == 0) {
-        xr = xr + f.xadv * tp + (f.fxx + three * f.fxx * isb) * epor;
-        yr = yr + f.yadv * tp + (f.fyy + three * f.fyy * isb) * epor;
+        xr = xr + f.xadv * tp + vfx;
+        yr = yr + f.yadv * tp + vfy;
       } else {
-        xr = xr - f.xadv * tp - (f.fxx + three * f.fxx * isb) * epor;
-        yr = yr - f.yadv * tp - (f.fyy + three * f.fyy * isb) * epor;
+        xr = xr - f.xadv * tp - vfx;
+        yr = yr - f.yadv * tp - vfy;
       }
     }
     const double edx = P.ce_dx[q], edy = P.ce_dy[q];
@@ -779,7 +793,7 @@ __global__ void __launch_bounds__(128) k_vdif_uv(const Dev P, int parts) {
       size_t q = C3(P, i, k);
       double uu = P.uf[q], vv = P.vf[q];
       if (fix) { uu = P.ua[i]; vv = P.va[i]; }
-      if (b == 3) { uu = 0.0; vv = 0.0; }
+      if (b == 3 && !P.gcy) { uu = 0.0; vv = 0.0; }
       if (b == 1) bc_solid3(P, i, uu, vv);
       P.uf[q] = uu;
       P.vf[q] = vv;

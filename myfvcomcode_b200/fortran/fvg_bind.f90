@@ -45,6 +45,7 @@ MODULE FVG_BIND
     REAL(C_DOUBLE) :: RHEAT, ZETA1, ZETA2
     INTEGER(C_INT32_T) :: LIMITER        ! 0 LIMITED_NO, 1 LIMITED_1, 2 slope limiter alone
     INTEGER(C_INT32_T) :: BAROPG_Z       ! 1: BAROCLINIC_PRESSURE_GRADIENT = 'z coordinates'
+    INTEGER(C_INT32_T) :: GHOST_CELLS    ! 0: GCN build, 1: GCY1 or GCY2 build
   END TYPE FVG_PARAMS_T
 
   TYPE, BIND(C) :: FVG_FORCING_T

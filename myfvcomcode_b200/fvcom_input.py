@@ -577,9 +577,10 @@ def _s(v, default=""):
 class FvcomRun:
     """An FVCOM case read from its run namelist (``<case>_run.nml``) and input files."""
 
-    def __init__(self, nml_path, input_dir=None, limiter="LIMITED_NO"):
-        """``limiter``: FVCOM's compile-time choice of the momentum advection limiter,
-        LIMITED_NO, LIMITED_1 or LIMITED_2 (the run namelist does not carry it)."""
+    def __init__(self, nml_path, input_dir=None, limiter="LIMITED_NO", ghost_cells="GCN"):
+        """``limiter`` and ``ghost_cells``: FVCOM's compile-time choices of the momentum
+        advection limiter (LIMITED_NO, LIMITED_1, LIMITED_2) and of the solid-boundary
+        treatment (GCN, GCY1, GCY2); the run namelist carries neither."""
         self.nml_path = os.path.abspath(nml_path)
         nml = read_namelist(nml_path)
         self.nml = nml
@@ -691,7 +692,8 @@ class FvcomRun:
                           sponge=spg, horcon=float(ph.get("HORIZONTAL_MIXING_COEFFICIENT", 0.2)),
                           z0b=float(ph.get("BOTTOM_ROUGHNESS_LENGTHSCALE", 0.001)),
                           rivers=rivers, river_location=rloc,
-                          static_ssh_adj=float(it.get("STATIC_SSH_ADJ", 0.0)), p_sigma=psig)
+                          static_ssh_adj=float(it.get("STATIC_SSH_ADJ", 0.0)), p_sigma=psig,
+                          ghost_cells=ghost_cells)
 
         tide = None
         if obc_nodes and _b(obc.get("OBC_ELEVATION_FORCING_ON")):

@@ -75,7 +75,8 @@ class Grid:
 
 def build_grid(vx_in, vy_in, nv_cw, h_in, kb, obc_nodes=(), obc_types=(),
                cor_lat=None, sponge=(), horcon=0.2, z0b=0.001,
-               rivers=None, river_location="node", static_ssh_adj=0.0, p_sigma=1.0):
+               rivers=None, river_location="node", static_ssh_adj=0.0, p_sigma=1.0,
+               ghost_cells="GCN"):
     """Build every mesh array the mode-split step reads.
 
     vx_in, vy_in, h_in: node coordinates (m) and depth (m), length M (0-based input).
@@ -89,7 +90,13 @@ def build_grid(vx_in, vy_in, nv_cw, h_in, kb, obc_nodes=(), obc_types=(),
     sponge: iterable of (node, radius, coefficient) as in the *_spg.dat file.
     horcon: HORIZONTAL_MIXING_COEFFICIENT (constant kind); z0b: BOTTOM_ROUGHNESS_LENGTHSCALE.
     rivers: list of dicts {"loc": node-or-cell (1-based), "dist": per-layer weights}.
+    ghost_cells: FVCOM's solid-boundary treatment: "GCN" (no ghost cell, gradients of
+      boundary cells are zero), "GCY1" (ghost cell at the foot of the perpendicular from
+      the cell centre to the boundary edge) or "GCY2" (ghost cell at the edge midpoint)
+      (SHAPE_COEF_GCN / SHAPE_COEF_GCY, shape_coef_gcy.F:29-655).
     """
+    if ghost_cells not in ("GCN", "GCY1", "GCY2"):
+        raise ValueError("ghost_cells must be GCN, GCY1 or GCY2")
     g = Grid()
     M = len(vx_in)
     N = len(nv_cw)
@@ -118,7 +125,11 @@ def build_grid(vx_in, vy_in, nv_cw, h_in, kb, obc_nodes=(), obc_types=(),
 
     _tge(g, list(obc_nodes))
     _cell_area(g)
-    _shape_coef(g)
+    if ghost_cells == "GCN":
+        _shape_coef(g)
+    else:
+        _shape_coef_gcy(g, ghost_cells)
+    g["GHOST_CELLS"] = ghost_cells
     _edge_len(g)
     _depth_gradient(g)
     _obc_setup(g, list(obc_nodes), list(obc_types))
@@ -419,6 +430,134 @@ def _shape_coef(g):
             delty = vy[nv[i, j1 - 1]] - vy[nv[i, j2 - 1]]
             alpha[i] = math.atan2(delty, deltx)
             alpha[i] = alpha[i] - pi7 / 2.0
+    ang1 = 359.9 / 180.0 * pi7
+    ang2 = -0.1 / 180.0 * pi7
+    ntve, nbve, isonb = g["NTVE"], g["NBVE"], g["ISONB"]
+    for i in range(1, M + 1):
+        nt = int(ntve[i])
+        if isonb[i] == 1 and nt > 2:
+            angle = alpha[nbve[i, nt - 1]] - alpha[nbve[i, 0]]
+            if angle > ang1:
+                angle = 100000.0
+            elif angle > pi7:
+                angle = angle - 2.0 * pi7
+            elif angle < -pi7:
+                angle = angle + 2.0 * pi7
+            elif angle < ang2:
+                angle = 100000.0
+            for j in range(2, nt):
+                ii = nbve[i, j - 1]
+                if isbce[ii] != 1:
+                    alpha[ii] = alpha[nbve[i, 0]] + angle / _f4(nt - 1) * _f4(j - 1)
+    g.a.update(A1U=a1u, A2U=a2u, AWX=awx, AWY=awy, AW0=aw0, ALPHA=alpha)
+
+
+def _foot(xa, ya, xb, yb, xc, yc):
+    """Foot of the perpendicular from (xc, yc) onto the line through (xa, ya) and (xb, yb),
+    in the reference's line-intersection form (shape_coef_gcy.F:117-125)."""
+    deltx = xa - xb
+    delty = ya - yb
+    aa1 = -delty
+    bb1 = deltx
+    cc1 = -aa1 * xa - bb1 * ya
+    aa2 = bb1
+    bb2 = -aa1
+    cc2 = -aa2 * xc - bb2 * yc
+    x = -(cc1 * bb2 - cc2 * bb1) / (aa1 * bb2 - aa2 * bb1)
+    y = -(cc1 * aa2 - cc2 * aa1) / (bb1 * aa2 - bb2 * aa1)
+    return x, y
+
+
+def _shape_coef_gcy(g, variant):
+    """SHAPE_COEF_GCY (shape_coef_gcy.F:29-655): the least-squares weights of every cell,
+    boundary cells included, with a ghost point in place of each missing neighbour: on a
+    solid edge the foot of the perpendicular from the centre (GCY1) or the edge midpoint
+    (GCY2), on an open-boundary edge twice the centre-to-foot offset.  The formulas are
+    the reference's, including its first A2U weight, which multiplies (X1+X2+X3) by the
+    sum of X squared where the GCN weights use the sum of X*Y."""
+    M, N = g["M"], g["N"]
+    vx, vy, nv, xc, yc = g["VX"], g["VY"], g["NV"], g["XC"], g["YC"]
+    nbe, isbce, art = g["NBE"], g["ISBCE"], g["ART"]
+    a1u = np.zeros((N + 1, 4))
+    a2u = np.zeros((N + 1, 4))
+    awx = np.zeros((N + 1, 3))
+    awy = np.zeros((N + 1, 3))
+    aw0 = np.zeros((N + 1, 3))
+    alpha = np.zeros(N + 1)
+    pi7 = 3.1415926
+
+    def node(i, j):  # node j (1-based) of cell i
+        return nv[i, j - 1]
+
+    def nbr(i, j):
+        return nbe[i, j - 1]
+
+    for i in range(1, N + 1):
+        b = isbce[i]
+        pts = [None, None, None]  # (x, y) offsets of the three neighbours or ghosts
+        if b == 0:
+            for j in range(1, 4):
+                pts[j - 1] = (xc[nbr(i, j)] - xc[i], yc[nbr(i, j)] - yc[i])
+        elif b in (1, 2):
+            jj = 0
+            for j in range(1, 4):
+                if nbr(i, j) == 0:
+                    jj = j
+            j1, j2 = _nxt(jj), _nxt2(jj)
+            na, nb_ = node(i, j1), node(i, j2)
+            if b == 2 or variant == "GCY1":
+                deltx = vx[na] - vx[nb_]
+                delty = vy[na] - vy[nb_]
+                alpha[i] = math.atan2(delty, deltx) - pi7 / 2.0
+                xt, yt = _foot(vx[na], vy[na], vx[nb_], vy[nb_], xc[i], yc[i])
+            else:
+                xt, yt = (vx[na] + vx[nb_]) / 2.0, (vy[na] + vy[nb_]) / 2.0
+            ghost = (xt - xc[i], yt - yc[i]) if b == 1 else ((xt - xc[i]) * 2.0, (yt - yc[i]) * 2.0)
+            for j in range(1, 4):
+                pts[j - 1] = ghost if j == jj else (xc[nbr(i, j)] - xc[i], yc[nbr(i, j)] - yc[i])
+        elif b == 3:
+            jj = 0
+            for j in range(1, 4):
+                if nbr(i, j) != 0:
+                    jj = j
+            j1, j2 = _nxt(jj), _nxt2(jj)
+            n0, na, nb_ = node(i, jj), node(i, j1), node(i, j2)
+            if variant == "GCY1":
+                xt1, yt1 = _foot(vx[n0], vy[n0], vx[nb_], vy[nb_], xc[i], yc[i])
+                xt2, yt2 = _foot(vx[n0], vy[n0], vx[na], vy[na], xc[i], yc[i])
+            else:
+                xt1, yt1 = (vx[n0] + vx[nb_]) / 2.0, (vy[n0] + vy[nb_]) / 2.0
+                xt2, yt2 = (vx[n0] + vx[na]) / 2.0, (vy[n0] + vy[na]) / 2.0
+            # slot j1 lies opposite node j1: the edge (jj, j2), ghost 1; slot j2: ghost 2
+            pts[jj - 1] = (xc[nbr(i, jj)] - xc[i], yc[nbr(i, jj)] - yc[i])
+            pts[j1 - 1] = (xt1 - xc[i], yt1 - yc[i])
+            pts[j2 - 1] = (xt2 - xc[i], yt2 - yc[i])
+        (x1, y1), (x2, y2), (x3, y3) = pts
+        x1 = x1 / 1000.0; x2 = x2 / 1000.0; x3 = x3 / 1000.0
+        y1 = y1 / 1000.0; y2 = y2 / 1000.0; y3 = y3 / 1000.0
+        delt = (x1 * y2 - x2 * y1) ** 2 + (x1 * y3 - x3 * y1) ** 2 + (x2 * y3 - x3 * y2) ** 2
+        delt = delt * 1000.0
+        sxy = x1 * y1 + x2 * y2 + x3 * y3
+        syy = y1 ** 2 + y2 ** 2 + y3 ** 2
+        sxx = x1 ** 2 + x2 ** 2 + x3 ** 2
+        sxx_b = x1 * x1 + x2 * x2 + x3 * x3
+        a1u[i, 0] = ((y1 + y2 + y3) * sxy - (x1 + x2 + x3) * syy) / delt
+        a1u[i, 1] = (syy * x1 - sxy * y1) / delt
+        a1u[i, 2] = (syy * x2 - sxy * y2) / delt
+        a1u[i, 3] = (syy * x3 - sxy * y3) / delt
+        a2u[i, 0] = ((x1 + x2 + x3) * sxx_b - (y1 + y2 + y3) * sxx) / delt
+        a2u[i, 1] = (sxx * y1 - sxy * x1) / delt
+        a2u[i, 2] = (sxx * y2 - sxy * x2) / delt
+        a2u[i, 3] = (sxx * y3 - sxy * x3) / delt
+        x1 = vx[nv[i, 0]] - xc[i]; x2 = vx[nv[i, 1]] - xc[i]; x3 = vx[nv[i, 2]] - xc[i]
+        y1 = vy[nv[i, 0]] - yc[i]; y2 = vy[nv[i, 1]] - yc[i]; y3 = vy[nv[i, 2]] - yc[i]
+        ai = (y2 - y3, y3 - y1, y1 - y2)
+        bi = (x3 - x2, x1 - x3, x2 - x1)
+        ci = (x2 * y3 - x3 * y2, x3 * y1 - x1 * y3, x1 * y2 - x2 * y1)
+        for j in range(3):
+            aw0[i, j] = -ci[j] / 2.0 / art[i]
+            awx[i, j] = -ai[j] / 2.0 / art[i]
+            awy[i, j] = -bi[j] / 2.0 / art[i]
     ang1 = 359.9 / 180.0 * pi7
     ang2 = -0.1 / 180.0 * pi7
     ntve, nbve, isonb = g["NTVE"], g["NBVE"], g["ISONB"]

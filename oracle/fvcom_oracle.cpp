@@ -291,6 +291,44 @@ struct Oracle {
   // =====================================================================================
   // ADVAVE_EDGE_GCN(XFLUX,YFLUX), LIMITED_NO branch (advave_edge_gcn.F:32-1145)
   // =====================================================================================
+  // Velocity of neighbour j (1..3) of cell c for the least-squares gradient.  GCN: the
+  // neighbour's value (the ghost cell 0 holds zero).  GCY where the neighbour is missing:
+  // GHOSTUV2/GHOSTUV3 (ghostuv.F:32-223), the cell's velocity projected on the boundary
+  // edge opposite node j, or, on an open-boundary cell, the cell's own velocity.
+  inline void nbr_uv(const double* U, const double* V, int c, int j, double& uk, double& vk) const {
+    const int k = NBE(c, j);
+    if (!P.ghost_cells || k != 0) {
+      uk = U[k];
+      vk = V[k];
+      return;
+    }
+    if (isbce[c] != 2) {
+      const int J1 = nxt(j), J2 = nxt2(j);
+      const double deltx = vx[NV(c, J1)] - vx[NV(c, J2)];
+      const double delty = vy[NV(c, J1)] - vy[NV(c, J2)];
+      const double a = std::atan2(delty, deltx);
+      const double ca = std::cos(a), sa = std::sin(a);
+      const double utmp = U[c] * ca + V[c] * sa;
+      const double vtmp = 0.0;
+      uk = utmp * ca - vtmp * sa;
+      vk = utmp * sa + vtmp * ca;
+    } else {
+      uk = U[c];
+      vk = V[c];
+    }
+  }
+  // COFA1, COFA2 (U) and COFA5, COFA6 (V) of cell c (advave_edge_gcn.F:634-637).
+  inline void cofa(const double* U, const double* V, int c, double& c1, double& c2, double& c5, double& c6) const {
+    double u1, v1, u2, v2, u3, v3;
+    nbr_uv(U, V, c, 1, u1, v1);
+    nbr_uv(U, V, c, 2, u2, v2);
+    nbr_uv(U, V, c, 3, u3, v3);
+    c1 = A1U(c, 1) * U[c] + A1U(c, 2) * u1 + A1U(c, 3) * u2 + A1U(c, 4) * u3;
+    c2 = A2U(c, 1) * U[c] + A2U(c, 2) * u1 + A2U(c, 3) * u2 + A2U(c, 4) * u3;
+    c5 = A1U(c, 1) * V[c] + A1U(c, 2) * v1 + A1U(c, 3) * v2 + A1U(c, 4) * v3;
+    c6 = A2U(c, 1) * V[c] + A2U(c, 2) * v1 + A2U(c, 3) * v2 + A2U(c, 4) * v3;
+  }
+
   // Phase one of the limited schemes (advave_edge_gcn.F:141-318, advection_edge_gcn.F:
   // 118-259, adv_uv_edge_gcn.F:152-330): per cell the smallest, over its wet edges, of
   // |U(IA)-U(IB)| / |U'+EPSILON|, at most 1, where U' = COFA1*XIJ + COFA2*YIJ is the
@@ -312,10 +350,8 @@ struct Oracle {
       for (int side = 0; side < 2; ++side) {
         int c = side == 0 ? ia : ib;
         int k1 = NBE(c, 1), k2 = NBE(c, 2), k3 = NBE(c, 3);
-        double cofa1 = A1U(c, 1) * U[c] + A1U(c, 2) * U[k1] + A1U(c, 3) * U[k2] + A1U(c, 4) * U[k3];
-        double cofa2 = A2U(c, 1) * U[c] + A2U(c, 2) * U[k1] + A2U(c, 3) * U[k2] + A2U(c, 4) * U[k3];
-        double cofa5 = A1U(c, 1) * V[c] + A1U(c, 2) * V[k1] + A1U(c, 3) * V[k2] + A1U(c, 4) * V[k3];
-        double cofa6 = A2U(c, 1) * V[c] + A2U(c, 2) * V[k1] + A2U(c, 3) * V[k2] + A2U(c, 4) * V[k3];
+        double cofa1, cofa2, cofa5, cofa6;
+        cofa(U, V, c, cofa1, cofa2, cofa5, cofa6);
         double xij = xijc[i] - xc[c], yij = yijc[i] - yc[c];
         lim(std::fabs(U[ia] - U[ib]), cofa1 * xij + cofa2 * yij, ualfa[c]);
         lim(std::fabs(V[ia] - V[ib]), cofa5 * xij + cofa6 * yij, valfa[c]);
@@ -357,17 +393,13 @@ struct Oracle {
       double elij = 0.5 * (el[j1] + el[j2]);
       if (iswetce[ia] * iswetc[ia] == 1 || iswetce[ib] * iswetc[ib] == 1) {
         int k1 = NBE(ia, 1), k2 = NBE(ia, 2), k3 = NBE(ia, 3);
-        double cofa1 = A1U(ia, 1) * ua[ia] + A1U(ia, 2) * ua[k1] + A1U(ia, 3) * ua[k2] + A1U(ia, 4) * ua[k3];
-        double cofa2 = A2U(ia, 1) * ua[ia] + A2U(ia, 2) * ua[k1] + A2U(ia, 3) * ua[k2] + A2U(ia, 4) * ua[k3];
-        double cofa5 = A1U(ia, 1) * va[ia] + A1U(ia, 2) * va[k1] + A1U(ia, 3) * va[k2] + A1U(ia, 4) * va[k3];
-        double cofa6 = A2U(ia, 1) * va[ia] + A2U(ia, 2) * va[k1] + A2U(ia, 3) * va[k2] + A2U(ia, 4) * va[k3];
+        double cofa1, cofa2, cofa5, cofa6;
+        cofa(ua.data(), va.data(), ia, cofa1, cofa2, cofa5, cofa6);
         double xija = xijc[i] - xc[ia];
         double yija = yijc[i] - yc[ia];
         k1 = NBE(ib, 1); k2 = NBE(ib, 2); k3 = NBE(ib, 3);
-        double cofa3 = A1U(ib, 1) * ua[ib] + A1U(ib, 2) * ua[k1] + A1U(ib, 3) * ua[k2] + A1U(ib, 4) * ua[k3];
-        double cofa4 = A2U(ib, 1) * ua[ib] + A2U(ib, 2) * ua[k1] + A2U(ib, 3) * ua[k2] + A2U(ib, 4) * ua[k3];
-        double cofa7 = A1U(ib, 1) * va[ib] + A1U(ib, 2) * va[k1] + A1U(ib, 3) * va[k2] + A1U(ib, 4) * va[k3];
-        double cofa8 = A2U(ib, 1) * va[ib] + A2U(ib, 2) * va[k1] + A2U(ib, 3) * va[k2] + A2U(ib, 4) * va[k3];
+        double cofa3, cofa4, cofa7, cofa8;
+        cofa(ua.data(), va.data(), ib, cofa3, cofa4, cofa7, cofa8);
         double xijb = xijc[i] - xc[ib];
         double yijb = yijc[i] - yc[ib];
         const bool L = P.limiter != 0;
@@ -409,8 +441,13 @@ struct Oracle {
     }
     for (int i = 1; i <= N; ++i) {
       if (isbce[i] == 2) {
-        xflux[i] = (xflux[i] + fluxobn[i] * ua[i]) * iucp[i];
-        yflux[i] = (yflux[i] + fluxobn[i] * va[i]) * iucp[i];
+        if (P.ghost_cells) {  // advave_edge_gcy.F
+          xflux[i] = xflux[i] + fluxobn[i] * ua[i] * iucp[i];
+          yflux[i] = yflux[i] + fluxobn[i] * va[i] * iucp[i];
+        } else {
+          xflux[i] = (xflux[i] + fluxobn[i] * ua[i]) * iucp[i];
+          yflux[i] = (yflux[i] + fluxobn[i] * va[i]) * iucp[i];
+        }
       }
     }
     if (NUMQBC > 0) {
@@ -500,9 +537,10 @@ struct Oracle {
   // BCOND_GCN(2,K) (bcond_gcn.F:325-406)
   void bcond_uv2d() {
     for (int i = 1; i <= N; ++i) {
-      if (isbce[i] == 3) { uaf[i] = 0.0; vaf[i] = 0.0; }
+      // GCY (bcond_gcy.F): river clamp only, no tangential projection, no corner zero
+      if (isbce[i] == 3 && !P.ghost_cells) { uaf[i] = 0.0; vaf[i] = 0.0; }
       if (isbce[i] == 1) {
-        if (!river_clamp(i, uaf[i], vaf[i])) tangential(i, uaf[i], vaf[i]);
+        if (!river_clamp(i, uaf[i], vaf[i]) && !P.ghost_cells) tangential(i, uaf[i], vaf[i]);
       }
     }
   }
@@ -611,9 +649,9 @@ struct Oracle {
     for (int i = 1; i <= N; ++i) {
       for (int k = 1; k <= KBM1; ++k) {
         size_t q = c3(i, k);
-        if (isbce[i] == 3) { uu[q] = 0.0; vv[q] = 0.0; }
+        if (isbce[i] == 3 && !P.ghost_cells) { uu[q] = 0.0; vv[q] = 0.0; }
         if (isbce[i] == 1) {
-          if (!river_clamp(i, uu[q], vv[q])) tangential(i, uu[q], vv[q]);
+          if (!river_clamp(i, uu[q], vv[q]) && !P.ghost_cells) tangential(i, uu[q], vv[q]);
         }
       }
     }
@@ -696,14 +734,10 @@ struct Oracle {
         double xijb = xijc[i] - xc[ib], yijb = yijc[i] - yc[ib];
         double dij = 0.5 * (dt[j1] * dz[n3(j1, k)] + dt[j2] * dz[n3(j2, k)]);
         const double *U_ = &u[c3(0, k)], *V_ = &v[c3(0, k)];
-        double cofa1 = A1U(ia, 1) * U_[ia] + A1U(ia, 2) * U_[k1] + A1U(ia, 3) * U_[k2] + A1U(ia, 4) * U_[k3];
-        double cofa2 = A2U(ia, 1) * U_[ia] + A2U(ia, 2) * U_[k1] + A2U(ia, 3) * U_[k2] + A2U(ia, 4) * U_[k3];
-        double cofa5 = A1U(ia, 1) * V_[ia] + A1U(ia, 2) * V_[k1] + A1U(ia, 3) * V_[k2] + A1U(ia, 4) * V_[k3];
-        double cofa6 = A2U(ia, 1) * V_[ia] + A2U(ia, 2) * V_[k1] + A2U(ia, 3) * V_[k2] + A2U(ia, 4) * V_[k3];
-        double cofa3 = A1U(ib, 1) * U_[ib] + A1U(ib, 2) * U_[k4] + A1U(ib, 3) * U_[k5] + A1U(ib, 4) * U_[k6];
-        double cofa4 = A2U(ib, 1) * U_[ib] + A2U(ib, 2) * U_[k4] + A2U(ib, 3) * U_[k5] + A2U(ib, 4) * U_[k6];
-        double cofa7 = A1U(ib, 1) * V_[ib] + A1U(ib, 2) * V_[k4] + A1U(ib, 3) * V_[k5] + A1U(ib, 4) * V_[k6];
-        double cofa8 = A2U(ib, 1) * V_[ib] + A2U(ib, 2) * V_[k4] + A2U(ib, 3) * V_[k5] + A2U(ib, 4) * V_[k6];
+        double cofa1, cofa2, cofa5, cofa6;
+        cofa(U_, V_, ia, cofa1, cofa2, cofa5, cofa6);
+        double cofa3, cofa4, cofa7, cofa8;
+        cofa(U_, V_, ib, cofa3, cofa4, cofa7, cofa8);
         double uij1, uij2, vij1, vij2;
         face_values(U_[ia], U_[ib], cofa1, cofa2, xija, yija, cofa3, cofa4, xijb, yijb, L ? ualfa[ia] : 1.0,
                     L ? ualfa[ib] : 1.0, uij1, uij2);
@@ -728,10 +762,17 @@ struct Oracle {
         double tpa = (double)(float)(1 - isbc[i]) * epor[ia];
         double tpb = (double)(float)(1 - isbc[i]) * epor[ib];
         double *X = &advx[c3(0, k)], *Y = &advy[c3(0, k)];
-        X[ia] = X[ia] + xadv * tpa + (fxx + 3.0 * fxx * isb) * epor[ia];
-        Y[ia] = Y[ia] + yadv * tpa + (fyy + 3.0 * fyy * isb) * epor[ia];
-        X[ib] = X[ib] - xadv * tpb - (fxx + 3.0 * fxx * isb) * epor[ib];
-        Y[ib] = Y[ib] - yadv * tpb - (fyy + 3.0 * fyy * isb) * epor[ib];
+        if (P.ghost_cells) {  // advection_edge_gcy.F: the viscous flux masked like the advective
+          X[ia] = X[ia] + xadv * tpa + fxx * tpa;
+          Y[ia] = Y[ia] + yadv * tpa + fyy * tpa;
+          X[ib] = X[ib] - xadv * tpb - fxx * tpb;
+          Y[ib] = Y[ib] - yadv * tpb - fyy * tpb;
+        } else {
+          X[ia] = X[ia] + xadv * tpa + (fxx + 3.0 * fxx * isb) * epor[ia];
+          Y[ia] = Y[ia] + yadv * tpa + (fyy + 3.0 * fyy * isb) * epor[ia];
+          X[ib] = X[ib] - xadv * tpb - (fxx + 3.0 * fxx * isb) * epor[ib];
+          Y[ib] = Y[ib] - yadv * tpb - (fyy + 3.0 * fyy * isb) * epor[ib];
+        }
       }
     }
 #pragma omp parallel for schedule(static)
@@ -1094,14 +1135,10 @@ struct Oracle {
         if (iswetct[ia] * iswetc[ia] == 1 || iswetct[ib] * iswetc[ib] == 1) {
           double xija = xijc[i] - xc[ia], yija = yijc[i] - yc[ia];
           double xijb = xijc[i] - xc[ib], yijb = yijc[i] - yc[ib];
-          double cofa1 = A1U(ia, 1) * U_[ia] + A1U(ia, 2) * U_[k1] + A1U(ia, 3) * U_[k2] + A1U(ia, 4) * U_[k3];
-          double cofa2 = A2U(ia, 1) * U_[ia] + A2U(ia, 2) * U_[k1] + A2U(ia, 3) * U_[k2] + A2U(ia, 4) * U_[k3];
-          double cofa5 = A1U(ia, 1) * V_[ia] + A1U(ia, 2) * V_[k1] + A1U(ia, 3) * V_[k2] + A1U(ia, 4) * V_[k3];
-          double cofa6 = A2U(ia, 1) * V_[ia] + A2U(ia, 2) * V_[k1] + A2U(ia, 3) * V_[k2] + A2U(ia, 4) * V_[k3];
-          double cofa3 = A1U(ib, 1) * U_[ib] + A1U(ib, 2) * U_[k4] + A1U(ib, 3) * U_[k5] + A1U(ib, 4) * U_[k6];
-          double cofa4 = A2U(ib, 1) * U_[ib] + A2U(ib, 2) * U_[k4] + A2U(ib, 3) * U_[k5] + A2U(ib, 4) * U_[k6];
-          double cofa7 = A1U(ib, 1) * V_[ib] + A1U(ib, 2) * V_[k4] + A1U(ib, 3) * V_[k5] + A1U(ib, 4) * V_[k6];
-          double cofa8 = A2U(ib, 1) * V_[ib] + A2U(ib, 2) * V_[k4] + A2U(ib, 3) * V_[k5] + A2U(ib, 4) * V_[k6];
+          double cofa1, cofa2, cofa5, cofa6;
+          cofa(U_, V_, ia, cofa1, cofa2, cofa5, cofa6);
+          double cofa3, cofa4, cofa7, cofa8;
+          cofa(U_, V_, ib, cofa3, cofa4, cofa7, cofa8);
           double uij1, uij2, vij1, vij2;
           face_values(U_[ia], U_[ib], cofa1, cofa2, xija, yija, cofa3, cofa4, xijb, yijb, L ? ualfa[ia] : 1.0,
                       L ? ualfa[ib] : 1.0, uij1, uij2);
@@ -1127,10 +1164,17 @@ struct Oracle {
           double isb = (double)isbc[i];
           double tpa = (double)(float)(1 - isbc[i]) * epor[ia];
           double tpb = (double)(float)(1 - isbc[i]) * epor[ib];
-          X[ia] = X[ia] + xadv * tpa + (fxx + 3.0 * fxx * isb) * epor[ia];
-          Y[ia] = Y[ia] + yadv * tpa + (fyy + 3.0 * fyy * isb) * epor[ia];
-          X[ib] = X[ib] - xadv * tpb - (fxx + 3.0 * fxx * isb) * epor[ib];
-          Y[ib] = Y[ib] - yadv * tpb - (fyy + 3.0 * fyy * isb) * epor[ib];
+          if (P.ghost_cells) {  // adv_uv_edge_gcy.F
+            X[ia] = X[ia] + xadv * tpa + fxx * tpa;
+            Y[ia] = Y[ia] + yadv * tpa + fyy * tpa;
+            X[ib] = X[ib] - xadv * tpb - fxx * tpb;
+            Y[ib] = Y[ib] - yadv * tpb - fyy * tpb;
+          } else {
+            X[ia] = X[ia] + xadv * tpa + (fxx + 3.0 * fxx * isb) * epor[ia];
+            Y[ia] = Y[ia] + yadv * tpa + (fyy + 3.0 * fyy * isb) * epor[ia];
+            X[ib] = X[ib] - xadv * tpb - (fxx + 3.0 * fxx * isb) * epor[ib];
+            Y[ib] = Y[ib] - yadv * tpb - (fyy + 3.0 * fyy * isb) * epor[ib];
+          }
         }
         PX[ia] = PX[ia] - grav_e[ia] * dt1[ia] * dz1[c3(ia, k)] * elij * dltyc[i];
         PY[ia] = PY[ia] + grav_e[ia] * dt1[ia] * dz1[c3(ia, k)] * elij * dltxc[i];
@@ -2116,6 +2160,7 @@ struct Oracle {
     cp(wsy, have_wind ? f->wstress_y : nullptr, n1);
     if (P.heating_on && !(P.rheat >= 0.0 && P.zeta1 > 0.0 && P.zeta2 > 0.0)) return FVG_ERR_ARG;
     if (P.limiter < 0 || P.limiter > 2) return FVG_ERR_ARG;
+    if (P.ghost_cells < 0 || P.ghost_cells > 1) return FVG_ERR_ARG;
     cp(swrad_w, P.heating_on && f ? f->swrad : nullptr, m1);
     cp(wtsurf_w, P.heating_on && f ? f->wtsurf : nullptr, m1);
     swrad.assign(m1, 0.0);

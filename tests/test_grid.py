@@ -72,3 +72,28 @@ def test_shape_coefficients_reproduce_linear_field():
         vals = np.array([u[i], u[k[0]], u[k[1]], u[k[2]]])
         assert abs(g["A1U"][i] @ vals - 2e-4) < 1e-9
         assert abs(g["A2U"][i] @ vals + 5e-5) < 1e-9
+
+
+def test_ghost_cell_coefficients():
+    """SHAPE_COEF_GCY: boundary cells get least-squares weights from their ghost points
+    (GCN leaves them zero); GCY1 and GCY2 differ only on solid-boundary cells; on interior
+    cells the weights equal GCN's except the first A2U weight, which the reference's GCY
+    routine forms with the sum of X squared in place of the sum of X*Y."""
+    import numpy as np
+    from myfvcomcode_b200 import cases
+    kw = dict(npts=1500, kb=5, lx=20000.0, ly=10000.0, seed=7)
+    g0 = cases.coastal_mesh(**kw)["grid"]
+    g1 = cases.coastal_mesh(ghost_cells="GCY1", **kw)["grid"]
+    g2 = cases.coastal_mesh(ghost_cells="GCY2", **kw)["grid"]
+    isbce = np.asarray(g0["ISBCE"])
+    solid = isbce == 1
+    obc = isbce == 2
+    interior = isbce == 0
+    interior[0] = False
+    assert solid.sum() > 10 and obc.sum() > 5
+    assert np.all(g0["A1U"][solid] == 0.0) and np.all(np.abs(g1["A1U"][solid]).sum(axis=1) > 0)
+    assert np.array_equal(g1["A1U"][interior], g0["A1U"][interior])
+    assert np.array_equal(g1["A2U"][interior][:, 1:], g0["A2U"][interior][:, 1:])
+    assert not np.array_equal(g1["A2U"][interior][:, 0], g0["A2U"][interior][:, 0])
+    assert np.array_equal(g1["A1U"][~solid & (isbce != 3)], g2["A1U"][~solid & (isbce != 3)])
+    assert not np.array_equal(g1["A1U"][solid], g2["A1U"][solid])

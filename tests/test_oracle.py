@@ -193,3 +193,23 @@ def test_z_level_pressure_gradient_on_flat_bottom():
     half_level = 0.5 * 9.81 * 1e-4 * deltz * 12.0 * g["DZ1"][1:, : g["KB"] - 1] * g["ART"][1:, None]
     assert np.abs(out["z coordinates"] - out["sigma levels"] - half_level).max() <= 1e-6 * scale
     assert np.abs(out["z coordinates uniform"]).max() <= 1e-12 * scale
+
+
+def test_ghost_cell_variants_run():
+    """GCY1 and GCY2 (ghost cells on the solid boundary) step the channel with an edge
+    river and the wet/dry coastal mesh; they differ from GCN and from each other."""
+    import numpy as np
+    from myfvcomcode_b200 import cases
+    from oracle.oracle import Oracle
+    for build, kw in ((cases.estuary_channel, dict(nx=24, ny=6, kb=6, lx=4800.0, ly=1200.0, IRAMP=10,
+                                                   river_location="edge")),
+                      (cases.coastal_mesh, dict(npts=1500, kb=7, lx=20000.0, ly=10000.0, seed=7, IRAMP=20))):
+        out = {}
+        for gc in ("GCN", "GCY1", "GCY2"):
+            o = Oracle(build(ghost_cells=gc, **kw))
+            o.run(10)
+            u = o.get("u")
+            assert np.isfinite(u).all() and np.isfinite(o.get("el")).all()
+            out[gc] = u
+        assert not np.array_equal(out["GCN"], out["GCY1"])
+        assert not np.array_equal(out["GCY1"], out["GCY2"])

@@ -264,3 +264,49 @@ def test_z_level_pressure_gradient_matches_oracle(case_name, request):
     b.run(20)
     bad = parity.compare(b, a, ["el", "ua", "va", "u", "v", "t1", "s1", "rho1"], rtol=1e-10)
     assert not bad, bad
+
+
+GCY_ROUTINES = [
+    ("BCOND_UV3D_SOLID", 0, ["u", "v"]),
+    ("ADVECTION3D", 0, ["advx", "advy"]),
+    ("INT_PRE_EXT", 0, ["adx2d", "ady2d", "drx2d", "dry2d", "advua", "advva", "pstx", "psty"]),
+    ("ADVAVE", 0, ["advua", "advva", "pstx", "psty"]),
+    ("BCOND_UV2D", 0, ["uaf", "vaf"]),
+    ("EXTERNAL_STEP", 1, ["el", "elf", "ua", "va", "d1", "uard", "egf", "fluxobn"]),
+    ("ADV_UV", 0, ["uf", "vf", "viscofm"]),
+    ("BCOND_UV3D", 0, ["uf", "vf"]),
+]
+
+
+@pytest.mark.parametrize("ghost", ["GCY1", "GCY2"])
+@pytest.mark.parametrize("case_name", ["channel_edge", "coastal"])
+def test_ghost_cells_match_oracle(case_name, ghost):
+    """GCY (ghost velocities in the gradients, the GCY flux masks, no tangential projection)
+    per routine bit for bit (EXTERNAL_STEP to 1e-13), 20 whole steps to 1e-10, and with
+    the LIMITED_1 scheme on top."""
+    from myfvcomcode_b200 import cases
+    from myfvcomcode_b200.engine import Fvcom
+    from oracle.oracle import Oracle
+    if case_name == "channel_edge":
+        base = cases.estuary_channel(nx=24, ny=6, kb=6, lx=4800.0, ly=1200.0, IRAMP=10,
+                                     river_location="edge", ghost_cells=ghost)
+    else:
+        base = cases.coastal_mesh(npts=1500, kb=7, lx=20000.0, ly=10000.0, seed=7, IRAMP=20, ghost_cells=ghost)
+    for lim in ("LIMITED_NO", "LIMITED_1"):
+        case = dict(base, params=dict(base["params"], LIMITER=lim))
+        ora, gpu = Oracle(case), Fvcom(case)
+        ora.run(4)
+        failures = {}
+        for name, arg, outs in GCY_ROUTINES:
+            parity.copy_state(ora, gpu)
+            gpu.routine(name, arg)
+            ora.routine(name, arg)
+            bad = parity.compare(gpu, ora, outs, rtol=1e-13 if name in TRANSCENDENTAL else 0.0)
+            if bad:
+                failures["%s(%d)" % (name, arg)] = bad
+        assert not failures, (lim, failures)
+        a, b = Oracle(case), Fvcom(case)
+        a.run(20)
+        b.run(20)
+        bad = parity.compare(b, a, ["el", "ua", "va", "u", "v", "t1", "s1"], rtol=1e-10)
+        assert not bad, (lim, bad)
