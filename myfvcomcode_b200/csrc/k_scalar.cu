@@ -310,10 +310,23 @@ __device__ inline R he_flux(const Dev& P, const HeCell<R>& hc, int he, int a, in
 }
 
 template <typename R>
+__device__ inline TRec<R> sel_trec(const TRec<R>& a, const TRec<R>& b, const TRec<R>& c, int j) {
+  TRec<R> r;
+  r.q = j == 0 ? a.q : (j == 1 ? b.q : c.q);
+  r.px = j == 0 ? a.px : (j == 1 ? b.px : c.px);
+  r.py = j == 0 ? a.py : (j == 1 ? b.py : c.py);
+  r.pxd = j == 0 ? a.pxd : (j == 1 ? b.pxd : c.pxd);
+  r.pyd = j == 0 ? a.pyd : (j == 1 ? b.pyd : c.pyd);
+  r.rmin = j == 0 ? a.rmin : (j == 1 ? b.rmin : c.rmin);
+  r.rmax = j == 0 ? a.rmax : (j == 1 ? b.rmax : c.rmax);
+  return r;
+}
+
+template <typename R>
 __device__ inline int pos3(const HeCell<R>& hc, int n) { return n == hc.nd[0] ? 0 : (n == hc.nd[1] ? 1 : 2); }
 
 template <typename R, int MODE>
-__global__ void __launch_bounds__(256) k_he_adv(const Dev P, int parts) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_he_adv(const Dev P, int parts) {
   typedef typename Mesh<R>::R2 R2;
   int c = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (c > P.N) return;
@@ -332,21 +345,23 @@ __global__ void __launch_bounds__(256) k_he_adv(const Dev P, int parts) {
       pb[s] = nb == nd0 ? 0 : (nb == nd1 ? 1 : 2);
     }
   }
+  // Each of the cell's three nodes ends two of its half-edges: its record is loaded once
+  // per tracer and layer and handed to both.
   for (int k = kb; k <= ke; ++k) {
     HeCell<R> hc;
     he_cell_load<R, MODE>(P, c, k, hc);
     R2* EX = Mesh<R>::ex2(P) + (size_t)(k - 1) * P.ncvs;
-    for (int s = 0; s < 3; ++s) {
-      const int na = sel3i(hc.nd, pa[s]), nb = sel3i(hc.nd, pb[s]);
-      R e0 = 0, e1 = 0;
-      if (do0)
-        e0 = he_flux<R, MODE>(P, hc, hes[s], pa[s], pb[s], load_trec<R, MODE>(P, na, k, 0),
-                              load_trec<R, MODE>(P, nb, k, 0), nullptr);
-      if (do1)
-        e1 = he_flux<R, MODE>(P, hc, hes[s], pa[s], pb[s], load_trec<R, MODE>(P, na, k, 1),
-                              load_trec<R, MODE>(P, nb, k, 1), nullptr);
-      EX[hes[s]] = mk2(e0, e1);
+    R e[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    for (int t = 0; t < 2; ++t) {
+      if (!(t == 0 ? do0 : do1)) continue;
+      const TRec<R> r0 = load_trec<R, MODE>(P, hc.nd[0], k, t);
+      const TRec<R> r1 = load_trec<R, MODE>(P, hc.nd[1], k, t);
+      const TRec<R> r2 = load_trec<R, MODE>(P, hc.nd[2], k, t);
+      for (int s = 0; s < 3; ++s)
+        e[t][s] = he_flux<R, MODE>(P, hc, hes[s], pa[s], pb[s], sel_trec(r0, r1, r2, pa[s]),
+                                   sel_trec(r0, r1, r2, pb[s]), nullptr);
     }
+    for (int s = 0; s < 3; ++s) EX[hes[s]] = mk2(e[0][s], e[1][s]);
   }
 }
 
