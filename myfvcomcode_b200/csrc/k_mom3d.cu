@@ -193,8 +193,18 @@ __global__ void __launch_bounds__(256) k_alfa3(const Dev P) {
 }
 
 // q: the edge's slot in the cell slot table (offsets and DLTXC/DLTYC of the edge).
-template <typename R, bool LIM>
-__device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib, int k, R dij, bool exflux_form) {
+// The cell's own side of its edges on one layer, loaded once for its three edges.
+template <typename R>
+struct Own3 {
+  G3<R> g;
+  R u, v, art, cc;
+};
+
+// OWN (FP32 form, no limiter): `own` holds the values of the cell on the edge's `side`
+// (0: IA, 1: IB), so that only the other cell is gathered.
+template <typename R, bool LIM, bool OWN = false>
+__device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib, int k, R dij, bool exflux_form,
+                                         const Own3<R>& own = Own3<R>(), int side = 0) {
   typedef Mesh<R> Mh;
   const R half = (R)0.5, one = (R)1.0;
   const double* U = P.u + C3(P, 0, k);
@@ -203,14 +213,42 @@ __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib,
   R xijb = Mh::s_xob(P, q), yijb = Mh::s_yob(P, q);
   G3<R> ga, gb;
   R uij1, vij1, uij2, vij2;
+  R arta, artb, cca, ccb;
   if constexpr (!LIM) {
-    ga = load_g3<R>(P, ia, k);
-    uij1 = (R)U[ia] + ga.ux * xija + ga.uy * yija;
-    vij1 = (R)V[ia] + ga.vx * xija + ga.vy * yija;
-    gb = load_g3<R>(P, ib, k);
-    uij2 = (R)U[ib] + gb.ux * xijb + gb.uy * yijb;
-    vij2 = (R)V[ib] + gb.vx * xijb + gb.vy * yijb;
+    if constexpr (OWN) {
+      const int o = side == 0 ? ib : ia;
+      const G3<R> go = load_g3<R>(P, o, k);
+      const R uo = (R)U[o], vo = (R)V[o];
+      ga = side == 0 ? own.g : go;
+      gb = side == 0 ? go : own.g;
+      const R ua = side == 0 ? own.u : uo, va = side == 0 ? own.v : vo;
+      const R ub = side == 0 ? uo : own.u, vb = side == 0 ? vo : own.v;
+      uij1 = ua + ga.ux * xija + ga.uy * yija;
+      vij1 = va + ga.vx * xija + ga.vy * yija;
+      uij2 = ub + gb.ux * xijb + gb.uy * yijb;
+      vij2 = vb + gb.vx * xijb + gb.vy * yijb;
+      const R arto = Mh::art(P, o), cco = Mh::cc_hvc(P, o);
+      arta = side == 0 ? own.art : arto;
+      artb = side == 0 ? arto : own.art;
+      cca = side == 0 ? own.cc : cco;
+      ccb = side == 0 ? cco : own.cc;
+    } else {
+      ga = load_g3<R>(P, ia, k);
+      uij1 = (R)U[ia] + ga.ux * xija + ga.uy * yija;
+      vij1 = (R)V[ia] + ga.vx * xija + ga.vy * yija;
+      gb = load_g3<R>(P, ib, k);
+      uij2 = (R)U[ib] + gb.ux * xijb + gb.uy * yijb;
+      vij2 = (R)V[ib] + gb.vx * xijb + gb.vy * yijb;
+      arta = Mh::art(P, ia);
+      artb = Mh::art(P, ib);
+      cca = Mh::cc_hvc(P, ia);
+      ccb = Mh::cc_hvc(P, ib);
+    }
   } else {
+    arta = Mh::art(P, ia);
+    artb = Mh::art(P, ib);
+    cca = Mh::cc_hvc(P, ia);
+    ccb = Mh::cc_hvc(P, ib);
     ga = load_g3<R>(P, ia, k);
     gb = load_g3<R>(P, ib, k);
     const size_t qa = C3(P, ia, k), qb = C3(P, ib, k);
@@ -221,9 +259,8 @@ __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib,
   }
   R uij = half * (uij1 + uij2);
   R vij = half * (vij1 + vij2);
-  R viscof1 = Mh::art(P, ia) * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + half * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
-  R viscof2 = Mh::art(P, ib) * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + half * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
-  const R cca = Mh::cc_hvc(P, ia), ccb = Mh::cc_hvc(P, ib);
+  R viscof1 = arta * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + half * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
+  R viscof2 = artb * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + half * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
   R viscof = ((R)P.fact * half * (viscof1 * cca + viscof2 * ccb) + (R)P.fm1 * half * (cca + ccb)) / (R)P.hprnu;
   R txx = (ga.ux + gb.ux) * viscof;
   R tyy = (ga.vy + gb.vy) * viscof;
@@ -282,6 +319,16 @@ __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
   const size_t n1 = P.N + 1;
   const R epor = (R)P.epor[i], three = (R)3.0;
   R xr = 0, yr = 0;
+    // FP32 form without a limiter: the cell's own side of its three edges, once
+    constexpr bool OWN = !LIM && sizeof(R) == 4;
+    Own3<R> own;
+    if constexpr (OWN) {
+      own.g = load_g3<R>(P, i, k);
+      own.u = (R)P.u[C3(P, i, k)];
+      own.v = (R)P.v[C3(P, i, k)];
+      own.art = Mesh<R>::art(P, i);
+      own.cc = Mesh<R>::cc_hvc(P, i);
+    }
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;
     const int code = P.ce_code[q], side = code & 1, isbc = (code >> 1) & 1;
@@ -289,7 +336,7 @@ __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
     if (!(P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1)) continue;
     const int j1 = P.ce_j1[q], j2 = P.ce_j2[q];
     R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
-    EdgeFlux<R> f = edge_flux3<R, LIM>(P, q, ia, ib, k, dij, false);
+    EdgeFlux<R> f = edge_flux3<R, LIM, OWN>(P, q, ia, ib, k, dij, false, own, side);
     R isb = (R)isbc;
     R tp = (R)((double)(float)(1 - isbc) * P.epor[i]);
     // viscous part: GCN (fxx + 3 fxx ISBC) EPOR; GCY (advection_edge_gcy.F) fxx TPA
@@ -632,6 +679,16 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
   R xr = 0, yr = 0, vmr = 0;
   const double dz1i = P.dz1[C3(P, i, k)];
   const double gdd = P.grav_e[i] * P.dt1[i] * dz1i;
+    // FP32 form without a limiter: the cell's own side of its three edges, once
+    constexpr bool OWN = !LIM && sizeof(R) == 4;
+    Own3<R> own;
+    if constexpr (OWN) {
+      own.g = load_g3<R>(P, i, k);
+      own.u = (R)P.u[C3(P, i, k)];
+      own.v = (R)P.v[C3(P, i, k)];
+      own.art = Mesh<R>::art(P, i);
+      own.cc = Mesh<R>::cc_hvc(P, i);
+    }
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;
     const int code = P.ce_code[q], side = code & 1, isbc = (code >> 1) & 1;
@@ -640,7 +697,7 @@ __global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
     double elij = 0.5 * (P.egf[j1] + P.egf[j2]);
     R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
     if (P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1) {
-      EdgeFlux<R> f = edge_flux3<R, LIM>(P, q, ia, ib, k, dij, true);
+      EdgeFlux<R> f = edge_flux3<R, LIM, OWN>(P, q, ia, ib, k, dij, true, own, side);
       vmr = vmr + f.viscof;
       R isb = (R)isbc;
       R tp = (R)((double)(float)(1 - isbc) * P.epor[i]);
