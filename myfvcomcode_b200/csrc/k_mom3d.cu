@@ -779,6 +779,29 @@ __global__ void __launch_bounds__(128) k_vdif_uv(const Dev P, int parts) {
   if (i > P.N) return;
   const int KB = P.KB, KBM1 = P.KBM1, KBM2 = P.KBM2;
   const double DTI = P.dti;
+  // With VU_BC3 in the same launch the sponge and BCOND_GCN(3,0) are applied to each
+  // solved value before it is stored (per element they follow in the reference's order),
+  // which saves two passes over UF and VF.
+  const bool fused = (parts & VU_VDIF) && (parts & VU_BC3);
+  const bool fix = P.h1[i] <= P.static_ssh_adj;
+  const int b = P.isbce[i];
+  const double sp = P.cc_sponge[i];
+  auto bc3 = [&](double& uu, double& vv) {
+    if (fix) { uu = P.ua[i]; vv = P.va[i]; }
+    if (b == 3 && !P.gcy) { uu = 0.0; vv = 0.0; }
+    if (b == 1) bc_solid3(P, i, uu, vv);
+  };
+  // the sponge of vdif_uv.F's end, then (fused) BCOND_GCN(3,0), then the store
+  auto finish = [&](int k, double uu, double vv) {
+    const size_t q = C3(P, i, k);
+    if (fused) {
+      uu = uu / (1.0 + sp * (uu * uu));
+      vv = vv / (1.0 + sp * (vv * vv));
+      bc3(uu, vv);
+    }
+    P.uf[q] = uu;
+    P.vf[q] = vv;
+  };
   if (parts & VU_VDIF) {
     if (P.iswetc[i] == 1) {
       double vhu[kMaxKB], vhpu[kMaxKB], vhv[kMaxKB], vhpv[kMaxKB];
@@ -815,43 +838,35 @@ __global__ void __launch_bounds__(128) k_vdif_uv(const Dev P, int parts) {
       double dzb = P.dz1[C3(P, i, KBM1)];
       double ufk = (cb * vhpu[KBM2] - P.uf[C3(P, i, KBM1)]) / (tps * DTI / (-dzb * d1) - 1.0 - (vhu[KBM2] - 1.0) * cb);
       double vfk = (cb * vhpv[KBM2] - P.vf[C3(P, i, KBM1)]) / (tps * DTI / (-dzb * d1) - 1.0 - (vhv[KBM2] - 1.0) * cb);
-      P.uf[C3(P, i, KBM1)] = ufk;
-      P.vf[C3(P, i, KBM1)] = vfk;
+      finish(KBM1, ufk, vfk);
       for (int k = 2; k <= KBM1; ++k) {
         int ki = KB - k;
         ufk = (vhu[ki] * ufk + vhpu[ki]);
         vfk = (vhv[ki] * vfk + vhpv[ki]);
-        P.uf[C3(P, i, ki)] = ufk;
-        P.vf[C3(P, i, ki)] = vfk;
+        finish(ki, ufk, vfk);
       }
       P.wubot[i] = -tps * ub;
       P.wvbot[i] = -tps * vb;
     } else {
-      for (int k = 2; k <= KBM1; ++k) {
-        int ki = KB - k;
-        P.uf[C3(P, i, ki)] = 0.0;
-        P.vf[C3(P, i, ki)] = 0.0;
-      }
+      for (int k = 2; k <= KBM1; ++k) finish(KB - k, 0.0, 0.0);
+      if (fused) finish(KBM1, P.uf[C3(P, i, KBM1)], P.vf[C3(P, i, KBM1)]);
       P.wubot[i] = 0.0;
       P.wvbot[i] = 0.0;
     }
-    double sp = P.cc_sponge[i];
-    for (int k = 1; k <= KBM1; ++k) {
-      size_t q = C3(P, i, k);
-      double uu = P.uf[q], vv = P.vf[q];
-      P.uf[q] = uu / (1.0 + sp * (uu * uu));
-      P.vf[q] = vv / (1.0 + sp * (vv * vv));
+    if (!fused) {
+      for (int k = 1; k <= KBM1; ++k) {
+        size_t q = C3(P, i, k);
+        double uu = P.uf[q], vv = P.vf[q];
+        P.uf[q] = uu / (1.0 + sp * (uu * uu));
+        P.vf[q] = vv / (1.0 + sp * (vv * vv));
+      }
     }
   }
-  if (parts & VU_BC3) {
-    bool fix = P.h1[i] <= P.static_ssh_adj;
-    int b = P.isbce[i];
+  if ((parts & VU_BC3) && !fused) {
     for (int k = 1; k <= KBM1; ++k) {
       size_t q = C3(P, i, k);
       double uu = P.uf[q], vv = P.vf[q];
-      if (fix) { uu = P.ua[i]; vv = P.va[i]; }
-      if (b == 3 && !P.gcy) { uu = 0.0; vv = 0.0; }
-      if (b == 1) bc_solid3(P, i, uu, vv);
+      bc3(uu, vv);
       P.uf[q] = uu;
       P.vf[q] = vv;
     }
