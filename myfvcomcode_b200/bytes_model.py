@@ -66,8 +66,10 @@ def ledger(grid, isplit, wet_dry, precision="fp64"):
                         + edge_geo + M * D, 1)
     g["baropg"] = (M * K * 2 * D + N * KB * 2 * D + N * K * 7 * D + N * 10 * D + M * 3 * D, 1)
     g["int_advave"] = (N * (cell_lsq // N + 16 * D + 4 * X) + edge_geo + pg_extra + M * 3 * D, 1)
-    g["adjust2"] = (N * K * 5 * D + N * 6 * D, 1)
-    g["vertvl_flux"] = (N * K * 3 * D + M * K * D + halfedge_csr + NCV * (I + 2 * D) + N * D, 1)
+    # ADJUST2D3D(2) also writes VERTVL_EDGE's half-edge fluxes (CELL_HE, DLTXE/YE read
+    # once per cell); the node kernel sums them in half-edge order.
+    g["adjust2"] = (N * K * 5 * D + N * 6 * D + NCV * K * D + NCV * (I + 2 * D), 1)
+    g["vertvl_flux"] = (NCV * K * D + M * K * D + halfedge_csr, 1)
     g["vertvl_col"] = (M * K * 2 * D + M * KB * D + M * K * 2 * D + M * 10 * D + I * ntve + N * 2 * D, 1)
     g["w_viscofh"] = (M * KB * D + N * KB * D + N * K * 2 * D + M * K * D + M * 3 * D
                       + ntve * (I + 4 * D) + N * I, 1)

@@ -226,7 +226,7 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   }
   launch_ext_finish(P, s, 4, p.wetting_drying_on);
   mk.mark(s, G_EXT_UPD);
-  launch_adjust2(P, s);
+  launch_adjust2(P, s, AJ_ADJUST | AJ_HE_FLUX);
   mk.mark(s, G_ADJ2);
   launch_vertvl_flux(P, s);
   mk.mark(s, G_VV_FLUX);
@@ -427,6 +427,14 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
     std::vector<int> ptr, ent;
     build_csr(nl, ptr, ent);
     UPI(node_he_ptr, ptr.data(), ptr.size()); UPI(node_he, ent.data(), ent.size());
+    {
+      size_t w = 0;
+      for (auto& l : nl) w = std::max(w, l.size());
+      std::vector<int> ell(std::max<size_t>(w, 1) * ms, 0);
+      for (size_t i = 0; i < m1; ++i)
+        for (size_t j = 0; j < nl[i].size(); ++j) ell[j * ms + i] = nl[i][j];
+      UPI(node_he_ell, ell.data(), ell.size());
+    }
     std::vector<int> ce(3 * n1, 0);
     for (size_t i = 1; i < n1; ++i) {
       if (cl[i].size() != 3) { h->err = "cell without exactly three edges"; return fail(FVG_ERR_BOUNDS); }
@@ -654,6 +662,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   for (int q = 0; q < 4; ++q)
     if ((rc = dalloc(h, &P.g3[q], ns * KB))) return fail(rc);
   if ((rc = dalloc(h, (double**)&P.ex2, (size_t)P.ncvs * KB * 2))) return fail(rc);
+  P.he_vflux = (double*)P.ex2;
 
   // ---- schedule ----
   h->sched_cap = 256;
@@ -1162,7 +1171,7 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
       break;
     case FVG_R_ADJUST2D3D:
       if (arg == 1) launch_cell_pre(P, s, CP_ADJUST1);
-      else launch_adjust2(P, s);
+      else launch_adjust2(P, s, AJ_ADJUST);
       break;
     case FVG_R_BCOND_UV3D_SOLID: launch_cell_pre(P, s, CP_BC5); break;
     case FVG_R_BROUGH:
@@ -1189,6 +1198,7 @@ int fvg_run_routine(fvg_handle* h, int32_t r, int32_t arg) {
       launch_int_reset(P, s);
       break;
     case FVG_R_VERTVL:
+      launch_adjust2(P, s, AJ_HE_FLUX);
       launch_vertvl_flux(P, s);
       launch_vertvl_col(P, s, VC_WTS);
       launch_w_viscofh(P, s, 1, 0);

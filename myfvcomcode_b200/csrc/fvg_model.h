@@ -102,6 +102,9 @@ struct Dev {
   const double *dltxe, *dltye, *dltxncve, *dltyncve;
   // ----- gather lists -----
   const int *node_he_ptr, *node_he;   // node -> half-edges (id*2 + side), ascending id
+  // The same lists transposed: entry j of node i at j*ms + i, so that the threads of
+  // consecutive nodes read entry j in one coalesced load (count = ptr[i+1] - ptr[i]).
+  const int* node_he_ell;
   const int *cell_edge;               // cell -> its 3 edges (id*2 + side), ascending id
   // Slot table of the cell edge loops, slot s of cell i at s*(N+1) + i (edges in the order
   // of cell_edge): code = edge*4 + ISBC*2 + side, the two cells, the two nodes, the edge
@@ -154,6 +157,9 @@ struct Dev {
   // VDIF_Q between its passes: PROD, GH, DTEF, the q2l DTEF (node 3-D) and UTAU2 (node)
   double *vq_prod, *vq_gh, *vq_dtef, *vq_dtefl, *vq_ut;
   double2* ex2;                              // half-edge fluxes of both advected tracers (ncvs x KB)
+  // VERTVL_EDGE's EXFLUX of each half-edge and layer (KBM1 x ncvs); it lives in the
+  // allocation of ex2, which is free between ADJUST2D3D and the next advection.
+  double* he_vflux;
   double* g2d[4];                            // least-squares gradient of UA, VA per cell (COFA1/2/5/6)
   // Slope limiters of the limited schemes, UALFA and VALFA: per cell of the 2-D mode
   // (N+1) and per cell and layer of the 3-D mode (ns x KB); index 0 holds 1.
@@ -358,7 +364,9 @@ void launch_advection3d(const Dev& P, cudaStream_t s);
 void launch_baropg(const Dev& P, cudaStream_t s, int do_baropg, int do_sums);
 void launch_phy_baropg(const Dev& P, cudaStream_t s);
 void launch_int_reset(const Dev& P, cudaStream_t s);
-void launch_adjust2(const Dev& P, cudaStream_t s);
+// ADJUST2D3D(2) (AJ_ADJUST) and the half-edge fluxes of VERTVL_EDGE (AJ_HE_FLUX)
+enum Adjust2Parts { AJ_ADJUST = 1, AJ_HE_FLUX = 2 };
+void launch_adjust2(const Dev& P, cudaStream_t s, int parts);
 void launch_vertvl_flux(const Dev& P, cudaStream_t s);
 enum VertvlColParts { VC_WTS = 1, VC_WD2 = 2, VC_RHO_ROUNDTRIP = 4, VC_BOT_NODE = 8 };
 void launch_vertvl_col(const Dev& P, cudaStream_t s, int parts);

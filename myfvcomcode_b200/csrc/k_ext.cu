@@ -173,8 +173,9 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   if (parts & EN_FINISH_PREV) ext_update_node(P, i, (parts >> 8) & 7);
   double x = 0.0;
   if (parts & EN_EXTEL) {
-    for (int q = P.node_he_ptr[i]; q < P.node_he_ptr[i + 1]; ++q) {
-      int e = P.node_he[q];
+    const int n = P.node_he_ptr[i + 1] - P.node_he_ptr[i];
+    for (int j = 0; j < n; ++j) {
+      int e = P.node_he_ell[(size_t)j * P.ms + i];
       double exflux = P.exf2d[e >> 1];
       x = (e & 1) ? x + exflux : x - exflux;
     }

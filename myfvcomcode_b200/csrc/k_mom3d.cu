@@ -470,29 +470,62 @@ __global__ void k_int_reset(const Dev P) {
   if (i >= 1 && i <= P.iobcn) P.uard_obcn[i] = 0.0;
 }
 
-// ADJUST2D3D(2) (adjust2d3d.F:65-92), one thread per cell column.
-__global__ void k_adjust2(const Dev P) {
+// ADJUST2D3D(2) (adjust2d3d.F:65-92), one thread per cell column (AJ_ADJUST), and the
+// EXFLUX of VERTVL_EDGE (vertvl_edge.F:68-90) for the cell's three half-edges and every
+// layer from the adjusted U, V (AJ_HE_FLUX): DT1*DZ1*(-U*DLTYE + V*DLTXE) into he_vflux,
+// which the node kernel sums in half-edge order.
+__global__ void k_adjust2(const Dev P, int parts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i > P.N) return;
-  double ud = P.uard[i] / (double)(float)P.isplit;
-  double vd = P.vard[i] / (double)(float)P.isplit;
-  P.uard[i] = ud;
-  P.vard[i] = vd;
-  if (i == 0) return;
-  if (P.iswetct[i] * P.iswetc[i] != 1) return;
-  double ut = 0.0, vt = 0.0;
-  for (int k = 1; k <= P.KBM1; ++k) {
-    size_t q = C3(P, i, k);
-    ut = ut + P.u[q] * P.dz1[q];
-    vt = vt + P.v[q] * P.dz1[q];
+  const bool adj = parts & AJ_ADJUST;
+  double ud = 0.0, vd = 0.0;
+  if (adj) {
+    ud = P.uard[i] / (double)(float)P.isplit;
+    vd = P.vard[i] / (double)(float)P.isplit;
+    P.uard[i] = ud;
+    P.vard[i] = vd;
   }
-  double dt1 = P.dt1[i];
-  ut = ut * dt1;
-  vt = vt * dt1;
+  if (i == 0) return;
+  const bool wet = adj && P.iswetct[i] * P.iswetc[i] == 1;
+  const double dt1 = P.dt1[i];
+  double ut = 0.0, vt = 0.0;
+  if (wet) {
+    for (int k = 1; k <= P.KBM1; ++k) {
+      size_t q = C3(P, i, k);
+      ut = ut + P.u[q] * P.dz1[q];
+      vt = vt + P.v[q] * P.dz1[q];
+    }
+    ut = ut * dt1;
+    vt = vt * dt1;
+  }
+  if (!(parts & AJ_HE_FLUX)) {
+    if (!wet) return;
+    for (int k = 1; k <= P.KBM1; ++k) {
+      size_t q = C3(P, i, k);
+      P.u[q] = P.u[q] - (ut - ud) / dt1;
+      P.v[q] = P.v[q] - (vt - vd) / dt1;
+    }
+    return;
+  }
+  int he[3];
+  double dy[3], dx[3];
+  for (int s = 0; s < 3; ++s) {
+    he[s] = P.cell_he[3 * i + s];
+    dy[s] = P.dltye[he[s]];
+    dx[s] = P.dltxe[he[s]];
+  }
   for (int k = 1; k <= P.KBM1; ++k) {
     size_t q = C3(P, i, k);
-    P.u[q] = P.u[q] - (ut - ud) / dt1;
-    P.v[q] = P.v[q] - (vt - vd) / dt1;
+    double uu = P.u[q], vv = P.v[q];
+    if (wet) {
+      uu = uu - (ut - ud) / dt1;
+      vv = vv - (vt - vd) / dt1;
+      P.u[q] = uu;
+      P.v[q] = vv;
+    }
+    const double dij = dt1 * P.dz1[q];
+    double* F = P.he_vflux + (size_t)(k - 1) * P.ncvs;
+    for (int s = 0; s < 3; ++s) F[he[s]] = dij * (-uu * dy[s] + vv * dx[s]);
   }
 }
 
@@ -501,31 +534,30 @@ __global__ void k_adjust2(const Dev P) {
 // node's half-edges in ascending order.  Result in the scratch field.
 // -------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_vertvl_flux(const Dev P) {
-  // One thread per (node, layer): the half-edge chain of the 8 layer threads of a node
-  // resolves in parallel, which suits this short gather better than a layer loop.
+  // One thread per (node, layer); the 8 layer threads of a node share its list entries
+  // in L1, and the entries of 32 consecutive nodes arrive in one load.
   int i = blockIdx.x * 32 + threadIdx.x + 1;
   int k = blockIdx.y * 8 + threadIdx.y + 1;
   if (i > P.M || k > P.KBM1) return;
   {
   double x = 0.0;
   if (P.isonb[i] != 2) {
-    // EXFLUX of one half-edge; the entries are fetched two at a time and added in order
-    auto flux = [&](int he) {
-      const int c = P.ntrg[he];
-      const double dij = P.dt1[c] * P.dz1[C3(P, c, k)];
-      return dij * (-P.u[C3(P, c, k)] * P.dltye[he] + P.v[C3(P, c, k)] * P.dltxe[he]);
-    };
-    const int q1 = P.node_he_ptr[i + 1];
-    int q = P.node_he_ptr[i];
-    for (; q + 2 <= q1; q += 2) {
-      const int e0 = P.node_he[q], e1 = P.node_he[q + 1];
-      const double f0 = flux(e0 >> 1), f1 = flux(e1 >> 1);
+    const double* F = P.he_vflux + (size_t)(k - 1) * P.ncvs;
+    const int* L = P.node_he_ell + i;
+    const size_t ms = P.ms;
+    const int n = P.node_he_ptr[i + 1] - P.node_he_ptr[i];
+    int j = 0;
+    for (; j + 4 <= n; j += 4) {
+      const int e0 = L[j * ms], e1 = L[(j + 1) * ms], e2 = L[(j + 2) * ms], e3 = L[(j + 3) * ms];
+      const double f0 = F[e0 >> 1], f1 = F[e1 >> 1], f2 = F[e2 >> 1], f3 = F[e3 >> 1];
       x = (e0 & 1) ? x + f0 : x - f0;
       x = (e1 & 1) ? x + f1 : x - f1;
+      x = (e2 & 1) ? x + f2 : x - f2;
+      x = (e3 & 1) ? x + f3 : x - f3;
     }
-    for (; q < q1; ++q) {
-      const int e = P.node_he[q];
-      const double f = flux(e >> 1);
+    for (; j < n; ++j) {
+      const int e = L[j * ms];
+      const double f = F[e >> 1];
       x = (e & 1) ? x + f : x - f;
     }
   }
@@ -1058,7 +1090,7 @@ void launch_int_reset(const Dev& P, cudaStream_t s) {
   int n = (P.M > P.N ? P.M : P.N) + 1;
   k_int_reset<<<nblk(n, 256), 256, 0, s>>>(P);
 }
-void launch_adjust2(const Dev& P, cudaStream_t s) { k_adjust2<<<nblk(P.N + 1, 128), 128, 0, s>>>(P); }
+void launch_adjust2(const Dev& P, cudaStream_t s, int parts) { k_adjust2<<<nblk(P.N + 1, 128), 128, 0, s>>>(P, parts); }
 void launch_vertvl_flux(const Dev& P, cudaStream_t s) {
   k_vertvl_flux<<<dim3(nblk(P.M, 32), nblk(P.KBM1, 8)), dim3(32, 8), 0, s>>>(P);
 }
