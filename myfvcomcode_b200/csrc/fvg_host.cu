@@ -487,6 +487,23 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
       }
     }
     UPI(cell_he, chv.data(), chv.size());
+    // VERTVL_EDGE's node lists over the (slot, cell) positions of the half-edge fluxes:
+    // entry j of node i at j*ms + i, code = (slot*ns + cell)*2 + side, ascending half-edge id
+    std::vector<int> slot(v1, 0);
+    for (size_t i = 1; i < n1; ++i)
+      for (int s2 = 0; s2 < 3; ++s2) slot[chv[3 * i + s2]] = s2;
+    std::vector<std::vector<int>> vl(m1);
+    for (int he = 1; he <= m->ncv; ++he) {
+      const long pos = (long)slot[he] * (long)ns + m->ntrg[he];
+      vl[m->niec[he]].push_back((int)(pos * 2 + 0));
+      vl[m->niec[v1 + he]].push_back((int)(pos * 2 + 1));
+    }
+    size_t w = 1;
+    for (auto& l : vl) w = std::max(w, l.size());
+    std::vector<int> ell(w * ms, 0);
+    for (size_t i = 0; i < m1; ++i)
+      for (size_t j = 0; j < vl[i].size(); ++j) ell[j * ms + i] = vl[i][j];
+    UPI(node_vpos_ell, ell.data(), ell.size());
   }
   // open boundary
   {
@@ -661,7 +678,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   if ((rc = dalloc(h, &P.exf2d, v1))) return fail(rc);
   for (int q = 0; q < 4; ++q)
     if ((rc = dalloc(h, &P.g3[q], ns * KB))) return fail(rc);
-  if ((rc = dalloc(h, (double**)&P.ex2, (size_t)P.ncvs * KB * 2))) return fail(rc);
+  if ((rc = dalloc(h, (double**)&P.ex2, std::max((size_t)P.ncvs * KB * 2, 3 * ns * KB)))) return fail(rc);
   P.he_vflux = (double*)P.ex2;
 
   // ---- schedule ----

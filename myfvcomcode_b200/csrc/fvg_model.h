@@ -105,6 +105,9 @@ struct Dev {
   // The same lists transposed: entry j of node i at j*ms + i, so that the threads of
   // consecutive nodes read entry j in one coalesced load (count = ptr[i+1] - ptr[i]).
   const int* node_he_ell;
+  // VERTVL_EDGE's node lists, transposed the same way: code = (slot*ns + cell)*2 + side,
+  // the position of the half-edge flux in he_vflux, in ascending half-edge id.
+  const int* node_vpos_ell;
   const int *cell_edge;               // cell -> its 3 edges (id*2 + side), ascending id
   // Slot table of the cell edge loops, slot s of cell i at s*(N+1) + i (edges in the order
   // of cell_edge): code = edge*4 + ISBC*2 + side, the two cells, the two nodes, the edge
@@ -157,8 +160,9 @@ struct Dev {
   // VDIF_Q between its passes: PROD, GH, DTEF, the q2l DTEF (node 3-D) and UTAU2 (node)
   double *vq_prod, *vq_gh, *vq_dtef, *vq_dtefl, *vq_ut;
   double2* ex2;                              // half-edge fluxes of both advected tracers (ncvs x KB)
-  // VERTVL_EDGE's EXFLUX of each half-edge and layer (KBM1 x ncvs); it lives in the
-  // allocation of ex2, which is free between ADJUST2D3D and the next advection.
+  // VERTVL_EDGE's EXFLUX of each half-edge and layer, at (k-1)*3*ns + slot*ns + cell for
+  // the cell's half-edge in slot `slot` of cell_he; it lives in the allocation of ex2,
+  // which is free between ADJUST2D3D and the next advection.
   double* he_vflux;
   double* g2d[4];                            // least-squares gradient of UA, VA per cell (COFA1/2/5/6)
   // Slope limiters of the limited schemes, UALFA and VALFA: per cell of the 2-D mode

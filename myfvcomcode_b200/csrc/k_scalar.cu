@@ -390,9 +390,11 @@ __device__ inline double obc_xflux_adv(const Dev& P, int i, int k, int t) {
 // half-edge order (the order of the reference's scatter into XFLUX).
 // The loads are issued four entries at a time (codes, then fluxes) and added in order.
 template <typename R>
-__device__ inline double2 gather_he(const Dev& P, int q0, int q1, int k) {
+__device__ inline double2 gather_he(const Dev& P, int i, int n, int k) {
   typedef typename Mesh<R>::R2 R2;
   const R2* EX = Mesh<R>::ex2(P) + (size_t)(k - 1) * P.ncvs;
+  const int* L = P.node_he_ell + i;
+  const size_t ms = P.ms;
   R x0 = 0, x1 = 0;
   auto add = [&](int code, R2 e) {
     if (code & 1) {
@@ -403,17 +405,17 @@ __device__ inline double2 gather_he(const Dev& P, int q0, int q1, int k) {
       x1 = x1 + e.y;
     }
   };
-  int q = q0;
-  for (; q + 4 <= q1; q += 4) {
-    const int c0 = P.node_he[q], c1 = P.node_he[q + 1], c2 = P.node_he[q + 2], c3 = P.node_he[q + 3];
+  int j = 0;
+  for (; j + 4 <= n; j += 4) {
+    const int c0 = L[j * ms], c1 = L[(j + 1) * ms], c2 = L[(j + 2) * ms], c3 = L[(j + 3) * ms];
     const R2 e0 = EX[c0 >> 1], e1 = EX[c1 >> 1], e2 = EX[c2 >> 1], e3 = EX[c3 >> 1];
     add(c0, e0);
     add(c1, e1);
     add(c2, e2);
     add(c3, e3);
   }
-  for (; q < q1; ++q) {
-    const int c = P.node_he[q];
+  for (; j < n; ++j) {
+    const int c = L[j * ms];
     add(c, EX[c >> 1]);
   }
   return make_double2((double)x0, (double)x1);
@@ -427,9 +429,9 @@ __global__ void __launch_bounds__(256) k_gather_q(const Dev P, int parts) {
   int kb, ke;
   col_range(P, 2, P.KBM1, kb, ke);
   const bool wet = P.iswetn[i] * P.iswetnt[i] == 1;
-  const int q0 = P.node_he_ptr[i], q1 = P.node_he_ptr[i + 1];
+  const int nhe = P.node_he_ptr[i + 1] - P.node_he_ptr[i];
   for (int k = kb; k <= ke; ++k) {
-  const double2 xs = gather_he<R>(P, q0, q1, k);
+  const double2 xs = gather_he<R>(P, i, nhe, k);
   for (int t = 0; t < 2; ++t) {
     if (!(parts & (t == 0 ? AD_Q2 : AD_Q2L))) continue;
     const double* Q = (t == 0 ? P.q2 : P.q2l);
@@ -531,6 +533,9 @@ __device__ inline void vq_stress(const Dev& P, int i, double& utau2, double& wub
   wvb = wvb / fn;
 }
 
+// AUX: the learned closure's inputs or the closure samples are written (P.closure or
+// P.clos_samp); without them the kernel is instantiated without those paths.
+template <bool AUX>
 __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
   using namespace vq;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -549,7 +554,7 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
   const double l0 = SURFL * utau2 / P.grav_n[i];
   if (kb == 1) P.vq_ut[i] = utau2;
   if (ke == KB) P.q2f[n3(KB)] = sqrt(wub * wub + wvb * wvb) * P.const1;
-  float* const cs = P.clos_samp;
+  float* const cs = AUX ? P.clos_samp : nullptr;
   const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
   auto samp = [&](int f, int k, double v) { cs[(size_t)f * ss + (size_t)(k - 2) * P.M + (i - 1)] = (float)v; };
   // ring means of U, V on the level above the first interior level of the chunk
@@ -587,13 +592,13 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
         ring_mean(k, uk, vk);
         const double den = P.dzz[n3(k - 1)] * d;
         const double shear2 = ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den);
-        if (P.closure) {
+        if (AUX && P.closure) {
           const float fv[CLOS_IN] = {(float)boygr, (float)shear2, (float)d, (float)P.z[q], (float)sqrt(utau2),
                                      (float)sqrt(sqrt(wub * wub + wvb * wvb)), (float)q2, (float)q2l};
           const size_t r = (size_t)(k - 2) * P.M + (i - 1);
           for (int f = 0; f < CLOS_IN; ++f) P.clos_feat[(size_t)f * ss + r] = fv[f];
         }
-        if (cs) {
+        if (AUX && cs) {
           samp(0, k, boygr);
           samp(1, k, shear2);
           samp(2, k, d);
@@ -638,7 +643,9 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
 }
 
 // The q2 and q2l tridiagonal sweeps of one column (vdif_q.F:372-431), and the column's
-// envelope flag of the learned closure.
+// envelope flag of the learned closure.  The two sweeps are independent: blockIdx.y = 0
+// runs the q2 sweep, 1 the q2l sweep.  The forward elimination loads the coefficients of
+// four levels before it runs their (serial) recurrence.
 __global__ void __launch_bounds__(128) k_vdif_q_sweep(const Dev P) {
   using namespace vq;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -647,8 +654,9 @@ __global__ void __launch_bounds__(128) k_vdif_q_sweep(const Dev P) {
   const double DTI = P.dti;
   const double d = P.d[i];
   const bool wet = P.iswetn[i] == 1;
+  const bool q2l = blockIdx.y == 1;
   auto n3 = [&](int k) { return N3(P, i, k); };
-  if (P.closure) {
+  if (P.closure && !q2l) {
     bool in_env = wet;
     const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
     for (int k = 2; k <= KBM1 && in_env; ++k) {
@@ -662,42 +670,49 @@ __global__ void __launch_bounds__(128) k_vdif_q_sweep(const Dev P) {
   }
   if (!wet) return;
   double vh[kMaxKBs], vhp[kMaxKBs];
-  auto Acoef = [&](int k) {
-    return -0.5 * DTI * (P.kq[n3(k + 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k)] * d * d);
-  };
-  auto Ccoef = [&](int k) {
-    return -0.5 * DTI * (P.kq[n3(k - 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k - 1)] * d * d);
-  };
-  double* Q2F = P.q2f;
-  double* Q2LF = P.q2lf;
   vh[1] = 0.0;
-  vhp[1] = P.vhp1c * P.vq_ut[i];
-  for (int k = 2; k <= KBM1; ++k) {
-    const double a = Acoef(k), c = Ccoef(k);
-    const double p = 1. / (a + c * (1. - vh[k - 1]) - (2. * DTI * P.vq_dtef[n3(k)] + 1.));
+  vhp[1] = q2l ? 0.0 : P.vhp1c * P.vq_ut[i];
+  double* QF = q2l ? P.q2lf : P.q2f;
+  // the coefficients of level k: A, C, the diagonal term and the source of the equation
+  auto coef = [&](int k, double& a, double& c, double& e, double& r, double& qf) {
+    a = -0.5 * DTI * (P.kq[n3(k + 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k)] * d * d);
+    c = -0.5 * DTI * (P.kq[n3(k - 1)] + P.kq[n3(k)] + 2.0 * P.umol) / (P.dzz[n3(k - 1)] * P.dz[n3(k - 1)] * d * d);
+    if (q2l) {
+      e = DTI * P.vq_dtefl[n3(k)] + 1.;
+      r = DTI * (-P.vq_prod[n3(k)] * P.l[n3(k)] * E1);
+    } else {
+      e = 2. * DTI * P.vq_dtef[n3(k)] + 1.;
+      r = -2. * DTI * P.vq_prod[n3(k)];
+    }
+    qf = QF[n3(k)];
+  };
+  auto step = [&](int k, double a, double c, double e, double r, double qf) {
+    const double p = 1. / (a + c * (1. - vh[k - 1]) - e);
     vh[k] = a * p;
-    vhp[k] = (-2. * DTI * P.vq_prod[n3(k)] + c * vhp[k - 1] - Q2F[n3(k)]) * p;
+    vhp[k] = (r + c * vhp[k - 1] - qf) * p;
+  };
+  int k = 2;
+  for (; k + 3 <= KBM1; k += 4) {
+    double a[4], c[4], e[4], r[4], qf[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) coef(k + u, a[u], c[u], e[u], r[u], qf[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) step(k + u, a[u], c[u], e[u], r[u], qf[u]);
+  }
+  for (; k <= KBM1; ++k) {
+    double a, c, e, r, qf;
+    coef(k, a, c, e, r, qf);
+    step(k, a, c, e, r, qf);
   }
   for (int k = 1; k <= KBM1; ++k) {
     int ki = KB - k;
-    Q2F[n3(ki)] = vh[ki] * Q2F[n3(ki + 1)] + vhp[ki];
-  }
-  vh[1] = 0.0;
-  vhp[1] = 0.0;
-  for (int k = 2; k <= KBM1; ++k) {
-    const double a = Acoef(k), c = Ccoef(k);
-    const double p = 1. / (a + c * (1. - vh[k - 1]) - (DTI * P.vq_dtefl[n3(k)] + 1.));
-    vh[k] = a * p;
-    vhp[k] = (DTI * (-P.vq_prod[n3(k)] * P.l[n3(k)] * E1) + c * vhp[k - 1] - Q2LF[n3(k)]) * p;
-  }
-  for (int k = 1; k <= KBM1; ++k) {
-    int ki = KB - k;
-    Q2LF[n3(ki)] = vh[ki] * Q2LF[n3(ki + 1)] + vhp[ki];
+    QF[n3(ki)] = vh[ki] * QF[n3(ki + 1)] + vhp[ki];
   }
 }
 
 // Positivity of the new Q2F/Q2LF, the stability functions and KQ, KM, KH
 // (vdif_q.F:443-491), per (node, level); then Q2 = Q2F, Q2L = Q2LF.
+template <bool AUX>
 __global__ void __launch_bounds__(256) k_vdif_q_coef(const Dev P, int copy_back) {
   using namespace vq;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -708,7 +723,7 @@ __global__ void __launch_bounds__(256) k_vdif_q_coef(const Dev P, int copy_back)
   const double COEF4 = 18.0 * A1 * A1 + 9.0 * A1 * A2;
   const double COEF5 = 9.0 * A1 * A2;
   const bool wet = P.iswetn[i] == 1;
-  float* const cs = P.clos_samp;
+  float* const cs = AUX ? P.clos_samp : nullptr;
   const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
   auto samp = [&](int f, int k, double v) { cs[(size_t)f * ss + (size_t)(k - 2) * P.M + (i - 1)] = (float)v; };
   for (int k = kb; k <= ke; ++k) {
@@ -729,13 +744,13 @@ __global__ void __launch_bounds__(256) k_vdif_q_coef(const Dev P, int copy_back)
     double kn = P.l[q] * sqrt(P.q2[q]);
     bool interior_by_network = false;
     if (k >= 2 && k <= KBM1) {
-      if (cs) {
+      if (AUX && cs) {
         samp(8, k, kn * KAPPA * sm);
         samp(9, k, kn * sm);
         samp(10, k, kn * sh * P.vprnu);
         samp(11, k, wet ? 1.0 : 0.0);
       }
-      if (P.closure) {
+      if (AUX && P.closure) {
         // interior levels are finished by the network kernel (k_closure_mlp)
         const size_t r = (size_t)(k - 2) * P.M + (i - 1);
         P.clos_plain[r] = kn * KAPPA * sm;
@@ -784,9 +799,9 @@ __global__ void __launch_bounds__(256) k_gather_ts(const Dev P, int parts) {
   col_range(P, 1, P.KBM1, kb, ke);
   const bool wet = P.iswetn[i] * P.iswetnt[i] == 1;
   const int ob = P.node_obc[i];
-  const int q0 = P.node_he_ptr[i], q1 = P.node_he_ptr[i + 1];
+  const int nhe = P.node_he_ptr[i + 1] - P.node_he_ptr[i];
   for (int k = kb; k <= ke; ++k) {
-  const double2 xs = gather_he<R>(P, q0, q1, k);
+  const double2 xs = gather_he<R>(P, i, nhe, k);
   for (int t = 0; t < 2; ++t) {
     if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
     const double* F1 = (t == 0 ? P.t1 : P.s1);
@@ -1137,9 +1152,10 @@ void launch_fct_q(const Dev& P, cudaStream_t s, int parts) {
   k_fct_q<<<g, b, 0, s>>>(P, parts);
 }
 void launch_vdif_q(const Dev& P, cudaStream_t s, int copy_back) {
-  k_vdif_q_levels<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P);
-  k_vdif_q_sweep<<<nblk(P.M, 128), 128, 0, s>>>(P);
-  k_vdif_q_coef<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P, copy_back);
+  const bool aux = P.closure || P.clos_samp;
+  (aux ? k_vdif_q_levels<true> : k_vdif_q_levels<false>)<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P);
+  k_vdif_q_sweep<<<dim3(nblk(P.M, 128), 2), 128, 0, s>>>(P);
+  (aux ? k_vdif_q_coef<true> : k_vdif_q_coef<false>)<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P, copy_back);
   if (!P.closure) launch_vdif_q_shallow(P, s);
 }
 void launch_turb_update(const Dev& P, cudaStream_t s) {
