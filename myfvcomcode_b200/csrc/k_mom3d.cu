@@ -507,12 +507,11 @@ __global__ void k_adjust2(const Dev P, int parts) {
     }
     return;
   }
-  int he[3];
   double dy[3], dx[3];
   for (int s = 0; s < 3; ++s) {
-    he[s] = P.cell_he[3 * i + s];
-    dy[s] = P.dltye[he[s]];
-    dx[s] = P.dltxe[he[s]];
+    const int he = P.cell_he[3 * i + s];
+    dy[s] = P.dltye[he];
+    dx[s] = P.dltxe[he];
   }
   for (int k = 1; k <= P.KBM1; ++k) {
     size_t q = C3(P, i, k);
@@ -524,8 +523,8 @@ __global__ void k_adjust2(const Dev P, int parts) {
       P.v[q] = vv;
     }
     const double dij = dt1 * P.dz1[q];
-    double* F = P.he_vflux + (size_t)(k - 1) * P.ncvs;
-    for (int s = 0; s < 3; ++s) F[he[s]] = dij * (-uu * dy[s] + vv * dx[s]);
+    double* F = P.he_vflux + (size_t)(k - 1) * 3 * P.ns + i;
+    for (int s = 0; s < 3; ++s) F[(size_t)s * P.ns] = dij * (-uu * dy[s] + vv * dx[s]);
   }
 }
 
@@ -542,8 +541,8 @@ __global__ void __launch_bounds__(256) k_vertvl_flux(const Dev P) {
   {
   double x = 0.0;
   if (P.isonb[i] != 2) {
-    const double* F = P.he_vflux + (size_t)(k - 1) * P.ncvs;
-    const int* L = P.node_he_ell + i;
+    const double* F = P.he_vflux + (size_t)(k - 1) * 3 * P.ns;
+    const int* L = P.node_vpos_ell + i;
     const size_t ms = P.ms;
     const int n = P.node_he_ptr[i + 1] - P.node_he_ptr[i];
     int j = 0;
@@ -699,7 +698,7 @@ __global__ void __launch_bounds__(256) k_w_viscofh(const Dev P, int do_w, int do
 // pressure gradient, Coriolis, river momentum and the explicit update to UF/VF.
 // -------------------------------------------------------------------------------------
 template <typename R, bool LIM>
-__global__ void __launch_bounds__(256) k_adv_uv(const Dev P) {
+__global__ void __launch_bounds__(256, (sizeof(R) == 4 && !LIM) ? 4 : 1) k_adv_uv(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
   int kb, ke;
@@ -854,15 +853,29 @@ __global__ void __launch_bounds__(128) k_vdif_uv(const Dev P, int parts) {
       vhv[1] = a1 / (a1 - 1.0);
       vhpu[1] = (-DTI * wus * tmp / (-P.dz1[C3(P, i, 1)] * d1) - P.uf[C3(P, i, 1)]) / (a1 - 1.0);
       vhpv[1] = (-DTI * wvs * tmp / (-P.dz1[C3(P, i, 1)] * d1) - P.vf[C3(P, i, 1)]) / (a1 - 1.0);
-      for (int k = 2; k <= KBM2; ++k) {
-        double ak = Acoef(k), ck = Ccoef(k);
+      // the forward elimination; the loads of four levels are issued before their steps
+      auto step = [&](int k, double ak, double ck, double uk, double vk) {
         double pu = 1.0 / (ak + ck * (1.0 - vhu[k - 1]) - 1.0);
         double pv = 1.0 / (ak + ck * (1.0 - vhv[k - 1]) - 1.0);
         vhu[k] = ak * pu;
         vhv[k] = ak * pv;
-        vhpu[k] = (ck * vhpu[k - 1] - P.uf[C3(P, i, k)]) * pu;
-        vhpv[k] = (ck * vhpv[k - 1] - P.vf[C3(P, i, k)]) * pv;
+        vhpu[k] = (ck * vhpu[k - 1] - uk) * pu;
+        vhpv[k] = (ck * vhpv[k - 1] - vk) * pv;
+      };
+      int k = 2;
+      for (; k + 3 <= KBM2; k += 4) {
+        double ak[4], ck[4], uk[4], vk[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          ak[u] = Acoef(k + u);
+          ck[u] = Ccoef(k + u);
+          uk[u] = P.uf[C3(P, i, k + u)];
+          vk[u] = P.vf[C3(P, i, k + u)];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) step(k + u, ak[u], ck[u], uk[u], vk[u]);
       }
+      for (; k <= KBM2; ++k) step(k, Acoef(k), Ccoef(k), P.uf[C3(P, i, k)], P.vf[C3(P, i, k)]);
       double ub = P.u[C3(P, i, KBM1)], vb = P.v[C3(P, i, KBM1)];
       double tps = P.cbc[i] * sqrt(ub * ub + vb * vb);
       P.tps[i] = tps;

@@ -875,7 +875,8 @@ __global__ void __launch_bounds__(256) k_fct_ts(const Dev P, int parts) {
 }
 
 // -------------------------------------------------------------------------------------
-// VDIF_TS(1,TF1) and VDIF_TS(2,SF1) (vdif_ts.F:78-337), one thread per node column.
+// VDIF_TS(1,TF1) and VDIF_TS(2,SF1) (vdif_ts.F:78-337), one thread per node column and
+// tracer (blockIdx.y 0: T, 1: S).
 // With surface heating (HEATING_TYPE 'flux', vdif_ts.F:118-150) the temperature column
 // takes the net heat flux WTSURF, held at zero while cooling water at or below -2 C,
 // and the short-wave flux RAD(K) = SWRAD*(RHEAT*EXP(Z*D/ZETA1) + (1-RHEAT)*EXP(Z*D/ZETA2))
@@ -895,8 +896,9 @@ __global__ void __launch_bounds__(128) k_vdif_ts(const Dev P, int parts) {
   auto CF = [&](int k) { double fkh = P.kh[n3(k)]; return -DTI * (fkh + UMOLPR) / (P.dz[n3(k)] * P.dzz[n3(k - 1)] * d * d); };
   const double khbottom = P.kh[n3(KBM1)];
   const bool update = P.iswetn[i] * P.iswetnt[i] == 1;
-  for (int t = 0; t < 2; ++t) {
-    if (!(parts & (t == 0 ? AD_T : AD_S))) continue;
+  {
+    const int t = blockIdx.y;  // 0: temperature, 1: salinity (independent columns)
+    if (!(parts & (t == 0 ? AD_T : AD_S))) return;
     double* F = (t == 0 ? P.tf1 : P.sf1);
     double vhf[kMaxKBs], vhpf[kMaxKBs];
     const double sasurf = 0.0;
@@ -922,13 +924,33 @@ __global__ void __launch_bounds__(128) k_vdif_ts(const Dev P, int parts) {
     vhf[1] = af1 / (af1 - 1.);
     vhpf[1] = -DTI * (sasurf + wfsurf - swradf + rad_k - rad_k1) / (-P.dz[n3(1)] * d) - F[n3(1)];
     vhpf[1] = vhpf[1] / (af1 - 1.);
-    for (int k = 2; k <= KBM2; ++k) {
+    // level k's coefficients and source, then its step of the (serial) recurrence; the
+    // loads of four levels are issued before their steps
+    auto coef = [&](int k, double& af, double& cf, double& fk, double& r) {
       rad_k = rad_k1;
       rad_k1 = RAD(k + 1);
-      double af = AF(k), cf = CF(k);
+      af = AF(k);
+      cf = CF(k);
+      fk = F[n3(k)];
+      r = DTI * (rad_k - rad_k1) / (d * P.dz[n3(k)]);
+    };
+    auto step = [&](int k, double af, double cf, double fk, double r) {
       double p = 1. / (af + cf * (1. - vhf[k - 1]) - 1.);
       vhf[k] = af * p;
-      vhpf[k] = (cf * vhpf[k - 1] - F[n3(k)] + DTI * (rad_k - rad_k1) / (d * P.dz[n3(k)])) * p;
+      vhpf[k] = (cf * vhpf[k - 1] - fk + r) * p;
+    };
+    int k = 2;
+    for (; k + 3 <= KBM2; k += 4) {
+      double af[4], cf[4], fk[4], r[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) coef(k + u, af[u], cf[u], fk[u], r[u]);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) step(k + u, af[u], cf[u], fk[u], r[u]);
+    }
+    for (; k <= KBM2; ++k) {
+      double af, cf, fk, r;
+      coef(k, af, cf, fk, r);
+      step(k, af, cf, fk, r);
     }
     if (P.isonb[i] != 2 && update) {
       double pfx = t == 0 ? P.pfpxb_t[i] : P.pfpxb_s[i];
@@ -1178,9 +1200,9 @@ void launch_fct_ts(const Dev& P, cudaStream_t s, int parts) {
 }
 void launch_vdif_ts(const Dev& P, cudaStream_t s, int parts) {
   if (P.heating_on)
-    k_vdif_ts<true><<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
+    k_vdif_ts<true><<<dim3(nblk(P.M, 128), 2), 128, 0, s>>>(P, parts);
   else
-    k_vdif_ts<false><<<nblk(P.M, 128), 128, 0, s>>>(P, parts);
+    k_vdif_ts<false><<<dim3(nblk(P.M, 128), 2), 128, 0, s>>>(P, parts);
 }
 void launch_bcond_ts(const Dev& P, cudaStream_t s, int parts) {
   k_bcond_ts_riv<<<1, 128, 0, s>>>(P);
