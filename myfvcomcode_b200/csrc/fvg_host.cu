@@ -427,14 +427,6 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
     std::vector<int> ptr, ent;
     build_csr(nl, ptr, ent);
     UPI(node_he_ptr, ptr.data(), ptr.size()); UPI(node_he, ent.data(), ent.size());
-    {
-      size_t w = 0;
-      for (auto& l : nl) w = std::max(w, l.size());
-      std::vector<int> ell(std::max<size_t>(w, 1) * ms, 0);
-      for (size_t i = 0; i < m1; ++i)
-        for (size_t j = 0; j < nl[i].size(); ++j) ell[j * ms + i] = nl[i][j];
-      UPI(node_he_ell, ell.data(), ell.size());
-    }
     std::vector<int> ce(3 * n1, 0);
     for (size_t i = 1; i < n1; ++i) {
       if (cl[i].size() != 3) { h->err = "cell without exactly three edges"; return fail(FVG_ERR_BOUNDS); }
@@ -487,11 +479,23 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
       }
     }
     UPI(cell_he, chv.data(), chv.size());
-    // VERTVL_EDGE's node lists over the (slot, cell) positions of the half-edge fluxes:
-    // entry j of node i at j*ms + i, code = (slot*ns + cell)*2 + side, ascending half-edge id
+    // Half-edge positions pos = slot*ns + cell; the node lists over positions, entry j of
+    // node i at j*ms + i, code = pos*2 + side, ascending half-edge id; the metrics by position
     std::vector<int> slot(v1, 0);
+    std::vector<double> hg(18 * ns, 0.0);
     for (size_t i = 1; i < n1; ++i)
-      for (int s2 = 0; s2 < 3; ++s2) slot[chv[3 * i + s2]] = s2;
+      for (int s2 = 0; s2 < 3; ++s2) {
+        const int he = chv[3 * i + s2];
+        slot[he] = s2;
+        const size_t pos = (size_t)s2 * ns + i, pl = 3 * ns;
+        hg[pos] = m->dltxe[he];
+        hg[pl + pos] = m->dltye[he];
+        hg[2 * pl + pos] = m->dltxncve[he];
+        hg[3 * pl + pos] = m->dltyncve[he];
+        hg[4 * pl + pos] = m->dltxncve[vi1 + he];
+        hg[5 * pl + pos] = m->dltyncve[vi1 + he];
+      }
+    UPD(hg, hg.data(), hg.size());
     std::vector<std::vector<int>> vl(m1);
     for (int he = 1; he <= m->ncv; ++he) {
       const long pos = (long)slot[he] * (long)ns + m->ntrg[he];
@@ -649,7 +653,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   for (double** pp : {&P.vq_prod, &P.vq_gh, &P.vq_dtef, &P.vq_dtefl})
     if ((rc = dalloc(h, pp, ms * KB))) return fail(rc);
   if ((rc = dalloc(h, &P.vq_ut, ms))) return fail(rc);
-  P.ncvs = (int)pad32(m->ncv + 1);
+  P.ncvs = (int)(3 * ns);  // half-edge arrays by position, pos = slot*ns + cell
   for (int q = 0; q < 4; ++q) {
     if ((rc = dalloc(h, &P.g2d[q], n1))) return fail(rc);
   }
@@ -675,10 +679,10 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
       if ((rc = upload(h, &P.alfa3[q], ones.data(), (size_t)P.ns * KB))) return fail(rc);
     }
   }
-  if ((rc = dalloc(h, &P.exf2d, v1))) return fail(rc);
+  if ((rc = dalloc(h, &P.exf2d, 3 * ns))) return fail(rc);
   for (int q = 0; q < 4; ++q)
     if ((rc = dalloc(h, &P.g3[q], ns * KB))) return fail(rc);
-  if ((rc = dalloc(h, (double**)&P.ex2, std::max((size_t)P.ncvs * KB * 2, 3 * ns * KB)))) return fail(rc);
+  if ((rc = dalloc(h, (double**)&P.ex2, (size_t)P.ncvs * KB * 2))) return fail(rc);
   P.he_vflux = (double*)P.ex2;
 
   // ---- schedule ----
@@ -962,7 +966,6 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
   if (mode == FVG_PREC_FP32_FLUX && !P.f.ex2) {
     int rc;
     const size_t ms = P.ms, ns = P.ns, KB = P.KB, n1 = P.N + 1, e1 = P.NE + 1;
-    const size_t v1 = P.NCV + 1, vi1 = P.NCV_I + 1;
     F32& f = P.f;
     auto fail = [&](int r) { return r; };
     for (int q = 0; q < 4; ++q) {
@@ -988,12 +991,9 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     if ((rc = dalloc(h, &f.cc_hvc, n1))) return fail(rc);
     if ((rc = dalloc(h, &f.a1u, 4 * n1))) return fail(rc);
     if ((rc = dalloc(h, &f.a2u, 4 * n1))) return fail(rc);
-    if ((rc = dalloc(h, &f.dltxe, v1))) return fail(rc);
-    if ((rc = dalloc(h, &f.dltye, v1))) return fail(rc);
-    if ((rc = dalloc(h, &f.dltxncve, 2 * vi1))) return fail(rc);
-    if ((rc = dalloc(h, &f.dltyncve, 2 * vi1))) return fail(rc);
     for (float** pp : {&f.ce_xoa, &f.ce_yoa, &f.ce_xob, &f.ce_yob, &f.ce_dx, &f.ce_dy})
       if ((rc = dalloc(h, pp, 3 * n1))) return fail(rc);
+    if ((rc = dalloc(h, &f.hg, 6 * (size_t)P.ncvs))) return fail(rc);
     launch_make_f32(P, h->stream);
     CK(cudaGetLastError());
   }

@@ -46,8 +46,8 @@ struct F32 {
   float* npk;  // node records of the ring gradients, 16 floats per (node, layer)
   float2* ex2;
   float *xo, *yo, *dltxc, *dltyc, *art, *cc_hvc, *a1u, *a2u;
-  float *dltxe, *dltye, *dltxncve, *dltyncve;
   float *ce_xoa, *ce_yoa, *ce_xob, *ce_yob, *ce_dx, *ce_dy;
+  float* hg;  // the half-edge metrics by position, as Dev::hg
 };
 
 // Input and output scaling of the learned closure's network, and the training envelope.
@@ -102,12 +102,15 @@ struct Dev {
   const double *dltxe, *dltye, *dltxncve, *dltyncve;
   // ----- gather lists -----
   const int *node_he_ptr, *node_he;   // node -> half-edges (id*2 + side), ascending id
-  // The same lists transposed: entry j of node i at j*ms + i, so that the threads of
-  // consecutive nodes read entry j in one coalesced load (count = ptr[i+1] - ptr[i]).
-  const int* node_he_ell;
-  // VERTVL_EDGE's node lists, transposed the same way: code = (slot*ns + cell)*2 + side,
-  // the position of the half-edge flux in he_vflux, in ascending half-edge id.
+  // Half-edge data by position: half-edge cell_he[3*c + s] (slot s of cell c) sits at
+  // pos = s*ns + c, so that the threads of consecutive cells touch consecutive entries.
+  // node_vpos_ell: the lists of node_he over positions and transposed, entry j of node i
+  // at j*ms + i, code = pos*2 + side, ascending half-edge id (count = ptr[i+1] - ptr[i]);
+  // the threads of consecutive nodes read entry j in one coalesced load.
   const int* node_vpos_ell;
+  // Metrics by position, plane j at j*ncvs: DLTXE, DLTYE, DLTXNCVE and DLTYNCVE of the
+  // NIEC(he,1) side, DLTXNCVE and DLTYNCVE of the NIEC(he,2) side.
+  const double* hg;
   const int *cell_edge;               // cell -> its 3 edges (id*2 + side), ascending id
   // Slot table of the cell edge loops, slot s of cell i at s*(N+1) + i (edges in the order
   // of cell_edge): code = edge*4 + ISBC*2 + side, the two cells, the two nodes, the edge
@@ -159,18 +162,17 @@ struct Dev {
   double* budget;                            // 3 doubles
   // VDIF_Q between its passes: PROD, GH, DTEF, the q2l DTEF (node 3-D) and UTAU2 (node)
   double *vq_prod, *vq_gh, *vq_dtef, *vq_dtefl, *vq_ut;
-  double2* ex2;                              // half-edge fluxes of both advected tracers (ncvs x KB)
-  // VERTVL_EDGE's EXFLUX of each half-edge and layer, at (k-1)*3*ns + slot*ns + cell for
-  // the cell's half-edge in slot `slot` of cell_he; it lives in the allocation of ex2,
-  // which is free between ADJUST2D3D and the next advection.
+  double2* ex2;                              // half-edge fluxes of both tracers (ncvs x KB, by position)
+  // VERTVL_EDGE's EXFLUX of each half-edge position and layer, at (k-1)*ncvs + pos; it
+  // lives in the allocation of ex2, which is free between ADJUST2D3D and the next advection.
   double* he_vflux;
   double* g2d[4];                            // least-squares gradient of UA, VA per cell (COFA1/2/5/6)
   // Slope limiters of the limited schemes, UALFA and VALFA: per cell of the 2-D mode
   // (N+1) and per cell and layer of the 3-D mode (ns x KB); index 0 holds 1.
   double *alfa2[2], *alfa3[2];
-  double* exf2d;                             // EXTEL_EDGE flux of each half-edge (NCV+1)
+  double* exf2d;                             // EXTEL_EDGE flux of each half-edge position (ncvs)
   double* g3[4];                             // least-squares gradient of U, V per cell and layer (ns x KB)
-  int ncvs;                                  // layer stride of ex (>= NCV+1)
+  int ncvs;                                  // layer stride of the half-edge arrays by position (3*ns)
   // Precision form (fvg_set_precision): 0 = FP64 everywhere; 1 = the edge fluxes and
   // advection (ADVAVE's edge loop, the 3-D momentum edge fluxes, ADV_Q/ADV_T/ADV_S with
   // FCT) in FP32 arithmetic over FP32 scratch and FP32 copies of their mesh metrics.
@@ -260,15 +262,12 @@ template <> struct Mesh<double> {
   __device__ static double cc_hvc(const Dev& P, int c) { return P.cc_hvc[c]; }
   __device__ static double a1u(const Dev& P, size_t q) { return P.a1u[q]; }
   __device__ static double a2u(const Dev& P, size_t q) { return P.a2u[q]; }
-  __device__ static double dltxe(const Dev& P, size_t q) { return P.dltxe[q]; }
-  __device__ static double dltye(const Dev& P, size_t q) { return P.dltye[q]; }
-  __device__ static double dltxncve(const Dev& P, size_t q) { return P.dltxncve[q]; }
-  __device__ static double dltyncve(const Dev& P, size_t q) { return P.dltyncve[q]; }
   __device__ static double* g2d(const Dev& P, int q) { return P.g2d[q]; }
   __device__ static double* alfa2(const Dev& P, int q) { return P.alfa2[q]; }
   __device__ static double* alfa3(const Dev& P, int q) { return P.alfa3[q]; }
   __device__ static double* g3(const Dev& P, int q) { return P.g3[q]; }
   __device__ static double2* ex2(const Dev& P) { return P.ex2; }
+  __device__ static double hg(const Dev& P, int j, size_t pos) { return P.hg[(size_t)j * P.ncvs + pos]; }
 };
 template <> struct Mesh<float> {
   typedef float2 R2;
@@ -288,15 +287,12 @@ template <> struct Mesh<float> {
   __device__ static float cc_hvc(const Dev& P, int c) { return P.f.cc_hvc[c]; }
   __device__ static float a1u(const Dev& P, size_t q) { return P.f.a1u[q]; }
   __device__ static float a2u(const Dev& P, size_t q) { return P.f.a2u[q]; }
-  __device__ static float dltxe(const Dev& P, size_t q) { return P.f.dltxe[q]; }
-  __device__ static float dltye(const Dev& P, size_t q) { return P.f.dltye[q]; }
-  __device__ static float dltxncve(const Dev& P, size_t q) { return P.f.dltxncve[q]; }
-  __device__ static float dltyncve(const Dev& P, size_t q) { return P.f.dltyncve[q]; }
   __device__ static float* g2d(const Dev& P, int q) { return P.f.g2d[q]; }
   __device__ static float* alfa2(const Dev& P, int q) { return P.f.alfa2[q]; }
   __device__ static float* alfa3(const Dev& P, int q) { return P.f.alfa3[q]; }
   __device__ static float* g3(const Dev& P, int q) { return P.f.g3[q]; }
   __device__ static float2* ex2(const Dev& P) { return P.f.ex2; }
+  __device__ static float hg(const Dev& P, int j, size_t pos) { return P.f.hg[(size_t)j * P.ncvs + pos]; }
 };
 // Limited schemes (advave_edge_gcn.F:226-229, 300-303, 340-357): the slope limiter of one
 // cell and edge, min(ALFA, min(1, |U(IA)-U(IB)| / |U'+EPSILON|)), EPSILON of the form's type.

@@ -77,8 +77,8 @@ __device__ inline Grad<R> load_grad(const Dev& P, int c) {
 __device__ inline void store_exf(const Dev& P, int c) {
   double d1 = P.d1[c], u = P.ua[c], v = P.va[c];
   for (int s = 0; s < 3; ++s) {
-    int he = P.cell_he[3 * c + s];
-    P.exf2d[he] = d1 * (-u * P.dltye[he] + v * P.dltxe[he]);
+    const size_t pos = (size_t)s * P.ns + c;
+    P.exf2d[pos] = d1 * (-u * Mesh<double>::hg(P, 1, pos) + v * Mesh<double>::hg(P, 0, pos));
   }
 }
 
@@ -129,8 +129,8 @@ __device__ inline void ext_update_cell(const Dev& P, int i, int K, double u, dou
     P.vard[i] = P.vard[i] + v * dd1;
   }
   for (int s = 0; s < 3; ++s) {
-    int he = P.cell_he[3 * i + s];
-    P.exf2d[he] = dd1 * (-u * P.dltye[he] + v * P.dltxe[he]);
+    const size_t pos = (size_t)s * P.ns + i;
+    P.exf2d[pos] = dd1 * (-u * Mesh<double>::hg(P, 1, pos) + v * Mesh<double>::hg(P, 0, pos));
   }
 }
 
@@ -175,7 +175,7 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   if (parts & EN_EXTEL) {
     const int n = P.node_he_ptr[i + 1] - P.node_he_ptr[i];
     for (int j = 0; j < n; ++j) {
-      int e = P.node_he_ell[(size_t)j * P.ms + i];
+      int e = P.node_vpos_ell[(size_t)j * P.ms + i];
       double exflux = P.exf2d[e >> 1];
       x = (e & 1) ? x + exflux : x - exflux;
     }
@@ -580,7 +580,7 @@ __global__ void k_edge_offsets_f32(const Dev P) {
 }
 void launch_make_f32(const Dev& P, cudaStream_t s) {
   auto cvt = [&](const double* a, float* b, size_t n) { k_d2f<<<296, 256, 0, s>>>(a, b, n); };
-  const size_t n1 = P.N + 1, e1 = P.NE + 1, v1 = P.NCV + 1, vi1 = P.NCV_I + 1;
+  const size_t n1 = P.N + 1, e1 = P.NE + 1;
   k_edge_offsets_f32<<<nblk(P.NE + 1, 256), 256, 0, s>>>(P);
   cvt(P.dltxc, P.f.dltxc, e1);
   cvt(P.dltyc, P.f.dltyc, e1);
@@ -588,16 +588,13 @@ void launch_make_f32(const Dev& P, cudaStream_t s) {
   cvt(P.cc_hvc, P.f.cc_hvc, n1);
   cvt(P.a1u, P.f.a1u, 4 * n1);
   cvt(P.a2u, P.f.a2u, 4 * n1);
-  cvt(P.dltxe, P.f.dltxe, v1);
-  cvt(P.dltye, P.f.dltye, v1);
-  cvt(P.dltxncve, P.f.dltxncve, 2 * vi1);
-  cvt(P.dltyncve, P.f.dltyncve, 2 * vi1);
   cvt(P.ce_xoa, P.f.ce_xoa, 3 * n1);
   cvt(P.ce_yoa, P.f.ce_yoa, 3 * n1);
   cvt(P.ce_xob, P.f.ce_xob, 3 * n1);
   cvt(P.ce_yob, P.f.ce_yob, 3 * n1);
   cvt(P.ce_dx, P.f.ce_dx, 3 * n1);
   cvt(P.ce_dy, P.f.ce_dy, 3 * n1);
+  cvt(P.hg, P.f.hg, 6 * (size_t)P.ncvs);
 }
 void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);

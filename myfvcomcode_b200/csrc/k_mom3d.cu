@@ -509,9 +509,9 @@ __global__ void k_adjust2(const Dev P, int parts) {
   }
   double dy[3], dx[3];
   for (int s = 0; s < 3; ++s) {
-    const int he = P.cell_he[3 * i + s];
-    dy[s] = P.dltye[he];
-    dx[s] = P.dltxe[he];
+    const size_t pos = (size_t)s * P.ns + i;
+    dy[s] = Mesh<double>::hg(P, 1, pos);
+    dx[s] = Mesh<double>::hg(P, 0, pos);
   }
   for (int k = 1; k <= P.KBM1; ++k) {
     size_t q = C3(P, i, k);
@@ -523,7 +523,7 @@ __global__ void k_adjust2(const Dev P, int parts) {
       P.v[q] = vv;
     }
     const double dij = dt1 * P.dz1[q];
-    double* F = P.he_vflux + (size_t)(k - 1) * 3 * P.ns + i;
+    double* F = P.he_vflux + (size_t)(k - 1) * P.ncvs + i;
     for (int s = 0; s < 3; ++s) F[(size_t)s * P.ns] = dij * (-uu * dy[s] + vv * dx[s]);
   }
 }
@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(256) k_vertvl_flux(const Dev P) {
   {
   double x = 0.0;
   if (P.isonb[i] != 2) {
-    const double* F = P.he_vflux + (size_t)(k - 1) * 3 * P.ns;
+    const double* F = P.he_vflux + (size_t)(k - 1) * P.ncvs;
     const int* L = P.node_vpos_ell + i;
     const size_t ms = P.ms;
     const int n = P.node_he_ptr[i + 1] - P.node_he_ptr[i];

@@ -231,7 +231,8 @@ __device__ inline void fct_level_bounds(const Dev& P, int i, int k, const double
 // half-edges run from its centroid to its edge midpoints and each separates two of the
 // cell's own nodes, so the node data (tracer value, ring gradients and extrema, mixing
 // coefficient) is loaded once for the three half-edges.  Each half-edge flux EXFLUX is
-// evaluated once, in the reference's expression order, and stored by half-edge number.
+// evaluated once, in the reference's expression order, and stored at the half-edge's
+// position slot*ns + cell.
 // Phase 2 (k_gather_*, one thread per node and layer) sums the node's half-edge fluxes
 // with their signs in ascending half-edge order -- the order of the reference's scatter --
 // and applies the vertical flux, the update and the FCT clamp.
@@ -278,18 +279,30 @@ template <typename R>
 __device__ inline R sel3(const R* v, int j) { return j == 0 ? v[0] : (j == 1 ? v[1] : v[2]); }
 __device__ inline int sel3i(const int* v, int j) { return j == 0 ? v[0] : (j == 1 ? v[1] : v[2]); }
 
-// EXFLUX of half-edge he for tracer t, in R; a and b are the positions of NIEC(he,1) and
-// NIEC(he,2) among the cell's nodes, ra and rb their data.  xadv receives EXFLUX-FXX-FYY.
-template <typename R, int MODE>
-__device__ inline R he_flux(const Dev& P, const HeCell<R>& hc, int he, int a, int b, const TRec<R>& ra,
-                            const TRec<R>& rb, R* xadv) {
+// Metrics of one half-edge (DLTXE, DLTYE and the DLTXNCVE/DLTYNCVE of both sides), read
+// by position (coalesced over the threads of consecutive cells).
+template <typename R>
+struct HeGeo {
+  R dx, dy, xa, ya, xb, yb;
+};
+template <typename R>
+__device__ inline HeGeo<R> he_geo(const Dev& P, size_t pos) {
   typedef Mesh<R> Mh;
+  return HeGeo<R>{Mh::hg(P, 0, pos), Mh::hg(P, 1, pos), Mh::hg(P, 2, pos),
+                  Mh::hg(P, 3, pos), Mh::hg(P, 4, pos), Mh::hg(P, 5, pos)};
+}
+
+// EXFLUX of a half-edge with metrics g for tracer t, in R; a and b are the positions of
+// NIEC(he,1) and NIEC(he,2) among the cell's nodes, ra and rb their data.  xadv receives
+// EXFLUX-FXX-FYY.
+template <typename R, int MODE>
+__device__ inline R he_flux(const Dev& P, const HeCell<R>& hc, const HeGeo<R>& g, int a, int b, const TRec<R>& ra,
+                            const TRec<R>& rb, R* xadv) {
   const R half = (R)0.5, one = (R)1.0;
-  const size_t vi1 = P.NCV_I + 1;
-  const R dltxe = Mh::dltxe(P, he), dltye = Mh::dltye(P, he);
+  const R dltxe = g.dx, dltye = g.dy;
   R un = hc.vq * dltxe - hc.uq * dltye;
-  R fij1 = ra.q + Mh::dltxncve(P, he) * ra.px + Mh::dltyncve(P, he) * ra.py;
-  R fij2 = rb.q + Mh::dltxncve(P, vi1 + he) * rb.px + Mh::dltyncve(P, vi1 + he) * rb.py;
+  R fij1 = ra.q + g.xa * ra.px + g.ya * ra.py;
+  R fij2 = rb.q + g.xb * rb.px + g.yb * rb.py;
   R q1min = fmin(ra.rmin, ra.q), q1max = fmax(ra.rmax, ra.q);
   R q2min = fmin(rb.rmin, rb.q), q2max = fmax(rb.rmax, rb.q);
   if (fij1 < q1min) fij1 = q1min;
@@ -334,23 +347,23 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_he_adv(const De
   col_range(P, MODE == 0 ? 2 : 1, P.KBM1, kb, ke);
   const size_t v1 = P.NCV + 1;
   const bool do0 = parts & (MODE == 0 ? AD_Q2 : AD_T), do1 = parts & (MODE == 0 ? AD_Q2L : AD_S);
-  int hes[3], pa[3], pb[3];
+  int pa[3], pb[3];
   {
     int nd0 = P.nv[c], nd1 = P.nv[(size_t)(P.N + 1) + c];
     for (int s = 0; s < 3; ++s) {
       int he = P.cell_he[3 * c + s];
-      hes[s] = he;
       int na = P.niec[he], nb = P.niec[v1 + he];
       pa[s] = na == nd0 ? 0 : (na == nd1 ? 1 : 2);
       pb[s] = nb == nd0 ? 0 : (nb == nd1 ? 1 : 2);
     }
   }
   // Each of the cell's three nodes ends two of its half-edges: its record is loaded once
-  // per tracer and layer and handed to both.
+  // per tracer and layer and handed to both.  The metrics and the fluxes are by position
+  // s*ns + c.
   for (int k = kb; k <= ke; ++k) {
     HeCell<R> hc;
     he_cell_load<R, MODE>(P, c, k, hc);
-    R2* EX = Mesh<R>::ex2(P) + (size_t)(k - 1) * P.ncvs;
+    R2* EX = Mesh<R>::ex2(P) + (size_t)(k - 1) * P.ncvs + c;
     R e[2][3] = {{0, 0, 0}, {0, 0, 0}};
     for (int t = 0; t < 2; ++t) {
       if (!(t == 0 ? do0 : do1)) continue;
@@ -358,10 +371,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_he_adv(const De
       const TRec<R> r1 = load_trec<R, MODE>(P, hc.nd[1], k, t);
       const TRec<R> r2 = load_trec<R, MODE>(P, hc.nd[2], k, t);
       for (int s = 0; s < 3; ++s)
-        e[t][s] = he_flux<R, MODE>(P, hc, hes[s], pa[s], pb[s], sel_trec(r0, r1, r2, pa[s]),
-                                   sel_trec(r0, r1, r2, pb[s]), nullptr);
+        e[t][s] = he_flux<R, MODE>(P, hc, he_geo<R>(P, (size_t)s * P.ns + c), pa[s], pb[s],
+                                   sel_trec(r0, r1, r2, pa[s]), sel_trec(r0, r1, r2, pb[s]), nullptr);
     }
-    for (int s = 0; s < 3; ++s) EX[hes[s]] = mk2(e[0][s], e[1][s]);
+    for (int s = 0; s < 3; ++s) EX[(size_t)s * P.ns] = mk2(e[0][s], e[1][s]);
   }
 }
 
@@ -375,12 +388,13 @@ __device__ inline double obc_xflux_adv(const Dev& P, int i, int k, int t) {
     int code = P.node_he[q];
     int he = code >> 1;
     int c = P.ntrg[he];
+    const int sl = P.cell_he[3 * c] == he ? 0 : (P.cell_he[3 * c + 1] == he ? 1 : 2);
     HeCell<R> hc;
     he_cell_load<R, 1>(P, c, k, hc);
     const int na = P.niec[he], nb = P.niec[v1 + he];
     R part;
-    he_flux<R, 1>(P, hc, he, pos3(hc, na), pos3(hc, nb), load_trec<R, 1>(P, na, k, t),
-                  load_trec<R, 1>(P, nb, k, t), &part);
+    he_flux<R, 1>(P, hc, he_geo<R>(P, (size_t)sl * P.ns + c), pos3(hc, na), pos3(hc, nb),
+                  load_trec<R, 1>(P, na, k, t), load_trec<R, 1>(P, nb, k, t), &part);
     xa = (code & 1) ? xa - part : xa + part;
   }
   return (double)xa;
@@ -393,7 +407,7 @@ template <typename R>
 __device__ inline double2 gather_he(const Dev& P, int i, int n, int k) {
   typedef typename Mesh<R>::R2 R2;
   const R2* EX = Mesh<R>::ex2(P) + (size_t)(k - 1) * P.ncvs;
-  const int* L = P.node_he_ell + i;
+  const int* L = P.node_vpos_ell + i;
   const size_t ms = P.ms;
   R x0 = 0, x1 = 0;
   auto add = [&](int code, R2 e) {
