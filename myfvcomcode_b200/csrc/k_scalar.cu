@@ -29,16 +29,19 @@ __device__ inline double TRIEY(const Dev& P, int i, int j) { return P.dltytrie[(
 template <typename R>
 struct TRec {
   R q, px, py, pxd, pyd, rmin, rmax;
+  R vf;  // FP32 records: the node's VISCOFH on the record's layer or level (else unused)
 };
 
 // Storage of the ring gradients and extrema by arithmetic type.  FP64: six arrays per
 // tracer (P.gq, P.gt).  FP32: one 32-byte record per tracer and (node, layer) in P.f.npk,
-// record r = (K-1)*ms + I holding {value, PX, PY, PXD, PYD, min, max, 0} for tracer t at
-// floats 16r + 8t, read and written as two float4.
+// record r = (K-1)*ms + I holding {value, PX, PY, PXD, PYD, min, max, VF} for tracer t at
+// floats 16r + 8t, read and written as two float4; VF is the node's VISCOFH on the layer
+// (T, S) or interpolated to the level (Q2, Q2L) as the half-edge fluxes take it, so that
+// they need not gather it.
 template <typename R> struct NodeRec;
 template <> struct NodeRec<double> {
   __device__ static void store(const Dev& P, int mode, int t, size_t q, double, double px, double py, double pxd,
-                               double pyd, double mn, double mx) {
+                               double pyd, double mn, double mx, double) {
     double* const* G = mode == 0 ? P.gq[t] : P.gt[t];
     G[0][q] = px;
     G[1][q] = py;
@@ -49,7 +52,7 @@ template <> struct NodeRec<double> {
   }
   __device__ static TRec<double> load(const Dev& P, int mode, int t, size_t q, double qv) {
     double* const* G = mode == 0 ? P.gq[t] : P.gt[t];
-    return TRec<double>{qv, G[0][q], G[1][q], G[2][q], G[3][q], G[4][q], G[5][q]};
+    return TRec<double>{qv, G[0][q], G[1][q], G[2][q], G[3][q], G[4][q], G[5][q], 0.0};
   }
   __device__ static void minmax(const Dev& P, int mode, int t, size_t q, double& mn, double& mx) {
     double* const* G = mode == 0 ? P.gq[t] : P.gt[t];
@@ -62,15 +65,15 @@ template <> struct NodeRec<float> {
     return reinterpret_cast<float4*>(P.f.npk + 16 * q + 8 * t);
   }
   __device__ static void store(const Dev& P, int, int t, size_t q, float qv, float px, float py, float pxd,
-                               float pyd, float mn, float mx) {
+                               float pyd, float mn, float mx, float vf) {
     float4* r = rec(P, t, q);
     r[0] = make_float4(qv, px, py, pxd);
-    r[1] = make_float4(pyd, mn, mx, 0.f);
+    r[1] = make_float4(pyd, mn, mx, vf);
   }
   __device__ static TRec<float> load(const Dev& P, int, int t, size_t q, double) {
     const float4* r = rec(P, t, q);
     const float4 a = r[0], b = r[1];
-    return TRec<float>{a.x, a.y, a.z, a.w, b.x, b.y, b.z};
+    return TRec<float>{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
   }
   __device__ static void minmax(const Dev& P, int, int t, size_t q, double& mn, double& mx) {
     const float4 b = rec(P, t, q)[1];
@@ -166,9 +169,19 @@ __global__ void __launch_bounds__(256) k_grad(const Dev P, int which) {
       w1 = w2;
     }
     const size_t q = N3(P, i, k);
+    // the node's mixing coefficient as the half-edge fluxes take it (FP32 records)
+    R vf = 0;
+    if (sizeof(R) == 4) {
+      if (which == 0) {
+        const size_t qm = N3(P, i, k - 1);
+        vf = (R)((P.viscofh[q] * P.dz[qm] + P.viscofh[qm] * P.dz[q]) / (P.dz[q] + P.dz[qm]));
+      } else {
+        vf = (R)P.viscofh[q];
+      }
+    }
     for (int t = 0; t < 2; ++t) {
       const R gx = px[t] / art2, gy = py[t] / art2, gxd = pxd[t] / art2, gyd = pyd[t] / art2;
-      NodeRec<R>::store(P, which, t, q, qi[t], gx, gy, gxd, gyd, rmin[t], rmax[t]);
+      NodeRec<R>::store(P, which, t, q, qi[t], gx, gy, gxd, gyd, rmin[t], rmax[t], vf);
       if (which == 1 && k == P.KBM1) {
         if (t == 0) { P.pfpxb_t[i] = (double)gx; P.pfpyb_t[i] = (double)gy; }
         else { P.pfpxb_s[i] = (double)gx; P.pfpyb_s[i] = (double)gy; }
@@ -263,6 +276,8 @@ __device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell<R>& hc) {
   for (int j = 0; j < 3; ++j) {
     int n = P.nv[j * n1 + c];
     hc.nd[j] = n;
+    hc.nn[j] = (R)P.nn_hvc[n];
+    if (sizeof(R) == 4) continue;  // FP32: VISCOFH travels in the node records
     size_t q = N3(P, n, k);
     if (MODE == 0) {
       size_t qm = N3(P, n, k - 1);
@@ -270,7 +285,6 @@ __device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell<R>& hc) {
     } else {
       hc.vf[j] = (R)P.viscofh[q];
     }
-    hc.nn[j] = (R)P.nn_hvc[n];
   }
 }
 
@@ -309,7 +323,8 @@ __device__ inline R he_flux(const Dev& P, const HeCell<R>& hc, const HeGeo<R>& g
   if (fij1 > q1max) fij1 = q1max;
   if (fij2 < q2min) fij2 = q2min;
   if (fij2 > q2max) fij2 = q2max;
-  const R vfa = sel3(hc.vf, a), vfb = sel3(hc.vf, b), nna = sel3(hc.nn, a), nnb = sel3(hc.nn, b);
+  const R vfa = sizeof(R) == 4 ? ra.vf : sel3(hc.vf, a), vfb = sizeof(R) == 4 ? rb.vf : sel3(hc.vf, b);
+  const R nna = sel3(hc.nn, a), nnb = sel3(hc.nn, b);
   R viscof = (R)P.fact * half * (vfa * nna + vfb * nnb) + (R)P.fm1 * half * (nna + nnb);
   if (MODE == 0) viscof = viscof / (R)P.hprnu;
   R txx = half * (ra.pxd + rb.pxd) * viscof;
@@ -332,6 +347,7 @@ __device__ inline TRec<R> sel_trec(const TRec<R>& a, const TRec<R>& b, const TRe
   r.pyd = j == 0 ? a.pyd : (j == 1 ? b.pyd : c.pyd);
   r.rmin = j == 0 ? a.rmin : (j == 1 ? b.rmin : c.rmin);
   r.rmax = j == 0 ? a.rmax : (j == 1 ? b.rmax : c.rmax);
+  r.vf = j == 0 ? a.vf : (j == 1 ? b.vf : c.vf);
   return r;
 }
 
