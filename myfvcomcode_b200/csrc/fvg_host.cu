@@ -457,6 +457,14 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
           dy[q] = m->dltyc[e];
         }
       UPI(ce_code, cc.data(), S3); UPI(ce_ia, ca.data(), S3); UPI(ce_ib, cb.data(), S3);
+      std::vector<int> c4(4 * S3);
+      for (size_t q = 0; q < S3; ++q) {
+        c4[4 * q] = cc[q];
+        c4[4 * q + 1] = ca[q];
+        c4[4 * q + 2] = cb[q];
+        c4[4 * q + 3] = cj1[q];
+      }
+      UPI(ce_i4, c4.data(), c4.size());
       UPI(ce_j1, cj1.data(), S3); UPI(ce_j2, cj2.data(), S3);
       UPD(ce_xoa, xa.data(), S3); UPD(ce_yoa, ya.data(), S3); UPD(ce_xob, xb.data(), S3);
       UPD(ce_yob, yb.data(), S3); UPD(ce_dx, dx.data(), S3); UPD(ce_dy, dy.data(), S3);
@@ -994,6 +1002,8 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     for (float** pp : {&f.ce_xoa, &f.ce_yoa, &f.ce_xob, &f.ce_yob, &f.ce_dx, &f.ce_dy})
       if ((rc = dalloc(h, pp, 3 * n1))) return fail(rc);
     if ((rc = dalloc(h, &f.hg, 6 * (size_t)P.ncvs))) return fail(rc);
+    if ((rc = dalloc(h, (float**)&f.ce_geo, 4 * 3 * n1))) return fail(rc);
+    if ((rc = dalloc(h, (float**)&f.ce_dd, 2 * 3 * n1))) return fail(rc);
     launch_make_f32(P, h->stream);
     CK(cudaGetLastError());
   }

@@ -48,6 +48,9 @@ struct F32 {
   float *xo, *yo, *dltxc, *dltyc, *art, *cc_hvc, *a1u, *a2u;
   float *ce_xoa, *ce_yoa, *ce_xob, *ce_yob, *ce_dx, *ce_dy;
   float* hg;  // the half-edge metrics by position, as Dev::hg
+  // The slot table's metrics packed per slot: {XOA, YOA, XOB, YOB} and {DX, DY}
+  float4* ce_geo;
+  float2* ce_dd;
 };
 
 // Input and output scaling of the learned closure's network, and the training envelope.
@@ -116,6 +119,7 @@ struct Dev {
   // of cell_edge): code = edge*4 + ISBC*2 + side, the two cells, the two nodes, the edge
   // offsets XIJC-XC / YIJC-YC of both cells, DLTXC, DLTYC.  Read coalesced by cell.
   const int *ce_code, *ce_ia, *ce_ib, *ce_j1, *ce_j2;
+  const int4* ce_i4;  // the same slot as {code, IA, IB, J1} in one 16-byte load
   const double *ce_xoa, *ce_yoa, *ce_xob, *ce_yob, *ce_dx, *ce_dy;
   const int *cell_he;                 // cell -> its 3 control-volume half-edges (NTRG(he) == cell)
   // ----- open boundary -----
@@ -256,6 +260,10 @@ template <> struct Mesh<double> {
   __device__ static double s_yob(const Dev& P, size_t q) { return P.ce_yob[q]; }
   __device__ static double s_dx(const Dev& P, size_t q) { return P.ce_dx[q]; }
   __device__ static double s_dy(const Dev& P, size_t q) { return P.ce_dy[q]; }
+  __device__ static double4 s_geo(const Dev& P, size_t q) {
+    return make_double4(P.ce_xoa[q], P.ce_yoa[q], P.ce_xob[q], P.ce_yob[q]);
+  }
+  __device__ static double2 s_dd(const Dev& P, size_t q) { return make_double2(P.ce_dx[q], P.ce_dy[q]); }
   __device__ static double dltxc(const Dev& P, int e) { return P.dltxc[e]; }
   __device__ static double dltyc(const Dev& P, int e) { return P.dltyc[e]; }
   __device__ static double art(const Dev& P, int c) { return P.art[c]; }
@@ -281,6 +289,8 @@ template <> struct Mesh<float> {
   __device__ static float s_yob(const Dev& P, size_t q) { return P.f.ce_yob[q]; }
   __device__ static float s_dx(const Dev& P, size_t q) { return P.f.ce_dx[q]; }
   __device__ static float s_dy(const Dev& P, size_t q) { return P.f.ce_dy[q]; }
+  __device__ static float4 s_geo(const Dev& P, size_t q) { return P.f.ce_geo[q]; }
+  __device__ static float2 s_dd(const Dev& P, size_t q) { return P.f.ce_dd[q]; }
   __device__ static float dltxc(const Dev& P, int e) { return P.f.dltxc[e]; }
   __device__ static float dltyc(const Dev& P, int e) { return P.f.dltyc[e]; }
   __device__ static float art(const Dev& P, int c) { return P.f.art[c]; }

@@ -263,10 +263,11 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
   const double ged1 = P.grav_e[i] * P.d1[i];
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;
-    const int code = P.ce_code[q];
+    const int4 ci = P.ce_i4[q];  // {code, IA, IB, J1}
+    const int code = ci.x;
     const int side = code & 1;
-    const int ia = P.ce_ia[q], ib = P.ce_ib[q];
-    const int j1 = P.ce_j1[q], j2 = P.ce_j2[q];
+    const int ia = ci.y, ib = ci.z;
+    const int j1 = ci.w, j2 = P.ce_j2[q];
     R dij = (R)(0.5 * (P.d[j1] + P.d[j2]));
     double elij = 0.5 * (P.el[j1] + P.el[j2]);
     const int o = side == 0 ? ib : ia;  // the other cell of the edge
@@ -297,14 +298,11 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
         gb = side == 0 ? go : gi;
         const R uia = side == 0 ? ui : uo, via = side == 0 ? vi : vo;
         const R uib = side == 0 ? uo : ui, vib = side == 0 ? vo : vi;
-        R xij = Mh::s_xoa(P, q);
-        R yij = Mh::s_yoa(P, q);
-        uij1 = uia + ga.ux * xij + ga.uy * yij;
-        vij1 = via + ga.vx * xij + ga.vy * yij;
-        xij = Mh::s_xob(P, q);
-        yij = Mh::s_yob(P, q);
-        uij2 = uib + gb.ux * xij + gb.uy * yij;
-        vij2 = vib + gb.vx * xij + gb.vy * yij;
+        const auto G = Mh::s_geo(P, q);  // XOA, YOA, XOB, YOB
+        uij1 = uia + ga.ux * G.x + ga.uy * G.y;
+        vij1 = via + ga.vx * G.x + ga.vy * G.y;
+        uij2 = uib + gb.ux * G.z + gb.uy * G.w;
+        vij2 = vib + gb.vx * G.z + gb.vy * G.w;
         const R arto = Mh::art(P, o), cco = Mh::cc_hvc(P, o);
         arta = side == 0 ? arti : arto;
         artb = side == 0 ? arto : arti;
@@ -326,7 +324,8 @@ __device__ inline void advave_cell(const Dev& P, int i, double& xfo, double& yfo
       }
       R uij = half * (uij1 + uij2);
       R vij = half * (vij1 + vij2);
-      const R dltxc = Mh::s_dx(P, q), dltyc = Mh::s_dy(P, q);
+      const auto DD = Mh::s_dd(P, q);
+      const R dltxc = DD.x, dltyc = DD.y;
       R un = -uij * dltyc + vij * dltxc;
       R viscof1 = arta * sqrt(ga.ux * ga.ux + ga.vy * ga.vy + half * ((ga.uy + ga.vx) * (ga.uy + ga.vx)));
       R viscof2 = artb * sqrt(gb.ux * gb.ux + gb.vy * gb.vy + half * ((gb.uy + gb.vx) * (gb.uy + gb.vx)));
@@ -578,6 +577,13 @@ __global__ void k_edge_offsets_f32(const Dev P) {
   P.f.xo[e1 + e] = xb;
   P.f.yo[e1 + e] = yb;
 }
+// FP32 slot metrics packed per slot, each value rounded once from FP64
+__global__ void k_pack_slots_f32(const Dev P) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 3 * (size_t)(P.N + 1)) return;
+  P.f.ce_geo[q] = make_float4((float)P.ce_xoa[q], (float)P.ce_yoa[q], (float)P.ce_xob[q], (float)P.ce_yob[q]);
+  P.f.ce_dd[q] = make_float2((float)P.ce_dx[q], (float)P.ce_dy[q]);
+}
 void launch_make_f32(const Dev& P, cudaStream_t s) {
   auto cvt = [&](const double* a, float* b, size_t n) { k_d2f<<<296, 256, 0, s>>>(a, b, n); };
   const size_t n1 = P.N + 1, e1 = P.NE + 1;
@@ -595,6 +601,7 @@ void launch_make_f32(const Dev& P, cudaStream_t s) {
   cvt(P.ce_dx, P.f.ce_dx, 3 * n1);
   cvt(P.ce_dy, P.f.ce_dy, 3 * n1);
   cvt(P.hg, P.f.hg, 6 * (size_t)P.ncvs);
+  k_pack_slots_f32<<<nblk(3 * (P.N + 1), 256), 256, 0, s>>>(P);
 }
 void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);

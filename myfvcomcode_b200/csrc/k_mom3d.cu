@@ -209,8 +209,9 @@ __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib,
   const R half = (R)0.5, one = (R)1.0;
   const double* U = P.u + C3(P, 0, k);
   const double* V = P.v + C3(P, 0, k);
-  R xija = Mh::s_xoa(P, q), yija = Mh::s_yoa(P, q);
-  R xijb = Mh::s_xob(P, q), yijb = Mh::s_yob(P, q);
+  const auto G = Mh::s_geo(P, q);  // XOA, YOA, XOB, YOB
+  R xija = G.x, yija = G.y;
+  R xijb = G.z, yijb = G.w;
   G3<R> ga, gb;
   R uij1, vij1, uij2, vij2;
   R arta, artb, cca, ccb;
@@ -265,7 +266,8 @@ __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib,
   R txx = (ga.ux + gb.ux) * viscof;
   R tyy = (ga.vy + gb.vy) * viscof;
   R txy = half * (ga.uy + gb.uy + ga.vx + gb.vx) * viscof;
-  const R dltxc = Mh::s_dx(P, q), dltyc = Mh::s_dy(P, q);
+  const auto DD = Mh::s_dd(P, q);
+  const R dltxc = DD.x, dltyc = DD.y;
   EdgeFlux<R> f;
   f.fxx = dij * (txx * dltyc - txy * dltxc);
   f.fyy = dij * (txy * dltyc - tyy * dltxc);
@@ -310,7 +312,7 @@ __device__ inline void river3(const Dev& P, int i, int k, double& x, double& y) 
 // edges in ascending edge number.
 // -------------------------------------------------------------------------------------
 template <typename R, bool LIM>
-__global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
+__global__ void __launch_bounds__(256, (sizeof(R) == 4 && !LIM) ? 4 : 1) k_advection3d(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
   int kb, ke;
@@ -331,10 +333,11 @@ __global__ void __launch_bounds__(256) k_advection3d(const Dev P) {
     }
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;
-    const int code = P.ce_code[q], side = code & 1, isbc = (code >> 1) & 1;
-    const int ia = P.ce_ia[q], ib = P.ce_ib[q];
+    const int4 ci = P.ce_i4[q];  // {code, IA, IB, J1}
+    const int code = ci.x, side = code & 1, isbc = (code >> 1) & 1;
+    const int ia = ci.y, ib = ci.z;
     if (!(P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1)) continue;
-    const int j1 = P.ce_j1[q], j2 = P.ce_j2[q];
+    const int j1 = ci.w, j2 = P.ce_j2[q];
     R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
     EdgeFlux<R> f = edge_flux3<R, LIM, OWN>(P, q, ia, ib, k, dij, false, own, side);
     R isb = (R)isbc;
@@ -722,9 +725,10 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && !LIM) ? 4 : 1) k_adv_u
     }
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;
-    const int code = P.ce_code[q], side = code & 1, isbc = (code >> 1) & 1;
-    const int ia = P.ce_ia[q], ib = P.ce_ib[q];
-    const int j1 = P.ce_j1[q], j2 = P.ce_j2[q];
+    const int4 ci = P.ce_i4[q];  // {code, IA, IB, J1}
+    const int code = ci.x, side = code & 1, isbc = (code >> 1) & 1;
+    const int ia = ci.y, ib = ci.z;
+    const int j1 = ci.w, j2 = P.ce_j2[q];
     double elij = 0.5 * (P.egf[j1] + P.egf[j2]);
     R dij = (R)(0.5 * (P.dt[j1] * P.dz[N3(P, j1, k)] + P.dt[j2] * P.dz[N3(P, j2, k)]));
     if (P.iswetct[ia] * P.iswetc[ia] == 1 || P.iswetct[ib] * P.iswetc[ib] == 1) {
