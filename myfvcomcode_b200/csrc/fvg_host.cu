@@ -384,6 +384,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   UPI(isonb, m->isonb, m1); UPI(ntsn, m->ntsn, m1); UPI(ntve, m->ntve, m1);
   UPI(nbsn, m->nbsn, m1 * m->nbsn_cols); UPI(nbve, m->nbve, m1 * m->nbve_cols); UPI(nbvt, m->nbvt, m1 * m->nbve_cols);
   UPD(dltxtrie, m->dltxtrie, m1 * m->trie_cols); UPD(dltytrie, m->dltytrie, m1 * m->trie_cols);
+  P.trie_n = (int)(m1 * m->trie_cols);
   UPD(dltxecec, m->dltxecec, m1 * m->trie_cols); UPD(dltyecec, m->dltyecec, m1 * m->trie_cols);
   UPD(dltxnec, m->dltxnec, m1 * m->trie_cols); UPD(dltynec, m->dltynec, m1 * m->trie_cols);
   UP3(z, m->z, m1, ms); UP3(zz, m->zz, m1, ms); UP3(dz, m->dz, m1, ms); UP3(dzz, m->dzz, m1, ms);
@@ -1001,9 +1002,11 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     if ((rc = dalloc(h, &f.a2u, 4 * n1))) return fail(rc);
     for (float** pp : {&f.ce_xoa, &f.ce_yoa, &f.ce_xob, &f.ce_yob, &f.ce_dx, &f.ce_dy})
       if ((rc = dalloc(h, pp, 3 * n1))) return fail(rc);
-    if ((rc = dalloc(h, &f.hg, 6 * (size_t)P.ncvs))) return fail(rc);
     if ((rc = dalloc(h, (float**)&f.ce_geo, 4 * 3 * n1))) return fail(rc);
     if ((rc = dalloc(h, (float**)&f.ce_dd, 2 * 3 * n1))) return fail(rc);
+    if ((rc = dalloc(h, (float**)&f.hg4, 4 * (size_t)P.ncvs))) return fail(rc);
+    if ((rc = dalloc(h, (float**)&f.hg2, 2 * (size_t)P.ncvs))) return fail(rc);
+    if ((rc = dalloc(h, (float**)&f.trie, 2 * (size_t)P.trie_n))) return fail(rc);
     launch_make_f32(P, h->stream);
     CK(cudaGetLastError());
   }

@@ -47,10 +47,14 @@ struct F32 {
   float2* ex2;
   float *xo, *yo, *dltxc, *dltyc, *art, *cc_hvc, *a1u, *a2u;
   float *ce_xoa, *ce_yoa, *ce_xob, *ce_yob, *ce_dx, *ce_dy;
-  float* hg;  // the half-edge metrics by position, as Dev::hg
   // The slot table's metrics packed per slot: {XOA, YOA, XOB, YOB} and {DX, DY}
   float4* ce_geo;
   float2* ce_dd;
+  // The half-edge metrics packed per position: {DLTXE, DLTYE, XNCVE a, YNCVE a} and
+  // {XNCVE b, YNCVE b}; the ring-edge metrics per (ring slot, node): {DLTYTRIE, DLTXTRIE}
+  float4* hg4;
+  float2* hg2;
+  float2* trie;
 };
 
 // Input and output scaling of the learned closure's network, and the training envelope.
@@ -90,6 +94,7 @@ struct Dev {
   const double *vx, *vy, *h, *art1, *art2, *grav_n, *nn_hvc, *cos_sita, *sin_sita, *phpn;
   const int *isonb, *ntsn, *ntve, *nbsn, *nbve, *nbvt;
   const double *dltxtrie, *dltytrie, *dltxecec, *dltyecec, *dltxnec, *dltynec;
+  int trie_n;  // entries of DLTXTRIE/DLTYTRIE: (M+1) x ring columns
   const double *z, *zz, *dz, *dzz;  // 3-D node (ms stride)
   // ----- mesh, cells -----
   const double *xc, *yc, *art, *cor, *grav_e, *cc_hvc, *cc_sponge, *cc_z0b, *epor, *iucp;
@@ -302,7 +307,6 @@ template <> struct Mesh<float> {
   __device__ static float* alfa3(const Dev& P, int q) { return P.f.alfa3[q]; }
   __device__ static float* g3(const Dev& P, int q) { return P.f.g3[q]; }
   __device__ static float2* ex2(const Dev& P) { return P.f.ex2; }
-  __device__ static float hg(const Dev& P, int j, size_t pos) { return P.f.hg[(size_t)j * P.ncvs + pos]; }
 };
 // Limited schemes (advave_edge_gcn.F:226-229, 300-303, 340-357): the slope limiter of one
 // cell and edge, min(ALFA, min(1, |U(IA)-U(IB)| / |U'+EPSILON|)), EPSILON of the form's type.

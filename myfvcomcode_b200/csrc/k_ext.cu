@@ -584,6 +584,16 @@ __global__ void k_pack_slots_f32(const Dev P) {
   P.f.ce_geo[q] = make_float4((float)P.ce_xoa[q], (float)P.ce_yoa[q], (float)P.ce_xob[q], (float)P.ce_yob[q]);
   P.f.ce_dd[q] = make_float2((float)P.ce_dx[q], (float)P.ce_dy[q]);
 }
+// FP32 half-edge metrics per position and ring-edge metrics, packed, rounded once
+__global__ void k_pack_he_f32(const Dev P) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t pl = P.ncvs;
+  if (q < pl) {
+    P.f.hg4[q] = make_float4((float)P.hg[q], (float)P.hg[pl + q], (float)P.hg[2 * pl + q], (float)P.hg[3 * pl + q]);
+    P.f.hg2[q] = make_float2((float)P.hg[4 * pl + q], (float)P.hg[5 * pl + q]);
+  }
+  if (q < (size_t)P.trie_n) P.f.trie[q] = make_float2((float)P.dltytrie[q], (float)P.dltxtrie[q]);
+}
 void launch_make_f32(const Dev& P, cudaStream_t s) {
   auto cvt = [&](const double* a, float* b, size_t n) { k_d2f<<<296, 256, 0, s>>>(a, b, n); };
   const size_t n1 = P.N + 1, e1 = P.NE + 1;
@@ -600,8 +610,8 @@ void launch_make_f32(const Dev& P, cudaStream_t s) {
   cvt(P.ce_yob, P.f.ce_yob, 3 * n1);
   cvt(P.ce_dx, P.f.ce_dx, 3 * n1);
   cvt(P.ce_dy, P.f.ce_dy, 3 * n1);
-  cvt(P.hg, P.f.hg, 6 * (size_t)P.ncvs);
   k_pack_slots_f32<<<nblk(3 * (P.N + 1), 256), 256, 0, s>>>(P);
+  k_pack_he_f32<<<nblk(P.ncvs > P.trie_n ? P.ncvs : P.trie_n, 256), 256, 0, s>>>(P);
 }
 void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);

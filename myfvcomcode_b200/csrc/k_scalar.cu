@@ -139,7 +139,15 @@ __global__ void __launch_bounds__(256) k_grad(const Dev P, int which) {
     for (int j = 1; j <= nt - 1; ++j) {
       const int i2 = NBSN(P, i, j + 1);
       const int w2 = which == 0 ? 1 : P.iswetn[i2];
-      const R ty = (R)TRIEY(P, i, j), tx = (R)TRIEX(P, i, j);
+      R ty, tx;
+      if constexpr (sizeof(R) == 4) {
+        const float2 tr = P.f.trie[(size_t)(j - 1) * (P.M + 1) + i];
+        ty = tr.x;
+        tx = tr.y;
+      } else {
+        ty = TRIEY(P, i, j);
+        tx = TRIEX(P, i, j);
+      }
       for (int t = 0; t < 2; ++t) {
         const R q2 = (R)Q[t][i2];
         if (j >= 2) {
@@ -302,8 +310,14 @@ struct HeGeo {
 template <typename R>
 __device__ inline HeGeo<R> he_geo(const Dev& P, size_t pos) {
   typedef Mesh<R> Mh;
-  return HeGeo<R>{Mh::hg(P, 0, pos), Mh::hg(P, 1, pos), Mh::hg(P, 2, pos),
-                  Mh::hg(P, 3, pos), Mh::hg(P, 4, pos), Mh::hg(P, 5, pos)};
+  if constexpr (sizeof(R) == 4) {
+    const float4 a = P.f.hg4[pos];
+    const float2 b = P.f.hg2[pos];
+    return HeGeo<R>{a.x, a.y, a.z, a.w, b.x, b.y};
+  } else {
+    return HeGeo<R>{Mh::hg(P, 0, pos), Mh::hg(P, 1, pos), Mh::hg(P, 2, pos),
+                    Mh::hg(P, 3, pos), Mh::hg(P, 4, pos), Mh::hg(P, 5, pos)};
+  }
 }
 
 // EXFLUX of a half-edge with metrics g for tracer t, in R; a and b are the positions of
