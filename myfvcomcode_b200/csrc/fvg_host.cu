@@ -397,6 +397,12 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
     UPD(h1, h1.data(), n1);
   }
   UPI(nv, m->nv, n1 * 3); UPI(nbe, m->nbe, n1 * 3); UPI(isbce, m->isbce, n1);
+  {
+    std::vector<int> nb4(4 * n1, 0);
+    for (size_t c = 0; c < n1; ++c)
+      for (int j = 0; j < 3; ++j) nb4[4 * c + j] = m->nbe[j * n1 + c];
+    UPI(nbe4, nb4.data(), nb4.size());
+  }
   UPD(a1u, m->a1u, n1 * 4); UPD(a2u, m->a2u, n1 * 4); UPD(awx, m->awx, n1 * 3); UPD(awy, m->awy, n1 * 3);
   UP3(z1, m->z1, n1, ns); UP3(zz1, m->zz1, n1, ns); UP3(dz1, m->dz1, n1, ns); UP3(dzz1, m->dzz1, n1, ns);
   UPI(iec, m->iec, e1 * 2); UPI(ienode, m->ienode, e1 * 2); UPI(isbc, m->isbc, e1);
@@ -1007,6 +1013,8 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     if ((rc = dalloc(h, (float**)&f.hg4, 4 * (size_t)P.ncvs))) return fail(rc);
     if ((rc = dalloc(h, (float**)&f.hg2, 2 * (size_t)P.ncvs))) return fail(rc);
     if ((rc = dalloc(h, (float**)&f.trie, 2 * (size_t)P.trie_n))) return fail(rc);
+    if ((rc = dalloc(h, (float**)&f.a1u4, 4 * n1))) return fail(rc);
+    if ((rc = dalloc(h, (float**)&f.a2u4, 4 * n1))) return fail(rc);
     launch_make_f32(P, h->stream);
     CK(cudaGetLastError());
   }

@@ -55,6 +55,8 @@ struct F32 {
   float4* hg4;
   float2* hg2;
   float2* trie;
+  // A1U and A2U of each cell packed: {A(c,1), A(c,2), A(c,3), A(c,4)}
+  float4 *a1u4, *a2u4;
 };
 
 // Input and output scaling of the learned closure's network, and the training envelope.
@@ -101,6 +103,7 @@ struct Dev {
   const double *sin_alpha, *cos_alpha;
   double* h1;  // H1(0) is reset by EXTUV_EDGE
   const int *nv, *nbe, *isbce;
+  const int4* nbe4;  // NBE of each cell packed: {NBE(c,1), NBE(c,2), NBE(c,3), 0}
   const double *a1u, *a2u, *awx, *awy;
   const double *z1, *zz1, *dz1, *dzz1;  // 3-D cell (ns stride)
   // ----- edges / half-edges -----
@@ -308,6 +311,26 @@ template <> struct Mesh<float> {
   __device__ static float* g3(const Dev& P, int q) { return P.f.g3[q]; }
   __device__ static float2* ex2(const Dev& P) { return P.f.ex2; }
 };
+// The cell's NBE and its least-squares coefficients A1U(c,1..4), A2U(c,1..4) in the
+// form's type (FP32: one packed load each).
+template <typename R>
+__device__ inline void lsq_coef(const Dev& P, int c, int& k1, int& k2, int& k3, R* a, R* b) {
+  const int4 nb = P.nbe4[c];
+  k1 = nb.x;
+  k2 = nb.y;
+  k3 = nb.z;
+  if constexpr (sizeof(R) == 4) {
+    const float4 A = P.f.a1u4[c], B = P.f.a2u4[c];
+    a[0] = A.x; a[1] = A.y; a[2] = A.z; a[3] = A.w;
+    b[0] = B.x; b[1] = B.y; b[2] = B.z; b[3] = B.w;
+  } else {
+    const size_t n1 = P.N + 1;
+    for (int j = 0; j < 4; ++j) {
+      a[j] = P.a1u[j * n1 + c];
+      b[j] = P.a2u[j * n1 + c];
+    }
+  }
+}
 // Limited schemes (advave_edge_gcn.F:226-229, 300-303, 340-357): the slope limiter of one
 // cell and edge, min(ALFA, min(1, |U(IA)-U(IB)| / |U'+EPSILON|)), EPSILON of the form's type.
 template <typename R>

@@ -30,10 +30,10 @@ struct Grad {
 template <typename R>
 __device__ inline Grad<R> cell_grad(const Dev& P, int c, const double* U, const double* V) {
   typedef Mesh<R> Mh;
-  const size_t n1 = P.N + 1;
-  int k1 = P.nbe[c], k2 = P.nbe[n1 + c], k3 = P.nbe[2 * n1 + c];
-  R a1 = Mh::a1u(P, c), a2 = Mh::a1u(P, n1 + c), a3 = Mh::a1u(P, 2 * n1 + c), a4 = Mh::a1u(P, 3 * n1 + c);
-  R b1 = Mh::a2u(P, c), b2 = Mh::a2u(P, n1 + c), b3 = Mh::a2u(P, 2 * n1 + c), b4 = Mh::a2u(P, 3 * n1 + c);
+  int k1, k2, k3;
+  R A[4], B[4];
+  lsq_coef<R>(P, c, k1, k2, k3, A, B);
+  const R a1 = A[0], a2 = A[1], a3 = A[2], a4 = A[3], b1 = B[0], b2 = B[1], b3 = B[2], b4 = B[3];
   R u0 = (R)U[c], u1 = (R)U[k1], u2 = (R)U[k2], u3 = (R)U[k3];
   R v0 = (R)V[c], v1 = (R)V[k1], v2 = (R)V[k2], v3 = (R)V[k3];
   if (P.gcy && (k1 == 0 || k2 == 0 || k3 == 0)) {
@@ -593,6 +593,11 @@ __global__ void k_pack_he_f32(const Dev P) {
     P.f.hg2[q] = make_float2((float)P.hg[4 * pl + q], (float)P.hg[5 * pl + q]);
   }
   if (q < (size_t)P.trie_n) P.f.trie[q] = make_float2((float)P.dltytrie[q], (float)P.dltxtrie[q]);
+  const size_t n1 = P.N + 1;
+  if (q < n1) {
+    P.f.a1u4[q] = make_float4((float)P.a1u[q], (float)P.a1u[n1 + q], (float)P.a1u[2 * n1 + q], (float)P.a1u[3 * n1 + q]);
+    P.f.a2u4[q] = make_float4((float)P.a2u[q], (float)P.a2u[n1 + q], (float)P.a2u[2 * n1 + q], (float)P.a2u[3 * n1 + q]);
+  }
 }
 void launch_make_f32(const Dev& P, cudaStream_t s) {
   auto cvt = [&](const double* a, float* b, size_t n) { k_d2f<<<296, 256, 0, s>>>(a, b, n); };
@@ -611,7 +616,9 @@ void launch_make_f32(const Dev& P, cudaStream_t s) {
   cvt(P.ce_dx, P.f.ce_dx, 3 * n1);
   cvt(P.ce_dy, P.f.ce_dy, 3 * n1);
   k_pack_slots_f32<<<nblk(3 * (P.N + 1), 256), 256, 0, s>>>(P);
-  k_pack_he_f32<<<nblk(P.ncvs > P.trie_n ? P.ncvs : P.trie_n, 256), 256, 0, s>>>(P);
+  size_t npk = P.ncvs > P.trie_n ? P.ncvs : P.trie_n;
+  if ((size_t)P.N + 1 > npk) npk = P.N + 1;
+  k_pack_he_f32<<<nblk(npk, 256), 256, 0, s>>>(P);
 }
 void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);

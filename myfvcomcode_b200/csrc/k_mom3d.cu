@@ -105,10 +105,10 @@ struct G3 {
 template <typename R>
 __device__ inline G3<R> grad3(const Dev& P, int c, const double* U, const double* V) {
   typedef Mesh<R> Mh;
-  const size_t n1 = P.N + 1;
-  int k1 = P.nbe[c], k2 = P.nbe[n1 + c], k3 = P.nbe[2 * n1 + c];
-  R a1 = Mh::a1u(P, c), a2 = Mh::a1u(P, n1 + c), a3 = Mh::a1u(P, 2 * n1 + c), a4 = Mh::a1u(P, 3 * n1 + c);
-  R b1 = Mh::a2u(P, c), b2 = Mh::a2u(P, n1 + c), b3 = Mh::a2u(P, 2 * n1 + c), b4 = Mh::a2u(P, 3 * n1 + c);
+  int k1, k2, k3;
+  R A[4], B[4];
+  lsq_coef<R>(P, c, k1, k2, k3, A, B);
+  const R a1 = A[0], a2 = A[1], a3 = A[2], a4 = A[3], b1 = B[0], b2 = B[1], b3 = B[2], b4 = B[3];
   R u0 = (R)U[c], u1 = (R)U[k1], u2 = (R)U[k2], u3 = (R)U[k3];
   R v0 = (R)V[c], v1 = (R)V[k1], v2 = (R)V[k2], v3 = (R)V[k3];
   if (P.gcy && (k1 == 0 || k2 == 0 || k3 == 0)) {
