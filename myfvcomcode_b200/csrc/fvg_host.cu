@@ -211,16 +211,19 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
       }
       const int prev =
           stage > 0 ? (EN_FINISH_PREV | (p.wetting_drying_on ? EN_WET_PREV : 0) | ((K == 1 ? 4 : K - 1) << 8)) : 0;
-      launch_ext_node(Q, s, iext, K, EN_EXTEL | EN_BC | EN_GRAD | (K == 1 ? EN_COPY_ELRK : 0) | prev);
+      // stage > 0: each kernel of the loop overlaps its launch with the previous one's tail
+      const int pdl = stage > 0 ? 1 : 0;
+      launch_ext_node(Q, s, iext, K, EN_EXTEL | EN_BC | EN_GRAD | (K == 1 ? EN_COPY_ELRK : 0) | prev, pdl);
       mk.mark(s, G_EXT_NODE);
       if (p.wetting_drying_on) {
-        launch_wet_cells(Q, s);  // its node part opens the next stage's node kernel
+        launch_wet_cells(Q, s, 1);  // its node part opens the next stage's node kernel
         mk.mark(s, G_WET);
       }
       if (P.limiter) launch_alfa2(Q, s);
       launch_ext_cell(Q, s, iext, K,
                       (p.wetting_drying_on ? 0 : EC_N2E) | EC_FLUXOBN | EC_ADVAVE | EC_EXTUV | EC_BC2 |
-                          (K == 1 ? EC_COPY_RK : 0) | EC_FINISH);
+                          (K == 1 ? EC_COPY_RK : 0) | EC_FINISH,
+                      P.limiter ? 0 : 1);
       mk.mark(s, G_EXT_CELL);
     }
   }

@@ -374,10 +374,13 @@ enum ExtNodeParts { EN_EXTEL = 1, EN_BC = 2, EN_COPY_ELRK = 4, EN_GRAD = 8, EN_F
 enum ExtCellParts { EC_N2E = 1, EC_FLUXOBN = 2, EC_ADVAVE = 4, EC_EXTUV = 8, EC_BC2 = 16, EC_COPY_RK = 32,
                     EC_INT_ADVAVE = 64, EC_FINISH = 128 };
 void launch_ext_finish(const Dev& P, cudaStream_t s, int K, int wet_prev);
-void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts);
+// pdl: launched as a programmatic dependent of the previous kernel in the stream (the
+// fused external loop); the kernel waits for that kernel's completion before it touches
+// memory, while its blocks are scheduled during the previous kernel's tail.
+void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts, int pdl = 0);
 void launch_wet_judge(const Dev& P, cudaStream_t s);
-void launch_wet_cells(const Dev& P, cudaStream_t s);
-void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts);
+void launch_wet_cells(const Dev& P, cudaStream_t s, int pdl = 0);
+void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts, int pdl = 0);
 void launch_alfa2(const Dev& P, cudaStream_t s);
 void launch_ext_update(const Dev& P, cudaStream_t s, int K);
 void launch_begin_step(const Dev& P, cudaStream_t s);

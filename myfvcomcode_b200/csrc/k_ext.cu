@@ -10,6 +10,28 @@
 
 namespace fvg {
 
+// Programmatic dependent launch: wait until the previous kernel in the stream has
+// completed and its writes are visible (a no-op when the kernel was launched without the
+// attribute), then let the next kernel's blocks be scheduled during this one's tail.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... KArgs, typename... Args>
+static void launch_maybe_pdl(int pdl, void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 __device__ __constant__ double dAlphaRK[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
 const double kAlphaRK[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
 #define ONE_THIRD (1.0 / 3.0)
@@ -160,6 +182,7 @@ __global__ void k_alfa2(const Dev P) {
 }
 
 __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
+  pdl_enter();
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   // threads 1..M take the nodes, threads M+1..M+N the cells' least-squares gradients of
   // the current UA, VA for ADVAVE of this stage (one job per thread)
@@ -226,6 +249,7 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
 // forms itself from h and ELF.  Then nodes: the node flag and the clamp of ELF.
 // -------------------------------------------------------------------------------------
 __global__ void k_wet_cells(const Dev P) {
+  pdl_enter();
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
   int n1 = P.nv[i], n2 = P.nv[(size_t)(P.N + 1) + i], n3 = P.nv[(size_t)2 * (P.N + 1) + i];
@@ -401,6 +425,7 @@ __device__ inline void bc_solid(const Dev& P, int i, int rj, double& uu, double&
 // -------------------------------------------------------------------------------------
 template <typename R, bool LIM>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_ext_cell(const Dev P, int iext, int K, int parts) {
+  pdl_enter();
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
   const size_t n1 = P.N + 1;
@@ -543,9 +568,9 @@ __global__ void k_begin_step(const Dev P, int advance) {
 
 static inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
-void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
+void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts, int pdl) {
   int n = (parts & EN_GRAD) ? P.M + P.N : P.M;
-  k_ext_node<<<nblk(n, 256), 256, 0, s>>>(P, iext, K, parts);
+  launch_maybe_pdl(pdl, k_ext_node, dim3(nblk(n, 256)), dim3(256), s, P, iext, K, parts);
 }
 void launch_ext_prep(const Dev& P, cudaStream_t s) { k_ext_prep<<<nblk(P.N, 256), 256, 0, s>>>(P); }
 void launch_alfa2(const Dev& P, cudaStream_t s) {
@@ -624,12 +649,16 @@ void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);
   k_wet_nodes<<<nblk(P.M, 256), 256, 0, s>>>(P);
 }
-void launch_wet_cells(const Dev& P, cudaStream_t s) { k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P); }
-void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts) {
+void launch_wet_cells(const Dev& P, cudaStream_t s, int pdl) {
+  launch_maybe_pdl(pdl, k_wet_cells, dim3(nblk(P.N, 256)), dim3(256), s, P);
+}
+void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts, int pdl) {
+  void (*k)(const Dev, int, int, int);
   if (P.prec)
-    (P.limiter ? k_ext_cell<float, true> : k_ext_cell<float, false>)<<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
+    k = P.limiter ? k_ext_cell<float, true> : k_ext_cell<float, false>;
   else
-    (P.limiter ? k_ext_cell<double, true> : k_ext_cell<double, false>)<<<nblk(P.N, 128), 128, 0, s>>>(P, iext, K, parts);
+    k = P.limiter ? k_ext_cell<double, true> : k_ext_cell<double, false>;
+  launch_maybe_pdl(pdl, k, dim3(nblk(P.N, 128)), dim3(128), s, P, iext, K, parts);
 }
 void launch_ext_update(const Dev& P, cudaStream_t s, int K) {
   int n = P.M > P.N ? P.M : P.N;
