@@ -164,8 +164,9 @@ def barrier(pg, local):
         pg.barrier()
 
 
-def cpu_rate(case, seconds, warm=1, cap=None):
-    """Oracle (FP64 CPU restatement) throughput on all host threads, bounded sample."""
+def cpu_rate(case, seconds, warm=1, cap=None, keep=False):
+    """Oracle (FP64 CPU restatement) throughput on all host threads, bounded sample.
+    With ``keep`` the stepped oracle is returned too (for the parity check)."""
     from oracle.oracle import Oracle, max_threads
     o = Oracle(case)
     o.run(warm)
@@ -181,7 +182,64 @@ def cpu_rate(case, seconds, warm=1, cap=None):
     g = case["grid"]
     steps = n + 1
     rate = g["N"] * (g["KB"] - 1) * steps / (dt + t1)
+    if keep:
+        return rate, max_threads(), steps, dt + t1, o
+    o.close()
     return rate, max_threads(), steps, dt + t1
+
+
+def cpu_rate_single_core(case):
+    """One internal step of the oracle on one host thread (after one warm-up step)."""
+    from oracle.oracle import Oracle, max_threads, set_threads
+    nt = max_threads()
+    set_threads(1)
+    try:
+        o = Oracle(case)
+        o.run(1)
+        t0 = time.perf_counter()
+        o.run(1)
+        dt = time.perf_counter() - t0
+        o.close()
+    finally:
+        set_threads(nt)
+    g = case["grid"]
+    return g["N"] * (g["KB"] - 1) / dt, dt
+
+
+PARITY_FIELDS = ("el", "ua", "va", "u", "v", "w", "t1", "s1", "q2", "q2l", "km", "kh")
+
+
+def parity_vs_oracle(case, ora, steps):
+    """The plain FP64 library stepped ``steps`` internal steps from the same cold start as
+    the oracle ``ora``: per field the max-normalised difference max|a-b|/max|b|, the
+    largest per-element relative difference |a-b|/max(|b|, 1e-6 max|b|), and whether the
+    two are bitwise equal; the wet/dry flags compared exactly."""
+    import numpy as np
+    from myfvcomcode_b200.engine import Fvcom
+    gpu = Fvcom(case)
+    gpu.run(steps)
+    g = case["grid"]
+    node_fields = ("el", "t1", "s1", "q2", "q2l", "km", "kh")
+    out, bitwise = {}, True
+    for n in PARITY_FIELDS:
+        a, b = gpu.get(n), ora.get(n)
+        L = g["M"] + 1 if n in node_fields else g["N"] + 1
+        a = a.reshape((L, -1), order="F")[1:]
+        b = b.reshape((L, -1), order="F")[1:]
+        d = np.abs(a - b)
+        scale = float(np.abs(b).max())
+        floor = max(1e-6 * scale, 1e-300)
+        eq = bool(np.array_equal(a, b))
+        bitwise = bitwise and eq
+        out[n] = {"max_norm": float(d.max()) / max(scale, 1e-300),
+                  "per_element": float((d / np.maximum(np.abs(b), floor)).max()), "bitwise": eq}
+    wet = all(np.array_equal(gpu.get(n), ora.get(n)) for n in ("iswetn", "iswetc"))
+    same_clock = gpu.clock() == ora.clock()
+    gpu.close()
+    worst = max(v["max_norm"] for v in out.values())
+    return {"steps": steps, "against": "oracle (FP64 CPU restatement), same cold start",
+            "form": "plain FP64", "max_rel": worst, "bitwise": bitwise, "wet_dry_flags_equal": wet,
+            "clock_equal": same_clock, "fields": out}
 
 
 def run_ensemble(args, world, rank, local, pg):
@@ -276,6 +334,47 @@ def run_ensemble(args, world, rank, local, pg):
         pg.close()
 
 
+def e2e_leg(f, case, args, pg, local, world):
+    """The metric end to end through the public C ABI with host buffers: per step the wind
+    stress is copied in from pinned host memory, fvg_internal_step runs, and the surface
+    elevation is read back; wall clock, max over ranks."""
+    import ctypes as C
+    import torch
+    from myfvcomcode_b200.abi import wind_stress
+    g = case["grid"]
+    lib = f.lib
+    ws = wind_stress(case)
+    n1 = g["N"] + 1
+    hx = torch.zeros(n1, dtype=torch.float64).pin_memory()
+    hy = torch.zeros(n1, dtype=torch.float64).pin_memory()
+    if ws is not None:
+        hx.copy_(torch.from_numpy(ws[0]))
+        hy.copy_(torch.from_numpy(ws[1]))
+    hel = torch.zeros(g["M"] + 1, dtype=torch.float64).pin_memory()
+    dp = C.POINTER(C.c_double)
+    lib.fvg_set_field.argtypes = [C.c_void_p, C.c_char_p, dp, C.c_int64]
+    lib.fvg_get_field.argtypes = [C.c_void_p, C.c_char_p, dp, C.c_int64]
+    px = C.cast(hx.data_ptr(), dp)
+    py = C.cast(hy.data_ptr(), dp)
+    pe = C.cast(hel.data_ptr(), dp)
+    ne = max(3, args.steps // 2)
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        rc = lib.fvg_set_field(f.h, b"wstress_x", px, n1)
+        rc |= lib.fvg_set_field(f.h, b"wstress_y", py, n1)
+        rc |= lib.fvg_internal_step(f.h)
+        rc |= lib.fvg_get_field(f.h, b"el", pe, g["M"] + 1)
+        if rc:
+            raise SystemExit("end-to-end leg: a C-ABI call failed")
+    te = time.perf_counter() - t0
+    te = reduce_max(pg, te, local)
+    return {"value": g["N"] * (g["KB"] - 1) * ne * world / te, "unit": "cell-layer updates/s",
+            "h2d_bytes_per_step": 2 * n1 * 8, "d2h_bytes_per_step": (g["M"] + 1) * 8,
+            "steps": ne, "api": "fvg_set_field(wstress_x/y) + fvg_internal_step + fvg_get_field(el), "
+                                "pinned host buffers, wall clock"}
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
@@ -293,6 +392,7 @@ def main():
             return
         steps = max(1, min(args.steps, 5))
         rate, cores, n, secs = cpu_rate(case, 1e9, warm=min(max(args.warmup, 0), 1), cap=steps - 1)
+        rate1, secs1 = cpu_rate_single_core(case)
         line = {"impl": "reference", "metric": metric, "value": rate, "unit": "cell-layer updates/s",
                 "n_gpus": args.gpus, "steps": n, "warmup": min(args.warmup, 1),
                 "ms_per_step": 1e3 * secs / n, "higher_is_better": True, "scaling": "weak",
@@ -300,7 +400,10 @@ def main():
                 "cpu_baseline": {"value": rate, "unit": "cell-layer updates/s", "cores": cores, "kind": "port",
                                  "sample": "%d internal steps of the full workload after one warm-up step, "
                                            "FP64 CPU restatement of the reference (OpenMP over layers and "
-                                           "columns)" % n},
+                                           "columns)" % n,
+                                 "single_core": {"value": rate1, "unit": "cell-layer updates/s", "cores": 1,
+                                                 "sample": "1 internal step (%.1f s) after one warm-up "
+                                                           "step, one host thread" % secs1}},
                 "e2e": {"value": rate, "unit": "cell-layer updates/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -353,6 +456,7 @@ def main():
     value = cells_layers * args.steps * world / (t_ms / 1e3)
 
     plain = None
+    fp = None
     if args.precision != "fp64" and not args.no_plain:
         fp, tp_ms, _ = timed_handle("fp64")
         plain = {"value": cells_layers * args.steps * world / (tp_ms / 1e3), "ms_per_step": tp_ms / args.steps,
@@ -363,11 +467,21 @@ def main():
         n_done = fp.clock()[0]
         if f.clock()[0] == n_done:
             plain["error_of_chosen_form"] = dict(compare(fp, f), internal_steps=n_done)
-        fp.close()
+        # The one-day error report is embedded only when it was made from the library
+        # sources and case generator this run is built from (its recorded stamp).
+        from myfvcomcode_b200.precision_report import sources_stamp
         day = os.path.join(ROOT, "myfvcomcode_b200", "data", "precision_error_coastal200k_k40_1day.json")
         if os.path.exists(day):
             with open(day) as fh:
-                plain["error_after_1_day"] = json.load(fh).get("errors_vs_fp64")
+                rep = json.load(fh)
+            stamp = sources_stamp()
+            if rep.get("sources_sha256") == stamp:
+                plain["error_after_1_day"] = {"errors_vs_fp64": rep.get("errors_vs_fp64"),
+                                              "budget_drift": rep.get("budget_drift"),
+                                              "sources_sha256": stamp, "made_at_commit": rep.get("commit")}
+            else:
+                plain["error_after_1_day"] = {"stale": "report made from other sources (%s), this build %s"
+                                              % (str(rep.get("sources_sha256"))[:12], stamp[:12])}
         cfg["plain_fp64"] = plain
 
     # per-kernel-group device time (plain launches with events between groups)
@@ -396,42 +510,23 @@ def main():
 
     e2e = None
     if not args.no_e2e:
-        from myfvcomcode_b200.abi import wind_stress
-        ws = wind_stress(case)
-        n1 = g["N"] + 1
-        hx = torch.zeros(n1, dtype=torch.float64).pin_memory()
-        hy = torch.zeros(n1, dtype=torch.float64).pin_memory()
-        if ws is not None:
-            hx.copy_(torch.from_numpy(ws[0]))
-            hy.copy_(torch.from_numpy(ws[1]))
-        hel = torch.zeros(g["M"] + 1, dtype=torch.float64).pin_memory()
-        dp = C.POINTER(C.c_double)
-        lib.fvg_set_field.argtypes = [C.c_void_p, C.c_char_p, dp, C.c_int64]
-        lib.fvg_get_field.argtypes = [C.c_void_p, C.c_char_p, dp, C.c_int64]
-        px = C.cast(hx.data_ptr(), dp)
-        py = C.cast(hy.data_ptr(), dp)
-        pe = C.cast(hel.data_ptr(), dp)
-        ne = max(3, args.steps // 2)
-        barrier(pg, local)
-        t0 = time.perf_counter()
-        for _ in range(ne):
-            lib.fvg_set_field(f.h, b"wstress_x", px, n1)
-            lib.fvg_set_field(f.h, b"wstress_y", py, n1)
-            lib.fvg_internal_step(f.h)
-            lib.fvg_get_field(f.h, b"el", pe, g["M"] + 1)
-        te = time.perf_counter() - t0
-        te = reduce_max(pg, te, local)
-        e2e = {"value": cells_layers * ne * world / te, "unit": "cell-layer updates/s",
-               "h2d_bytes_per_step": 2 * n1 * 8, "d2h_bytes_per_step": (g["M"] + 1) * 8,
-               "steps": ne, "api": "fvg_set_field(wstress_x/y) + fvg_internal_step + fvg_get_field(el), "
-                                   "pinned host buffers, wall clock"}
+        e2e = e2e_leg(f, case, args, pg, local, world)
+    if plain is not None and fp is not None:
+        if not args.no_e2e:
+            plain["e2e"] = e2e_leg(fp, case, args, pg, local, world)
+        fp.close()
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, n, secs = cpu_rate(case, args.cpu_seconds)
+        rate, cores, n, secs, ora = cpu_rate(case, args.cpu_seconds, keep=True)
         cpu = {"value": rate, "unit": "cell-layer updates/s", "cores": cores, "kind": "port",
                "sample": "%d internal steps (%.1f s) of the full workload after one warm-up step, FP64 "
                          "CPU restatement of the reference on %d threads" % (n, secs, cores)}
+        # the oracle of the CPU leg has stepped the full workload from its cold start:
+        # the plain FP64 library, stepped as far from the same cold start, against it
+        parity = parity_vs_oracle(case, ora, ora.clock()[0])
+        ora.close()
 
     if rank == 0:
         line = {"metric": metric, "value": value, "unit": "cell-layer updates/s", "n_gpus": world,
@@ -439,7 +534,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "f32 fluxes, f64 state",
                 "data": "synthetic", "config": cfg, "clocks": clocks, "e2e": e2e, "roofline": roof,
-                "cpu_baseline": cpu, "gpu_launches": int(lib.fvg_kernels_per_step(f.h)) * args.steps}
+                "cpu_baseline": cpu, "parity": parity,
+                "gpu_launches": int(lib.fvg_kernels_per_step(f.h)) * args.steps}
         print(json.dumps(line), flush=True)
     f.close()
     if pg is not None:

@@ -294,8 +294,11 @@ int fvg_mlp_forward_bf16(fvg_mlp* q, const float* x, int32_t n, float* out);
 #define FVG_CLOSURE_NORM_FLOATS 55
 int fvg_set_closure(fvg_handle* h, int32_t mode, const float* params, int32_t nparams, const float* norm,
                     int32_t nnorm);
-/* Columns that used the network in the last step, and the count of tensor-core waits
-   that ran out (0 unless the device misbehaved; results are then incomplete). */
+/* Columns that used the network in the last step, and the closure's error word: 0, or
+   nonzero once a bounded tensor-core wait ran out (1; 2 if the wait for the outstanding
+   MMAs before freeing tensor memory ran out as well).  Rows of a block whose wait ran
+   out take MY2.5's values, and fvg_run / fvg_internal_step return FVG_ERR_TIMEOUT while
+   the word is set; fvg_set_closure clears it. */
 int fvg_closure_status(fvg_handle* h, int32_t* columns_on_network, int32_t* wait_timeouts);
 /* Launch shape of the 3-D gather kernels (results do not depend on it):
    "col_threads" = entities (threads) per block, 32..256 in steps of 32 (default 128);
@@ -341,9 +344,12 @@ int fvg_budget(fvg_handle* h, double out[3]);
    and dz are (0:M, >=KBM1) column-major with leading dimension M+1 (FVCOM's layout, ghost
    row 0), all in device memory of the current device.  The scratch is a fixed 393,240-
    byte device array: M above 4,194,304 returns FVG_ERR_CAPACITY; KBM1 must be 1..63.
-   Runs on `stream` (a cudaStream_t; NULL for the default stream) and waits for it.  The
-   first call on a device sets up the scratch address; make it before any stream capture.
-   Calls that overlap on one device share the scratch and race. */
+   Runs on `stream` (a cudaStream_t; NULL for the default stream), waits for it and
+   copies the three sums into `out` before it returns.  The first call on a device sets
+   up the scratch address; make it before any stream capture.  That first call also loads
+   the library's device code on the device (CUDA loads modules lazily), which reserves
+   device memory for the code and the scratch array: make it early in the run, before
+   HBM fills up.  Calls that overlap on one device share the scratch and race. */
 int fvg_budget_fields(const double* d, const double* art1, const double* t1, const double* s1,
                       const double* dz, int32_t m, int32_t kbm1, void* stream, double out[3]);
 

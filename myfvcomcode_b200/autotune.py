@@ -2,8 +2,12 @@
 
 The 3-D gather kernels run one thread per cell or node walking ``col_layers`` consecutive
 layers, ``col_threads`` threads per block (``fvg_set_tuning``).  Their results do not
-depend on the shape, so the tuner times candidate shapes on a throw-away handle of the
-same case (the caller's model state is never advanced) and returns the fastest.
+depend on the shape, so the tuner times candidate shapes and returns the fastest.
+
+Without ``engine`` the candidates run on a throw-away handle of the same case, and no
+model of the caller's is advanced.  With ``engine=f`` they run on ``f`` itself, which is
+advanced by (warmup + steps) internal steps per candidate; callers that compare forms
+(``bench.py``) tune every handle the same way so that they stay step for step alike.
 """
 from __future__ import annotations
 

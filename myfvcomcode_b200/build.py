@@ -50,18 +50,38 @@ def needs_build():
 
 
 def build(force=False, verbose=False, extra=()):
+    """Compile every csrc/*.cu to an object (in parallel, one nvcc per file) and link
+    them into libfvg.so."""
     if not force and not needs_build():
         return LIB
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    obj_dir = os.path.join(HERE, "lib", "_build")
+    os.makedirs(obj_dir, exist_ok=True)
     cu = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    cmd = [_nvcc(), "-ccbin", _host_cxx()] + NVCC_FLAGS + list(extra) + ["-o", LIB + ".tmp"] + cu
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs = []
+    objs = []
+    for src in cu:
+        obj = os.path.join(obj_dir, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        cmd = [_nvcc(), "-ccbin", _host_cxx()] + compile_flags + list(extra) + ["-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    errs = []
+    for src, pr in procs:
+        out, err = pr.communicate()
+        if pr.returncode != 0:
+            errs.append(src + ":\n" + out + err)
+        elif verbose and err:
+            print(err, file=sys.stderr)
+    if errs:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errs))
+    cmd = [_nvcc(), "-ccbin", _host_cxx(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+           "-Xcompiler", "-fPIC", "-o", LIB + ".tmp"] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-    if verbose and r.stderr:
-        print(r.stderr, file=sys.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -20,7 +20,13 @@
 //
 // Set-up: the first call on a device looks up the scratch array's device address with
 // cudaGetSymbolAddress (with that device current) and caches it; later calls on that
-// device reuse it.  Make one call on each device before any stream capture begins.
+// device reuse it.  Make one call on each device before any stream capture begins.  With
+// CUDA's lazy module loading, that first call (its symbol lookup and first launches) is
+// also what loads this library's device code on the device, and loading reserves device
+// memory for the code and for g_budget_scratch.  "Allocates nothing" therefore holds from
+// the second call on: a caller that will fill HBM makes the first call early.
+//
+// Every call waits for its stream and copies the result to host memory before returning.
 //
 // Nothing has to start at zero: the tile kernel writes every partial that the final
 // kernel reads, earlier on the same stream, and the final kernel writes the result.

@@ -826,6 +826,18 @@ static void finish_chunk(fvg_handle* h, int c) {
   h->ramp = h->prm.iramp != 0 ? std::tanh((double)h->iint / (double)h->prm.iramp) : 1.0;
 }
 
+// The learned closure's error word, read after the steps have run: a bounded wait of the
+// tensor-core kernel that ran out (its rows then took MY2.5's values) fails the call.
+static int closure_check(fvg_handle* h) {
+  if (!h->P.closure || !h->P.clos_err) return FVG_OK;
+  int e = 0;
+  CK(cudaMemcpy(&e, h->P.clos_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e == 0) return FVG_OK;
+  h->err = "learned closure: a bounded tensor-core wait ran out (error word " + std::to_string(e) +
+           "); the affected rows took MY2.5's values";
+  return FVG_ERR_TIMEOUT;
+}
+
 static int run_steps(fvg_handle* h, int32_t nsteps, int mode, double* group_ms, double* total_ms) {
   if (!h || nsteps < 0) return FVG_ERR_ARG;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -887,7 +899,7 @@ static int run_steps(fvg_handle* h, int32_t nsteps, int mode, double* group_ms, 
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
   }
-  return FVG_OK;
+  return closure_check(h);
 }
 
 int fvg_run(fvg_handle* h, int32_t nsteps) { return run_steps(h, nsteps, 0, nullptr, nullptr); }

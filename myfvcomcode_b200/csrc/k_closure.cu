@@ -158,8 +158,10 @@ __device__ inline float feat_transform(const ClosNorm& nm, int f, float x) {
 }  // namespace
 
 // The tile pipeline shared by the closure and the standalone forward pass.  load(r, v)
-// fills the 8 standardised inputs of row r; store(r, o) receives the 3 network outputs
-// (bias included).  err receives 1 if a wait ran out (results then incomplete).
+// fills the 8 standardised inputs of row r; store(r, o, true) receives the 3 network
+// outputs (bias included).  If an mbarrier wait runs out, err receives 1 and every row of
+// the block that has not been stored yet (the current tile and all later ones) gets
+// store(r, nullptr, false), so that the caller can write its fallback for that row.
 template <class Load, class Store, class Need>
 __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nrows, Load load, Store store, Need need,
                                     int* err) {
@@ -196,10 +198,15 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int r = tile * ROWS + t;
     const bool live = r < nrows;
+    // after a wait ran out, the rest of the block's rows take the fallback
+    if (abort_flag) {
+      if (live) store(r, nullptr, false);
+      continue;
+    }
     // a tile none of whose rows uses the network skips the tensor cores
     if (!__syncthreads_or(live && need(r))) {
       float o[16] = {};
-      if (live) store(r, o);
+      if (live) store(r, o, true);
       continue;
     }
     float v[HID];
@@ -251,14 +258,22 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
         fence_before();
         if (live) {
           for (int c = 0; c < 3; ++c) o[c] += b3[c];
-          store(r, o);
+          store(r, o, true);
         }
         __syncthreads();
       }
     }
-    if (abort_flag) break;
+    // the wait of this tile ran out: none of its rows was stored
+    if (abort_flag && live) store(r, nullptr, false);
   }
-  // give the tensor memory back (every issued MMA has completed or the wait ran out)
+  // After a wait ran out, one commit is still outstanding: wait for it once more (again
+  // bounded) so that the MMAs writing this block's columns are done before they are freed.
+  // If that wait runs out too, err holds 2 and the columns are freed regardless: a CTA
+  // must release its tensor memory before it exits, and the step's result is already
+  // reported as failed.
+  if (abort_flag && t == 0) {
+    if (!mbar_wait(&mbar, (phase + 1) & 1)) atomicExch(err, 2);  // the phase that ran out
+  }
   fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -276,10 +291,10 @@ __global__ void __launch_bounds__(ROWS, 1) k_closure_mlp(const Dev P, int* err) 
 #pragma unroll
     for (int f = 0; f < CLOS_IN; ++f) v[f] = feat_transform(nm, f, P.clos_feat[(size_t)f * S + r]);
   };
-  auto store = [&](int r, const float* o) {
+  auto store = [&](int r, const float* o, bool net_ok) {
     const int k = r / P.M + 2, i = r % P.M + 1;
     const size_t q = N3(P, i, k);
-    const bool use_net = P.clos_env[i] != 0;
+    const bool use_net = net_ok && P.clos_env[i] != 0;
     double nw[3];
     for (int c = 0; c < 3; ++c) {
       if (use_net) {
@@ -305,8 +320,8 @@ __global__ void __launch_bounds__(ROWS, 1) k_mlp_tc_forward(const void* wimg, co
 #pragma unroll
     for (int f = 0; f < CLOS_IN; ++f) v[f] = x[(size_t)r * CLOS_IN + f];
   };
-  auto store = [&](int r, const float* o) {
-    for (int c = 0; c < 3; ++c) out[(size_t)r * 3 + c] = o[c];
+  auto store = [&](int r, const float* o, bool net_ok) {
+    for (int c = 0; c < 3; ++c) out[(size_t)r * 3 + c] = net_ok ? o[c] : __int_as_float(0x7fc00000);
   };
   auto need = [](int) { return true; };
   mlp_tc_tiles(wimg, bias, n, load, store, need, err);

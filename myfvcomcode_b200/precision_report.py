@@ -13,11 +13,39 @@ themselves in this flow.
 from __future__ import annotations
 
 import argparse
+import glob
+import hashlib
 import json
 import math
+import os
+import subprocess
 import time
 
 import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def sources_stamp():
+    """sha256 over everything the report's numbers depend on: the CUDA sources, the C-ABI
+    header, and the host code that builds the case and its mesh metrics."""
+    files = sorted(glob.glob(os.path.join(_HERE, "csrc", "*.cu")) + glob.glob(os.path.join(_HERE, "csrc", "*.h")))
+    files += [os.path.join(_HERE, "..", "include", "fvg.h")]
+    files += [os.path.join(_HERE, n) for n in ("cases.py", "grid.py", "startup.py", "abi.py", "build.py")]
+    h = hashlib.sha256()
+    for fn in files:
+        h.update(os.path.basename(fn).encode())
+        with open(fn, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()
+
+
+def _commit():
+    try:
+        return subprocess.run(["git", "-C", _HERE, "rev-parse", "--short=12", "HEAD"], capture_output=True,
+                              text=True, timeout=10).stdout.strip() or None
+    except Exception:
+        return None
 
 
 def _interior(engine, name):
@@ -72,7 +100,8 @@ def run(case, steps, modes=("fp64", "fp32flux", "fp64_twin"), chunk=200):
                       for i, k in enumerate(("volume", "heat", "salt"))}
         engines[m] = f
     ref = engines[modes[0]]
-    report = {"case": case["name"], "internal_steps": steps,
+    report = {"case": case["name"], "internal_steps": steps, "sources_sha256": sources_stamp(),
+              "commit": _commit(),
               "simulated_hours": steps * case["params"]["DTE"] * case["params"]["ISPLIT"] / 3600.0,
               "budget_drift": budgets, "wall_s": times, "errors_vs_" + modes[0]: {}}
     for m in modes[1:]:
@@ -100,6 +129,7 @@ def main():
     ap.add_argument("--npts", type=int, default=200000)
     ap.add_argument("--hours", type=float, default=24.0)
     ap.add_argument("--md", default=None)
+    ap.add_argument("--json", default=None, help="also write the report to this file")
     args = ap.parse_args()
     from . import cases
     case = cases.coastal_mesh(npts=args.npts)
@@ -107,6 +137,9 @@ def main():
     steps = int(round(args.hours * 3600.0 / dti))
     rep = run(case, steps)
     print(json.dumps(rep))
+    if args.json:
+        with open(args.json, "w") as fh:
+            json.dump(rep, fh)
     if args.md:
         with open(args.md, "w") as fh:
             fh.write(markdown(rep))

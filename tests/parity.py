@@ -1,4 +1,13 @@
-"""Helpers shared by the parity tests: field lists, state transfer and comparison."""
+"""Helpers shared by the parity tests: field lists, state transfer and comparison.
+
+Two measures of a difference between the library's field ``a`` and the oracle's ``b``:
+
+* max-normalised: max|a - b| / max|b| over the field (``compare``'s ``rtol``), a norm
+  that grants every element the field's largest magnitude;
+* per element: max over elements of |a_i - b_i| / max(|b_i|, 1e-6 max|b|), i.e. each
+  element's own relative error, with elements below a millionth of the field's scale
+  held to that floor instead of their own (near-zero) size (``errors``).
+"""
 from __future__ import annotations
 
 import numpy as np
@@ -75,3 +84,18 @@ def compare(gpu, ora, names, rtol=0.0, tracer=1):
             if not d <= rtol:
                 bad[n] = d
     return bad
+
+
+def errors(gpu, ora, names, tracer=1):
+    """{name: {"max_norm": ..., "per_element": ..., "bitwise": bool}} for ``names``."""
+    out = {}
+    for n in names:
+        a = interior(gpu, n, gpu.get(gpu_name(n, tracer))).astype(np.float64)
+        b = interior(ora, n, ora.get(n)).astype(np.float64)
+        d = np.abs(a - b)
+        scale = float(np.abs(b).max()) if b.size else 0.0
+        floor = max(1e-6 * scale, 1e-300)
+        out[n] = {"max_norm": float(d.max()) / max(scale, 1e-300) if b.size else 0.0,
+                  "per_element": float((d / np.maximum(np.abs(b), floor)).max()) if b.size else 0.0,
+                  "bitwise": bool(np.array_equal(a, b, equal_nan=True))}
+    return out

@@ -14,7 +14,9 @@ import pytest
 
 from myfvcomcode_b200 import cases, fvcom_input as fi
 
-ESTUARY = "/root/reference/Examples/Estuary/run/tst_run.nml"
+# The reference's own Estuary example (Examples/Estuary/run/tst_run.nml of the FVCOM
+# tree), located by FVCOM_ESTUARY_NML; the test that reads it is skipped when unset.
+ESTUARY = os.environ.get("FVCOM_ESTUARY_NML", "")
 
 NML_TEXT = """
  &NML_CASE
@@ -202,7 +204,8 @@ def test_history_written_every_interval(tmp_path, small_channel):
         assert list(nc.variables["iint"][:]) == [0, 10, 20]
 
 
-@pytest.mark.skipif(not os.path.exists(ESTUARY), reason="the reference's Estuary example is not present")
+@pytest.mark.skipif(not ESTUARY or not os.path.exists(ESTUARY),
+                    reason="FVCOM_ESTUARY_NML does not name the reference's Estuary example")
 def test_reads_the_estuary_example():
     from oracle.oracle import Oracle
     run = fi.FvcomRun(ESTUARY)
