@@ -2,7 +2,10 @@
 
 --fmad=false keeps every multiply and add separately rounded so the kernels follow the
 reference's expression order bit for bit; division and square root stay IEEE-rounded
-(the nvcc defaults -prec-div=true -prec-sqrt=true).
+(the nvcc defaults -prec-div=true -prec-sqrt=true).  The kernel sources that hold FP32
+instantiations of the precision form (F32_UNITS) are compiled a second time with
+-DFVG_F32_TU and --fmad=true: those kernels are not bit-matched to anything, and
+multiply-add contraction only removes roundings from them.
 """
 from __future__ import annotations
 
@@ -21,6 +24,9 @@ NVCC_FLAGS = [
     "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
     "-Xcompiler", "-fPIC,-O2", "-shared",
 ]
+
+
+F32_UNITS = ("k_ext.cu", "k_mom3d.cu", "k_scalar.cu")
 
 
 def _nvcc():
@@ -61,10 +67,14 @@ def build(force=False, verbose=False, extra=()):
     compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
     procs = []
     objs = []
-    for src in cu:
-        obj = os.path.join(obj_dir, os.path.basename(src)[:-3] + ".o")
+    units = [(src, os.path.basename(src)[:-3], compile_flags) for src in cu]
+    f32_flags = [("--fmad=true" if f == "--fmad=false" else f) for f in compile_flags] + ["-DFVG_F32_TU"]
+    units += [(src, os.path.basename(src)[:-3] + "_f32", f32_flags) for src in cu
+              if os.path.basename(src) in F32_UNITS]
+    for src, name, flags in units:
+        obj = os.path.join(obj_dir, name + ".o")
         objs.append(obj)
-        cmd = [_nvcc(), "-ccbin", _host_cxx()] + compile_flags + list(extra) + ["-c", "-o", obj, src]
+        cmd = [_nvcc(), "-ccbin", _host_cxx()] + flags + list(extra) + ["-c", "-o", obj, src]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))

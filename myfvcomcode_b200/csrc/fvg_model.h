@@ -431,3 +431,33 @@ void launch_final(const Dev& P, cudaStream_t s, int parts);
 void launch_budget(const Dev& P, cudaStream_t s);
 
 }  // namespace fvg
+
+// The precision form's FP32 flux kernels, compiled separately with multiply-add
+// contraction (the FP64 kernels keep --fmad=false for their bitwise parity).  Launchers
+// of kernels that have an FP32 instantiation forward to these when P.prec is set.
+namespace fvg_f32 {
+using fvg::Dev;
+void launch_alfa2(const Dev& P, cudaStream_t s);
+void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts, int pdl);
+void launch_grad3(const Dev& P, cudaStream_t s);
+void launch_advection3d(const Dev& P, cudaStream_t s);
+void launch_adv_uv(const Dev& P, cudaStream_t s);
+void launch_grad(const Dev& P, cudaStream_t s, int which);
+void launch_adv_q(const Dev& P, cudaStream_t s, int parts);
+void launch_adv_ts(const Dev& P, cudaStream_t s, int parts);
+}  // namespace fvg_f32
+
+// RF: the arithmetic type of the flux kernels this translation unit launches.
+#ifdef FVG_F32_TU
+using RF = float;
+#define FVG_F32_FORWARD(call)
+#else
+using RF = double;
+#define FVG_F32_FORWARD(call) \
+  do {                          \
+    if (P.prec) {               \
+      fvg_f32::call;            \
+      return;                   \
+    }                           \
+  } while (0)
+#endif

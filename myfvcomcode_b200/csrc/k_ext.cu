@@ -8,7 +8,15 @@
 // --fmad=false so no multiply-add is contracted.
 #include "fvg_model.h"
 
+// The FP32 instantiations of the precision form's flux kernels are compiled from this
+// same source a second time with -DFVG_F32_TU and multiply-add contraction (build.py),
+// into namespace fvg_f32; the FP64 translation unit forwards their launches there.
+#ifdef FVG_F32_TU
+namespace fvg_f32 {
+using namespace fvg;
+#else
 namespace fvg {
+#endif
 
 // Programmatic dependent launch: wait until the previous kernel in the stream has
 // completed and its writes are visible (a no-op when the kernel was launched without the
@@ -33,7 +41,9 @@ static void launch_maybe_pdl(int pdl, void (*k)(KArgs...), dim3 grid, dim3 block
 }
 
 __device__ __constant__ double dAlphaRK[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
+#ifndef FVG_F32_TU
 const double kAlphaRK[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
+#endif
 #define ONE_THIRD (1.0 / 3.0)
 
 __device__ inline const double* sched_row(const Dev& P) {
@@ -574,10 +584,8 @@ void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts, i
 }
 void launch_ext_prep(const Dev& P, cudaStream_t s) { k_ext_prep<<<nblk(P.N, 256), 256, 0, s>>>(P); }
 void launch_alfa2(const Dev& P, cudaStream_t s) {
-  if (P.prec)
-    k_alfa2<float><<<nblk(P.N, 128), 128, 0, s>>>(P);
-  else
-    k_alfa2<double><<<nblk(P.N, 128), 128, 0, s>>>(P);
+  FVG_F32_FORWARD(launch_alfa2(P, s));
+  k_alfa2<RF><<<nblk(P.N, 128), 128, 0, s>>>(P);
 }
 
 // FP32 copies of the mesh metrics the precision form's flux kernels read.
@@ -653,11 +661,9 @@ void launch_wet_cells(const Dev& P, cudaStream_t s, int pdl) {
   launch_maybe_pdl(pdl, k_wet_cells, dim3(nblk(P.N, 256)), dim3(256), s, P);
 }
 void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts, int pdl) {
+  FVG_F32_FORWARD(launch_ext_cell(P, s, iext, K, parts, pdl));
   void (*k)(const Dev, int, int, int);
-  if (P.prec)
-    k = P.limiter ? k_ext_cell<float, true> : k_ext_cell<float, false>;
-  else
-    k = P.limiter ? k_ext_cell<double, true> : k_ext_cell<double, false>;
+  k = P.limiter ? k_ext_cell<RF, true> : k_ext_cell<RF, false>;
   launch_maybe_pdl(pdl, k, dim3(nblk(P.N, 128)), dim3(128), s, P, iext, K, parts);
 }
 void launch_ext_update(const Dev& P, cudaStream_t s, int K) {
@@ -671,4 +677,4 @@ void launch_ext_finish(const Dev& P, cudaStream_t s, int K, int wet_prev) {
 void launch_begin_step(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 1); }
 void launch_set_qdis(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 0); }
 
-}  // namespace fvg
+}  // namespace fvg / fvg_f32

@@ -10,7 +10,15 @@
 // shared by the eight warps through L1.
 #include "fvg_model.h"
 
+// The FP32 instantiations of the precision form's flux kernels are compiled from this
+// same source a second time with -DFVG_F32_TU and multiply-add contraction (build.py),
+// into namespace fvg_f32; the FP64 translation unit forwards their launches there.
+#ifdef FVG_F32_TU
+namespace fvg_f32 {
+using namespace fvg;
+#else
 namespace fvg {
+#endif
 
 #define ONE_THIRD (1.0 / 3.0)
 constexpr int kMaxKB = 64;
@@ -948,23 +956,16 @@ void launch_cell_pre(const Dev& P, cudaStream_t s, int parts) {
   k_cell_pre<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);
 }
 void launch_grad3(const Dev& P, cudaStream_t s) {
-  if (P.prec)
-    k_grad3<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
-  else
-    k_grad3<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  FVG_F32_FORWARD(launch_grad3(P, s));
+  k_grad3<RF><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 static void launch_alfa3(const Dev& P, cudaStream_t s) {
-  if (P.prec)
-    k_alfa3<float><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
-  else
-    k_alfa3<double><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  k_alfa3<RF><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_advection3d(const Dev& P, cudaStream_t s) {
+  FVG_F32_FORWARD(launch_advection3d(P, s));
   if (P.limiter) launch_alfa3(P, s);
-  if (P.prec)
-    (P.limiter ? k_advection3d<float, true> : k_advection3d<float, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
-  else
-    (P.limiter ? k_advection3d<double, true> : k_advection3d<double, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  (P.limiter ? k_advection3d<RF, true> : k_advection3d<RF, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 // -------------------------------------------------------------------------------------
 // PHY_BAROPG (phy_baropg.F:37-151), BAROCLINIC_PRESSURE_GRADIENT = 'z coordinates'.
@@ -1119,14 +1120,12 @@ void launch_w_viscofh(const Dev& P, cudaStream_t s, int do_w, int do_visc) {
   k_w_viscofh<<<col_grid(P, n, P.KB), P.col_bc, 0, s>>>(P, do_w, do_visc);
 }
 void launch_adv_uv(const Dev& P, cudaStream_t s) {
+  FVG_F32_FORWARD(launch_adv_uv(P, s));
   if (P.limiter) launch_alfa3(P, s);
-  if (P.prec)
-    (P.limiter ? k_adv_uv<float, true> : k_adv_uv<float, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
-  else
-    (P.limiter ? k_adv_uv<double, true> : k_adv_uv<double, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
+  (P.limiter ? k_adv_uv<RF, true> : k_adv_uv<RF, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
 void launch_vdif_uv(const Dev& P, cudaStream_t s, int parts) {
   k_vdif_uv<<<nblk(P.N, 128), 128, 0, s>>>(P, parts);
 }
 
-}  // namespace fvg
+}  // namespace fvg / fvg_f32

@@ -13,7 +13,15 @@
 // transported in the same launches since neither reads the other's update.
 #include "fvg_model.h"
 
+// The FP32 instantiations of the precision form's flux kernels are compiled from this
+// same source a second time with -DFVG_F32_TU and multiply-add contraction (build.py),
+// into namespace fvg_f32; the FP64 translation unit forwards their launches there.
+#ifdef FVG_F32_TU
+namespace fvg_f32 {
+using namespace fvg;
+#else
 namespace fvg {
+#endif
 
 #define ONE_THIRD (1.0 / 3.0)
 constexpr int kMaxKBs = 64;
@@ -1198,20 +1206,14 @@ __global__ void k_budget_final(const double* part, int nb, double* out) {
 }
 
 void launch_grad(const Dev& P, cudaStream_t s, int which) {
+  FVG_F32_FORWARD(launch_grad(P, s, which));
   const dim3 g = col_grid(P, P.M, which == 0 ? P.KBM1 - 1 : P.KBM1);
-  if (P.prec)
-    k_grad<float><<<g, P.col_bc, 0, s>>>(P, which);
-  else
-    k_grad<double><<<g, P.col_bc, 0, s>>>(P, which);
+  k_grad<RF><<<g, P.col_bc, 0, s>>>(P, which);
 }
 void launch_adv_q(const Dev& P, cudaStream_t s, int parts) {
-  if (P.prec) {
-    k_he_adv<float, 0><<<col_grid(P, P.N, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
-    k_gather_q<float><<<col_grid(P, P.M, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
-  } else {
-    k_he_adv<double, 0><<<col_grid(P, P.N, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
-    k_gather_q<double><<<col_grid(P, P.M, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
-  }
+  FVG_F32_FORWARD(launch_adv_q(P, s, parts));
+  k_he_adv<RF, 0><<<col_grid(P, P.N, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
+  k_gather_q<RF><<<col_grid(P, P.M, P.KBM1 - 1), P.col_bc, 0, s>>>(P, parts);
 }
 void launch_fct_q(const Dev& P, cudaStream_t s, int parts) {
   dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1 - 1, 8));
@@ -1230,13 +1232,9 @@ void launch_turb_update(const Dev& P, cudaStream_t s) {
   k_turb_update<<<g, b, 0, s>>>(P);
 }
 void launch_adv_ts(const Dev& P, cudaStream_t s, int parts) {
-  if (P.prec) {
-    k_he_adv<float, 1><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P, parts);
-    k_gather_ts<float><<<col_grid(P, P.M, P.KBM1), P.col_bc, 0, s>>>(P, parts);
-  } else {
-    k_he_adv<double, 1><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P, parts);
-    k_gather_ts<double><<<col_grid(P, P.M, P.KBM1), P.col_bc, 0, s>>>(P, parts);
-  }
+  FVG_F32_FORWARD(launch_adv_ts(P, s, parts));
+  k_he_adv<RF, 1><<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P, parts);
+  k_gather_ts<RF><<<col_grid(P, P.M, P.KBM1), P.col_bc, 0, s>>>(P, parts);
 }
 void launch_fct_ts(const Dev& P, cudaStream_t s, int parts) {
   dim3 b(32, 8), g(nblk(P.M, 32), nblk(P.KBM1, 8));
@@ -1263,4 +1261,4 @@ void launch_budget(const Dev& P, cudaStream_t s) {
   k_budget_final<<<1, 32, 0, s>>>(P.budget + 3, nb, P.budget);
 }
 
-}  // namespace fvg
+}  // namespace fvg / fvg_f32

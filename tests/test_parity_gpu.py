@@ -241,8 +241,7 @@ def test_limited_schemes_match_oracle(case_name, limiter, request):
         bad = parity.compare(gpu, ora, outs, rtol=1e-13 if name in TRANSCENDENTAL else 0.0)
         if bad:
             failures["%s(%d)" % (name, arg)] = bad
-    gpu.close()
-    return failures
+    assert not failures, failures
     a, b = Oracle(case), Fvcom(case)
     a.run(20)
     b.run(20)
