@@ -451,6 +451,7 @@ def main():
     cfg["precision"] = {"fp64": "plain FP64",
                         "fp32flux": "FP32 edge fluxes/advection/FCT; FP64 elevation update, "
                                     "column solves, state and budgets"}[args.precision]
+    cfg["compact_stage_kernel"] = bool(f.get_tuning("compact"))
     cfg["tiling"] = {"col_threads": f.get_tuning("col_threads"), "col_layers": f.get_tuning("col_layers"),
                      "autotuned": not args.no_tune}
     value = cells_layers * args.steps * world / (t_ms / 1e3)
@@ -491,7 +492,8 @@ def main():
     nprof = 2
     lib.fvg_profile(f.h, nprof, gms, C.byref(tot))
     names = [lib.fvg_profile_group_name(i).decode() for i in range(ng)]
-    led = bytes_model.ledger(g, p["ISPLIT"], bool(p["WETTING_DRYING_ON"]), args.precision)
+    compact = bool(f.get_tuning("compact"))
+    led = bytes_model.ledger(g, p["ISPLIT"], bool(p["WETTING_DRYING_ON"]), args.precision, compact)
     groups = {names[i]: gms[i] / nprof for i in range(ng) if gms[i] > 0}
     dom = max(groups, key=groups.get)
     b_launch, n_launch = led[dom]
@@ -499,7 +501,7 @@ def main():
     achieved = b_launch / (dur / 1e3) / 1e9
     peak, peak_kind = peak_hbm()
     traffic = traffic_table().get((dom, case["name"]))
-    step_b = bytes_model.step_bytes(g, p["ISPLIT"], bool(p["WETTING_DRYING_ON"]), args.precision)
+    step_b = bytes_model.step_bytes(g, p["ISPLIT"], bool(p["WETTING_DRYING_ON"]), args.precision, compact)
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
             "algorithmic_bytes_per_launch": b_launch, "launch_ms": dur,

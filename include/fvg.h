@@ -302,7 +302,11 @@ int fvg_set_closure(fvg_handle* h, int32_t mode, const float* params, int32_t np
 int fvg_closure_status(fvg_handle* h, int32_t* columns_on_network, int32_t* wait_timeouts);
 /* Launch shape of the 3-D gather kernels (results do not depend on it):
    "col_threads" = entities (threads) per block, 32..256 in steps of 32 (default 128);
-   "col_layers"  = consecutive layers each thread walks, 1..KB (default 8). */
+   "col_layers"  = consecutive layers each thread walks, 1..KB (default 8);
+   "compact"     = 1 (default) lets the precision form's Runge-Kutta stages use the
+                   compact cell kernel where fvg_set_precision found the mesh's edge metrics
+                   to be the ones its coordinates define; 0 keeps the general kernel.
+                   fvg_get_tuning("compact") reports whether the compact kernel is in use. */
 int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value);
 int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value);
 

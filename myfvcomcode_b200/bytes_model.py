@@ -22,13 +22,18 @@ def sizes(grid):
                 K=grid["KB"] - 1, ntsn=int(grid["NTSN"][1:].sum()), ntve=int(grid["NTVE"][1:].sum()))
 
 
-def ledger(grid, isplit, wet_dry, precision="fp64"):
+def ledger(grid, isplit, wet_dry, precision="fp64", compact=False):
     """{group: (bytes per launch, launches per internal step)}
 
     ``precision`` "fp32flux" counts the arrays that form keeps in FP32 at 4 bytes: the
     least-squares and node-ring gradients (A1U/A2U, the 2-D and 3-D cell gradients,
     PTPX.. with the ring extrema), the edge offsets, DLTXC/DLTYC, ART, CC_HVC and the
-    control-volume metrics read by the flux kernels.  FP64 state is counted at 8 bytes.
+    control-volume metrics read by the flux kernels.  FP64 state is counted at 8 bytes
+    in both forms (ADVX/ADVY, UF/VF/VISCOFM and DZ1 among them).
+
+    ``compact`` (precision form only): the Runge-Kutta stages' cell kernel is the compact
+    one, whose records replace the slot table's metrics and EXTUV's fixed inputs (see
+    ``ext_cell_compact``).
     """
     s = sizes(grid)
     M, N, NE, NCV, K, KB = s["M"], s["N"], s["NE"], s["NCV"], s["K"], s["KB"]
@@ -57,12 +62,15 @@ def ledger(grid, isplit, wet_dry, precision="fp64"):
     g["ext_node"] = (M * (I + I + 3 * D) + halfedge_csr + NCV * (I + 2 * D) + N * 3 * D + M * 5 * D + wet_node, st)
     g["ext_cell"] = (N * (cell_lsq // N + 22 * D + 4 * X + 6 * I) + N * 8 * D + edge_geo + pg_extra
                      + M * 4 * D + N * (6 * D + 3 * I), st)
+    if compact and precision == "fp32flux":
+        g["ext_cell"] = (ext_cell_compact(N, M, isplit), st)
     g["ext_update"] = (M * (6 * D + I) + N * (10 * D + (2 * I if wet_dry else 0)), 1)
     if wet_dry:
         g["wet_judge"] = (N * (3 * I + I + D) + M * D, st)
     # ---- 3-D, once per internal step ----
     g["cell_pre"] = (N * K * 4 * D + N * K * D + N * 12 * D, 1)              # U,V rw; DZ1; 2-D
-    g["advection3d"] = (N * K * 2 * D + N * K * 2 * X + M * K * D + cell_lsq + N * 6 * D + N * 4 * X
+    # U, V read and ADVX, ADVY written per cell and layer (FP64 in both forms)
+    g["advection3d"] = (N * K * 4 * D + M * K * D + cell_lsq + N * 6 * D + N * 4 * X
                         + edge_geo + M * D, 1)
     g["baropg"] = (M * K * 2 * D + N * KB * 2 * D + N * K * 7 * D + N * 10 * D + M * 3 * D, 1)
     g["int_advave"] = (N * (cell_lsq // N + 16 * D + 4 * X) + edge_geo + pg_extra + M * 3 * D, 1)
@@ -73,7 +81,8 @@ def ledger(grid, isplit, wet_dry, precision="fp64"):
     g["vertvl_col"] = (M * K * 2 * D + M * KB * D + M * K * 2 * D + M * 10 * D + I * ntve + N * 2 * D, 1)
     g["w_viscofh"] = (M * KB * D + N * KB * D + N * K * 2 * D + M * K * D + M * 3 * D
                       + ntve * (I + 4 * D) + N * I, 1)
-    g["adv_uv"] = (N * K * 7 * D + N * K * 2 * X + N * D + M * K * D + cell_lsq + N * 10 * D + N * 4 * X
+    # U, V, W, DZ1, DRHOX, DRHOY read and UF, VF, VISCOFM written per cell and layer
+    g["adv_uv"] = (N * K * 9 * D + N * D + M * K * D + cell_lsq + N * 10 * D + N * 4 * X
                    + edge_geo + M * 2 * D, 1)
     g["vdif_uv"] = (N * KB * D + N * K * 10 * D + N * 20 * D + M * 3 * D, 1)
     g["grad_q"] = (M * K * 2 * D + M * K * 12 * X + ring + M * 2 * D, 1)
@@ -89,5 +98,21 @@ def ledger(grid, isplit, wet_dry, precision="fp64"):
     return g
 
 
-def step_bytes(grid, isplit, wet_dry, precision="fp64"):
-    return sum(b * n for b, n in ledger(grid, isplit, wet_dry, precision).values())
+def ext_cell_compact(N, M, isplit):
+    """Bytes of one launch of the compact stage kernel, averaged over the 4*ISPLIT stages.
+
+    Per cell: the flag word, UA, VA, the two wet flags, D1, the packed FP32 gradient
+    {UX, UY, VX, VY}, {ART, CC_HVC} in FP32, {XC, YC}, three 16-byte slots, the two
+    32-byte records of EXTUV's terms, UARK, VARK, ELRK1, ELF1 read; UAF, VAF, EL1, D1
+    and the three half-edge continuity fluxes written.  Per node: {VX, VY}, D, EL read.
+    The first stage of each external step also reads EL1 and writes UARK, VARK, ELRK1
+    (instead of reading them); the last stage writes ADVUA, ADVVA, PSTX, PSTY.
+    """
+    per_cell = I + 2 * D + 2 * I + D + 16 + 8 + 16 + 3 * 16 + 2 * 32 + 4 * D + 4 * D + 3 * D
+    st = 4 * isplit
+    extra = (isplit * D + 4 * D) / st
+    return int(N * (per_cell + extra) + M * (16 + 2 * D))
+
+
+def step_bytes(grid, isplit, wet_dry, precision="fp64", compact=False):
+    return sum(b * n for b, n in ledger(grid, isplit, wet_dry, precision, compact).values())

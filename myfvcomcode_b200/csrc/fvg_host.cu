@@ -52,6 +52,10 @@ struct fvg_handle {
   cudaGraph_t graph = nullptr;
   bool use_graph = true;
   int clos_grid = 148;
+  // compact external stage of the precision form: allowed (tuning key "compact") and
+  // possible (the mesh check of fvg_set_precision passed)
+  int compact_allowed = 1;
+  int compact_ok = 0;
 };
 
 #define CK(call)                                                                      \
@@ -189,7 +193,7 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   launch_ext_prep(P, s);
   if (P.limiter) launch_alfa2(P, s);
   mk.mark(s, G_BAROPG);
-  launch_ext_cell(P, s, 1, 1, EC_INT_ADVAVE);
+  launch_ext_cell(P, s, 1, 1, EC_INT_ADVAVE | EC_COMPACT);
   launch_int_reset(P, s);
   mk.mark(s, G_INT_ADVAVE);
   // The ISPLIT x 4 Runge-Kutta stages.  Instead of copying UAF to UA and ISWETC to
@@ -222,7 +226,8 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
       if (P.limiter) launch_alfa2(Q, s);
       launch_ext_cell(Q, s, iext, K,
                       (p.wetting_drying_on ? 0 : EC_N2E) | EC_FLUXOBN | EC_ADVAVE | EC_EXTUV | EC_BC2 |
-                          (K == 1 ? EC_COPY_RK : 0) | EC_FINISH,
+                          (K == 1 ? EC_COPY_RK : 0) | EC_FINISH | EC_COMPACT |
+                          (iext == p.isplit && K == 4 ? EC_LAST : 0),
                       P.limiter ? 0 : 1);
       mk.mark(s, G_EXT_CELL);
     }
@@ -998,10 +1003,9 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     const size_t ms = P.ms, ns = P.ns, KB = P.KB, n1 = P.N + 1, e1 = P.NE + 1;
     F32& f = P.f;
     auto fail = [&](int r) { return r; };
-    for (int q = 0; q < 4; ++q) {
-      if ((rc = dalloc(h, &f.g2d[q], n1))) return fail(rc);
+    for (int q = 0; q < 4; ++q)
       if ((rc = dalloc(h, &f.g3[q], ns * KB))) return fail(rc);
-    }
+    if ((rc = dalloc(h, (float**)&f.g2d4, 4 * n1))) return fail(rc);
     if (P.limiter) {
       std::vector<float> ones(std::max(n1, ns * KB), 1.0f);
       for (int q = 0; q < 2; ++q) {
@@ -1032,8 +1036,26 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     if ((rc = dalloc(h, (float**)&f.a2u4, 4 * n1))) return fail(rc);
     launch_make_f32(P, h->stream);
     CK(cudaGetLastError());
+    // records of the compact stage kernel, used where the mesh's edge metrics are the ones
+    // its coordinates define (checked here, bit for bit)
+    if ((rc = dalloc(h, (int**)&f.slot4, 4 * 3 * n1))) return fail(rc);
+    if ((rc = dalloc(h, (double**)&f.vxy, 2 * ((size_t)P.M + 1)))) return fail(rc);
+    if ((rc = dalloc(h, (double**)&f.xyc, 2 * n1))) return fail(rc);
+    if ((rc = dalloc(h, (float**)&f.artcc, 2 * n1))) return fail(rc);
+    if ((rc = dalloc(h, (double**)&f.exc0, 4 * n1))) return fail(rc);
+    if ((rc = dalloc(h, (double**)&f.exc1, 4 * n1))) return fail(rc);
+    if ((rc = dalloc(h, &f.cflag, n1))) return fail(rc);
+    int* d_bad = nullptr;
+    if ((rc = dalloc(h, &d_bad, 1))) return fail(rc);
+    launch_make_compact(P, h->stream, d_bad);
+    CK(cudaGetLastError());
+    int bad = -1;
+    CK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->compact_ok = (bad == 0 && !P.limiter && !P.gcy) ? 1 : 0;
   }
   P.prec = mode;
+  P.f.compact = (mode == FVG_PREC_FP32_FLUX && h->compact_ok && h->compact_allowed) ? 1 : 0;
   // The captured step holds the other precision's kernels: capture again.
   CK(cudaStreamSynchronize(h->stream));
   if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
@@ -1145,6 +1167,9 @@ int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value) {
   } else if (k == "col_layers") {
     if (value < 1 || value > h->P.KB) { h->err = "col_layers must be 1..KB"; return FVG_ERR_ARG; }
     h->P.col_lc = value;
+  } else if (k == "compact") {
+    h->compact_allowed = value != 0;
+    h->P.f.compact = (h->P.prec == FVG_PREC_FP32_FLUX && h->compact_ok && h->compact_allowed) ? 1 : 0;
   } else {
     h->err = "unknown tuning key " + k;
     return FVG_ERR_ARG;
@@ -1161,6 +1186,7 @@ int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value) {
   std::string k(key);
   if (k == "col_threads") *value = h->P.col_bc;
   else if (k == "col_layers") *value = h->P.col_lc;
+  else if (k == "compact") *value = h->P.f.compact;
   else return FVG_ERR_ARG;
   return FVG_OK;
 }

@@ -41,7 +41,7 @@ struct SchedLayout {
 // and rounded once: xo[e] = XIJC(e)-XC(IEC(e,1)), xo[NE+1+e] = XIJC(e)-XC(IEC(e,2)), the
 // same for y.
 struct F32 {
-  float *g2d[4], *g3[4];
+  float* g3[4];
   float *alfa2[2], *alfa3[2];  // slope limiters UALFA, VALFA (see Dev)
   float* npk;  // node records of the ring gradients, 16 floats per (node, layer)
   float2* ex2;
@@ -57,6 +57,23 @@ struct F32 {
   float2* trie;
   // A1U and A2U of each cell packed: {A(c,1), A(c,2), A(c,3), A(c,4)}
   float4 *a1u4, *a2u4;
+  // Least-squares gradient of UA, VA per cell packed: {UX, UY, VX, VY}
+  float4* g2d4;
+  // Compact external stage (compact != 0; set up by fvg_set_precision after checking that
+  // the mesh's edge metrics are the ones its node and cell coordinates define, bit for
+  // bit: DLTXC = VX(IENODE2)-VX(IENODE1), XIJC = (VX(IENODE1)+VX(IENODE2))/2, DLTXE =
+  // XIJC-XC of the half-edge's cell, the same in y).  slot4: per (slot s, cell c) at
+  // s*(N+1)+c {code, the other cell, IENODE1, IENODE2}; vxy {VX, VY} per node; xyc {XC, YC}
+  // per cell; artcc {ART, CC_HVC} in FP32; exc0 per internal step {ADX2D+DRX2D-WUBOT*ART,
+  // ADY2D+DRY2D-WVBOT*ART, 0.001*WSX*ART, 0.001*WSY*ART}; exc1 {COR*ART, ART, H1, GRAV_E};
+  // cflag: ISBCE in bits 0-1, IUCP = 1 bit 2, EPOR = 1 bit 3, river momentum entries bit
+  // 4, open-boundary flux entries bit 5, a sponge coefficient bit 6.
+  int compact;
+  int4* slot4;
+  double2 *vxy, *xyc;
+  float2* artcc;
+  double4 *exc0, *exc1;
+  int* cflag;
 };
 
 // Input and output scaling of the learned closure's network, and the training envelope.
@@ -305,7 +322,6 @@ template <> struct Mesh<float> {
   __device__ static float cc_hvc(const Dev& P, int c) { return P.f.cc_hvc[c]; }
   __device__ static float a1u(const Dev& P, size_t q) { return P.f.a1u[q]; }
   __device__ static float a2u(const Dev& P, size_t q) { return P.f.a2u[q]; }
-  __device__ static float* g2d(const Dev& P, int q) { return P.f.g2d[q]; }
   __device__ static float* alfa2(const Dev& P, int q) { return P.f.alfa2[q]; }
   __device__ static float* alfa3(const Dev& P, int q) { return P.f.alfa3[q]; }
   __device__ static float* g3(const Dev& P, int q) { return P.f.g3[q]; }
@@ -371,8 +387,11 @@ enum ExtNodeParts { EN_EXTEL = 1, EN_BC = 2, EN_COPY_ELRK = 4, EN_GRAD = 8, EN_F
 // EC_FINISH: end with the cell part of the stage's update (EL1, D1, the stage sums, the
 // next stage's continuity fluxes from the new UAF, VAF), UA/VA being swapped with
 // UAF/VAF between stages instead of copied.
+// EC_COMPACT: the stage loop of an internal step may use the compact FP32 kernel (when
+// F32::compact is set); EC_LAST: the last stage of that loop (the compact kernel writes
+// ADVUA, ADVVA, PSTX, PSTY only there and in the internal-step ADVAVE call).
 enum ExtCellParts { EC_N2E = 1, EC_FLUXOBN = 2, EC_ADVAVE = 4, EC_EXTUV = 8, EC_BC2 = 16, EC_COPY_RK = 32,
-                    EC_INT_ADVAVE = 64, EC_FINISH = 128 };
+                    EC_INT_ADVAVE = 64, EC_FINISH = 128, EC_COMPACT = 256, EC_LAST = 512 };
 void launch_ext_finish(const Dev& P, cudaStream_t s, int K, int wet_prev);
 // pdl: launched as a programmatic dependent of the previous kernel in the stream (the
 // fused external loop); the kernel waits for that kernel's completion before it touches
@@ -386,6 +405,9 @@ void launch_ext_update(const Dev& P, cudaStream_t s, int K);
 void launch_begin_step(const Dev& P, cudaStream_t s);
 void launch_ext_prep(const Dev& P, cudaStream_t s);
 void launch_make_f32(const Dev& P, cudaStream_t s);
+// Fill the compact external stage's records and count (into *mismatch, device memory)
+// the mesh metrics that differ from the ones the coordinates define.
+void launch_make_compact(const Dev& P, cudaStream_t s, int* mismatch);
 void launch_closure(const Dev& P, cudaStream_t s, int* err, int grid);
 void launch_vdif_q_shallow(const Dev& P, cudaStream_t s);
 size_t closure_smem_bytes();

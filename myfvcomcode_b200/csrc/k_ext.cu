@@ -86,10 +86,14 @@ __device__ inline Grad<R> cell_grad(const Dev& P, int c, const double* U, const 
 template <typename R>
 __device__ inline void store_grad_t(const Dev& P, int c) {
   Grad<R> g = cell_grad<R>(P, c, P.ua, P.va);
-  Mesh<R>::g2d(P, 0)[c] = g.ux;
-  Mesh<R>::g2d(P, 1)[c] = g.uy;
-  Mesh<R>::g2d(P, 2)[c] = g.vx;
-  Mesh<R>::g2d(P, 3)[c] = g.vy;
+  if constexpr (sizeof(R) == 4) {
+    P.f.g2d4[c] = make_float4(g.ux, g.uy, g.vx, g.vy);
+  } else {
+    Mesh<R>::g2d(P, 0)[c] = g.ux;
+    Mesh<R>::g2d(P, 1)[c] = g.uy;
+    Mesh<R>::g2d(P, 2)[c] = g.vx;
+    Mesh<R>::g2d(P, 3)[c] = g.vy;
+  }
 }
 __device__ inline void store_grad(const Dev& P, int c) {
   if (P.prec) store_grad_t<float>(P, c);
@@ -98,10 +102,18 @@ __device__ inline void store_grad(const Dev& P, int c) {
 template <typename R>
 __device__ inline Grad<R> load_grad(const Dev& P, int c) {
   Grad<R> g;
-  g.ux = Mesh<R>::g2d(P, 0)[c];
-  g.uy = Mesh<R>::g2d(P, 1)[c];
-  g.vx = Mesh<R>::g2d(P, 2)[c];
-  g.vy = Mesh<R>::g2d(P, 3)[c];
+  if constexpr (sizeof(R) == 4) {
+    const float4 a = P.f.g2d4[c];
+    g.ux = a.x;
+    g.uy = a.y;
+    g.vx = a.z;
+    g.vy = a.w;
+  } else {
+    g.ux = Mesh<R>::g2d(P, 0)[c];
+    g.uy = Mesh<R>::g2d(P, 1)[c];
+    g.vx = Mesh<R>::g2d(P, 2)[c];
+    g.vy = Mesh<R>::g2d(P, 3)[c];
+  }
   return g;
 }
 // EXTEL_EDGE half-edge flux EXFLUX = DIJ*(-UIJ*DLTYE+VIJ*DLTXE) (extel_edge.F:86-94) of the
@@ -529,6 +541,218 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_ext_cell(const 
   }
 }
 
+#ifdef FVG_F32_TU
+// -------------------------------------------------------------------------------------
+// Compact cell kernel of the precision form's stage loop (F32::compact; no limiter, GCN).
+// The same steps as k_ext_cell<float, false> -- FLUX_OBN, ADVAVE's edge loop in FP32 with
+// the FP64 surface-slope pressure gradient, EXTUV_EDGE and BCOND_GCN(2) in FP64, the cell
+// part of the stage's update -- over smaller records:
+//   * a slot is {code, other cell, IENODE1, IENODE2}; the edge's geometry is formed in FP64
+//     from the node and cell coordinates (XIJC = (VX1+VX2)/2, DLTXC = VX2-VX1, the offsets
+//     XIJC-XC rounded once to FP32, DLTXE = XIJC-XC of this cell for the continuity flux),
+//     values fvg_set_precision has checked equal, bit for bit, to the mesh's own metrics;
+//   * EXTUV's terms that stay fixed over the external loop are summed once per internal
+//     step (exc0, exc1, written by the internal-step ADVAVE call of this kernel), so that a
+//     stage reads five FP64 values per cell for them instead of thirteen;
+//   * ADVUA, ADVVA, PSTX, PSTY, which no later stage reads, are stored by the last stage
+//     (EC_LAST) and the internal-step call only.
+// -------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 8) k_ext_cell_c(const Dev P, int iext, int K, int parts) {
+  pdl_enter();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > P.N) return;
+  const size_t n1 = P.N + 1;
+  const int fl = P.f.cflag[i];
+  const int isbce = fl & 3;
+  const double ua_i = P.ua[i], va_i = P.va[i];
+  if (parts & EC_COPY_RK) {
+    P.uark[i] = ua_i;
+    P.vark[i] = va_i;
+    P.elrk1[i] = P.el1[i];
+  }
+  double elf1 = 0.0;
+  if (parts & EC_N2E) {
+    elf1 = ONE_THIRD * (P.elf[P.nv[i]] + P.elf[P.nv[n1 + i]] + P.elf[P.nv[2 * n1 + i]]);
+    P.elf1[i] = elf1;
+  } else if (parts & (EC_EXTUV | EC_FINISH)) {
+    elf1 = P.elf1[i];
+  }
+  double fob = 0.0;
+  if (parts & EC_FLUXOBN) {
+    if (fl & 32) fob = fluxobn_cell(P, i, K);
+    if ((fl & 32) || isbce == 2) P.fluxobn[i] = fob;
+  } else if (isbce == 2) {
+    fob = P.fluxobn[i];
+  }
+  const int weti = P.iswetce[i] * P.iswetc[i];
+  const double d1i = P.d1[i];
+  // {COR*ART, ART, H1, GRAV_E}: formed by the internal-step call below, read by the stages
+  const double4 e1 = (parts & EC_INT_ADVAVE) ? make_double4(0.0, 0.0, 0.0, P.grav_e[i]) : P.f.exc1[i];
+  double xf = 0.0, yf = 0.0, px = 0.0, py = 0.0;
+  if (parts & (EC_ADVAVE | EC_INT_ADVAVE)) {
+    const float half = 0.5f, one = 1.0f;
+    const double ged1 = e1.w * d1i;
+    const float4 gi4 = P.f.g2d4[i];
+    const float2 aci = P.f.artcc[i];
+    const double2 xyi = P.f.xyc[i];
+    const float ui = (float)ua_i, vi = (float)va_i;
+    const float epor = (fl & 8) ? 1.0f : 0.0f, iucp = (fl & 4) ? 1.0f : 0.0f;
+    float xr = 0.f, yr = 0.f;
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const int4 sl = P.f.slot4[(size_t)s * n1 + i];  // {code, other cell, IENODE1, IENODE2}
+      const int code = sl.x, side = code & 1, o = sl.y, j1 = sl.z, j2 = sl.w;
+      const double2 v1 = P.f.vxy[j1], v2 = P.f.vxy[j2];
+      const double xijc = (v1.x + v2.x) / 2.0, yijc = (v1.y + v2.y) / 2.0;
+      const double dltxc = v2.x - v1.x, dltyc = v2.y - v1.y;
+      const float dij = (float)(0.5 * (P.d[j1] + P.d[j2]));
+      const double elij = 0.5 * (P.el[j1] + P.el[j2]);
+      if (weti == 1 || P.iswetce[o] * P.iswetc[o] == 1) {
+        const float4 go4 = P.f.g2d4[o];
+        const float2 aco = P.f.artcc[o];
+        const double2 xyo = P.f.xyc[o];
+        const float uo = (float)P.ua[o], vo = (float)P.va[o];
+        const float xoi = (float)(xijc - xyi.x), yoi = (float)(yijc - xyi.y);
+        const float xoo = (float)(xijc - xyo.x), yoo = (float)(yijc - xyo.y);
+        // side 0: this cell is IA; side 1: this cell is IB
+        const float4 ga = side == 0 ? gi4 : go4, gb = side == 0 ? go4 : gi4;
+        const float uia = side == 0 ? ui : uo, via = side == 0 ? vi : vo;
+        const float uib = side == 0 ? uo : ui, vib = side == 0 ? vo : vi;
+        const float xa = side == 0 ? xoi : xoo, ya = side == 0 ? yoi : yoo;
+        const float xb = side == 0 ? xoo : xoi, yb = side == 0 ? yoo : yoi;
+        const float arta = side == 0 ? aci.x : aco.x, artb = side == 0 ? aco.x : aci.x;
+        const float cca = side == 0 ? aci.y : aco.y, ccb = side == 0 ? aco.y : aci.y;
+        // ga = {UX, UY, VX, VY} of IA, gb of IB
+        const float uij1 = uia + ga.x * xa + ga.y * ya;
+        const float vij1 = via + ga.z * xa + ga.w * ya;
+        const float uij2 = uib + gb.x * xb + gb.y * yb;
+        const float vij2 = vib + gb.z * xb + gb.w * yb;
+        const float uij = half * (uij1 + uij2);
+        const float vij = half * (vij1 + vij2);
+        const float dx = (float)dltxc, dy = (float)dltyc;
+        const float un = -uij * dy + vij * dx;
+        const float viscof1 = arta * sqrtf(ga.x * ga.x + ga.w * ga.w + half * ((ga.y + ga.z) * (ga.y + ga.z)));
+        const float viscof2 = artb * sqrtf(gb.x * gb.x + gb.w * gb.w + half * ((gb.y + gb.z) * (gb.y + gb.z)));
+        const float viscof =
+            ((float)P.fact * half * (viscof1 * cca + viscof2 * ccb) + (float)P.fm1 * half * (cca + ccb)) / (float)P.hprnu;
+        const float txx = (ga.x + gb.x) * viscof;
+        const float tyy = (ga.w + gb.w) * viscof;
+        const float txy = half * (ga.y + gb.y + ga.z + gb.z) * viscof;
+        const float fxx = dij * (txx * dy - txy * dx);
+        const float fyy = dij * (txy * dy - tyy * dx);
+        const float sg = fsign1(un);
+        const float xadv = dij * un * ((one - sg) * uij2 + (one + sg) * uij1) * half;
+        const float yadv = dij * un * ((one - sg) * vij2 + (one + sg) * vij1) * half;
+        const float nb = one - (float)((code >> 1) & 1);
+        if (side == 0) {
+          xr = xr + (xadv + fxx * epor) * nb * iucp;
+          yr = yr + (yadv + fyy * epor) * nb * iucp;
+        } else {
+          xr = xr - (xadv + fxx * epor) * nb * iucp;
+          yr = yr - (yadv + fyy * epor) * nb * iucp;
+        }
+      }
+      if (side == 0) {
+        px = px - ged1 * elij * dltyc;
+        py = py + ged1 * elij * dltxc;
+      } else {
+        px = px + ged1 * elij * dltyc;
+        py = py - ged1 * elij * dltxc;
+      }
+    }
+    const float w = (float)weti;
+    xf = (double)(xr * w);
+    yf = (double)(yr * w);
+    if (isbce == 2) {
+      const double iu = (fl & 4) ? 1.0 : 0.0;
+      xf = (xf + fob * ua_i) * iu;
+      yf = (yf + fob * va_i) * iu;
+    }
+    if (fl & 16) {
+      for (int q = P.cell_riv_ptr[i]; q < P.cell_riv_ptr[i + 1]; ++q) {
+        int k = P.cell_riv[q] >> 1;
+        double vlctyq = P.qdis[k] / P.qarea[k];
+        if (P.river_location == 0) {
+          xf = xf - 0.5 * P.qdis[k] * vlctyq * P.cos_angleq[k];
+          yf = yf - 0.5 * P.qdis[k] * vlctyq * P.sin_angleq[k];
+        } else {
+          double temp = P.qdis[k] * vlctyq;
+          xf = xf - temp * P.cos_angleq[k];
+          yf = yf - temp * P.sin_angleq[k];
+        }
+      }
+    }
+    if (parts & (EC_LAST | EC_INT_ADVAVE)) {
+      P.advua[i] = xf;
+      P.advva[i] = yf;
+      P.pstx[i] = px;
+      P.psty[i] = py;
+    }
+    if (parts & EC_INT_ADVAVE) {
+      // ADX2D -= ADVUA (internal_step.F:387-392), then EXTUV's fixed terms of the coming
+      // external loop
+      const double adx = P.adx2d[i] - xf, ady = P.ady2d[i] - yf;
+      P.adx2d[i] = adx;
+      P.ady2d[i] = ady;
+      const double art = P.art[i];
+      const double wx = P.have_wind ? 0.001 * P.wsx[i] * art : 0.0;
+      const double wy = P.have_wind ? 0.001 * P.wsy[i] * art : 0.0;
+      P.f.exc0[i] = make_double4(adx + P.drx2d[i] - P.wubot[i] * art, ady + P.dry2d[i] - P.wvbot[i] * art, wx, wy);
+      P.f.exc1[i] = make_double4(P.cor[i] * art, art, P.h1[i], P.grav_e[i]);
+    }
+  }
+  if (parts & (EC_EXTUV | EC_BC2)) {
+    double uaf = 0.0, vaf = 0.0;
+    if (parts & EC_EXTUV) {
+      if (weti == 1) {
+        const double4 e0 = P.f.exc0[i];
+        const double ramp = sched_row(P)[P.sl.ramp_ext(iext)];
+        const double resx = e0.x + xf + px - e1.x * va_i * d1i - ramp * e0.z;
+        const double resy = e0.y + yf + py + e1.x * ua_i * d1i - ramp * e0.w;
+        const double a = dAlphaRK[K];
+        const double uark = (parts & EC_COPY_RK) ? ua_i : P.uark[i];
+        const double vark = (parts & EC_COPY_RK) ? va_i : P.vark[i];
+        const double elrk1 = (parts & EC_COPY_RK) ? P.el1[i] : P.elrk1[i];
+        uaf = (uark * (e1.z + elrk1) - a * P.dte * resx / e1.y) / (e1.z + elf1);
+        vaf = (vark * (e1.z + elrk1) - a * P.dte * resy / e1.y) / (e1.z + elf1);
+      }
+      if (fl & 64) {
+        const double sp = P.cc_sponge[i];
+        uaf = uaf / (1.0 + sp * (uaf * uaf));
+        vaf = vaf / (1.0 + sp * (vaf * vaf));
+      }
+    } else {
+      uaf = P.uaf[i];
+      vaf = P.vaf[i];
+    }
+    if (parts & EC_BC2) {
+      if (isbce == 3) { uaf = 0.0; vaf = 0.0; }
+      if (isbce == 1) bc_solid(P, i, P.cell_bcriv[i], uaf, vaf);
+    }
+    P.uaf[i] = uaf;
+    P.vaf[i] = vaf;
+    if (parts & EC_FINISH) {
+      // cell part of the stage's update (ext_update_cell) with DLTXE, DLTYE = XIJC-XC
+      P.el1[i] = elf1;
+      const double dd1 = e1.z + elf1;
+      P.d1[i] = dd1;
+      if (K == 3) {
+        P.uard[i] = P.uard[i] + uaf * dd1;
+        P.vard[i] = P.vard[i] + vaf * dd1;
+      }
+      const double2 xyi = P.f.xyc[i];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const int4 sl = P.f.slot4[(size_t)s * n1 + i];
+        const double2 v1 = P.f.vxy[sl.z], v2 = P.f.vxy[sl.w];
+        const double dxe = (v1.x + v2.x) / 2.0 - xyi.x, dye = (v1.y + v2.y) / 2.0 - xyi.y;
+        P.exf2d[(size_t)s * P.ns + i] = dd1 * (-uaf * dye + vaf * dxe);
+      }
+    }
+  }
+}
+#endif  // FVG_F32_TU
+
 // -------------------------------------------------------------------------------------
 // external_step.F:333-436: EL=ELF, EL1=N2E2D(EL), D, D1, UA=UAF, DTFA, the K==3 sums
 // for the 3-D correction, the K==4 open-boundary transport and WD_UPDATE(1).
@@ -653,6 +877,48 @@ void launch_make_f32(const Dev& P, cudaStream_t s) {
   if ((size_t)P.N + 1 > npk) npk = P.N + 1;
   k_pack_he_f32<<<nblk(npk, 256), 256, 0, s>>>(P);
 }
+#ifndef FVG_F32_TU
+// Records of the compact stage kernel, and the count of mesh metrics that differ from the
+// values the kernel forms from the coordinates (then the compact kernel is not used).
+__global__ void k_make_compact(const Dev P, int* mismatch) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= P.M) P.f.vxy[i] = make_double2(P.vx[i], P.vy[i]);
+  if (i > P.N) return;
+  P.f.xyc[i] = make_double2(P.xc[i], P.yc[i]);
+  P.f.artcc[i] = make_float2((float)P.art[i], (float)P.cc_hvc[i]);
+  if (i == 0) return;
+  const size_t n1 = P.N + 1;
+  int bad = 0;
+  for (int s = 0; s < 3; ++s) {
+    const size_t q = (size_t)s * n1 + i;
+    const int code = P.ce_code[q], ia = P.ce_ia[q], ib = P.ce_ib[q], j1 = P.ce_j1[q], j2 = P.ce_j2[q];
+    const int side = code & 1;
+    if ((side == 0 ? ia : ib) != i) ++bad;
+    P.f.slot4[q] = make_int4(code, side == 0 ? ib : ia, j1, j2);
+    const double xijc = (P.vx[j1] + P.vx[j2]) / 2.0, yijc = (P.vy[j1] + P.vy[j2]) / 2.0;
+    if (xijc - P.xc[ia] != P.ce_xoa[q] || yijc - P.yc[ia] != P.ce_yoa[q]) ++bad;
+    if (xijc - P.xc[ib] != P.ce_xob[q] || yijc - P.yc[ib] != P.ce_yob[q]) ++bad;
+    if (P.vx[j2] - P.vx[j1] != P.ce_dx[q] || P.vy[j2] - P.vy[j1] != P.ce_dy[q]) ++bad;
+    const size_t pos = (size_t)s * P.ns + i;
+    if (P.hg[pos] != xijc - P.xc[i] || P.hg[P.ncvs + pos] != yijc - P.yc[i]) ++bad;
+  }
+  const double iu = P.iucp[i], ep = P.epor[i];
+  if (!(iu == 0.0 || iu == 1.0) || !(ep == 0.0 || ep == 1.0)) ++bad;
+  int fl = P.isbce[i] & 3;
+  if (iu == 1.0) fl |= 4;
+  if (ep == 1.0) fl |= 8;
+  if (P.cell_riv_ptr[i + 1] > P.cell_riv_ptr[i]) fl |= 16;
+  if (P.cell_obc_ptr[i + 1] > P.cell_obc_ptr[i]) fl |= 32;
+  if (P.cc_sponge[i] != 0.0) fl |= 64;
+  P.f.cflag[i] = fl;
+  if (bad) atomicAdd(mismatch, bad);
+}
+void launch_make_compact(const Dev& P, cudaStream_t s, int* mismatch) {
+  const int n = (P.M > P.N ? P.M : P.N) + 1;
+  k_make_compact<<<nblk(n, 256), 256, 0, s>>>(P, mismatch);
+}
+#endif
+
 void launch_wet_judge(const Dev& P, cudaStream_t s) {
   k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);
   k_wet_nodes<<<nblk(P.M, 256), 256, 0, s>>>(P);
@@ -663,6 +929,12 @@ void launch_wet_cells(const Dev& P, cudaStream_t s, int pdl) {
 void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts, int pdl) {
   FVG_F32_FORWARD(launch_ext_cell(P, s, iext, K, parts, pdl));
   void (*k)(const Dev, int, int, int);
+#ifdef FVG_F32_TU
+  if ((parts & EC_COMPACT) && P.f.compact && !P.limiter && !P.gcy) {
+    launch_maybe_pdl(pdl, k_ext_cell_c, dim3(nblk(P.N, 128)), dim3(128), s, P, iext, K, parts);
+    return;
+  }
+#endif
   k = P.limiter ? k_ext_cell<RF, true> : k_ext_cell<RF, false>;
   launch_maybe_pdl(pdl, k, dim3(nblk(P.N, 128)), dim3(128), s, P, iext, K, parts);
 }
