@@ -306,7 +306,12 @@ int fvg_closure_status(fvg_handle* h, int32_t* columns_on_network, int32_t* wait
    "compact"     = 1 (default) lets the precision form's Runge-Kutta stages use the
                    compact cell kernel where fvg_set_precision found the mesh's edge metrics
                    to be the ones its coordinates define; 0 keeps the general kernel.
-                   fvg_get_tuning("compact") reports whether the compact kernel is in use. */
+                   fvg_get_tuning("compact") reports whether the compact kernel is in use;
+   "staged"      = 2 runs ADVECTION_EDGE_GCN and ADV_UV_EDGE_GCN (LIMITED_NO, GCN) as the
+                   tile-staged kernels (neighbour cells in shared memory, each edge
+                   evaluated once per tile); 1 (default) only the FP64 ADV_UV, where the
+                   staged kernel measured faster; 0 keeps one thread per cell everywhere.
+                   Results do not depend on it (bit for bit in FP64). */
 int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value);
 int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value);
 

@@ -6,6 +6,7 @@
 // as a fixed kernel sequence; the sequence is captured once into a CUDA graph and
 // replayed, with the per-step scalars (RAMP, tidal phase arguments) supplied through a
 // device schedule table that the host fills ahead of each batch of steps.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -103,6 +104,91 @@ int upload3(fvg_handle* h, double** p, const double* src, size_t rows, int kb, s
 }
 
 inline size_t pad32(size_t n) { return (n + 31) / 32 * 32; }
+
+// Cell tiles of the staged momentum kernels (struct Tiles): recursive coordinate bisection
+// of the cell centroids, the larger extent split at a multiple of the tile size.  cl[i]:
+// cell i's edges (edge*2 + side) in ascending edge order; iec: IEC (NE+1, 2) column-major.
+struct TileBuild {
+  std::vector<int> ptr, nc, eptr, cells;
+  std::vector<int> edges, slots;  // 4 ints per entry
+  int cap_cells = 0, cap_edges = 0;
+};
+void rcb(std::vector<int>& ids, size_t b, size_t e, const double* xc, const double* yc, std::vector<size_t>& cuts) {
+  const size_t n = e - b;
+  if (n <= (size_t)fvg::kTileCells) {
+    cuts.push_back(e);
+    return;
+  }
+  double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+  for (size_t q = b; q < e; ++q) {
+    x0 = std::min(x0, xc[ids[q]]); x1 = std::max(x1, xc[ids[q]]);
+    y0 = std::min(y0, yc[ids[q]]); y1 = std::max(y1, yc[ids[q]]);
+  }
+  const bool byx = (x1 - x0) >= (y1 - y0);
+  const size_t ntile = (n + fvg::kTileCells - 1) / fvg::kTileCells;
+  const size_t mid = b + ((ntile + 1) / 2) * fvg::kTileCells;
+  auto key = [&](int c) { return byx ? std::make_pair(xc[c], c) : std::make_pair(yc[c], c); };
+  std::nth_element(ids.begin() + b, ids.begin() + mid, ids.begin() + e,
+                   [&](int a, int c) { return key(a) < key(c); });
+  rcb(ids, b, mid, xc, yc, cuts);
+  rcb(ids, mid, e, xc, yc, cuts);
+}
+void build_tiles(int N, int NE, const double* xc, const double* yc, const int* iec, const int* ienode,
+                 const int* isbc, const std::vector<std::vector<int>>& cl, TileBuild& tb) {
+  const size_t e1 = (size_t)NE + 1;
+  std::vector<int> ids(N);
+  for (int i = 0; i < N; ++i) ids[i] = i + 1;
+  std::vector<size_t> cuts;
+  rcb(ids, 0, ids.size(), xc, yc, cuts);
+  std::vector<int> local((size_t)N + 1, -1), elocal(e1, -1);
+  size_t b = 0;
+  tb.ptr.push_back(0);
+  tb.eptr.push_back(0);
+  for (size_t cut : cuts) {
+    std::vector<int> own(ids.begin() + b, ids.begin() + cut);
+    b = cut;
+    std::sort(own.begin(), own.end());
+    std::vector<int> all(own), elist;
+    for (size_t j = 0; j < own.size(); ++j) local[own[j]] = (int)j;
+    for (int c : own)
+      for (int code : cl[c]) {
+        const int e = code >> 1, side = code & 1;
+        const int o = side == 0 ? iec[e1 + e] : iec[e];
+        if (local[o] < 0) {
+          local[o] = (int)all.size();
+          all.push_back(o);
+        }
+        if (elocal[e] < 0) {
+          elocal[e] = (int)elist.size();
+          elist.push_back(e);
+        }
+      }
+    for (int e : elist) {
+      tb.edges.push_back(e);
+      tb.edges.push_back(local[iec[e]] | (local[iec[e1 + e]] << 16));
+      tb.edges.push_back(ienode[e]);
+      tb.edges.push_back(ienode[e1 + e]);
+    }
+    for (int c : own) {
+      for (int sl = 0; sl < 3; ++sl) {
+        const int code = cl[c][sl], e = code >> 1;
+        tb.slots.push_back(elocal[e] | ((code & 1) << 16) | ((isbc[e] != 0 ? 1 : 0) << 17));
+      }
+      tb.slots.push_back(0);
+    }
+    for (int c : all) tb.cells.push_back(c);
+    tb.nc.push_back((int)own.size());
+    tb.ptr.push_back((int)tb.cells.size());
+    // own cells' slot entries are padded to the tile's cell count (halo entries unused)
+    for (size_t j = own.size(); j < all.size(); ++j)
+      for (int w = 0; w < 4; ++w) tb.slots.push_back(0);
+    tb.eptr.push_back((int)(tb.edges.size() / 4));
+    tb.cap_cells = std::max(tb.cap_cells, (int)all.size());
+    tb.cap_edges = std::max(tb.cap_edges, (int)elist.size());
+    for (int c : all) local[c] = -1;
+    for (int e : elist) elocal[e] = -1;
+  }
+}
 
 int build_csr(const std::vector<std::vector<int>>& lists, std::vector<int>& ptr, std::vector<int>& ent) {
   ptr.assign(lists.size() + 1, 0);
@@ -483,6 +569,29 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
       UPI(ce_j1, cj1.data(), S3); UPI(ce_j2, cj2.data(), S3);
       UPD(ce_xoa, xa.data(), S3); UPD(ce_yoa, ya.data(), S3); UPD(ce_xob, xb.data(), S3);
       UPD(ce_yob, yb.data(), S3); UPD(ce_dx, dx.data(), S3); UPD(ce_dy, dy.data(), S3);
+    }
+    // cell tiles of the staged momentum flux kernels
+    {
+      TileBuild tb;
+      build_tiles(N, m->ne, m->xc, m->yc, m->iec, m->ienode, m->isbc, cl, tb);
+      if (tb.cap_edges >= (1 << 16) || tb.cap_cells >= (1 << 16)) {
+        h->err = "tile builder: a tile with too many edges";
+        return fail(FVG_ERR_BOUNDS);
+      }
+      P.tl.n = (int)tb.nc.size();
+      P.tl.cap_cells = tb.cap_cells;
+      P.tl.cap_edges = tb.cap_edges;
+      UPI(tl.ptr, tb.ptr.data(), tb.ptr.size());
+      UPI(tl.nc, tb.nc.data(), tb.nc.size());
+      UPI(tl.eptr, tb.eptr.data(), tb.eptr.size());
+      UPI(tl.cells, tb.cells.data(), tb.cells.size());
+      UPI(tl.edges, tb.edges.data(), tb.edges.size());
+      UPI(tl.slots, tb.slots.data(), tb.slots.size());
+      P.staged = 1;
+      if (staged_setup() || fvg_f32::staged_setup()) {
+        h->err = "cannot configure the staged momentum kernels";
+        return fail(FVG_ERR_CUDA);
+      }
     }
     std::vector<std::vector<int>> ch(n1);
     for (int he = 1; he <= m->ncv; ++he) ch[m->ntrg[he]].push_back(he);
@@ -1167,6 +1276,9 @@ int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value) {
   } else if (k == "col_layers") {
     if (value < 1 || value > h->P.KB) { h->err = "col_layers must be 1..KB"; return FVG_ERR_ARG; }
     h->P.col_lc = value;
+  } else if (k == "staged") {
+    if (value < 0 || value > 2) { h->err = "staged must be 0, 1 or 2"; return FVG_ERR_ARG; }
+    h->P.staged = value;
   } else if (k == "compact") {
     h->compact_allowed = value != 0;
     h->P.f.compact = (h->P.prec == FVG_PREC_FP32_FLUX && h->compact_ok && h->compact_allowed) ? 1 : 0;
@@ -1187,6 +1299,7 @@ int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value) {
   if (k == "col_threads") *value = h->P.col_bc;
   else if (k == "col_layers") *value = h->P.col_lc;
   else if (k == "compact") *value = h->P.f.compact;
+  else if (k == "staged") *value = h->P.staged;
   else return FVG_ERR_ARG;
   return FVG_OK;
 }

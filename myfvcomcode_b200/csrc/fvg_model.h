@@ -87,6 +87,21 @@ struct ClosNorm {
   float tmean[3], tstd[3], teps;
 };
 
+// Cell tiles of the staged 3-D momentum flux kernels.  The cells are split by recursive
+// coordinate bisection of their centroids into compact tiles of at most kTileCells cells
+// (cells ascending within a tile).  Tile t owns entries ptr[t] .. ptr[t+1]-1 of `cells`:
+// its nc[t] own cells, then its halo (the other cells of its cells' edges, the ghost cell
+// 0 included where an edge has one).  Its edges are entries eptr[t] .. eptr[t+1]-1 of
+// `edges`, each {edge number, local IA | local IB << 16, IENODE1, IENODE2}, local indices
+// counting from ptr[t]; own cell j's three edges in slot order are slots[ptr[t]+j], each
+// {local edge | side << 16 | ISBC << 17} (w unused).
+constexpr int kTileCells = 128;
+struct Tiles {
+  int n, cap_cells, cap_edges;
+  const int *ptr, *nc, *eptr, *cells;
+  const int4 *edges, *slots;
+};
+
 // Device pointers and sizes, passed by value to kernels.
 struct Dev {
   int M, N, KB, KBM1, KBM2, NE, NCV, NCV_I, ms, ns;
@@ -224,6 +239,10 @@ struct Dev {
   double* clos_plain;
   int* clos_env;
   int* clos_err;
+  Tiles tl;
+  // 1: ADVECTION_EDGE_GCN and ADV_UV_EDGE_GCN run as the tile-staged kernels (no limiter,
+  // GCN); 0: one thread per cell gathering its neighbours (tuning key "staged").
+  int staged;
   // Column tiling of the 3-D gather kernels: col_bc threads (entities) per block, each
   // walking col_lc consecutive layers, so the entity's index chain (cell -> edge ->
   // neighbour) is resolved from cache after the first layer.  Results do not depend on it.
@@ -434,6 +453,7 @@ enum VertvlColParts { VC_WTS = 1, VC_WD2 = 2, VC_RHO_ROUNDTRIP = 4, VC_BOT_NODE 
 void launch_vertvl_col(const Dev& P, cudaStream_t s, int parts);
 void launch_w_viscofh(const Dev& P, cudaStream_t s, int do_w, int do_visc);
 void launch_adv_uv(const Dev& P, cudaStream_t s);
+int staged_setup();  // shared-memory limit of the tile-staged momentum kernels; 0 on success
 enum VdifUvParts { VU_VDIF = 1, VU_BC3 = 2, VU_WREAL = 4 };
 void launch_vdif_uv(const Dev& P, cudaStream_t s, int parts);
 
@@ -467,6 +487,7 @@ void launch_adv_uv(const Dev& P, cudaStream_t s);
 void launch_grad(const Dev& P, cudaStream_t s, int which);
 void launch_adv_q(const Dev& P, cudaStream_t s, int parts);
 void launch_adv_ts(const Dev& P, cudaStream_t s, int parts);
+int staged_setup();
 }  // namespace fvg_f32
 
 // RF: the arithmetic type of the flux kernels this translation unit launches.

@@ -315,6 +315,20 @@ __device__ inline void river3(const Dev& P, int i, int k, double& x, double& y) 
   }
 }
 
+// The end of ADVECTION_EDGE_GCN for cell i on layer k once its three edges are summed
+// into xr, yr (advection_edge_gcn.F:674-708): wet mask, open-boundary cells, rivers.
+template <typename R>
+__device__ inline void advection3d_tail(const Dev& P, int i, int k, R xr, R yr) {
+  double x = (double)xr, y = (double)yr;
+  double w = (double)(P.iswetct[i] * P.iswetc[i]);
+  x = x * w;
+  y = y * w;
+  if (P.isbce[i] == 2) { x = 0.0; y = 0.0; }
+  river3(P, i, k, x, y);
+  P.advx[C3(P, i, k)] = x;
+  P.advy[C3(P, i, k)] = y;
+}
+
 // -------------------------------------------------------------------------------------
 // ADVECTION_EDGE_GCN (advection_edge_gcn.F:397-708): per cell and layer, the cell's three
 // edges in ascending edge number.
@@ -361,14 +375,7 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && !LIM) ? 4 : 1) k_advec
       yr = yr - f.yadv * tp - vfy;
     }
   }
-  double x = (double)xr, y = (double)yr;
-  double w = (double)(P.iswetct[i] * P.iswetc[i]);
-  x = x * w;
-  y = y * w;
-  if (P.isbce[i] == 2) { x = 0.0; y = 0.0; }
-  river3(P, i, k, x, y);
-  P.advx[C3(P, i, k)] = x;
-  P.advy[C3(P, i, k)] = y;
+  advection3d_tail<R>(P, i, k, xr, yr);
   }
 }
 
@@ -703,6 +710,60 @@ __global__ void __launch_bounds__(256) k_w_viscofh(const Dev P, int do_w, int do
   }
 }
 
+// The end of ADV_UV_EDGE_GCN for cell i on layer k once its three edges are summed into
+// xr, yr, vmr and the pressure-gradient terms into px, py (adv_uv_edge_gcn.F:884-1193):
+// wet mask, vertical advection, DRHOX, Coriolis, open-boundary cells, rivers, the update
+// to UF, VF and VISCOFM.
+template <typename R>
+__device__ inline void adv_uv_tail(const Dev& P, int i, int k, R xr, R yr, R vmr, double px, double py,
+                                   double dz1i) {
+  double x = (double)xr, y = (double)yr, vm = (double)vmr;
+  bool wet = P.iswetct[i] * P.iswetc[i] == 1;
+  double w = (double)(P.iswetct[i] * P.iswetc[i]);
+  x = x * w;
+  y = y * w;
+  px = px * w;
+  py = py * w;
+  x = x + px;
+  y = y + py;
+  size_t q = C3(P, i, k);
+  if (wet) {
+    const double *U = P.u, *V = P.v, *W = P.w, *DZ1 = P.dz1;
+    double xfv, yfv;
+    if (k == 1) {
+      size_t qp = C3(P, i, k + 1);
+      xfv = -W[qp] * (U[q] * DZ1[qp] + U[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
+      yfv = -W[qp] * (V[q] * DZ1[qp] + V[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
+    } else if (k == P.KBM1) {
+      size_t qm = C3(P, i, k - 1);
+      xfv = W[q] * (U[q] * DZ1[qm] + U[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]);
+      yfv = W[q] * (V[q] * DZ1[qm] + V[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]);
+    } else {
+      size_t qm = C3(P, i, k - 1), qp = C3(P, i, k + 1);
+      xfv = W[q] * (U[q] * DZ1[qm] + U[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]) -
+            W[qp] * (U[q] * DZ1[qp] + U[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
+      yfv = W[q] * (V[q] * DZ1[qm] + V[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]) -
+            W[qp] * (V[q] * DZ1[qp] + V[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
+    }
+    x = x + xfv * P.art[i] + P.drhox[q] - P.cor[i] * V[q] * P.dt1[i] * DZ1[q] * P.art[i];
+    y = y + yfv * P.art[i] + P.drhoy[q] + P.cor[i] * U[q] * P.dt1[i] * DZ1[q] * P.art[i];
+  }
+  if (P.isbce[i] == 2) { x = 0.0; y = 0.0; }
+  river3(P, i, k, x, y);
+  double uf, vf;
+  if (wet) {
+    double d1 = P.d1[i];
+    uf = P.u[q] * P.dt1[i] / d1 - P.dti * x / P.art[i] / (d1 * dz1i);
+    vf = P.v[q] * P.dt1[i] / d1 - P.dti * y / P.art[i] / (d1 * dz1i);
+  } else {
+    uf = 0.0;
+    vf = 0.0;
+  }
+  P.uf[q] = uf;
+  P.vf[q] = vf;
+  P.viscofm[q] = vm / P.art[i];
+}
+
 // -------------------------------------------------------------------------------------
 // ADV_UV_EDGE_GCN (adv_uv_edge_gcn.F:124-1193): horizontal advection/diffusion, the
 // internal barotropic pressure gradient from EGF, vertical advection, baroclinic
@@ -763,52 +824,221 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && !LIM) ? 4 : 1) k_adv_u
       py = py - gdd * elij * edx;
     }
   }
-  double x = (double)xr, y = (double)yr, vm = (double)vmr;
-  bool wet = P.iswetct[i] * P.iswetc[i] == 1;
-  double w = (double)(P.iswetct[i] * P.iswetc[i]);
-  x = x * w;
-  y = y * w;
-  px = px * w;
-  py = py * w;
-  x = x + px;
-  y = y + py;
-  size_t q = C3(P, i, k);
-  if (wet) {
-    const double *U = P.u, *V = P.v, *W = P.w, *DZ1 = P.dz1;
-    double xfv, yfv;
-    if (k == 1) {
-      size_t qp = C3(P, i, k + 1);
-      xfv = -W[qp] * (U[q] * DZ1[qp] + U[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
-      yfv = -W[qp] * (V[q] * DZ1[qp] + V[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
-    } else if (k == P.KBM1) {
-      size_t qm = C3(P, i, k - 1);
-      xfv = W[q] * (U[q] * DZ1[qm] + U[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]);
-      yfv = W[q] * (V[q] * DZ1[qm] + V[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]);
-    } else {
-      size_t qm = C3(P, i, k - 1), qp = C3(P, i, k + 1);
-      xfv = W[q] * (U[q] * DZ1[qm] + U[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]) -
-            W[qp] * (U[q] * DZ1[qp] + U[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
-      yfv = W[q] * (V[q] * DZ1[qm] + V[qm] * DZ1[q]) / (DZ1[q] + DZ1[qm]) -
-            W[qp] * (V[q] * DZ1[qp] + V[qp] * DZ1[q]) / (DZ1[q] + DZ1[qp]);
-    }
-    x = x + xfv * P.art[i] + P.drhox[q] - P.cor[i] * V[q] * P.dt1[i] * DZ1[q] * P.art[i];
-    y = y + yfv * P.art[i] + P.drhoy[q] + P.cor[i] * U[q] * P.dt1[i] * DZ1[q] * P.art[i];
+  adv_uv_tail<R>(P, i, k, xr, yr, vmr, px, py, dz1i);
   }
-  if (P.isbce[i] == 2) { x = 0.0; y = 0.0; }
-  river3(P, i, k, x, y);
-  double uf, vf;
-  if (wet) {
-    double d1 = P.d1[i];
-    uf = P.u[q] * P.dt1[i] / d1 - P.dti * x / P.art[i] / (d1 * dz1i);
-    vf = P.v[q] * P.dt1[i] / d1 - P.dti * y / P.art[i] / (d1 * dz1i);
+}
+
+// -------------------------------------------------------------------------------------
+// Tile-staged ADVECTION_EDGE_GCN (UV = false) and ADV_UV_EDGE_GCN (UV = true), LIMITED_NO
+// and GCN.  One CTA per cell tile (struct Tiles) and chunk of layers.  Per layer, the
+// tile's cells and their halo -- U, V and the least-squares gradient, with ART, CC_HVC and
+// the wet flags staged once -- are loaded into shared memory; every edge of the tile is
+// evaluated once from there into shared memory (an interior edge serves both its cells);
+// then each own cell sums its three edges in ascending edge number, as the reference's
+// scatter adds them, and finishes as the per-cell kernels do.  The edge arithmetic is
+// edge_flux3's term by term, so the FP64 instantiation equals the per-cell kernels bit
+// for bit.
+// -------------------------------------------------------------------------------------
+template <typename R>
+__device__ inline EdgeFlux<R> edge_flux_staged(const Dev& P, R ua, R va, const R* ga, R ub, R vb, const R* gb,
+                                               R arta, R artb, R cca, R ccb, R xija, R yija, R xijb, R yijb,
+                                               R dltxc, R dltyc, R dij, bool exflux_form) {
+  const R half = (R)0.5, one = (R)1.0;
+  // ga, gb: {UX, UY, VX, VY} of IA and IB
+  const R uij1 = ua + ga[0] * xija + ga[1] * yija;
+  const R vij1 = va + ga[2] * xija + ga[3] * yija;
+  const R uij2 = ub + gb[0] * xijb + gb[1] * yijb;
+  const R vij2 = vb + gb[2] * xijb + gb[3] * yijb;
+  R uij = half * (uij1 + uij2);
+  R vij = half * (vij1 + vij2);
+  R viscof1 = arta * sqrt(ga[0] * ga[0] + ga[3] * ga[3] + half * ((ga[1] + ga[2]) * (ga[1] + ga[2])));
+  R viscof2 = artb * sqrt(gb[0] * gb[0] + gb[3] * gb[3] + half * ((gb[1] + gb[2]) * (gb[1] + gb[2])));
+  R viscof = ((R)P.fact * half * (viscof1 * cca + viscof2 * ccb) + (R)P.fm1 * half * (cca + ccb)) / (R)P.hprnu;
+  R txx = (ga[0] + gb[0]) * viscof;
+  R tyy = (ga[3] + gb[3]) * viscof;
+  R txy = half * (ga[1] + gb[1] + ga[2] + gb[2]) * viscof;
+  EdgeFlux<R> f;
+  f.fxx = dij * (txx * dltyc - txy * dltxc);
+  f.fyy = dij * (txy * dltyc - tyy * dltxc);
+  f.viscof = viscof;
+  if (exflux_form) {
+    R exflux = dij * (-uij * dltyc + vij * dltxc);
+    R sg = fsign1(exflux);
+    f.xadv = exflux * ((one - sg) * uij2 + (one + sg) * uij1) * half;
+    f.yadv = exflux * ((one - sg) * vij2 + (one + sg) * vij1) * half;
   } else {
-    uf = 0.0;
-    vf = 0.0;
+    R un = vij * dltxc - uij * dltyc;
+    R sg = fsign1(un);
+    f.xadv = dij * un * ((one - sg) * uij2 + (one + sg) * uij1) * half;
+    f.yadv = dij * un * ((one - sg) * vij2 + (one + sg) * vij1) * half;
   }
-  P.uf[q] = uf;
-  P.vf[q] = vf;
-  P.viscofm[q] = vm / P.art[i];
+  return f;
+}
+
+// Shared memory of one CTA: FP64 DT of both edge nodes (and for UV ELIJ, DLTXC, DLTYC)
+// per edge; per cell U, V, UX, UY, VX, VY, ART, CC_HVC; per edge its six metrics and five
+// flux values; the cells' wet flags; per edge its two nodes, local cells and wet flag.
+template <typename R, bool UV>
+__host__ __device__ inline size_t staged_smem_bytes(int cc, int ec) {
+  return sizeof(double) * ((size_t)2 * ec + (UV ? (size_t)3 * ec : 0)) + sizeof(R) * ((size_t)8 * cc + (size_t)11 * ec) +
+         sizeof(int) * ((size_t)cc + (size_t)4 * ec);
+}
+
+template <typename R, bool UV>
+__global__ void __launch_bounds__(kTileCells, sizeof(R) == 4 ? 6 : 4) k_mom3d_staged(const Dev P) {
+  typedef Mesh<R> Mh;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const Tiles& T = P.tl;
+  const int t = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const int c0 = T.ptr[t], nall = T.ptr[t + 1] - c0, nc = T.nc[t];
+  const int e0 = T.eptr[t], ne = T.eptr[t + 1] - e0;
+  const int CC = T.cap_cells, EC = T.cap_edges;
+  double* s_dt = reinterpret_cast<double*>(sm_raw);   // [2][EC]
+  double* s_pg = s_dt + 2 * EC;                       // UV: [3][EC] ELIJ, DLTXC, DLTYC
+  R* s_c = reinterpret_cast<R*>(s_pg + (UV ? 3 * EC : 0));  // [8][CC]
+  R* s_e = s_c + 8 * CC;                              // [6][EC] XOA, YOA, XOB, YOB, DLTXC, DLTYC
+  R* s_f = s_e + 6 * EC;                              // [5][EC] XADV, YADV, FXX, FYY, VISCOF
+  int* s_w = reinterpret_cast<int*>(s_f + 5 * EC);    // [CC] ISWETCT*ISWETC
+  int* s_j = s_w + CC;                                // [3][EC] IENODE1, IENODE2, IA | IB << 16
+  int* s_ok = s_j + 3 * EC;                           // [EC] a side of the edge is wet
+
+  // fixed over the layers: the cells' ART, CC_HVC and wet flags, the edges' metrics
+  for (int q = tid; q < nall; q += nt) {
+    const int c = T.cells[c0 + q];
+    s_c[6 * CC + q] = Mh::art(P, c);
+    s_c[7 * CC + q] = Mh::cc_hvc(P, c);
+    s_w[q] = P.iswetct[c] * P.iswetc[c];
   }
+  __syncthreads();
+  for (int q = tid; q < ne; q += nt) {
+    const int4 ed = T.edges[e0 + q];  // {edge, IA | IB << 16, IENODE1, IENODE2}
+    const int e = ed.x, la = ed.y & 0xffff, lb = ed.y >> 16;
+    const int ia = T.cells[c0 + la], ib = T.cells[c0 + lb];
+    s_e[q] = Mh::xoa(P, e, ia);
+    s_e[EC + q] = Mh::yoa(P, e, ia);
+    s_e[2 * EC + q] = Mh::xob(P, e, ib);
+    s_e[3 * EC + q] = Mh::yob(P, e, ib);
+    s_e[4 * EC + q] = Mh::dltxc(P, e);
+    s_e[5 * EC + q] = Mh::dltyc(P, e);
+    s_dt[q] = P.dt[ed.z];
+    s_dt[EC + q] = P.dt[ed.w];
+    s_j[q] = ed.z;
+    s_j[EC + q] = ed.w;
+    s_j[2 * EC + q] = ed.y;
+    s_ok[q] = (s_w[la] == 1 || s_w[lb] == 1) ? 1 : 0;
+    if (UV) {
+      s_pg[q] = 0.5 * (P.egf[ed.z] + P.egf[ed.w]);
+      s_pg[EC + q] = P.dltxc[e];
+      s_pg[2 * EC + q] = P.dltyc[e];
+    }
+  }
+  const bool own = tid < nc;
+  const int4 sl = own ? T.slots[c0 + tid] : make_int4(0, 0, 0, 0);
+  const int i = own ? T.cells[c0 + tid] : 0;
+  int kb, ke;
+  col_range(P, 1, P.KBM1, kb, ke);
+  for (int k = kb; k <= ke; ++k) {
+    __syncthreads();
+    for (int q = tid; q < nall; q += nt) {
+      const size_t qq = C3(P, T.cells[c0 + q], k);
+      s_c[q] = (R)P.u[qq];
+      s_c[CC + q] = (R)P.v[qq];
+      s_c[2 * CC + q] = Mh::g3(P, 0)[qq];
+      s_c[3 * CC + q] = Mh::g3(P, 1)[qq];
+      s_c[4 * CC + q] = Mh::g3(P, 2)[qq];
+      s_c[5 * CC + q] = Mh::g3(P, 3)[qq];
+    }
+    __syncthreads();
+    for (int q = tid; q < ne; q += nt) {
+      if (!s_ok[q]) continue;
+      const int lab = s_j[2 * EC + q], la = lab & 0xffff, lb = lab >> 16;
+      const R dij = (R)(0.5 * (s_dt[q] * P.dz[N3(P, s_j[q], k)] + s_dt[EC + q] * P.dz[N3(P, s_j[EC + q], k)]));
+      const R ga[4] = {s_c[2 * CC + la], s_c[3 * CC + la], s_c[4 * CC + la], s_c[5 * CC + la]};
+      const R gb[4] = {s_c[2 * CC + lb], s_c[3 * CC + lb], s_c[4 * CC + lb], s_c[5 * CC + lb]};
+      const EdgeFlux<R> f = edge_flux_staged<R>(P, s_c[la], s_c[CC + la], ga, s_c[lb], s_c[CC + lb], gb,
+                                                s_c[6 * CC + la], s_c[6 * CC + lb], s_c[7 * CC + la],
+                                                s_c[7 * CC + lb], s_e[q], s_e[EC + q], s_e[2 * EC + q],
+                                                s_e[3 * EC + q], s_e[4 * EC + q], s_e[5 * EC + q], dij, UV);
+      s_f[q] = f.xadv;
+      s_f[EC + q] = f.yadv;
+      s_f[2 * EC + q] = f.fxx;
+      s_f[3 * EC + q] = f.fyy;
+      s_f[4 * EC + q] = f.viscof;
+    }
+    __syncthreads();
+    if (!own) continue;
+    const R epor = (R)P.epor[i], three = (R)3.0;
+    R xr = 0, yr = 0, vmr = 0;
+    double px = 0.0, py = 0.0, dz1i = 0.0, gdd = 0.0;
+    if (UV) {
+      dz1i = P.dz1[C3(P, i, k)];
+      gdd = P.grav_e[i] * P.dt1[i] * dz1i;
+    }
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const int w = s == 0 ? sl.x : (s == 1 ? sl.y : sl.z);
+      const int le = w & 0xffff, side = (w >> 16) & 1, isbc = (w >> 17) & 1;
+      if (s_ok[le]) {
+        if (UV) vmr = vmr + s_f[4 * EC + le];
+        const R isb = (R)isbc;
+        const R tp = (R)((double)(float)(1 - isbc) * P.epor[i]);
+        const R fxx = s_f[2 * EC + le], fyy = s_f[3 * EC + le];
+        const R vfx = (fxx + three * fxx * isb) * epor;
+        const R vfy = (fyy + three * fyy * isb) * epor;
+        if (side == 0) {
+          xr = xr + s_f[le] * tp + vfx;
+          yr = yr + s_f[EC + le] * tp + vfy;
+        } else {
+          xr = xr - s_f[le] * tp - vfx;
+          yr = yr - s_f[EC + le] * tp - vfy;
+        }
+      }
+      if (UV) {
+        const double elij = s_pg[le], edx = s_pg[EC + le], edy = s_pg[2 * EC + le];
+        if (side == 0) {
+          px = px - gdd * elij * edy;
+          py = py + gdd * elij * edx;
+        } else {
+          px = px + gdd * elij * edy;
+          py = py - gdd * elij * edx;
+        }
+      }
+    }
+    if (UV)
+      adv_uv_tail<R>(P, i, k, xr, yr, vmr, px, py, dz1i);
+    else
+      advection3d_tail<R>(P, i, k, xr, yr);
+  }
+}
+
+constexpr int kStagedSmemMax = 200 * 1024;
+template <typename R, bool UV>
+static void launch_mom3d_staged(const Dev& P, cudaStream_t s) {
+  const size_t smem = staged_smem_bytes<R, UV>(P.tl.cap_cells, P.tl.cap_edges);
+  const dim3 grid((unsigned)P.tl.n, (unsigned)((P.KBM1 + P.col_lc - 1) / P.col_lc));
+  k_mom3d_staged<R, UV><<<grid, kTileCells, smem, s>>>(P);
+}
+// Whether the staged kernel of ADVECTION (UV false) or ADV_UV (UV true) runs: LIMITED_NO,
+// GCN, a tile table whose shared memory fits one CTA, and P.staged = 2 (every staged
+// kernel), or P.staged = 1 (the default: only where it measured faster than the per-cell
+// kernel on the 200k-node, 40-layer coastal mesh, which is FP64 ADV_UV: 2.13 against
+// 2.52 ms per step; FP64 ADVECTION 1.35 against 1.26, FP32 ADVECTION 1.00 against 0.76,
+// FP32 ADV_UV 1.90 against 1.30).
+static bool staged_ok(const Dev& P, bool uv) {
+  const bool want = P.staged == 2 || (P.staged == 1 && uv && sizeof(RF) == 8);
+  return want && !P.limiter && !P.gcy && P.tl.n > 0 &&
+         staged_smem_bytes<double, true>(P.tl.cap_cells, P.tl.cap_edges) <= (size_t)kStagedSmemMax;
+}
+// Allow the staged kernels of this translation unit's arithmetic type up to
+// kStagedSmemMax bytes of dynamic shared memory (once, before any launch or capture).
+int staged_setup() {
+  if (cudaFuncSetAttribute(k_mom3d_staged<RF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kStagedSmemMax) != cudaSuccess)
+    return 1;
+  if (cudaFuncSetAttribute(k_mom3d_staged<RF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kStagedSmemMax) != cudaSuccess)
+    return 1;
+  return 0;
 }
 
 // -------------------------------------------------------------------------------------
@@ -964,6 +1194,10 @@ static void launch_alfa3(const Dev& P, cudaStream_t s) {
 }
 void launch_advection3d(const Dev& P, cudaStream_t s) {
   FVG_F32_FORWARD(launch_advection3d(P, s));
+  if (staged_ok(P, false)) {
+    launch_mom3d_staged<RF, false>(P, s);
+    return;
+  }
   if (P.limiter) launch_alfa3(P, s);
   (P.limiter ? k_advection3d<RF, true> : k_advection3d<RF, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }
@@ -1121,6 +1355,10 @@ void launch_w_viscofh(const Dev& P, cudaStream_t s, int do_w, int do_visc) {
 }
 void launch_adv_uv(const Dev& P, cudaStream_t s) {
   FVG_F32_FORWARD(launch_adv_uv(P, s));
+  if (staged_ok(P, true)) {
+    launch_mom3d_staged<RF, true>(P, s);
+    return;
+  }
   if (P.limiter) launch_alfa3(P, s);
   (P.limiter ? k_adv_uv<RF, true> : k_adv_uv<RF, false>)<<<col_grid(P, P.N, P.KBM1), P.col_bc, 0, s>>>(P);
 }

@@ -88,3 +88,20 @@ def test_compact_stage_kernel_matches_general_kernel(case_name, request):
         x, y = a.get(n), b.get(n)
         scale = max(float(np.abs(y).max()), 1e-12)
         assert np.abs(x - y).max() <= 1e-3 * scale, n
+
+
+def test_staged_momentum_kernels_in_precision_form(small_coastal):
+    """The FP32 instantiations of the tile-staged momentum kernels against the per-cell
+    FP32 kernels (same arithmetic; multiply-add contraction may differ): close."""
+    from myfvcomcode_b200.engine import Fvcom
+    a, b = Fvcom(small_coastal), Fvcom(small_coastal)
+    for f in (a, b):
+        f.set_precision("fp32flux")
+    a.set_tuning("staged", 2)
+    b.set_tuning("staged", 0)
+    a.run(4)
+    b.run(4)
+    for n in ("u", "v", "advx", "viscofm", "el"):
+        x, y = a.get(n), b.get(n)
+        scale = max(float(np.abs(y).max()), 1e-12)
+        assert np.abs(x - y).max() <= 1e-4 * scale, n
