@@ -53,6 +53,15 @@ def parse():
                     help="form timed for the headline value (fp32flux: FP32 edge fluxes and advection)")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip timing the plain FP64 path beside the chosen form")
+    ap.add_argument("--no-combined", action="store_true",
+                    help="skip the combined form (FP32 fluxes + learned closure + batched members)")
+    ap.add_argument("--combined-large", type=int, default=2,
+                    help="combined form: members on the 200k-node 40-layer mesh")
+    ap.add_argument("--combined-small", type=int, default=8,
+                    help="combined form: members on the 50k-node 30-layer mesh")
+    ap.add_argument("--combined-spinup", type=int, default=240,
+                    help="combined form: internal steps from the cold start before timing, so that the "
+                         "learned closure's columns have left the cold start's state (outside its envelope)")
     return ap.parse_args()
 
 
@@ -375,6 +384,77 @@ def e2e_leg(f, case, args, pg, local, world):
                                 "pinned host buffers, wall clock"}
 
 
+def combined_leg(args, case, plain_value, local):
+    """The chosen form of all three together, on one GPU: FP32 edge fluxes and advection,
+    the learned closure (the network trained on the 50k-node coastal mesh, MY2.5 as the
+    per-column fallback), and batching: perturbed members of the 200k-node 40-layer mesh
+    and of a 50k-node 30-layer mesh, each mesh's members as one union model, both models
+    stepped by one CUDA graph per internal step.  Member counts are a reduced ensemble
+    (``--combined-large`` and ``--combined-small``; the full 64 + 16 configuration is
+    ``--workload ensemble`` over several GPUs).  Returns the throughput over all members,
+    its ratio to the plain FP64 single-model rate, and member 0 of each mesh against its
+    own plain FP64 run after the same steps."""
+    from myfvcomcode_b200 import cases, closure, ensemble
+    from myfvcomcode_b200.engine import Fvcom, Group
+    from myfvcomcode_b200.precision_report import compare
+    trained = closure.load(os.path.join(ROOT, "myfvcomcode_b200", "data", "closure_coastal50k_8seeds.npz"))
+    bases = [("200k-k40", case, args.combined_large, 6),
+             ("50k-k30", cases.coastal_mesh(npts=50000, kb=31, seed=1234), args.combined_small, 5)]
+    models, unions, members = [], [], []
+    cells_layers = 0
+    for name, base, n, seed in bases:
+        if n <= 0:
+            continue
+        specs = ensemble.perturbed_members(base, n, seed=seed)
+        u = ensemble.union_case(base, specs)
+        f = Fvcom(u)
+        f.set_precision("fp32flux")
+        closure.attach(f, trained)
+        models.append(f)
+        unions.append((u, specs, base))
+        cells_layers += u["grid"]["N"] * (u["grid"]["KB"] - 1)
+        members.append({"mesh": name, "members": n})
+    grp = Group(models)
+    grp.run(max(args.warmup, args.combined_spinup))
+    t_ms = grp.time_steps(args.steps)
+    value = cells_layers * args.steps / (t_ms / 1e3)
+    errors = []
+    for f, (u, specs, base) in zip(models, unions):
+        n_done = f.clock()[0]
+        ref = Fvcom(ensemble.member_case(base, specs[0]))
+        ref.run(n_done)
+
+        class _Member:
+            KB = f.KB
+
+            def get(self, nm):
+                return ensemble.member_slice(u, 0, nm, f)
+
+            def get3(self, nm):
+                a = self.get(nm)
+                return a.reshape((a.size // self.KB, self.KB), order="F")
+        errors.append({"mesh": u["name"], "internal_steps": n_done,
+                       "columns_on_network": closure.status(f)["columns_on_network"],
+                       "member0_vs_plain_fp64": compare(ref, _Member())})
+        ref.close()
+    import ctypes as C
+    kps = 0
+    for f in models:
+        f.lib.fvg_kernels_per_step.argtypes = [C.c_void_p]
+        f.lib.fvg_kernels_per_step.restype = C.c_int32
+        kps += int(f.lib.fvg_kernels_per_step(f.h))
+    grp.close()
+    for f in models:
+        f.close()
+    return {"value": value, "unit": "cell-layer updates/s", "ms_per_step": t_ms / args.steps,
+            "vs_plain_fp64": value / plain_value if plain_value else None,
+            "form": "FP32 fluxes + learned closure (BF16 tensor cores, MY2.5 fallback) + batched members, "
+                    "one CUDA graph per internal step",
+            "members": members, "errors": errors, "gpu_launches": kps * args.steps,
+            "timing": "CUDA events around %d group steps after %d steps from the cold start"
+                      % (args.steps, max(args.warmup, args.combined_spinup))}
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
@@ -518,6 +598,10 @@ def main():
             plain["e2e"] = e2e_leg(fp, case, args, pg, local, world)
         fp.close()
 
+    combined = None
+    if world == 1 and args.workload == "coastal" and not args.no_combined:
+        combined = combined_leg(args, case, plain["value"] if plain else None, local)
+
     cpu = None
     parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -536,7 +620,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "f32 fluxes, f64 state",
                 "data": "synthetic", "config": cfg, "clocks": clocks, "e2e": e2e, "roofline": roof,
-                "cpu_baseline": cpu, "parity": parity,
+                "cpu_baseline": cpu, "parity": parity, "combined": combined,
                 "gpu_launches": int(lib.fvg_kernels_per_step(f.h)) * args.steps}
         print(json.dumps(line), flush=True)
     f.close()

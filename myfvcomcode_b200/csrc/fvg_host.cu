@@ -1206,7 +1206,7 @@ int fvg_set_closure(fvg_handle* h, int32_t mode, const float* params, int32_t np
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    h->clos_grid = 4 * nsm;
+    h->clos_grid = closure_ctas_per_sm() * nsm;
   }
   std::vector<uint8_t> img;
   std::vector<float> bias;

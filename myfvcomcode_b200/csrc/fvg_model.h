@@ -430,6 +430,7 @@ void launch_make_compact(const Dev& P, cudaStream_t s, int* mismatch);
 void launch_closure(const Dev& P, cudaStream_t s, int* err, int grid);
 void launch_vdif_q_shallow(const Dev& P, cudaStream_t s);
 size_t closure_smem_bytes();
+int closure_ctas_per_sm();
 size_t closure_weight_image_bytes();
 int closure_setup_attrs();
 void launch_mlp_tc_forward(const void* wimg, const float* bias, const float* x, int n, float* out, int* err, int grid,

@@ -45,9 +45,11 @@ constexpr int S_A1 = S_W3 + NOUT * HID * 2;         // 128 x 16 bf16, SBO 256
 constexpr int S_A2 = S_A1 + ROWS * K1 * 2;        // 128 x 64 bf16, SBO 1024
 constexpr int S_END = S_A2 + ROWS * HID * 2;
 constexpr int W_IMAGE = S_A1;                     // bytes of the weight image
-// TMEM columns: D1 [0,64), D2 [64,128), D3 [0,16) (D1 is read out before layer 3 runs);
-// 128 allocated, so four CTAs fit in an SM's 512 columns.
-constexpr uint32_t TMEM_COLS = 128;
+// TMEM columns: D1, D2 and D3 all at [0,64) -- each layer's accumulator is read out (and
+// the read waited for) before the next layer's MMA is issued -- so 64 columns are
+// allocated and eight CTAs fit in an SM's 512 columns.
+constexpr uint32_t TMEM_COLS = 64;
+constexpr int kCtasPerSm = 6;  // resident CTAs per SM the launch bounds ask for
 constexpr long kSpin = 1 << 22;  // bound of every mbarrier wait
 
 __device__ inline uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -146,6 +148,19 @@ __device__ inline void store_row(uint8_t* tile, int sbo, int r, const float* v) 
   }
 }
 
+// Sixteen values of row r into core-matrix columns c8 and c8+1 of an activation tile.
+__device__ inline void store_cols16(uint8_t* tile, int sbo, int r, int c8, const float* v) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint4 q;
+    q.x = pack_bf16(v[8 * h + 0], v[8 * h + 1]);
+    q.y = pack_bf16(v[8 * h + 2], v[8 * h + 3]);
+    q.z = pack_bf16(v[8 * h + 4], v[8 * h + 5]);
+    q.w = pack_bf16(v[8 * h + 6], v[8 * h + 7]);
+    *reinterpret_cast<uint4*>(tile + (r / 8) * sbo + (c8 + h) * CORE + (r % 8) * 16) = q;
+  }
+}
+
 // Network input transform of feature f: 0 identity, 1 log(x), 2 asinh(x / s).
 __device__ inline float feat_transform(const ClosNorm& nm, int f, float x) {
   float t = x;
@@ -209,7 +224,7 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
       if (live) store(r, o, true);
       continue;
     }
-    float v[HID];
+    float v[K1];
 #pragma unroll
     for (int f = 0; f < K1; ++f) v[f] = 0.f;
     if (live) load(r, v);
@@ -223,7 +238,7 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
         if (layer == 0) {
           mma_bf16(tm + 0, sdesc(s0 + S_A1, CORE, 256), sdesc(s0 + S_W1, CORE, 256), idesc_bf16(ROWS, HID), false);
         } else {
-          const uint32_t dcol = layer == 1 ? 64u : 0u;
+          const uint32_t dcol = 0u;
           const uint32_t bw = layer == 1 ? S_W2 : S_W3;
           const uint32_t idesc = idesc_bf16(ROWS, layer == 1 ? HID : NOUT);
           for (int s = 0; s < HID / 16; ++s)
@@ -242,13 +257,17 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
       if (abort_flag) break;
       fence_after();
       if (layer < 2) {
-        const uint32_t dcol = layer == 0 ? 0u : 64u;
         const float* bb = layer == 0 ? b1 : b2;
+        // sixteen accumulator columns at a time: bias, GELU, BF16 into the next layer's
+        // A tile (two core-matrix columns), so that few values are live at once
 #pragma unroll
-        for (int c = 0; c < HID / 16; ++c) tmem_ld16(tm + lane_off + dcol + 16 * c, v + 16 * c);
+        for (int c = 0; c < HID / 16; ++c) {
+          float w[16];
+          tmem_ld16(tm + lane_off + 16 * c, w);
 #pragma unroll
-        for (int j = 0; j < HID; ++j) v[j] = gelu(v[j] + bb[j]);
-        store_row<HID>(sm + S_A2, 1024, t, v);
+          for (int j = 0; j < 16; ++j) w[j] = gelu(w[j] + bb[16 * c + j]);
+          store_cols16(sm + S_A2, 1024, t, 2 * c, w);
+        }
         fence_async_smem();
         fence_before();
         __syncthreads();
@@ -283,7 +302,7 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
 }
 
 // The closure step: rows are (level K, node I) with r = (K-2)*M + (I-1).
-__global__ void __launch_bounds__(ROWS, 1) k_closure_mlp(const Dev P, int* err) {
+__global__ void __launch_bounds__(ROWS, kCtasPerSm) k_closure_mlp(const Dev P, int* err) {
   const int nrows = P.M * (P.KBM1 - 1);
   const size_t S = (size_t)nrows;
   const ClosNorm& nm = P.clos_norm;
@@ -314,7 +333,7 @@ __global__ void __launch_bounds__(ROWS, 1) k_closure_mlp(const Dev P, int* err) 
 }
 
 // Standalone BF16 forward pass on standardised inputs x [n][8] -> out [n][3].
-__global__ void __launch_bounds__(ROWS, 1) k_mlp_tc_forward(const void* wimg, const float* bias, const float* x,
+__global__ void __launch_bounds__(ROWS, kCtasPerSm) k_mlp_tc_forward(const void* wimg, const float* bias, const float* x,
                                                             int n, float* out, int* err) {
   auto load = [&](int r, float* v) {
 #pragma unroll
@@ -342,6 +361,7 @@ __global__ void k_closure_shallow(const Dev P) {
 }
 
 size_t closure_smem_bytes() { return (size_t)S_END; }
+int closure_ctas_per_sm() { return kCtasPerSm; }
 size_t closure_weight_image_bytes() { return (size_t)W_IMAGE; }
 
 void launch_vdif_q_shallow(const Dev& P, cudaStream_t s) {

@@ -135,8 +135,16 @@ __device__ inline void store_exf(const Dev& P, int c) {
 __device__ inline void wet_node(const Dev& P, int i, const int* cwet) {
   double e = P.elf[i];
   int wet = ((P.h[i] + e - P.min_depth) < 1.0e-5) ? 0 : 1;
-  int s = 0;
-  for (int j = 1; j <= P.ntve[i]; ++j) s += cwet[P.nbve[(size_t)(j - 1) * (P.M + 1) + i]];
+  // the ring's cell flags, four entries' indices and then their flags loaded at a time
+  const int nt = P.ntve[i];
+  const size_t m1 = P.M + 1;
+  const int* L = P.nbve + i;
+  int s = 0, j = 0;
+  for (; j + 4 <= nt; j += 4) {
+    const int c0 = L[j * m1], c1 = L[(j + 1) * m1], c2 = L[(j + 2) * m1], c3 = L[(j + 3) * m1];
+    s += cwet[c0] + cwet[c1] + cwet[c2] + cwet[c3];
+  }
+  for (; j < nt; ++j) s += cwet[L[j * m1]];
   if (s == 0) wet = 0;
   P.iswetn[i] = wet;
   P.elf[i] = fmax(e, -P.h[i] + P.min_depth);
@@ -213,18 +221,33 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
     if ((parts & EN_GRAD) && c <= P.N) store_grad(P, c);
     return;
   }
-  // the previous stage's node judgement, its cell flags now in ISWETCE (roles swapped)
-  if (parts & EN_WET_PREV) wet_node(P, i, P.iswetce);
-  if (parts & EN_FINISH_PREV) ext_update_node(P, i, (parts >> 8) & 7);
+  // EXTEL's sum first: its loads (the previous cell kernel's half-edge fluxes) do not
+  // depend on the node updates below, which then overlap with them
   double x = 0.0;
   if (parts & EN_EXTEL) {
+    // the half-edge fluxes in ascending half-edge order; four entries' codes and then
+    // their fluxes are loaded at a time, and added in order
     const int n = P.node_he_ptr[i + 1] - P.node_he_ptr[i];
-    for (int j = 0; j < n; ++j) {
-      int e = P.node_vpos_ell[(size_t)j * P.ms + i];
-      double exflux = P.exf2d[e >> 1];
+    const int* L = P.node_vpos_ell + i;
+    const size_t ms = P.ms;
+    int j = 0;
+    for (; j + 4 <= n; j += 4) {
+      const int e0 = L[j * ms], e1 = L[(j + 1) * ms], e2 = L[(j + 2) * ms], e3 = L[(j + 3) * ms];
+      const double f0 = P.exf2d[e0 >> 1], f1 = P.exf2d[e1 >> 1], f2 = P.exf2d[e2 >> 1], f3 = P.exf2d[e3 >> 1];
+      x = (e0 & 1) ? x + f0 : x - f0;
+      x = (e1 & 1) ? x + f1 : x - f1;
+      x = (e2 & 1) ? x + f2 : x - f2;
+      x = (e3 & 1) ? x + f3 : x - f3;
+    }
+    for (; j < n; ++j) {
+      const int e = L[j * ms];
+      const double exflux = P.exf2d[e >> 1];
       x = (e & 1) ? x + exflux : x - exflux;
     }
   }
+  // the previous stage's node judgement, its cell flags now in ISWETCE (roles swapped)
+  if (parts & EN_WET_PREV) wet_node(P, i, P.iswetce);
+  if (parts & EN_FINISH_PREV) ext_update_node(P, i, (parts >> 8) & 7);
   if (parts & EN_COPY_ELRK) P.elrk[i] = P.el[i];
   const double alpha = dAlphaRK[K];
   int ob = P.node_obc[i];
