@@ -1112,8 +1112,7 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     const size_t ms = P.ms, ns = P.ns, KB = P.KB, n1 = P.N + 1, e1 = P.NE + 1;
     F32& f = P.f;
     auto fail = [&](int r) { return r; };
-    for (int q = 0; q < 4; ++q)
-      if ((rc = dalloc(h, &f.g3[q], ns * KB))) return fail(rc);
+    if ((rc = dalloc(h, (float**)&f.g34, 4 * ns * KB))) return fail(rc);
     if ((rc = dalloc(h, (float**)&f.g2d4, 4 * n1))) return fail(rc);
     if (P.limiter) {
       std::vector<float> ones(std::max(n1, ns * KB), 1.0f);

@@ -41,7 +41,7 @@ struct SchedLayout {
 // and rounded once: xo[e] = XIJC(e)-XC(IEC(e,1)), xo[NE+1+e] = XIJC(e)-XC(IEC(e,2)), the
 // same for y.
 struct F32 {
-  float* g3[4];
+  float4* g34;  // least-squares gradient of U, V per cell and layer {UX, UY, VX, VY} (ns x KB)
   float *alfa2[2], *alfa3[2];  // slope limiters UALFA, VALFA (see Dev)
   float* npk;  // node records of the ring gradients, 16 floats per (node, layer)
   float2* ex2;
@@ -311,6 +311,7 @@ template <> struct Mesh<double> {
   __device__ static double dltxc(const Dev& P, int e) { return P.dltxc[e]; }
   __device__ static double dltyc(const Dev& P, int e) { return P.dltyc[e]; }
   __device__ static double art(const Dev& P, int c) { return P.art[c]; }
+  __device__ static double2 artcc(const Dev& P, int c) { return make_double2(P.art[c], P.cc_hvc[c]); }
   __device__ static double cc_hvc(const Dev& P, int c) { return P.cc_hvc[c]; }
   __device__ static double a1u(const Dev& P, size_t q) { return P.a1u[q]; }
   __device__ static double a2u(const Dev& P, size_t q) { return P.a2u[q]; }
@@ -338,12 +339,12 @@ template <> struct Mesh<float> {
   __device__ static float dltxc(const Dev& P, int e) { return P.f.dltxc[e]; }
   __device__ static float dltyc(const Dev& P, int e) { return P.f.dltyc[e]; }
   __device__ static float art(const Dev& P, int c) { return P.f.art[c]; }
+  __device__ static float2 artcc(const Dev& P, int c) { return P.f.artcc[c]; }  // {ART, CC_HVC}
   __device__ static float cc_hvc(const Dev& P, int c) { return P.f.cc_hvc[c]; }
   __device__ static float a1u(const Dev& P, size_t q) { return P.f.a1u[q]; }
   __device__ static float a2u(const Dev& P, size_t q) { return P.f.a2u[q]; }
   __device__ static float* alfa2(const Dev& P, int q) { return P.f.alfa2[q]; }
   __device__ static float* alfa3(const Dev& P, int q) { return P.f.alfa3[q]; }
-  __device__ static float* g3(const Dev& P, int q) { return P.f.g3[q]; }
   __device__ static float2* ex2(const Dev& P) { return P.f.ex2; }
 };
 // The cell's NBE and its least-squares coefficients A1U(c,1..4), A2U(c,1..4) in the

@@ -144,10 +144,18 @@ template <typename R>
 __device__ inline G3<R> load_g3(const Dev& P, int c, int k) {
   size_t q = C3(P, c, k);
   G3<R> g;
-  g.ux = Mesh<R>::g3(P, 0)[q];
-  g.uy = Mesh<R>::g3(P, 1)[q];
-  g.vx = Mesh<R>::g3(P, 2)[q];
-  g.vy = Mesh<R>::g3(P, 3)[q];
+  if constexpr (sizeof(R) == 4) {
+    const float4 a = P.f.g34[q];
+    g.ux = a.x;
+    g.uy = a.y;
+    g.vx = a.z;
+    g.vy = a.w;
+  } else {
+    g.ux = P.g3[0][q];
+    g.uy = P.g3[1][q];
+    g.vx = P.g3[2][q];
+    g.vy = P.g3[3][q];
+  }
   return g;
 }
 
@@ -162,10 +170,14 @@ __global__ void __launch_bounds__(256) k_grad3(const Dev P) {
   for (int k = kb; k <= ke; ++k) {
     G3<R> g = grad3<R>(P, i, P.u + C3(P, 0, k), P.v + C3(P, 0, k));
     size_t q = C3(P, i, k);
-    Mesh<R>::g3(P, 0)[q] = g.ux;
-    Mesh<R>::g3(P, 1)[q] = g.uy;
-    Mesh<R>::g3(P, 2)[q] = g.vx;
-    Mesh<R>::g3(P, 3)[q] = g.vy;
+    if constexpr (sizeof(R) == 4) {
+      P.f.g34[q] = make_float4(g.ux, g.uy, g.vx, g.vy);
+    } else {
+      P.g3[0][q] = g.ux;
+      P.g3[1][q] = g.uy;
+      P.g3[2][q] = g.vx;
+      P.g3[3][q] = g.vy;
+    }
   }
 }
 
@@ -236,7 +248,8 @@ __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib,
       vij1 = va + ga.vx * xija + ga.vy * yija;
       uij2 = ub + gb.ux * xijb + gb.uy * yijb;
       vij2 = vb + gb.vx * xijb + gb.vy * yijb;
-      const R arto = Mh::art(P, o), cco = Mh::cc_hvc(P, o);
+      const auto aco = Mh::artcc(P, o);
+      const R arto = aco.x, cco = aco.y;
       arta = side == 0 ? own.art : arto;
       artb = side == 0 ? arto : own.art;
       cca = side == 0 ? own.cc : cco;
@@ -350,8 +363,9 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && !LIM) ? 4 : 1) k_advec
       own.g = load_g3<R>(P, i, k);
       own.u = (R)P.u[C3(P, i, k)];
       own.v = (R)P.v[C3(P, i, k)];
-      own.art = Mesh<R>::art(P, i);
-      own.cc = Mesh<R>::cc_hvc(P, i);
+      const auto aci = Mesh<R>::artcc(P, i);
+      own.art = aci.x;
+      own.cc = aci.y;
     }
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;
@@ -789,8 +803,9 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && !LIM) ? 4 : 1) k_adv_u
       own.g = load_g3<R>(P, i, k);
       own.u = (R)P.u[C3(P, i, k)];
       own.v = (R)P.v[C3(P, i, k)];
-      own.art = Mesh<R>::art(P, i);
-      own.cc = Mesh<R>::cc_hvc(P, i);
+      const auto aci = Mesh<R>::artcc(P, i);
+      own.art = aci.x;
+      own.cc = aci.y;
     }
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;
@@ -940,13 +955,15 @@ __global__ void __launch_bounds__(kTileCells, sizeof(R) == 4 ? 6 : 4) k_mom3d_st
   for (int k = kb; k <= ke; ++k) {
     __syncthreads();
     for (int q = tid; q < nall; q += nt) {
-      const size_t qq = C3(P, T.cells[c0 + q], k);
+      const int c = T.cells[c0 + q];
+      const size_t qq = C3(P, c, k);
       s_c[q] = (R)P.u[qq];
       s_c[CC + q] = (R)P.v[qq];
-      s_c[2 * CC + q] = Mh::g3(P, 0)[qq];
-      s_c[3 * CC + q] = Mh::g3(P, 1)[qq];
-      s_c[4 * CC + q] = Mh::g3(P, 2)[qq];
-      s_c[5 * CC + q] = Mh::g3(P, 3)[qq];
+      const G3<R> g = load_g3<R>(P, c, k);
+      s_c[2 * CC + q] = g.ux;
+      s_c[3 * CC + q] = g.uy;
+      s_c[4 * CC + q] = g.vx;
+      s_c[5 * CC + q] = g.vy;
     }
     __syncthreads();
     for (int q = tid; q < ne; q += nt) {
