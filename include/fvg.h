@@ -296,16 +296,18 @@ int fvg_set_closure(fvg_handle* h, int32_t mode, const float* params, int32_t np
                     int32_t nnorm);
 /* Columns that used the network in the last step, and the closure's error word: 0, or
    nonzero once a bounded tensor-core wait ran out (1; 2 if the wait for the outstanding
-   MMAs before freeing tensor memory ran out as well).  Rows of a block whose wait ran
-   out take MY2.5's values, and fvg_run / fvg_internal_step return FVG_ERR_TIMEOUT while
-   the word is set; fvg_set_closure clears it. */
+   MMAs before freeing tensor memory ran out as well).  Network rows of a block whose
+   wait ran out keep their previous coefficients (columns outside the envelope have MY2.5's
+   as always), and fvg_run / fvg_internal_step return FVG_ERR_TIMEOUT while the word is
+   set; fvg_set_closure clears it. */
 int fvg_closure_status(fvg_handle* h, int32_t* columns_on_network, int32_t* wait_timeouts);
 /* Launch shape of the 3-D gather kernels (results do not depend on it):
    "col_threads" = entities (threads) per block, 32..256 in steps of 32 (default 128);
    "col_layers"  = consecutive layers each thread walks, 1..KB (default 8);
    "compact"     = 1 (default) lets the precision form's Runge-Kutta stages use the
                    compact cell kernel where fvg_set_precision found the mesh's edge metrics
-                   to be the ones its coordinates define; 0 keeps the general kernel.
+                   to be the ones its coordinates define (2: the same kernel held to 80
+                   registers instead of 64); 0 keeps the general kernel.
                    fvg_get_tuning("compact") reports whether the compact kernel is in use;
    "staged"      = 2 runs ADVECTION_EDGE_GCN and ADV_UV_EDGE_GCN (LIMITED_NO, GCN) as the
                    tile-staged kernels (neighbour cells in shared memory, each edge

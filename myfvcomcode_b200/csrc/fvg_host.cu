@@ -240,10 +240,10 @@ void fill_routine_row(const fvg_handle* h, double* row) {
 const char* kGroupNames[] = {"cell_pre", "advection3d", "baropg", "int_advave", "ext_node", "wet_judge",
                              "ext_cell", "ext_update", "adjust2", "vertvl_flux", "vertvl_col", "w_viscofh",
                              "adv_uv", "vdif_uv", "grad_q", "adv_q", "vdif_q", "grad_ts", "adv_ts",
-                             "vdif_ts", "bcond_ts", "final"};
+                             "vdif_ts", "bcond_ts", "final", "closure"};
 enum { G_CELL_PRE, G_ADV3D, G_BAROPG, G_INT_ADVAVE, G_EXT_NODE, G_WET, G_EXT_CELL, G_EXT_UPD, G_ADJ2,
        G_VV_FLUX, G_VV_COL, G_W_VISC, G_ADV_UV, G_VDIF_UV, G_GRAD_Q, G_ADV_Q, G_VDIF_Q, G_GRAD_TS,
-       G_ADV_TS, G_VDIF_TS, G_BCOND_TS, G_FINAL, G_COUNT };
+       G_ADV_TS, G_VDIF_TS, G_BCOND_TS, G_FINAL, G_CLOSURE, G_COUNT };
 
 struct Marker {
   std::vector<cudaEvent_t>* ev = nullptr;
@@ -338,8 +338,11 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
   launch_adv_q(P, s, AD_Q2 | AD_Q2L | spc);
   mk.mark(s, G_ADV_Q);
   launch_vdif_q(P, s, 1);
-  if (P.closure) launch_closure(P, s, P.clos_err, h->clos_grid);
   mk.mark(s, G_VDIF_Q);
+  if (P.closure) {
+    launch_closure(P, s, P.clos_err, h->clos_grid);
+    mk.mark(s, G_CLOSURE);
+  }
   int ts = (p.temperature_active ? AD_T : 0) | (p.salinity_active ? AD_S : 0);
   if (ts) {
     launch_grad(P, s, 1);
@@ -1163,7 +1166,7 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     h->compact_ok = (bad == 0 && !P.limiter && !P.gcy) ? 1 : 0;
   }
   P.prec = mode;
-  P.f.compact = (mode == FVG_PREC_FP32_FLUX && h->compact_ok && h->compact_allowed) ? 1 : 0;
+  P.f.compact = (mode == FVG_PREC_FP32_FLUX && h->compact_ok) ? h->compact_allowed : 0;
   // The captured step holds the other precision's kernels: capture again.
   CK(cudaStreamSynchronize(h->stream));
   if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
@@ -1192,8 +1195,9 @@ int fvg_set_closure(fvg_handle* h, int32_t mode, const float* params, int32_t np
   int rc;
   if (!P.clos_feat) {
     if (closure_setup_attrs()) { h->err = "cannot configure the closure kernel"; return FVG_ERR_CUDA; }
-    if ((rc = dalloc(h, &P.clos_feat, (size_t)CLOS_IN * S))) return rc;
-    if ((rc = dalloc(h, &P.clos_plain, 3 * S))) return rc;
+    if ((rc = dalloc(h, &P.clos_feat, S))) return rc;
+    // one flag per level chunk and node: at most KB chunks (one level per thread)
+    if ((rc = dalloc(h, &P.clos_envc, (size_t)P.KB * ((size_t)P.M + 1)))) return rc;
     if ((rc = dalloc(h, &P.clos_env, (size_t)P.M + 1))) return rc;
     if ((rc = dalloc(h, &P.clos_err, 1))) return rc;
     float* b = nullptr;
@@ -1279,8 +1283,9 @@ int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value) {
     if (value < 0 || value > 2) { h->err = "staged must be 0, 1 or 2"; return FVG_ERR_ARG; }
     h->P.staged = value;
   } else if (k == "compact") {
-    h->compact_allowed = value != 0;
-    h->P.f.compact = (h->P.prec == FVG_PREC_FP32_FLUX && h->compact_ok && h->compact_allowed) ? 1 : 0;
+    if (value < 0 || value > 2) { h->err = "compact must be 0, 1 or 2"; return FVG_ERR_ARG; }
+    h->compact_allowed = value;
+    h->P.f.compact = (h->P.prec == FVG_PREC_FP32_FLUX && h->compact_ok) ? h->compact_allowed : 0;
   } else {
     h->err = "unknown tuning key " + k;
     return FVG_ERR_ARG;

@@ -228,15 +228,18 @@ struct Dev {
   // KN*SM, KN*SH*VPRNU that MY2.5 averages into KQ, KM, KH, and 1 for a wet node.
   float* clos_samp;
   // Learned closure (fvg_set_closure): 0 = MY2.5; 1 = the network with MY2.5 as the
-  // per-column fallback.  clos_feat: [8][M*(KBM1-1)] inputs, clos_plain: [3][...] MY2.5's
-  // new parts (FP64), clos_env: per node 1 = wet and inside the envelope; clos_w: the BF16
-  // weight image, clos_b: biases (64 + 64 + 16).
+  // per-column fallback.  clos_feat: per row r = (K-2)*M + (I-1) the eight network inputs
+  // already transformed and standardised, in BF16 (16 bytes, the MMA's A-operand row);
+  // clos_envc: per level chunk of VDIF_Q's level kernel and node, 1 if every interior
+  // level of the chunk lies inside the training envelope (chunk c at c*(M+1) + I);
+  // clos_env: per node 1 = wet and inside the envelope on every interior level; clos_w:
+  // the BF16 weight image, clos_b: biases (64 + 64 + 16).
   int closure;
   ClosNorm clos_norm;
   const void* clos_w;
   const float* clos_b;
-  float* clos_feat;
-  double* clos_plain;
+  uint4* clos_feat;
+  unsigned char* clos_envc;
   int* clos_env;
   int* clos_err;
   Tiles tl;
@@ -262,6 +265,16 @@ __device__ inline void col_range(const Dev& P, int k0, int klast, int& kb, int& 
 
 
 constexpr int CLOS_IN = 8, CLOS_OUT = 3, CLOS_PLANES = CLOS_IN + CLOS_OUT + 1;
+
+// The learned closure's input transform of feature f: kind 0 identity, 1 log(x),
+// 2 asinh(x / scale); then standardised.
+__device__ inline float clos_feat_transform(const ClosNorm& nm, int f, float x) {
+  float t = x;
+  const int kind = nm.kind[f];
+  if (kind == 1) t = logf(fmaxf(x, 1e-30f));
+  else if (kind == 2) t = asinhf(x / nm.scale[f]);
+  return (t - nm.mean[f]) / nm.std[f];
+}
 
 // index helpers
 __host__ __device__ inline size_t N3(const Dev& P, int i, int k) { return (size_t)(k - 1) * P.ms + i; }

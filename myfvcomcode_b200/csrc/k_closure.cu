@@ -2,14 +2,14 @@
 // on the 5th-generation tensor cores (tcgen05.mma, accumulators in tensor memory), fused
 // with the closure's update of KQ, KM, KH.
 //
-// VDIF_Q in learned mode (P.closure == 1) stores, for every node and interior level, the
-// eight network inputs and MY2.5's own new parts KN*KAPPA*SM, KN*SM, KN*SH*VPRNU
-// (clos_feat, the planes of fvg_closure_sample), and per column whether the node is wet
-// and all its inputs lie inside the training envelope (clos_env).  It leaves KQ, KM, KH
-// of the interior levels to k_closure_mlp, which for each (node, level) row takes the
-// network's prediction where the column is inside the envelope and MY2.5's value where it
-// is not (the per-column fallback), then averages with the old value as MY2.5 does:
-// K = 0.5*(new + K_old) (vdif_q.F:489-491).
+// VDIF_Q in learned mode (P.closure == 1) stores, for every wet node and interior level,
+// the eight network inputs transformed, standardised and rounded to BF16 (clos_feat: one
+// 16-byte row, the MMA's A-operand row as it goes into shared memory), and per column
+// whether the node is wet and all its inputs lie inside the training envelope (clos_env,
+// from per-chunk flags of VDIF_Q's level kernel).  VDIF_Q finishes every column outside
+// the envelope with MY2.5 (the per-column fallback) and leaves KQ, KM, KH of the interior
+// levels of the others to k_closure_mlp, which takes the network's prediction and
+// averages with the old value as MY2.5 does: K = 0.5*(new + K_old) (vdif_q.F:489-491).
 //
 // Tile scheme: a CTA of 128 threads owns tiles of 128 rows; thread t owns row t of the
 // tile and TMEM lane t.  For each layer the threads write their row's BF16 activations
@@ -161,25 +161,19 @@ __device__ inline void store_cols16(uint8_t* tile, int sbo, int r, int c8, const
   }
 }
 
-// Network input transform of feature f: 0 identity, 1 log(x), 2 asinh(x / s).
-__device__ inline float feat_transform(const ClosNorm& nm, int f, float x) {
-  float t = x;
-  const int kind = nm.kind[f];
-  if (kind == 1) t = logf(fmaxf(x, 1e-30f));
-  else if (kind == 2) t = asinhf(x / nm.scale[f]);
-  return (t - nm.mean[f]) / nm.std[f];
-}
 
 }  // namespace
 
-// The tile pipeline shared by the closure and the standalone forward pass.  load(r, v)
-// fills the 8 standardised inputs of row r; store(r, o, true) receives the 3 network
-// outputs (bias included).  If an mbarrier wait runs out, err receives 1 and every row of
-// the block that has not been stored yet (the current tile and all later ones) gets
-// store(r, nullptr, false), so that the caller can write its fallback for that row.
-template <class Load, class Store, class Need>
+// The tile pipeline shared by the closure and the standalone forward pass.  need(r): row r
+// goes through the network; load(r, v) fills the 8 standardised inputs of such a row (the
+// next tile's rows are fetched while the current tile runs); prefetch(r) is called while
+// the last layer's MMA runs, so that the caller can fetch what store needs; store(r, o,
+// true) receives the 3 network outputs (bias included).  If an mbarrier wait runs out, err
+// receives 1 and every row of the block that has not been stored yet (the current tile
+// and all later ones) gets store(r, nullptr, false).
+template <class Load, class Store, class Need, class Prefetch>
 __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nrows, Load load, Store store, Need need,
-                                    int* err) {
+                                    Prefetch prefetch, int* err) {
   extern __shared__ __align__(1024) uint8_t sm[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_base;
@@ -210,24 +204,36 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
   const float* b2 = bias + HID;
   const float* b3 = bias + 2 * HID;
 
+  // this thread's row of the next tile: whether it uses the network, and its inputs
+  float vn[K1];
+  bool nn = false;
+  auto fetch = [&](int tl) {
+    const int rr = tl * ROWS + t;
+#pragma unroll
+    for (int f = 0; f < K1; ++f) vn[f] = 0.f;
+    nn = tl < ntiles && rr < nrows && need(rr);
+    if (nn) load(rr, vn);
+  };
+  fetch(blockIdx.x);
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int r = tile * ROWS + t;
     const bool live = r < nrows;
-    // after a wait ran out, the rest of the block's rows take the fallback
+    float v[K1];
+#pragma unroll
+    for (int f = 0; f < K1; ++f) v[f] = vn[f];
+    const bool nd = nn;
+    fetch(tile + gridDim.x);
+    // after a wait ran out, the rest of the block's rows are not stored
     if (abort_flag) {
       if (live) store(r, nullptr, false);
       continue;
     }
     // a tile none of whose rows uses the network skips the tensor cores
-    if (!__syncthreads_or(live && need(r))) {
+    if (!__syncthreads_or(nd)) {
       float o[16] = {};
       if (live) store(r, o, true);
       continue;
     }
-    float v[K1];
-#pragma unroll
-    for (int f = 0; f < K1; ++f) v[f] = 0.f;
-    if (live) load(r, v);
     store_row<K1>(sm + S_A1, 256, t, v);
     fence_async_smem();
     fence_before();
@@ -247,6 +253,7 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
         }
         mma_commit(&mbar);
       }
+      if (layer == 2 && live && nd) prefetch(r);
       const bool ok = mbar_wait(&mbar, phase & 1);
       phase += 1;
       if (!ok) {
@@ -301,35 +308,47 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
   }
 }
 
-// The closure step: rows are (level K, node I) with r = (K-2)*M + (I-1).
+// The closure step: rows are (level K, node I) with r = (K-2)*M + (I-1).  VDIF_Q has
+// finished every column outside the envelope with MY2.5 and left the BF16 inputs of the
+// others in clos_feat; this kernel finishes the columns inside the envelope.  After a
+// wait ran out (store with net_ok false) a row keeps its coefficients, and the step
+// reports FVG_ERR_TIMEOUT.
 __global__ void __launch_bounds__(ROWS, kCtasPerSm) k_closure_mlp(const Dev P, int* err) {
   const int nrows = P.M * (P.KBM1 - 1);
-  const size_t S = (size_t)nrows;
   const ClosNorm& nm = P.clos_norm;
   auto load = [&](int r, float* v) {
+    const uint4 w = P.clos_feat[r];
+    const uint32_t u[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-    for (int f = 0; f < CLOS_IN; ++f) v[f] = feat_transform(nm, f, P.clos_feat[(size_t)f * S + r]);
+    for (int j = 0; j < 4; ++j) {
+      const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u[j]));
+      v[2 * j] = f.x;
+      v[2 * j + 1] = f.y;
+    }
+  };
+  double kold[3] = {0.0, 0.0, 0.0};  // KQ, KM, KH of the row, fetched during the last MMA
+  auto prefetch = [&](int r) {
+    const size_t q = N3(P, r % P.M + 1, r / P.M + 2);
+    kold[0] = P.kq[q];
+    kold[1] = P.km[q];
+    kold[2] = P.kh[q];
   };
   auto store = [&](int r, const float* o, bool net_ok) {
     const int k = r / P.M + 2, i = r % P.M + 1;
+    if (!net_ok || P.clos_env[i] == 0) return;
     const size_t q = N3(P, i, k);
-    const bool use_net = net_ok && P.clos_env[i] != 0;
     double nw[3];
     for (int c = 0; c < 3; ++c) {
-      if (use_net) {
-        float y = o[c] * nm.tstd[c] + nm.tmean[c];
-        nw[c] = (double)expf(y) - (double)nm.teps;
-        if (nw[c] < 0.0) nw[c] = 0.0;
-      } else {
-        nw[c] = P.clos_plain[(size_t)c * S + r];  // MY2.5, FP64
-      }
+      float y = o[c] * nm.tstd[c] + nm.tmean[c];
+      nw[c] = (double)expf(y) - (double)nm.teps;
+      if (nw[c] < 0.0) nw[c] = 0.0;
     }
-    P.kq[q] = 0.5 * (nw[0] + P.kq[q]);
-    P.km[q] = 0.5 * (nw[1] + P.km[q]);
-    P.kh[q] = 0.5 * (nw[2] + P.kh[q]);
+    P.kq[q] = 0.5 * (nw[0] + kold[0]);
+    P.km[q] = 0.5 * (nw[1] + kold[1]);
+    P.kh[q] = 0.5 * (nw[2] + kold[2]);
   };
   auto need = [&](int r) { return P.clos_env[r % P.M + 1] != 0; };
-  mlp_tc_tiles(P.clos_w, P.clos_b, nrows, load, store, need, err);
+  mlp_tc_tiles(P.clos_w, P.clos_b, nrows, load, store, need, prefetch, err);
 }
 
 // Standalone BF16 forward pass on standardised inputs x [n][8] -> out [n][3].
@@ -343,7 +362,8 @@ __global__ void __launch_bounds__(ROWS, kCtasPerSm) k_mlp_tc_forward(const void*
     for (int c = 0; c < 3; ++c) out[(size_t)r * 3 + c] = net_ok ? o[c] : __int_as_float(0x7fc00000);
   };
   auto need = [](int) { return true; };
-  mlp_tc_tiles(wimg, bias, n, load, store, need, err);
+  auto prefetch = [](int) {};
+  mlp_tc_tiles(wimg, bias, n, load, store, need, prefetch, err);
 }
 
 // VDIF_Q's averaging of shallow columns (vdif_q.F:494-512), after the per-level update of

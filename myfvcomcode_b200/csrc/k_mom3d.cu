@@ -248,8 +248,7 @@ __device__ inline EdgeFlux<R> edge_flux3(const Dev& P, size_t q, int ia, int ib,
       vij1 = va + ga.vx * xija + ga.vy * yija;
       uij2 = ub + gb.ux * xijb + gb.uy * yijb;
       vij2 = vb + gb.vx * xijb + gb.vy * yijb;
-      const auto aco = Mh::artcc(P, o);
-      const R arto = aco.x, cco = aco.y;
+      const R arto = Mh::art(P, o), cco = Mh::cc_hvc(P, o);
       arta = side == 0 ? own.art : arto;
       artb = side == 0 ? arto : own.art;
       cca = side == 0 ? own.cc : cco;
@@ -363,9 +362,8 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && !LIM) ? 4 : 1) k_advec
       own.g = load_g3<R>(P, i, k);
       own.u = (R)P.u[C3(P, i, k)];
       own.v = (R)P.v[C3(P, i, k)];
-      const auto aci = Mesh<R>::artcc(P, i);
-      own.art = aci.x;
-      own.cc = aci.y;
+      own.art = Mesh<R>::art(P, i);
+      own.cc = Mesh<R>::cc_hvc(P, i);
     }
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;
@@ -803,9 +801,8 @@ __global__ void __launch_bounds__(256, (sizeof(R) == 4 && !LIM) ? 4 : 1) k_adv_u
       own.g = load_g3<R>(P, i, k);
       own.u = (R)P.u[C3(P, i, k)];
       own.v = (R)P.v[C3(P, i, k)];
-      const auto aci = Mesh<R>::artcc(P, i);
-      own.art = aci.x;
-      own.cc = aci.y;
+      own.art = Mesh<R>::art(P, i);
+      own.cc = Mesh<R>::cc_hvc(P, i);
     }
   for (int s = 0; s < 3; ++s) {
     const size_t q = (size_t)s * n1 + i;

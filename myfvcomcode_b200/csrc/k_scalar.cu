@@ -11,6 +11,8 @@
 // each node's half-edge fluxes with their signs in ascending half-edge order, which
 // reproduces the reference's scatter sums bit for bit.  T and S (and Q2 and Q2L) are
 // transported in the same launches since neither reads the other's update.
+#include <cuda_bf16.h>
+
 #include "fvg_model.h"
 
 // The FP32 instantiations of the precision form's flux kernels are compiled from this
@@ -625,6 +627,7 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
   };
   double ukm1 = 0.0, vkm1 = 0.0;
   if (wet && kb <= KBM1) ring_mean(kb >= 2 ? kb - 1 : 1, ukm1, vkm1);
+  bool chunk_inside = wet;  // every interior level of this chunk inside the closure's envelope
   for (int k = kb; k <= ke; ++k) {
     const size_t q = n3(k);
     // positivity of the previous Q2F/Q2LF (vdif_q.F:144-149)
@@ -645,10 +648,20 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
         const double den = P.dzz[n3(k - 1)] * d;
         const double shear2 = ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den);
         if (AUX && P.closure) {
+          // the network's inputs: inside the envelope or not, then transformed,
+          // standardised and rounded to BF16 as the MMA takes them
           const float fv[CLOS_IN] = {(float)boygr, (float)shear2, (float)d, (float)P.z[q], (float)sqrt(utau2),
                                      (float)sqrt(sqrt(wub * wub + wvb * wvb)), (float)q2, (float)q2l};
-          const size_t r = (size_t)(k - 2) * P.M + (i - 1);
-          for (int f = 0; f < CLOS_IN; ++f) P.clos_feat[(size_t)f * ss + r] = fv[f];
+          uint32_t packed[4];
+          for (int f = 0; f < CLOS_IN; ++f) {
+            if (!(fv[f] >= P.clos_norm.lo[f] && fv[f] <= P.clos_norm.hi[f])) chunk_inside = false;
+          }
+          for (int f = 0; f < CLOS_IN; f += 2) {
+            const __nv_bfloat162 b = __floats2bfloat162_rn(clos_feat_transform(P.clos_norm, f, fv[f]),
+                                                           clos_feat_transform(P.clos_norm, f + 1, fv[f + 1]));
+            packed[f / 2] = *reinterpret_cast<const uint32_t*>(&b);
+          }
+          P.clos_feat[(size_t)(k - 2) * P.M + (i - 1)] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
         }
         if (AUX && cs) {
           samp(0, k, boygr);
@@ -692,6 +705,7 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
       P.vq_dtefl[q] = dtef * (1. + E2 * (x * x));
     }
   }
+  if (AUX && P.closure) P.clos_envc[(size_t)blockIdx.y * (P.M + 1) + i] = chunk_inside ? 1 : 0;
 }
 
 // The q2 and q2l tridiagonal sweeps of one column (vdif_q.F:372-431), and the column's
@@ -709,15 +723,10 @@ __global__ void __launch_bounds__(128) k_vdif_q_sweep(const Dev P) {
   const bool q2l = blockIdx.y == 1;
   auto n3 = [&](int k) { return N3(P, i, k); };
   if (P.closure && !q2l) {
+    // the column's envelope flag from the level kernel's per-chunk flags
     bool in_env = wet;
-    const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
-    for (int k = 2; k <= KBM1 && in_env; ++k) {
-      const size_t r = (size_t)(k - 2) * P.M + (i - 1);
-      for (int f = 0; f < CLOS_IN; ++f) {
-        const float v = P.clos_feat[(size_t)f * ss + r];
-        if (!(v >= P.clos_norm.lo[f] && v <= P.clos_norm.hi[f])) in_env = false;
-      }
-    }
+    const int nch = (P.KB + P.col_lc - 1) / P.col_lc;
+    for (int c = 0; c < nch && in_env; ++c) in_env = P.clos_envc[(size_t)c * (P.M + 1) + i] != 0;
     P.clos_env[i] = in_env ? 1 : 0;
   }
   if (!wet) return;
@@ -802,14 +811,9 @@ __global__ void __launch_bounds__(256) k_vdif_q_coef(const Dev P, int copy_back)
         samp(10, k, kn * sh * P.vprnu);
         samp(11, k, wet ? 1.0 : 0.0);
       }
-      if (AUX && P.closure) {
-        // interior levels are finished by the network kernel (k_closure_mlp)
-        const size_t r = (size_t)(k - 2) * P.M + (i - 1);
-        P.clos_plain[r] = kn * KAPPA * sm;
-        P.clos_plain[ss + r] = kn * sm;
-        P.clos_plain[2 * ss + r] = kn * sh * P.vprnu;
-        interior_by_network = true;
-      }
+      // interior levels of a column inside the envelope are finished by the network
+      // kernel (k_closure_mlp); every other column keeps MY2.5 here
+      if (AUX && P.closure && P.clos_env[i] != 0) interior_by_network = true;
     }
     if (!interior_by_network) {
       P.kq[q] = 0.5 * (kn * KAPPA * sm + P.kq[q]);
