@@ -306,8 +306,7 @@ int fvg_closure_status(fvg_handle* h, int32_t* columns_on_network, int32_t* wait
    "col_layers"  = consecutive layers each thread walks, 1..KB (default 8);
    "compact"     = 1 (default) lets the precision form's Runge-Kutta stages use the
                    compact cell kernel where fvg_set_precision found the mesh's edge metrics
-                   to be the ones its coordinates define (2: the same kernel held to 80
-                   registers instead of 64); 0 keeps the general kernel.
+                   to be the ones its coordinates define; 0 keeps the general kernel.
                    fvg_get_tuning("compact") reports whether the compact kernel is in use;
    "staged"      = 2 runs ADVECTION_EDGE_GCN and ADV_UV_EDGE_GCN (LIMITED_NO, GCN) as the
                    tile-staged kernels (neighbour cells in shared memory, each edge

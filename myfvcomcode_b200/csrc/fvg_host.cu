@@ -1283,8 +1283,7 @@ int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value) {
     if (value < 0 || value > 2) { h->err = "staged must be 0, 1 or 2"; return FVG_ERR_ARG; }
     h->P.staged = value;
   } else if (k == "compact") {
-    if (value < 0 || value > 2) { h->err = "compact must be 0, 1 or 2"; return FVG_ERR_ARG; }
-    h->compact_allowed = value;
+    h->compact_allowed = value != 0;
     h->P.f.compact = (h->P.prec == FVG_PREC_FP32_FLUX && h->compact_ok) ? h->compact_allowed : 0;
   } else {
     h->err = "unknown tuning key " + k;

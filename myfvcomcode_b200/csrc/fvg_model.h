@@ -267,12 +267,22 @@ __device__ inline void col_range(const Dev& P, int k0, int klast, int& kb, int& 
 constexpr int CLOS_IN = 8, CLOS_OUT = 3, CLOS_PLANES = CLOS_IN + CLOS_OUT + 1;
 
 // The learned closure's input transform of feature f: kind 0 identity, 1 log(x),
-// 2 asinh(x / scale); then standardised.
+// 2 asinh(x / scale); then standardised.  The result is rounded to BF16 (8 significant
+// bits) for the tensor cores, so the hardware logarithm (__logf, a few ulp of FP32) is
+// used, and asinh(y) = sign(y) log(|y| + sqrt(y^2 + 1)) through it, except for |y| < 2^-6
+// where asinh(y) = y (1 - y^2/6) to well below BF16's resolution, and |y| > 1e18, where
+// it is log(|y|) + log(2).
 __device__ inline float clos_feat_transform(const ClosNorm& nm, int f, float x) {
   float t = x;
   const int kind = nm.kind[f];
-  if (kind == 1) t = logf(fmaxf(x, 1e-30f));
-  else if (kind == 2) t = asinhf(x / nm.scale[f]);
+  if (kind == 1) {
+    t = __logf(fmaxf(x, 1e-30f));
+  } else if (kind == 2) {
+    const float y = x / nm.scale[f], a = fabsf(y);
+    const float s = a < 0.015625f ? a * (1.0f - a * a * (1.0f / 6.0f))
+                    : (a > 1.0e18f ? __logf(a) + 0.6931472f : __logf(a + sqrtf(a * a + 1.0f)));
+    t = copysignf(s, y);
+  }
   return (t - nm.mean[f]) / nm.std[f];
 }
 

@@ -3,10 +3,10 @@
 Both forms start from the same cold start of the same case and run the same number of
 internal steps on the device.  Reported per output (zeta, u, v, T, S): the maximum and
 RMS absolute difference over the interior entities and layers, and for each form the
-drift of the volume, heat and salt budgets (``fvg_budget``) over the run.  The control
-"fp64_twin" is FP64 again from an initial temperature perturbed by 1e-6 C (seeded): its
-difference from FP64 is what perturbations of the size of FP32 rounding grow to by
-themselves in this flow.
+drift of the volume, heat and salt budgets (``fvg_budget``) over the run.  The controls
+"fp64_twin" and "fp64_twin2" are FP64 again from initial temperatures perturbed by 1e-6 C
+(two seeds): their differences from FP64 are what perturbations of the size of FP32
+rounding grow to by themselves in this flow.
 
     python -m myfvcomcode_b200.precision_report [--npts 200000] [--hours 24] [--md FILE]
 """
@@ -76,14 +76,21 @@ def twin_case(case, amplitude=1e-6, seed=17):
     return c
 
 
-def run(case, steps, modes=("fp64", "fp32flux", "fp64_twin"), chunk=200):
+TWIN_SEEDS = {"fp64_twin": 17, "fp64_twin2": 29}
+
+
+def run(case, steps, modes=("fp64", "fp32flux", "fp64_twin", "fp64_twin2"), chunk=200):
+    """Every mode from the same cold start for ``steps`` internal steps; the twins are
+    FP64 from initial temperatures perturbed by 1e-6 C with different seeds (their
+    spread shows how far this flow's own sensitivity alone moves the fields)."""
     from .engine import Fvcom
     engines = {}
     budgets = {}
     times = {}
     for m in modes:
-        f = Fvcom(twin_case(case) if m == "fp64_twin" else case)
-        f.set_precision("fp64" if m == "fp64_twin" else m)
+        twin = m in TWIN_SEEDS
+        f = Fvcom(twin_case(case, seed=TWIN_SEEDS[m]) if twin else case)
+        f.set_precision("fp64" if twin else m)
         b0 = f.budget()
         t0 = time.perf_counter()
         done = 0
