@@ -239,6 +239,7 @@ def evaluate_on(case, trained, steps=200, precision="fp64"):
     err["KM_rel_rms"] = float(np.sqrt(np.mean((km_a - km_b) ** 2)) / np.sqrt(np.mean(km_a ** 2)))
     va, sa = group_ms(a, "vdif_q")
     vb, sb = group_ms(b, "vdif_q")
+    vb += group_ms(b, "closure")[0]  # the network kernel, its own profile group
     out = {"steps": steps, "errors_vs_my25": err, "columns_on_network": st["columns_on_network"],
            "nodes": case["grid"]["M"], "wait_timeouts": st["wait_timeouts"],
            "closure_step_ms": {"my25": va, "learned": vb}, "step_ms": {"my25": sa, "learned": sb}}
@@ -260,8 +261,16 @@ def main():
     ap.add_argument("--eval-npts", type=int, default=200000)
     ap.add_argument("--eval-steps", type=int, default=200)
     ap.add_argument("--source", default="channel", choices=["channel", "coastal"])
+    ap.add_argument("--load", default=None,
+                    help="evaluate a trained network (.npz from --out) instead of generating and training one")
     args = ap.parse_args()
     from . import cases
+    if args.load:
+        trained = load(args.load)
+        report = {"network": args.load,
+                  "coastal": evaluate_on(cases.coastal_mesh(npts=args.eval_npts), trained, args.eval_steps)}
+        print(json.dumps(report))
+        return
     t0 = time.time()
     X, Y = generate(args.samples, source=args.source)
     t1 = time.time()
