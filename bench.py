@@ -470,17 +470,28 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        steps = max(1, min(args.steps, 5))
-        rate, cores, n, secs = cpu_rate(case, 1e9, warm=min(max(args.warmup, 0), 1), cap=steps - 1)
+        # the requested warm-up and timed steps, each one internal step of the full workload
+        # (about 3 s on 16 host threads); at most 60 timed steps keep the arm within minutes
+        from oracle.oracle import Oracle, max_threads
+        steps = max(1, min(args.steps, 60))
+        warm = max(0, min(args.warmup, 10))
+        ora = Oracle(case)
+        ora.run(warm)
+        t0 = time.perf_counter()
+        ora.run(steps)
+        secs = time.perf_counter() - t0
+        ora.close()
+        n, cores = steps, max_threads()
+        rate = cells_layers * n / secs
         rate1, secs1 = cpu_rate_single_core(case)
         line = {"impl": "reference", "metric": metric, "value": rate, "unit": "cell-layer updates/s",
-                "n_gpus": args.gpus, "steps": n, "warmup": min(args.warmup, 1),
+                "n_gpus": args.gpus, "steps": n, "warmup": warm,
                 "ms_per_step": 1e3 * secs / n, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
                 "cpu_baseline": {"value": rate, "unit": "cell-layer updates/s", "cores": cores, "kind": "port",
-                                 "sample": "%d internal steps of the full workload after one warm-up step, "
+                                 "sample": "%d internal steps of the full workload after %d warm-up steps, "
                                            "FP64 CPU restatement of the reference (OpenMP over layers and "
-                                           "columns)" % n,
+                                           "columns)" % (n, warm),
                                  "single_core": {"value": rate1, "unit": "cell-layer updates/s", "cores": 1,
                                                  "sample": "1 internal step (%.1f s) after one warm-up "
                                                            "step, one host thread" % secs1}},

@@ -250,6 +250,14 @@ struct Dev {
   // walking col_lc consecutive layers, so the entity's index chain (cell -> edge ->
   // neighbour) is resolved from cache after the first layer.  Results do not depend on it.
   int col_bc, col_lc;
+  // L2 residency of the external loop (host side only): the loop's per-cell and per-node
+  // arrays lie in one allocation starting at l2_base, most reused first; the loop's
+  // launches carry an access-policy window over its first l2_bytes, whose lines L2 keeps
+  // in its persisting portion (fraction l2_hit of them) across the 40 stages of a step.
+  // l2_bytes = 0: no window.
+  void* l2_base;
+  size_t l2_bytes;
+  float l2_hit;
 };
 
 // Grid of a column-tiled kernel over n entities and nl layers.
@@ -436,6 +444,7 @@ enum ExtNodeParts { EN_EXTEL = 1, EN_BC = 2, EN_COPY_ELRK = 4, EN_GRAD = 8, EN_F
 enum ExtCellParts { EC_N2E = 1, EC_FLUXOBN = 2, EC_ADVAVE = 4, EC_EXTUV = 8, EC_BC2 = 16, EC_COPY_RK = 32,
                     EC_INT_ADVAVE = 64, EC_FINISH = 128, EC_COMPACT = 256, EC_LAST = 512 };
 void launch_ext_finish(const Dev& P, cudaStream_t s, int K, int wet_prev);
+void launch_l2_release(const Dev& P, cudaStream_t s);
 // pdl: launched as a programmatic dependent of the previous kernel in the stream (the
 // fused external loop); the kernel waits for that kernel's completion before it touches
 // memory, while its blocks are scheduled during the previous kernel's tail.

@@ -25,19 +25,35 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
+// The external loop's launches also carry the handle's L2 access-policy window (Dev::l2_*),
+// when it has one.
 template <typename... KArgs, typename... Args>
-static void launch_maybe_pdl(int pdl, void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+static void launch_maybe_pdl(int pdl, void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, const Dev& P,
+                             Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute at[2];
+  int n = 0;
+  if (pdl) {
+    at[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[n].val.programmaticStreamSerializationAllowed = 1;
+    ++n;
+  }
+  if (P.l2_bytes) {
+    at[n].id = cudaLaunchAttributeAccessPolicyWindow;
+    at[n].val.accessPolicyWindow.base_ptr = P.l2_base;
+    at[n].val.accessPolicyWindow.num_bytes = P.l2_bytes;
+    at[n].val.accessPolicyWindow.hitRatio = P.l2_hit;
+    at[n].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    at[n].val.accessPolicyWindow.missProp = cudaAccessPropertyNormal;
+    ++n;
+  }
   cfg.attrs = at;
-  cfg.numAttrs = pdl ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, k, args...);
+  cfg.numAttrs = n;
+  cudaLaunchKernelEx(&cfg, k, P, args...);
 }
 
 __device__ __constant__ double dAlphaRK[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
@@ -971,6 +987,35 @@ void launch_ext_finish(const Dev& P, cudaStream_t s, int K, int wet_prev) {
   int n = P.M > P.N ? P.M : P.N;
   k_ext_finish<<<nblk(n, 256), 256, 0, s>>>(P, K, wet_prev);
 }
+#ifndef FVG_F32_TU
+// One word of every 128-byte line of the external loop's L2 window, read under a window
+// whose hit property is normal: the lines the loop kept persisting return to normal
+// status, so that the rest of the step has the whole L2 (persisting lines otherwise stay
+// until other persisting accesses evict them).  The volatile loads are not removed.
+__global__ void k_l2_release(const char* base, size_t nlines) {
+  for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < nlines; l += (size_t)gridDim.x * blockDim.x) {
+    unsigned v;
+    asm volatile("ld.global.u32 %0, [%1];" : "=r"(v) : "l"(base + l * 128));
+  }
+}
+void launch_l2_release(const Dev& P, cudaStream_t s) {
+  if (!P.l2_bytes) return;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(148 * 4);
+  cfg.blockDim = dim3(256);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeAccessPolicyWindow;
+  at[0].val.accessPolicyWindow.base_ptr = P.l2_base;
+  at[0].val.accessPolicyWindow.num_bytes = P.l2_bytes;
+  at[0].val.accessPolicyWindow.hitRatio = 1.0f;
+  at[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyNormal;
+  at[0].val.accessPolicyWindow.missProp = cudaAccessPropertyNormal;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_l2_release, (const char*)P.l2_base, (P.l2_bytes + 127) / 128);
+}
+#endif
 void launch_begin_step(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 1); }
 void launch_set_qdis(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 0); }
 

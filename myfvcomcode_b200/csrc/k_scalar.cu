@@ -587,10 +587,12 @@ __device__ inline void vq_stress(const Dev& P, int i, double& utau2, double& wub
   wvb = wvb / fn;
 }
 
-// AUX: the learned closure's inputs or the closure samples are written (P.closure or
-// P.clos_samp); without them the kernel is instantiated without those paths.
-template <bool AUX>
-__global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
+// AUX bit 1: the learned closure's inputs are written (P.closure); bit 2: the closure
+// samples (P.clos_samp).  Each combination is its own instantiation, so that the plain
+// step and the learned step carry none of the other paths' registers; with either path
+// every instantiation is held to 64 registers (four blocks per SM).
+template <int AUX>
+__global__ void __launch_bounds__(256, 4) k_vdif_q_levels(const Dev P) {
   using namespace vq;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.M) return;
@@ -608,7 +610,7 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
   const double l0 = SURFL * utau2 / P.grav_n[i];
   if (kb == 1) P.vq_ut[i] = utau2;
   if (ke == KB) P.q2f[n3(KB)] = sqrt(wub * wub + wvb * wvb) * P.const1;
-  float* const cs = AUX ? P.clos_samp : nullptr;
+  float* const cs = (AUX & 2) ? P.clos_samp : nullptr;
   const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
   auto samp = [&](int f, int k, double v) { cs[(size_t)f * ss + (size_t)(k - 2) * P.M + (i - 1)] = (float)v; };
   // ring means of U, V on the level above the first interior level of the chunk
@@ -647,7 +649,7 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
         ring_mean(k, uk, vk);
         const double den = P.dzz[n3(k - 1)] * d;
         const double shear2 = ((uk - ukm1) * (uk - ukm1) + (vk - vkm1) * (vk - vkm1)) / (den * den);
-        if (AUX && P.closure) {
+        if (AUX & 1) {
           // the network's inputs: inside the envelope or not, then transformed,
           // standardised and rounded to BF16 as the MMA takes them
           const float fv[CLOS_IN] = {(float)boygr, (float)shear2, (float)d, (float)P.z[q], (float)sqrt(utau2),
@@ -663,7 +665,7 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
           }
           P.clos_feat[(size_t)(k - 2) * P.M + (i - 1)] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
         }
-        if (AUX && cs) {
+        if (AUX & 2) {
           samp(0, k, boygr);
           samp(1, k, shear2);
           samp(2, k, d);
@@ -705,7 +707,7 @@ __global__ void __launch_bounds__(256) k_vdif_q_levels(const Dev P) {
       P.vq_dtefl[q] = dtef * (1. + E2 * (x * x));
     }
   }
-  if (AUX && P.closure) P.clos_envc[(size_t)blockIdx.y * (P.M + 1) + i] = chunk_inside ? 1 : 0;
+  if (AUX & 1) P.clos_envc[(size_t)blockIdx.y * (P.M + 1) + i] = chunk_inside ? 1 : 0;
 }
 
 // The q2 and q2l tridiagonal sweeps of one column (vdif_q.F:372-431), and the column's
@@ -772,8 +774,10 @@ __global__ void __launch_bounds__(128) k_vdif_q_sweep(const Dev P) {
 }
 
 // Positivity of the new Q2F/Q2LF, the stability functions and KQ, KM, KH
-// (vdif_q.F:443-491), per (node, level); then Q2 = Q2F, Q2L = Q2LF.
-template <bool AUX>
+// (vdif_q.F:443-491), per (node, level); then Q2 = Q2F, Q2L = Q2LF.  AUX as for
+// k_vdif_q_levels; with the learned closure the interior levels of a column on the network
+// skip the stability functions, which k_closure_mlp replaces.
+template <int AUX>
 __global__ void __launch_bounds__(256) k_vdif_q_coef(const Dev P, int copy_back) {
   using namespace vq;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -784,14 +788,24 @@ __global__ void __launch_bounds__(256) k_vdif_q_coef(const Dev P, int copy_back)
   const double COEF4 = 18.0 * A1 * A1 + 9.0 * A1 * A2;
   const double COEF5 = 9.0 * A1 * A2;
   const bool wet = P.iswetn[i] == 1;
-  float* const cs = AUX ? P.clos_samp : nullptr;
+  float* const cs = (AUX & 2) ? P.clos_samp : nullptr;
   const size_t ss = (size_t)P.M * (size_t)(KBM1 - 1);
   auto samp = [&](int f, int k, double v) { cs[(size_t)f * ss + (size_t)(k - 2) * P.M + (i - 1)] = (float)v; };
+  // interior levels of a column inside the envelope are finished by the network kernel
+  // (k_closure_mlp); every other column keeps MY2.5 here
+  const bool on_network = (AUX & 1) && P.clos_env[i] != 0;
   for (int k = kb; k <= ke; ++k) {
     const size_t q = N3(P, i, k);
     if (k >= 2 && k <= KBM1 && (P.q2f[q] <= SMALL || P.q2lf[q] <= SMALL)) {
       P.q2f[q] = SMALL;
       P.q2lf[q] = SMALL;
+    }
+    if (!(AUX & 2) && on_network && k >= 2 && k <= KBM1) {
+      if (copy_back) {
+        P.q2[q] = P.q2f[q];
+        P.q2l[q] = P.q2lf[q];
+      }
+      continue;
     }
     const double gh = P.vq_gh[q];
     double stf = 1.0;
@@ -805,15 +819,13 @@ __global__ void __launch_bounds__(256) k_vdif_q_coef(const Dev P, int copy_back)
     double kn = P.l[q] * sqrt(P.q2[q]);
     bool interior_by_network = false;
     if (k >= 2 && k <= KBM1) {
-      if (AUX && cs) {
+      if (AUX & 2) {
         samp(8, k, kn * KAPPA * sm);
         samp(9, k, kn * sm);
         samp(10, k, kn * sh * P.vprnu);
         samp(11, k, wet ? 1.0 : 0.0);
       }
-      // interior levels of a column inside the envelope are finished by the network
-      // kernel (k_closure_mlp); every other column keeps MY2.5 here
-      if (AUX && P.closure && P.clos_env[i] != 0) interior_by_network = true;
+      interior_by_network = on_network;
     }
     if (!interior_by_network) {
       P.kq[q] = 0.5 * (kn * KAPPA * sm + P.kq[q]);
@@ -1224,10 +1236,14 @@ void launch_fct_q(const Dev& P, cudaStream_t s, int parts) {
   k_fct_q<<<g, b, 0, s>>>(P, parts);
 }
 void launch_vdif_q(const Dev& P, cudaStream_t s, int copy_back) {
-  const bool aux = P.closure || P.clos_samp;
-  (aux ? k_vdif_q_levels<true> : k_vdif_q_levels<false>)<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P);
+  const int aux = (P.closure ? 1 : 0) | (P.clos_samp ? 2 : 0);
+  void (*lv)(const Dev) = aux == 0 ? k_vdif_q_levels<0> : aux == 1 ? k_vdif_q_levels<1>
+                        : aux == 2 ? k_vdif_q_levels<2> : k_vdif_q_levels<3>;
+  void (*cf)(const Dev, int) = aux == 0 ? k_vdif_q_coef<0> : aux == 1 ? k_vdif_q_coef<1>
+                             : aux == 2 ? k_vdif_q_coef<2> : k_vdif_q_coef<3>;
+  lv<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P);
   k_vdif_q_sweep<<<dim3(nblk(P.M, 128), 2), 128, 0, s>>>(P);
-  (aux ? k_vdif_q_coef<true> : k_vdif_q_coef<false>)<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P, copy_back);
+  cf<<<col_grid(P, P.M, P.KB), P.col_bc, 0, s>>>(P, copy_back);
   if (!P.closure) launch_vdif_q_shallow(P, s);
 }
 void launch_turb_update(const Dev& P, cudaStream_t s) {

@@ -105,3 +105,27 @@ def test_staged_momentum_kernels_in_precision_form(small_coastal):
         x, y = a.get(n), b.get(n)
         scale = max(float(np.abs(y).max()), 1e-12)
         assert np.abs(x - y).max() <= 1e-4 * scale, n
+
+
+def test_l2_window_leaves_results_bitwise_unchanged(small_coastal):
+    """The external loop's arrays live in one allocation after the switch to the
+    precision form, and its launches carry an L2 access-policy window over them: a cache
+    hint only, so runs with the window and without it are bit for bit equal, and fields
+    read and written by name reach the moved arrays."""
+    from myfvcomcode_b200.engine import Fvcom
+    a, b = Fvcom(small_coastal), Fvcom(small_coastal)
+    ua0 = a.get("ua").copy()
+    for f in (a, b):
+        f.set_precision("fp32flux")
+    assert a.get_tuning("compact") == 1
+    assert np.array_equal(a.get("ua"), ua0)
+    b.set_tuning("l2_window_mb", 0)
+    assert b.get_tuning("l2_window_mb") == 0
+    a.run(4)
+    b.run(4)
+    for n in ("el", "ua", "va", "u", "v", "t1", "s1", "iswetc", "iswetn"):
+        assert np.array_equal(a.get(n), b.get(n)), n
+    el = a.get("el")
+    el[1] += 0.25
+    a.set("el", el)
+    assert np.array_equal(a.get("el"), el)
