@@ -313,15 +313,11 @@ int fvg_closure_status(fvg_handle* h, int32_t* columns_on_network, int32_t* wait
                    evaluated once per tile); 1 (default) only the FP64 ADV_UV, where the
                    staged kernel measured faster; 0 keeps one thread per cell everywhere.
                    Results do not depend on it (bit for bit in FP64);
-   "l2_window_mb" = L2 residency of the external loop with the compact cell kernel: the
-                   loop's per-cell and per-node arrays (moved into one allocation by
-                   fvg_set_precision) are kept in L2's persisting part across the 40
-                   Runge-Kutta stages, and returned to normal status after the loop.  -1
-                   (default) = as much as the device's persisting maximum, 0 = off, n =
-                   at most n MiB.  Sets the context's persisting L2 limit
-                   (cudaLimitPersistingL2CacheSize) to that size when it is lower.
-                   fvg_get_tuning reports the window in MiB.  A cache hint only: results
-                   do not depend on it (bit for bit). */
+   "stream_hints" = 1 (default): the external loop's stage kernels load the arrays a
+                   stage reads once (gather lists, slot records, EXTUV's fixed terms, the
+                   Runge-Kutta start values) evict-first in L2, so that the arrays they
+                   gather from neighbours stay in L2 from one stage to the next; 0 plain
+                   loads.  A cache hint only: results do not depend on it (bit for bit). */
 int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value);
 int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value);
 

@@ -57,13 +57,6 @@ struct fvg_handle {
   // possible (the mesh check of fvg_set_precision passed)
   int compact_allowed = 1;
   int compact_ok = 0;
-  // bytes of each allocation (relocation of the external loop's arrays)
-  std::map<void*, size_t> alloc_bytes;
-  // L2 residency of the external loop: the arrays' allocation, its size, and the window's
-  // cap in MiB (tuning key "l2_window_mb": -1 = the device's persisting maximum, 0 = off)
-  void* l2_arena = nullptr;
-  size_t l2_arena_bytes = 0;
-  int l2_mb = -1;
 };
 
 #define CK(call)                                                                      \
@@ -88,7 +81,6 @@ int dalloc(fvg_handle* h, T** p, size_t n) {
   }
   cudaMemset(q, 0, bytes);
   h->allocs.push_back(q);
-  h->alloc_bytes[q] = bytes;
   *p = (T*)q;
   return FVG_OK;
 }
@@ -327,7 +319,6 @@ void enqueue_internal_step(fvg_handle* h, cudaStream_t s, Marker mk = Marker()) 
     }
   }
   launch_ext_finish(P, s, 4, p.wetting_drying_on);
-  launch_l2_release(P, s);
   mk.mark(s, G_EXT_UPD);
   launch_adjust2(P, s, AJ_ADJUST | AJ_HE_FLUX);
   mk.mark(s, G_ADJ2);
@@ -399,6 +390,7 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   P.ms = (int)pad32(M + 1);
   P.ns = (int)pad32(N + 1);
   P.col_bc = 128;
+  P.ldcs = 1;
   P.col_lc = 8;
   P.prec = FVG_PREC_FP64;
   P.nbsn_cols = m->nbsn_cols; P.nbve_cols = m->nbve_cols; P.trie_cols = m->trie_cols;
@@ -857,8 +849,6 @@ void fvg_destroy(fvg_handle* h) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   for (void* p : h->allocs) cudaFree(p);
-  // lines of the freed window would otherwise hold the persisting part of L2
-  if (h->P.l2_bytes) cudaCtxResetPersistingL2Cache();
   if (h->h_sched) cudaFreeHost(h->h_sched);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -1046,7 +1036,6 @@ int32_t fvg_kernels_per_step(const fvg_handle* h) {
   const fvg_params& p = h->prm;
   int n = 1 + 1 + 2 + 2 + 2;                                // begin, cell_pre, grad3+adv3d, baropg+prep, int advave+reset
   n += p.isplit * 4 * (2 + (p.wetting_drying_on ? 1 : 0)) + 1; // RK stages, closing update
-  if (h->P.l2_bytes) n += 1;                                 // release of the L2 window
   if (p.limiter) n += p.isplit * 4 + 1 + 2;                  // slope limiters: stages, ADVAVE, 3-D
   if (p.baropg_z && !p.barotropic) n += 2;                   // PHY_BAROPG's two kernels
   n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv
@@ -1117,106 +1106,6 @@ int fvg_set_forcing(fvg_handle* h, const fvg_forcing* f) {
   return FVG_OK;
 }
 
-namespace {
-
-// The external loop's per-cell and per-node arrays (compact stage kernel, node kernel,
-// WET_JUDGE), most reused first: the gathered ones, which up to three neighbour cells or a
-// node's whole ring read in every stage, then those a stage reads once.
-std::vector<void**> l2_arrays(Dev& P) {
-  return {(void**)&P.ua,        (void**)&P.va,       (void**)&P.uaf,        (void**)&P.vaf,
-          (void**)&P.iswetc,    (void**)&P.iswetce,  (void**)&P.f.g2d4,     (void**)&P.f.artcc,
-          (void**)&P.f.xyc,     (void**)&P.f.vxy,    (void**)&P.el,         (void**)&P.elf,
-          (void**)&P.d,         (void**)&P.h,        (void**)&P.exf2d,      (void**)&P.nbe4,
-          (void**)&P.nv,        (void**)&P.d1,       (void**)&P.elf1,       (void**)&P.el1,
-          (void**)&P.f.slot4,   (void**)&P.f.cflag,  (void**)&P.f.exc0,     (void**)&P.f.exc1,
-          (void**)&P.f.a1u4,    (void**)&P.f.a2u4,   (void**)&P.uark,       (void**)&P.vark,
-          (void**)&P.elrk1,     (void**)&P.elrk,     (void**)&P.art1,       (void**)&P.dtfa,
-          (void**)&P.egf,       (void**)&P.iswetn,   (void**)&P.node_obc,   (void**)&P.node_he_ptr,
-          (void**)&P.node_vpos_ell, (void**)&P.ntve, (void**)&P.nbve,       (void**)&P.uard,
-          (void**)&P.vard};
-}
-
-inline size_t round256(size_t b) { return (b + 255) / 256 * 256; }
-
-// Moves the external loop's arrays into one allocation in the order of l2_arrays, so that
-// one access-policy window covers the most reused of them.  Contents, field names and
-// results are unchanged.  Without room for the allocation the arrays stay where they are.
-int l2_relocate(fvg_handle* h) {
-  Dev& P = h->P;
-  std::vector<void**> list = l2_arrays(P);
-  size_t total = 0;
-  for (void** pp : list) {
-    auto it = h->alloc_bytes.find(*pp);
-    if (it == h->alloc_bytes.end()) { h->err = "L2 relocation: an array of the external loop was not allocated here"; return FVG_ERR_ARG; }
-    total += round256(it->second);
-  }
-  void* arena = nullptr;
-  if (cudaMalloc(&arena, total) != cudaSuccess) {
-    cudaGetLastError();
-    return FVG_OK;
-  }
-  h->allocs.push_back(arena);
-  h->alloc_bytes[arena] = total;
-  std::vector<void*> old;
-  size_t off = 0;
-  for (void** pp : list) {
-    void* o = *pp;
-    const size_t b = h->alloc_bytes[o];
-    void* nw = (char*)arena + off;
-    CK(cudaMemcpyAsync(nw, o, b, cudaMemcpyDeviceToDevice, h->stream));
-    for (auto& kv : h->fields)
-      if (kv.second.d == o) kv.second.d = nw;
-    *pp = nw;
-    old.push_back(o);
-    off += round256(b);
-  }
-  CK(cudaStreamSynchronize(h->stream));
-  for (void* o : old) {
-    cudaFree(o);
-    h->alloc_bytes.erase(o);
-    h->allocs.erase(std::find(h->allocs.begin(), h->allocs.end(), o));
-  }
-  h->l2_arena = arena;
-  h->l2_arena_bytes = total;
-  return FVG_OK;
-}
-
-// The access-policy window of the external loop's launches: the first bytes of the
-// relocated arrays, as many as the persisting part of L2 holds (capped by the tuning key
-// "l2_window_mb"), all of them persisting.  Only in the compact stage kernel's form.
-void l2_window(fvg_handle* h) {
-  Dev& P = h->P;
-  P.l2_base = h->l2_arena;
-  P.l2_bytes = 0;
-  P.l2_hit = 0.0f;
-  if (!h->l2_arena || h->l2_mb == 0 || !P.f.compact) return;
-  int dev = 0, maxp = 0, maxw = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess || maxp <= 0 ||
-      maxw <= 0) {
-    cudaGetLastError();
-    return;
-  }
-  size_t cap = (size_t)maxp;
-  if (h->l2_mb > 0) cap = std::min(cap, (size_t)h->l2_mb << 20);
-  size_t limit = 0;
-  if (cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize) != cudaSuccess) { cudaGetLastError(); return; }
-  if (limit < cap) {
-    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, cap) != cudaSuccess ||
-        cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize) != cudaSuccess) {
-      cudaGetLastError();
-      return;
-    }
-  }
-  const size_t win = std::min(std::min(h->l2_arena_bytes, (size_t)maxw), std::min(cap, limit));
-  if (win == 0) return;
-  P.l2_bytes = win;
-  P.l2_hit = 1.0f;
-}
-
-}  // namespace
-
 int fvg_set_precision(fvg_handle* h, int32_t mode) {
   if (!h) return FVG_ERR_ARG;
   if (mode != FVG_PREC_FP64 && mode != FVG_PREC_FP32_FLUX) { h->err = "unknown precision mode"; return FVG_ERR_ARG; }
@@ -1276,11 +1165,9 @@ int fvg_set_precision(fvg_handle* h, int32_t mode) {
     CK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     h->compact_ok = (bad == 0 && !P.limiter && !P.gcy) ? 1 : 0;
-    if (h->compact_ok && (rc = l2_relocate(h))) return rc;
   }
   P.prec = mode;
   P.f.compact = (mode == FVG_PREC_FP32_FLUX && h->compact_ok) ? h->compact_allowed : 0;
-  l2_window(h);
   // The captured step holds the other precision's kernels: capture again.
   CK(cudaStreamSynchronize(h->stream));
   if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
@@ -1399,11 +1286,8 @@ int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value) {
   } else if (k == "compact") {
     h->compact_allowed = value != 0;
     h->P.f.compact = (h->P.prec == FVG_PREC_FP32_FLUX && h->compact_ok) ? h->compact_allowed : 0;
-    l2_window(h);
-  } else if (k == "l2_window_mb") {
-    if (value < -1) { h->err = "l2_window_mb must be -1 (device maximum), 0 (off) or a size in MiB"; return FVG_ERR_ARG; }
-    h->l2_mb = value;
-    l2_window(h);
+  } else if (k == "stream_hints") {
+    h->P.ldcs = value != 0;
   } else {
     h->err = "unknown tuning key " + k;
     return FVG_ERR_ARG;
@@ -1422,7 +1306,7 @@ int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value) {
   else if (k == "col_layers") *value = h->P.col_lc;
   else if (k == "compact") *value = h->P.f.compact;
   else if (k == "staged") *value = h->P.staged;
-  else if (k == "l2_window_mb") *value = (int32_t)(h->P.l2_bytes >> 20);
+  else if (k == "stream_hints") *value = h->P.ldcs;
   else return FVG_ERR_ARG;
   return FVG_OK;
 }

@@ -17,6 +17,7 @@
 // step.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -250,14 +251,10 @@ struct Dev {
   // walking col_lc consecutive layers, so the entity's index chain (cell -> edge ->
   // neighbour) is resolved from cache after the first layer.  Results do not depend on it.
   int col_bc, col_lc;
-  // L2 residency of the external loop (host side only): the loop's per-cell and per-node
-  // arrays lie in one allocation starting at l2_base, most reused first; the loop's
-  // launches carry an access-policy window over its first l2_bytes, whose lines L2 keeps
-  // in its persisting portion (fraction l2_hit of them) across the 40 stages of a step.
-  // l2_bytes = 0: no window.
-  void* l2_base;
-  size_t l2_bytes;
-  float l2_hit;
+  // 1: the external loop's stage kernels load what a stage reads once evict-first (ld1),
+  // so that the arrays gathered from neighbours stay in L2 between stages (tuning key
+  // "stream_hints"); results do not depend on it.
+  int ldcs;
 };
 
 // Grid of a column-tiled kernel over n entities and nl layers.
@@ -318,6 +315,21 @@ __device__ inline void ghost_uv(const Dev& P, const double* U, const double* V, 
 
 // RAMP of the current internal step, from its schedule row.
 __device__ inline double ramp_int(const Dev& P) { return P.sched[(size_t)P.ctl[0] * P.sl.len]; }
+
+// A load of an array that one pass reads once (CS: evict-first in L2, ld.global.cs), so
+// that the arrays the pass gathers from neighbours keep their L2 lines from one
+// Runge-Kutta stage to the next; a plain load otherwise.
+template <bool CS, class T>
+__device__ __forceinline__ T ld1(const T* p) {
+  if constexpr (!CS) {
+    return *p;
+  } else if constexpr (std::is_same<T, double4>::value) {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p)), b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+  } else {
+    return __ldcs(p);
+  }
+}
 
 // Mesh metrics and scratch of the edge-flux kernels by arithmetic type R.  The FP64
 // instantiation reads the FP64 arrays and forms the edge offsets as the reference does;
@@ -380,14 +392,14 @@ template <> struct Mesh<float> {
 };
 // The cell's NBE and its least-squares coefficients A1U(c,1..4), A2U(c,1..4) in the
 // form's type (FP32: one packed load each).
-template <typename R>
+template <typename R, bool CS = false>
 __device__ inline void lsq_coef(const Dev& P, int c, int& k1, int& k2, int& k3, R* a, R* b) {
-  const int4 nb = P.nbe4[c];
+  const int4 nb = ld1<CS>(P.nbe4 + c);
   k1 = nb.x;
   k2 = nb.y;
   k3 = nb.z;
   if constexpr (sizeof(R) == 4) {
-    const float4 A = P.f.a1u4[c], B = P.f.a2u4[c];
+    const float4 A = ld1<CS>(P.f.a1u4 + c), B = ld1<CS>(P.f.a2u4 + c);
     a[0] = A.x; a[1] = A.y; a[2] = A.z; a[3] = A.w;
     b[0] = B.x; b[1] = B.y; b[2] = B.z; b[3] = B.w;
   } else {
@@ -444,7 +456,6 @@ enum ExtNodeParts { EN_EXTEL = 1, EN_BC = 2, EN_COPY_ELRK = 4, EN_GRAD = 8, EN_F
 enum ExtCellParts { EC_N2E = 1, EC_FLUXOBN = 2, EC_ADVAVE = 4, EC_EXTUV = 8, EC_BC2 = 16, EC_COPY_RK = 32,
                     EC_INT_ADVAVE = 64, EC_FINISH = 128, EC_COMPACT = 256, EC_LAST = 512 };
 void launch_ext_finish(const Dev& P, cudaStream_t s, int K, int wet_prev);
-void launch_l2_release(const Dev& P, cudaStream_t s);
 // pdl: launched as a programmatic dependent of the previous kernel in the stream (the
 // fused external loop); the kernel waits for that kernel's completion before it touches
 // memory, while its blocks are scheduled during the previous kernel's tail.

@@ -44,7 +44,8 @@ constexpr int S_W2 = S_W1 + HID * K1 * 2;         // 64 x 64 bf16, SBO 1024
 constexpr int S_W3 = S_W2 + HID * HID * 2;        // 16 x 64 bf16, SBO 1024
 constexpr int S_A1 = S_W3 + NOUT * HID * 2;         // 128 x 16 bf16, SBO 256
 constexpr int S_A2 = S_A1 + ROWS * K1 * 2;        // 128 x 64 bf16, SBO 1024
-constexpr int S_END = S_A2 + ROWS * HID * 2;
+constexpr int S_B = S_A2 + ROWS * HID * 2;        // biases b1, b2, b3 (64 + 64 + 16 FP32)
+constexpr int S_END = S_B + (2 * HID + NOUT) * 4;
 constexpr int W_IMAGE = S_A1;                     // bytes of the weight image
 // TMEM columns: D1, D2 and D3 all at [0,64) -- each layer's accumulator is read out (and
 // the read waited for) before the next layer's MMA is issued -- so 64 columns are
@@ -186,6 +187,8 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
   const int ntiles = (nrows + ROWS - 1) / ROWS;
   // stage the weight image (bf16, core-matrix layout) and allocate TMEM
   for (int q = t; q < W_IMAGE / 16; q += ROWS) reinterpret_cast<uint4*>(sm)[q] = reinterpret_cast<const uint4*>(wimg)[q];
+  float* const sb = reinterpret_cast<float*>(sm + S_B);
+  for (int q = t; q < 2 * HID + NOUT; q += ROWS) sb[q] = q < 2 * HID + 3 ? bias[q] : 0.f;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
                  "r"(TMEM_COLS));
@@ -204,9 +207,10 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
   const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
   const uint32_t s0 = smem_u32(sm);
   uint32_t phase = 0;
-  const float* b1 = bias;
-  const float* b2 = bias + HID;
-  const float* b3 = bias + 2 * HID;
+  // the biases from shared memory, four at a time
+  const float4* const b1 = reinterpret_cast<const float4*>(sb);
+  const float4* const b2 = reinterpret_cast<const float4*>(sb + HID);
+  const float* const b3 = sb + 2 * HID;
 
   // this thread's row of the next tile: whether it uses the network, and its inputs
   float vn[K1];
@@ -258,17 +262,18 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
         mma_commit(&mbar);
       }
       if (layer == 2 && live && nd) prefetch(r);
-      const bool ok = mbar_wait(&mbar, phase & 1);
-      phase += 1;
-      if (!ok) {
-        atomicExch(&abort_flag, 1);
+      // one thread waits for the MMAs (the others wait at the barrier, issuing nothing);
+      // the barrier and each thread's tcgen05 fence then order the accumulator reads
+      if (t == 0 && !mbar_wait(&mbar, phase & 1)) {
+        abort_flag = 1;
         atomicExch(err, 1);
       }
+      phase += 1;
       __syncthreads();
       if (abort_flag) break;
       fence_after();
       if (layer < 2) {
-        const float* bb = layer == 0 ? b1 : b2;
+        const float4* bb = layer == 0 ? b1 : b2;
         // sixteen accumulator columns at a time: bias, GELU, BF16 into the next layer's
         // A tile (two core-matrix columns), so that few values are live at once
 #pragma unroll
@@ -277,7 +282,11 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
           tmem_ld16(tm + lane_off + 16 * c, w);
           uint32_t q[8];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) q[j] = gelu2_bf16(w[2 * j] + bb[16 * c + 2 * j], w[2 * j + 1] + bb[16 * c + 2 * j + 1]);
+          for (int j = 0; j < 4; ++j) {
+            const float4 b = bb[4 * c + j];
+            q[2 * j] = gelu2_bf16(w[4 * j] + b.x, w[4 * j + 1] + b.y);
+            q[2 * j + 1] = gelu2_bf16(w[4 * j + 2] + b.z, w[4 * j + 3] + b.w);
+          }
           store_cols16_bf16(sm + S_A2, 1024, t, 2 * c, q);
         }
         fence_async_smem();

@@ -25,35 +25,19 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
-// The external loop's launches also carry the handle's L2 access-policy window (Dev::l2_*),
-// when it has one.
 template <typename... KArgs, typename... Args>
-static void launch_maybe_pdl(int pdl, void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, const Dev& P,
-                             Args... args) {
+static void launch_maybe_pdl(int pdl, void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
-  cudaLaunchAttribute at[2];
-  int n = 0;
-  if (pdl) {
-    at[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[n].val.programmaticStreamSerializationAllowed = 1;
-    ++n;
-  }
-  if (P.l2_bytes) {
-    at[n].id = cudaLaunchAttributeAccessPolicyWindow;
-    at[n].val.accessPolicyWindow.base_ptr = P.l2_base;
-    at[n].val.accessPolicyWindow.num_bytes = P.l2_bytes;
-    at[n].val.accessPolicyWindow.hitRatio = P.l2_hit;
-    at[n].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-    at[n].val.accessPolicyWindow.missProp = cudaAccessPropertyNormal;
-    ++n;
-  }
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = n;
-  cudaLaunchKernelEx(&cfg, k, P, args...);
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, args...);
 }
 
 __device__ __constant__ double dAlphaRK[5] = {0.0, 0.25, 1.0 / 3.0, 0.5, 1.0};
@@ -75,12 +59,12 @@ struct Grad {
   R ux, uy, vx, vy;
 };
 
-template <typename R>
+template <typename R, bool CS = false>
 __device__ inline Grad<R> cell_grad(const Dev& P, int c, const double* U, const double* V) {
   typedef Mesh<R> Mh;
   int k1, k2, k3;
   R A[4], B[4];
-  lsq_coef<R>(P, c, k1, k2, k3, A, B);
+  lsq_coef<R, CS>(P, c, k1, k2, k3, A, B);
   const R a1 = A[0], a2 = A[1], a3 = A[2], a4 = A[3], b1 = B[0], b2 = B[1], b3 = B[2], b4 = B[3];
   R u0 = (R)U[c], u1 = (R)U[k1], u2 = (R)U[k2], u3 = (R)U[k3];
   R v0 = (R)V[c], v1 = (R)V[k1], v2 = (R)V[k2], v3 = (R)V[k3];
@@ -99,9 +83,9 @@ __device__ inline Grad<R> cell_grad(const Dev& P, int c, const double* U, const 
 }
 // Least-squares gradient of UA, VA of cell c (advave_edge_gcn.F:634-637, 699-702), stored
 // for the edge loop of the next ADVAVE call in the handle's precision.
-template <typename R>
+template <typename R, bool CS>
 __device__ inline void store_grad_t(const Dev& P, int c) {
-  Grad<R> g = cell_grad<R>(P, c, P.ua, P.va);
+  Grad<R> g = cell_grad<R, CS>(P, c, P.ua, P.va);
   if constexpr (sizeof(R) == 4) {
     P.f.g2d4[c] = make_float4(g.ux, g.uy, g.vx, g.vy);
   } else {
@@ -111,9 +95,10 @@ __device__ inline void store_grad_t(const Dev& P, int c) {
     Mesh<R>::g2d(P, 3)[c] = g.vy;
   }
 }
+template <bool CS>
 __device__ inline void store_grad(const Dev& P, int c) {
-  if (P.prec) store_grad_t<float>(P, c);
-  else store_grad_t<double>(P, c);
+  if (P.prec) store_grad_t<float, CS>(P, c);
+  else store_grad_t<double, CS>(P, c);
 }
 template <typename R>
 __device__ inline Grad<R> load_grad(const Dev& P, int c) {
@@ -148,19 +133,21 @@ __device__ inline void store_exf(const Dev& P, int c) {
 // (external_step.F:262-266).  One thread per node; the node's control-volume half-edges
 // are gathered in ascending half-edge number, the order of the reference's scatter.
 // Node part of WET_JUDGE for node i from the cell flags cwet of the same judgement.
+template <bool CS = false>
 __device__ inline void wet_node(const Dev& P, int i, const int* cwet) {
   double e = P.elf[i];
   int wet = ((P.h[i] + e - P.min_depth) < 1.0e-5) ? 0 : 1;
   // the ring's cell flags, four entries' indices and then their flags loaded at a time
-  const int nt = P.ntve[i];
+  const int nt = ld1<CS>(P.ntve + i);
   const size_t m1 = P.M + 1;
   const int* L = P.nbve + i;
   int s = 0, j = 0;
   for (; j + 4 <= nt; j += 4) {
-    const int c0 = L[j * m1], c1 = L[(j + 1) * m1], c2 = L[(j + 2) * m1], c3 = L[(j + 3) * m1];
+    const int c0 = ld1<CS>(L + j * m1), c1 = ld1<CS>(L + (j + 1) * m1), c2 = ld1<CS>(L + (j + 2) * m1),
+              c3 = ld1<CS>(L + (j + 3) * m1);
     s += cwet[c0] + cwet[c1] + cwet[c2] + cwet[c3];
   }
-  for (; j < nt; ++j) s += cwet[L[j * m1]];
+  for (; j < nt; ++j) s += cwet[ld1<CS>(L + j * m1)];
   if (s == 0) wet = 0;
   P.iswetn[i] = wet;
   P.elf[i] = fmax(e, -P.h[i] + P.min_depth);
@@ -169,15 +156,16 @@ __device__ inline void wet_node(const Dev& P, int i, const int* cwet) {
 // -------------------------------------------------------------------------------------
 // Node part of the update after stage K (external_step.F:333-436): EL = ELF, D, DTFA, and
 // the K == 3 and K == 4 sums.
+template <bool CS = false>
 __device__ inline void ext_update_node(const Dev& P, int i, int K) {
   double e = P.elf[i];
   P.el[i] = e;
   double dd = P.h[i] + e;
   P.d[i] = dd;
   P.dtfa[i] = dd;
-  if (K == 3) P.egf[i] = P.egf[i] + e / (double)P.isplit;
+  if (K == 3) P.egf[i] = ld1<CS>(P.egf + i) + e / (double)P.isplit;
   if (K == 4) {
-    int ob = P.node_obc[i];
+    int ob = ld1<CS>(P.node_obc + i);
     if (ob > 0) {
       double tmp = -(P.elf[i] - P.elrk[i]) * P.art1[i] / P.dte - P.xflux_obcn[ob];
       P.uard_obcn[ob] = P.uard_obcn[ob] + tmp / (double)(float)P.isplit;
@@ -227,6 +215,9 @@ __global__ void k_alfa2(const Dev P) {
   Mh::alfa2(P, 1)[c] = av;
 }
 
+// CS: the arrays the kernel reads once per stage (gather lists, pointers, per-node and
+// per-cell coefficients) are loaded evict-first (ld1).
+template <bool CS>
 __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   pdl_enter();
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -234,7 +225,7 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   // the current UA, VA for ADVAVE of this stage (one job per thread)
   if (i > P.M) {
     const int c = i - P.M;
-    if ((parts & EN_GRAD) && c <= P.N) store_grad(P, c);
+    if ((parts & EN_GRAD) && c <= P.N) store_grad<CS>(P, c);
     return;
   }
   // EXTEL's sum first: its loads (the previous cell kernel's half-edge fluxes) do not
@@ -243,12 +234,13 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
   if (parts & EN_EXTEL) {
     // the half-edge fluxes in ascending half-edge order; four entries' codes and then
     // their fluxes are loaded at a time, and added in order
-    const int n = P.node_he_ptr[i + 1] - P.node_he_ptr[i];
+    const int n = ld1<CS>(P.node_he_ptr + i + 1) - ld1<CS>(P.node_he_ptr + i);
     const int* L = P.node_vpos_ell + i;
     const size_t ms = P.ms;
     int j = 0;
     for (; j + 4 <= n; j += 4) {
-      const int e0 = L[j * ms], e1 = L[(j + 1) * ms], e2 = L[(j + 2) * ms], e3 = L[(j + 3) * ms];
+      const int e0 = ld1<CS>(L + j * ms), e1 = ld1<CS>(L + (j + 1) * ms), e2 = ld1<CS>(L + (j + 2) * ms),
+                e3 = ld1<CS>(L + (j + 3) * ms);
       const double f0 = P.exf2d[e0 >> 1], f1 = P.exf2d[e1 >> 1], f2 = P.exf2d[e2 >> 1], f3 = P.exf2d[e3 >> 1];
       x = (e0 & 1) ? x + f0 : x - f0;
       x = (e1 & 1) ? x + f1 : x - f1;
@@ -256,17 +248,17 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
       x = (e3 & 1) ? x + f3 : x - f3;
     }
     for (; j < n; ++j) {
-      const int e = L[j * ms];
+      const int e = ld1<CS>(L + j * ms);
       const double exflux = P.exf2d[e >> 1];
       x = (e & 1) ? x + exflux : x - exflux;
     }
   }
   // the previous stage's node judgement, its cell flags now in ISWETCE (roles swapped)
-  if (parts & EN_WET_PREV) wet_node(P, i, P.iswetce);
-  if (parts & EN_FINISH_PREV) ext_update_node(P, i, (parts >> 8) & 7);
+  if (parts & EN_WET_PREV) wet_node<CS>(P, i, P.iswetce);
+  if (parts & EN_FINISH_PREV) ext_update_node<CS>(P, i, (parts >> 8) & 7);
   if (parts & EN_COPY_ELRK) P.elrk[i] = P.el[i];
   const double alpha = dAlphaRK[K];
-  int ob = P.node_obc[i];
+  int ob = ld1<CS>(P.node_obc + i);
   if (parts & EN_EXTEL) {
     if (ob > 0) {
       P.xflux_obcn[ob] = x;
@@ -281,7 +273,7 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
         x = x - P.qdis[j] * P.rdisq[(size_t)(r & 1) * (P.numqbc + 1) + j];
     }
     double dtk = alpha * P.dte;
-    P.elf[i] = P.elrk[i] - dtk * x / P.art1[i];
+    P.elf[i] = ld1<CS>(P.elrk + i) - dtk * x / ld1<CS>(P.art1 + i);
   }
   if ((parts & EN_BC) && ob > 0) {
     int kind = P.obc_kind[ob];
@@ -309,11 +301,12 @@ __global__ void k_ext_node(const Dev P, int iext, int K, int parts) {
 // unclamped ELF of its nodes, and ELF1 is the mean of the clamped ELF, which each cell
 // forms itself from h and ELF.  Then nodes: the node flag and the clamp of ELF.
 // -------------------------------------------------------------------------------------
+template <bool CS>
 __global__ void k_wet_cells(const Dev P) {
   pdl_enter();
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
-  int n1 = P.nv[i], n2 = P.nv[(size_t)(P.N + 1) + i], n3 = P.nv[(size_t)2 * (P.N + 1) + i];
+  int n1 = ld1<CS>(P.nv + i), n2 = ld1<CS>(P.nv + (size_t)(P.N + 1) + i), n3 = ld1<CS>(P.nv + (size_t)2 * (P.N + 1) + i);
   double e1 = P.elf[n1], e2 = P.elf[n2], e3 = P.elf[n3];
   double dtmp = fmax(fmax(e1, e2), e3) + fmin(fmin(P.h[n1], P.h[n2]), P.h[n3]);
   P.iswetc[i] = ((dtmp - P.min_depth) < 1.0e-5) ? 0 : 1;
@@ -598,25 +591,30 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_ext_cell(const 
 // -------------------------------------------------------------------------------------
 // 64 registers (eight blocks per SM): held to 80 registers, six blocks, it measured slower
 // (1.89 against 1.76 ms per step).
+// CS: the records the stage reads once (flags, slots, EXTUV's fixed terms, the Runge-Kutta
+// start values, the cell's own D1/ELF1/EL1) are loaded evict-first (ld1), so that what
+// neighbours gather (UA, VA, the gradients, ART/CC_HVC, XC/YC, the nodes' VX/VY, D, EL,
+// the wet flags) keeps its L2 lines between stages.
+template <bool CS>
 __global__ void __launch_bounds__(128, 8) k_ext_cell_c(const Dev P, int iext, int K, int parts) {
   pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
   const size_t n1 = P.N + 1;
-  const int fl = P.f.cflag[i];
+  const int fl = ld1<CS>(P.f.cflag + i);
   const int isbce = fl & 3;
   const double ua_i = P.ua[i], va_i = P.va[i];
   if (parts & EC_COPY_RK) {
     P.uark[i] = ua_i;
     P.vark[i] = va_i;
-    P.elrk1[i] = P.el1[i];
+    P.elrk1[i] = ld1<CS>(P.el1 + i);
   }
   double elf1 = 0.0;
   if (parts & EC_N2E) {
-    elf1 = ONE_THIRD * (P.elf[P.nv[i]] + P.elf[P.nv[n1 + i]] + P.elf[P.nv[2 * n1 + i]]);
+    elf1 = ONE_THIRD * (P.elf[ld1<CS>(P.nv + i)] + P.elf[ld1<CS>(P.nv + n1 + i)] + P.elf[ld1<CS>(P.nv + 2 * n1 + i)]);
     P.elf1[i] = elf1;
   } else if (parts & (EC_EXTUV | EC_FINISH)) {
-    elf1 = P.elf1[i];
+    elf1 = ld1<CS>(P.elf1 + i);
   }
   double fob = 0.0;
   if (parts & EC_FLUXOBN) {
@@ -626,9 +624,9 @@ __global__ void __launch_bounds__(128, 8) k_ext_cell_c(const Dev P, int iext, in
     fob = P.fluxobn[i];
   }
   const int weti = P.iswetce[i] * P.iswetc[i];
-  const double d1i = P.d1[i];
+  const double d1i = ld1<CS>(P.d1 + i);
   // {COR*ART, ART, H1, GRAV_E}: formed by the internal-step call below, read by the stages
-  const double4 e1 = (parts & EC_INT_ADVAVE) ? make_double4(0.0, 0.0, 0.0, P.grav_e[i]) : P.f.exc1[i];
+  const double4 e1 = (parts & EC_INT_ADVAVE) ? make_double4(0.0, 0.0, 0.0, P.grav_e[i]) : ld1<CS>(P.f.exc1 + i);
   double xf = 0.0, yf = 0.0, px = 0.0, py = 0.0;
   if (parts & (EC_ADVAVE | EC_INT_ADVAVE)) {
     const float half = 0.5f, one = 1.0f;
@@ -641,7 +639,7 @@ __global__ void __launch_bounds__(128, 8) k_ext_cell_c(const Dev P, int iext, in
     float xr = 0.f, yr = 0.f;
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
-      const int4 sl = P.f.slot4[(size_t)s * n1 + i];  // {code, other cell, IENODE1, IENODE2}
+      const int4 sl = ld1<CS>(P.f.slot4 + (size_t)s * n1 + i);  // {code, other cell, IENODE1, IENODE2}
       const int code = sl.x, side = code & 1, o = sl.y, j1 = sl.z, j2 = sl.w;
       const double2 v1 = P.f.vxy[j1], v2 = P.f.vxy[j2];
       const double xijc = (v1.x + v2.x) / 2.0, yijc = (v1.y + v2.y) / 2.0;
@@ -746,14 +744,14 @@ __global__ void __launch_bounds__(128, 8) k_ext_cell_c(const Dev P, int iext, in
     double uaf = 0.0, vaf = 0.0;
     if (parts & EC_EXTUV) {
       if (weti == 1) {
-        const double4 e0 = P.f.exc0[i];
+        const double4 e0 = ld1<CS>(P.f.exc0 + i);
         const double ramp = sched_row(P)[P.sl.ramp_ext(iext)];
         const double resx = e0.x + xf + px - e1.x * va_i * d1i - ramp * e0.z;
         const double resy = e0.y + yf + py + e1.x * ua_i * d1i - ramp * e0.w;
         const double a = dAlphaRK[K];
-        const double uark = (parts & EC_COPY_RK) ? ua_i : P.uark[i];
-        const double vark = (parts & EC_COPY_RK) ? va_i : P.vark[i];
-        const double elrk1 = (parts & EC_COPY_RK) ? P.el1[i] : P.elrk1[i];
+        const double uark = (parts & EC_COPY_RK) ? ua_i : ld1<CS>(P.uark + i);
+        const double vark = (parts & EC_COPY_RK) ? va_i : ld1<CS>(P.vark + i);
+        const double elrk1 = (parts & EC_COPY_RK) ? ld1<CS>(P.el1 + i) : ld1<CS>(P.elrk1 + i);
         uaf = (uark * (e1.z + elrk1) - a * P.dte * resx / e1.y) / (e1.z + elf1);
         vaf = (vark * (e1.z + elrk1) - a * P.dte * resy / e1.y) / (e1.z + elf1);
       }
@@ -778,13 +776,13 @@ __global__ void __launch_bounds__(128, 8) k_ext_cell_c(const Dev P, int iext, in
       const double dd1 = e1.z + elf1;
       P.d1[i] = dd1;
       if (K == 3) {
-        P.uard[i] = P.uard[i] + uaf * dd1;
-        P.vard[i] = P.vard[i] + vaf * dd1;
+        P.uard[i] = ld1<CS>(P.uard + i) + uaf * dd1;
+        P.vard[i] = ld1<CS>(P.vard + i) + vaf * dd1;
       }
       const double2 xyi = P.f.xyc[i];
 #pragma unroll
       for (int s = 0; s < 3; ++s) {
-        const int4 sl = P.f.slot4[(size_t)s * n1 + i];
+        const int4 sl = ld1<CS>(P.f.slot4 + (size_t)s * n1 + i);
         const double2 v1 = P.f.vxy[sl.z], v2 = P.f.vxy[sl.w];
         const double dxe = (v1.x + v2.x) / 2.0 - xyi.x, dye = (v1.y + v2.y) / 2.0 - xyi.y;
         P.exf2d[(size_t)s * P.ns + i] = dd1 * (-uaf * dye + vaf * dxe);
@@ -827,7 +825,7 @@ __global__ void k_ext_finish(const Dev P, int K, int wet_prev) {
 __global__ void k_ext_prep(const Dev P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.N) return;
-  store_grad(P, i);
+  store_grad<false>(P, i);
   store_exf(P, i);
 }
 
@@ -845,7 +843,8 @@ static inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
 void launch_ext_node(const Dev& P, cudaStream_t s, int iext, int K, int parts, int pdl) {
   int n = (parts & EN_GRAD) ? P.M + P.N : P.M;
-  launch_maybe_pdl(pdl, k_ext_node, dim3(nblk(n, 256)), dim3(256), s, P, iext, K, parts);
+  launch_maybe_pdl(pdl, P.ldcs ? k_ext_node<true> : k_ext_node<false>, dim3(nblk(n, 256)), dim3(256), s, P, iext, K,
+                   parts);
 }
 void launch_ext_prep(const Dev& P, cudaStream_t s) { k_ext_prep<<<nblk(P.N, 256), 256, 0, s>>>(P); }
 void launch_alfa2(const Dev& P, cudaStream_t s) {
@@ -961,18 +960,19 @@ void launch_make_compact(const Dev& P, cudaStream_t s, int* mismatch) {
 #endif
 
 void launch_wet_judge(const Dev& P, cudaStream_t s) {
-  k_wet_cells<<<nblk(P.N, 256), 256, 0, s>>>(P);
+  k_wet_cells<false><<<nblk(P.N, 256), 256, 0, s>>>(P);
   k_wet_nodes<<<nblk(P.M, 256), 256, 0, s>>>(P);
 }
 void launch_wet_cells(const Dev& P, cudaStream_t s, int pdl) {
-  launch_maybe_pdl(pdl, k_wet_cells, dim3(nblk(P.N, 256)), dim3(256), s, P);
+  launch_maybe_pdl(pdl, P.ldcs ? k_wet_cells<true> : k_wet_cells<false>, dim3(nblk(P.N, 256)), dim3(256), s, P);
 }
 void launch_ext_cell(const Dev& P, cudaStream_t s, int iext, int K, int parts, int pdl) {
   FVG_F32_FORWARD(launch_ext_cell(P, s, iext, K, parts, pdl));
   void (*k)(const Dev, int, int, int);
 #ifdef FVG_F32_TU
   if ((parts & EC_COMPACT) && P.f.compact && !P.limiter && !P.gcy) {
-    launch_maybe_pdl(pdl, k_ext_cell_c, dim3(nblk(P.N, 128)), dim3(128), s, P, iext, K, parts);
+    launch_maybe_pdl(pdl, P.ldcs ? k_ext_cell_c<true> : k_ext_cell_c<false>, dim3(nblk(P.N, 128)), dim3(128), s, P,
+                     iext, K, parts);
     return;
   }
 #endif
@@ -987,35 +987,6 @@ void launch_ext_finish(const Dev& P, cudaStream_t s, int K, int wet_prev) {
   int n = P.M > P.N ? P.M : P.N;
   k_ext_finish<<<nblk(n, 256), 256, 0, s>>>(P, K, wet_prev);
 }
-#ifndef FVG_F32_TU
-// One word of every 128-byte line of the external loop's L2 window, read under a window
-// whose hit property is normal: the lines the loop kept persisting return to normal
-// status, so that the rest of the step has the whole L2 (persisting lines otherwise stay
-// until other persisting accesses evict them).  The volatile loads are not removed.
-__global__ void k_l2_release(const char* base, size_t nlines) {
-  for (size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x; l < nlines; l += (size_t)gridDim.x * blockDim.x) {
-    unsigned v;
-    asm volatile("ld.global.u32 %0, [%1];" : "=r"(v) : "l"(base + l * 128));
-  }
-}
-void launch_l2_release(const Dev& P, cudaStream_t s) {
-  if (!P.l2_bytes) return;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(148 * 4);
-  cfg.blockDim = dim3(256);
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeAccessPolicyWindow;
-  at[0].val.accessPolicyWindow.base_ptr = P.l2_base;
-  at[0].val.accessPolicyWindow.num_bytes = P.l2_bytes;
-  at[0].val.accessPolicyWindow.hitRatio = 1.0f;
-  at[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyNormal;
-  at[0].val.accessPolicyWindow.missProp = cudaAccessPropertyNormal;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_l2_release, (const char*)P.l2_base, (P.l2_bytes + 127) / 128);
-}
-#endif
 void launch_begin_step(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 1); }
 void launch_set_qdis(const Dev& P, cudaStream_t s) { k_begin_step<<<1, 32, 0, s>>>(P, 0); }
 

@@ -107,25 +107,19 @@ def test_staged_momentum_kernels_in_precision_form(small_coastal):
         assert np.abs(x - y).max() <= 1e-4 * scale, n
 
 
-def test_l2_window_leaves_results_bitwise_unchanged(small_coastal):
-    """The external loop's arrays live in one allocation after the switch to the
-    precision form, and its launches carry an L2 access-policy window over them: a cache
-    hint only, so runs with the window and without it are bit for bit equal, and fields
-    read and written by name reach the moved arrays."""
+def test_stream_hints_leave_results_bitwise_unchanged(small_coastal):
+    """The external loop's stage kernels load what a stage reads once evict-first in L2
+    (tuning key stream_hints, on by default): a cache hint only, so runs with and without
+    it are bit for bit equal, in the precision form and in plain FP64."""
     from myfvcomcode_b200.engine import Fvcom
-    a, b = Fvcom(small_coastal), Fvcom(small_coastal)
-    ua0 = a.get("ua").copy()
-    for f in (a, b):
-        f.set_precision("fp32flux")
-    assert a.get_tuning("compact") == 1
-    assert np.array_equal(a.get("ua"), ua0)
-    b.set_tuning("l2_window_mb", 0)
-    assert b.get_tuning("l2_window_mb") == 0
-    a.run(4)
-    b.run(4)
-    for n in ("el", "ua", "va", "u", "v", "t1", "s1", "iswetc", "iswetn"):
-        assert np.array_equal(a.get(n), b.get(n)), n
-    el = a.get("el")
-    el[1] += 0.25
-    a.set("el", el)
-    assert np.array_equal(a.get("el"), el)
+    for prec in ("fp32flux", "fp64"):
+        a, b = Fvcom(small_coastal), Fvcom(small_coastal)
+        for f in (a, b):
+            f.set_precision(prec)
+        assert a.get_tuning("stream_hints") == 1
+        b.set_tuning("stream_hints", 0)
+        assert b.get_tuning("stream_hints") == 0
+        a.run(4)
+        b.run(4)
+        for n in ("el", "ua", "va", "u", "v", "t1", "s1", "iswetc", "iswetn"):
+            assert np.array_equal(a.get(n), b.get(n)), (prec, n)
