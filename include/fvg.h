@@ -317,7 +317,11 @@ int fvg_closure_status(fvg_handle* h, int32_t* columns_on_network, int32_t* wait
                    stage reads once (gather lists, slot records, EXTUV's fixed terms, the
                    Runge-Kutta start values) evict-first in L2, so that the arrays they
                    gather from neighbours stay in L2 from one stage to the next; 0 plain
-                   loads.  A cache hint only: results do not depend on it (bit for bit). */
+                   loads.  A cache hint only: results do not depend on it (bit for bit);
+   "ext_grid"     = blocks per SM (1..8, default 8) of the external loop's compact cell
+                   kernel, launched as one wave whose threads walk the cells so that no
+                   partly filled last wave is left; 0 launches one thread per cell.
+                   Results do not depend on it. */
 int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value);
 int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value);
 

@@ -391,6 +391,13 @@ int fvg_create(const fvg_mesh* m, const fvg_params* prm, const fvg_forcing* f, f
   P.ns = (int)pad32(N + 1);
   P.col_bc = 128;
   P.ldcs = 1;
+  P.ext_grid = 8;
+  P.nsm = 148;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&P.nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      P.nsm = 148;
+  }
   P.col_lc = 8;
   P.prec = FVG_PREC_FP64;
   P.nbsn_cols = m->nbsn_cols; P.nbve_cols = m->nbve_cols; P.trie_cols = m->trie_cols;
@@ -1040,7 +1047,7 @@ int32_t fvg_kernels_per_step(const fvg_handle* h) {
   if (p.baropg_z && !p.barotropic) n += 2;                   // PHY_BAROPG's two kernels
   n += 1 + 1 + 1 + 1 + 2 + 1;                              // adjust2, vertvl x2, w/viscofh, grad3+adv_uv, vdif_uv
   n += 7;                                                  // grad_q, adv_q (2 phases), vdif_q (4 passes)
-  if (h->P.closure) n += 1;                                // learned closure
+  if (h->P.closure) n += 3;                                // learned closure (compaction x2, network)
   if (p.temperature_active || p.salinity_active)           // grad_ts, adv_ts (2 phases), vdif_ts,
     n += 5 + (h->P.iobcn > 0 ? 1 : 0);                     // bcond_ts (rivers, open boundary)
   n += 1;                                                  // final
@@ -1200,6 +1207,8 @@ int fvg_set_closure(fvg_handle* h, int32_t mode, const float* params, int32_t np
     // one flag per level chunk and node: at most KB chunks (one level per thread)
     if ((rc = dalloc(h, &P.clos_envc, (size_t)P.KB * ((size_t)P.M + 1)))) return rc;
     if ((rc = dalloc(h, &P.clos_env, (size_t)P.M + 1))) return rc;
+    if ((rc = dalloc(h, &P.clos_list, (size_t)P.M + 1))) return rc;
+    if ((rc = dalloc(h, &P.clos_cnt, (size_t)P.M / 1024 + 2))) return rc;
     if ((rc = dalloc(h, &P.clos_err, 1))) return rc;
     float* b = nullptr;
     if ((rc = dalloc(h, &b, 144))) return rc;
@@ -1288,6 +1297,9 @@ int fvg_set_tuning(fvg_handle* h, const char* key, int32_t value) {
     h->P.f.compact = (h->P.prec == FVG_PREC_FP32_FLUX && h->compact_ok) ? h->compact_allowed : 0;
   } else if (k == "stream_hints") {
     h->P.ldcs = value != 0;
+  } else if (k == "ext_grid") {
+    if (value < 0 || value > 8) { h->err = "ext_grid must be 0..8 blocks per SM"; return FVG_ERR_ARG; }
+    h->P.ext_grid = value;
   } else {
     h->err = "unknown tuning key " + k;
     return FVG_ERR_ARG;
@@ -1307,6 +1319,7 @@ int fvg_get_tuning(const fvg_handle* h, const char* key, int32_t* value) {
   else if (k == "compact") *value = h->P.f.compact;
   else if (k == "staged") *value = h->P.staged;
   else if (k == "stream_hints") *value = h->P.ldcs;
+  else if (k == "ext_grid") *value = h->P.ext_grid;
   else return FVG_ERR_ARG;
   return FVG_OK;
 }

@@ -242,6 +242,9 @@ struct Dev {
   uint4* clos_feat;
   unsigned char* clos_envc;
   int* clos_env;
+  // clos_list: [0] the number of columns on the network, [1..] their nodes ascending
+  // (compacted from clos_env each step); clos_cnt: per-block counts of the compaction
+  int *clos_list, *clos_cnt;
   int* clos_err;
   Tiles tl;
   // 1: ADVECTION_EDGE_GCN and ADV_UV_EDGE_GCN run as the tile-staged kernels (no limiter,
@@ -255,6 +258,10 @@ struct Dev {
   // so that the arrays gathered from neighbours stay in L2 between stages (tuning key
   // "stream_hints"); results do not depend on it.
   int ldcs;
+  // Blocks per SM of the compact stage kernel's grid-stride launch (tuning key
+  // "ext_grid", default 8: one full wave whose threads walk the cells); 0: one thread per
+  // cell.  nsm: the device's SM count.
+  int ext_grid, nsm;
 };
 
 // Grid of a column-tiled kernel over n entities and nl layers.

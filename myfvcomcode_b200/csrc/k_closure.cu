@@ -322,16 +322,76 @@ __device__ inline void mlp_tc_tiles(const void* wimg, const float* bias, int nro
   }
 }
 
-// The closure step: rows are (level K, node I) with r = (K-2)*M + (I-1).  VDIF_Q has
-// finished every column outside the envelope with MY2.5 and left the BF16 inputs of the
-// others in clos_feat; this kernel finishes the columns inside the envelope.  After a
-// wait ran out (store with net_ok false) a row keeps its coefficients, and the step
-// reports FVG_ERR_TIMEOUT.
+// Ordered compaction of the columns on the network (clos_env != 0) into clos_list, in two
+// passes over blocks of kListBlock nodes: per-block counts, then each block's offset (the
+// sum of the counts before it) plus an exclusive scan inside the block.  Nodes stay in
+// ascending order.
+constexpr int kListBlock = 1024;  // nodes per block: 256 threads x 4
+__device__ inline int block_exclusive_scan(int v, int* ws, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  int before = 0;
+  total = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    if (w < warp) before += ws[w];
+    total += ws[w];
+  }
+  return before + x - v;
+}
+__global__ void __launch_bounds__(256) k_clos_count(const Dev P) {
+  __shared__ int ws[8];
+  const int i0 = blockIdx.x * kListBlock + threadIdx.x * 4 + 1;
+  int c = 0;
+  for (int q = 0; q < 4; ++q) c += (i0 + q <= P.M && P.clos_env[i0 + q] != 0) ? 1 : 0;
+  int total;
+  block_exclusive_scan(c, ws, total);
+  if (threadIdx.x == 0) P.clos_cnt[blockIdx.x] = total;
+}
+__global__ void __launch_bounds__(256) k_clos_list(const Dev P) {
+  __shared__ int ws[8];
+  __shared__ int base;
+  if (threadIdx.x < 32) {
+    int b = 0;
+    for (int j = threadIdx.x; j < (int)blockIdx.x; j += 32) b += P.clos_cnt[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
+    if (threadIdx.x == 0) base = b;
+  }
+  const int i0 = blockIdx.x * kListBlock + threadIdx.x * 4 + 1;
+  bool on[4];
+  int c = 0;
+  for (int q = 0; q < 4; ++q) {
+    on[q] = i0 + q <= P.M && P.clos_env[i0 + q] != 0;
+    c += on[q] ? 1 : 0;
+  }
+  int total;
+  int pos = block_exclusive_scan(c, ws, total) + base;
+  for (int q = 0; q < 4; ++q)
+    if (on[q]) P.clos_list[1 + pos++] = i0 + q;
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) P.clos_list[0] = base + total;
+}
+
+// The closure step.  VDIF_Q has finished every column outside the envelope with MY2.5 and
+// left the BF16 inputs of the others in clos_feat (row (K-2)*M + (I-1)); this kernel
+// finishes the columns on the network: its rows are (level K, j-th column on the network)
+// with r = (K-2)*n + j, n = clos_list[0], node I = clos_list[1 + j].  After a wait ran out
+// (store with net_ok false) a row keeps its coefficients, and the step reports
+// FVG_ERR_TIMEOUT.
 __global__ void __launch_bounds__(ROWS, kCtasPerSm) k_closure_mlp(const Dev P, int* err) {
-  const int nrows = P.M * (P.KBM1 - 1);
+  const int nnet = P.clos_list[0];
+  const int nrows = nnet * (P.KBM1 - 1);
+  const int* const list = P.clos_list + 1;
   const ClosNorm& nm = P.clos_norm;
+  auto node_of = [&](int r) { return list[r % nnet]; };
   auto load = [&](int r, float* v) {
-    const uint4 w = P.clos_feat[r];
+    const uint4 w = P.clos_feat[(size_t)(r / nnet) * P.M + (node_of(r) - 1)];
     const uint32_t u[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -342,14 +402,14 @@ __global__ void __launch_bounds__(ROWS, kCtasPerSm) k_closure_mlp(const Dev P, i
   };
   double kold[3] = {0.0, 0.0, 0.0};  // KQ, KM, KH of the row, fetched during the last MMA
   auto prefetch = [&](int r) {
-    const size_t q = N3(P, r % P.M + 1, r / P.M + 2);
+    const size_t q = N3(P, node_of(r), r / nnet + 2);
     kold[0] = P.kq[q];
     kold[1] = P.km[q];
     kold[2] = P.kh[q];
   };
   auto store = [&](int r, const float* o, bool net_ok) {
-    const int k = r / P.M + 2, i = r % P.M + 1;
-    if (!net_ok || P.clos_env[i] == 0) return;
+    const int k = r / nnet + 2, i = node_of(r);
+    if (!net_ok) return;
     const size_t q = N3(P, i, k);
     double nw[3];
     for (int c = 0; c < 3; ++c) {
@@ -361,7 +421,7 @@ __global__ void __launch_bounds__(ROWS, kCtasPerSm) k_closure_mlp(const Dev P, i
     P.km[q] = 0.5 * (nw[1] + kold[1]);
     P.kh[q] = 0.5 * (nw[2] + kold[2]);
   };
-  auto need = [&](int r) { return P.clos_env[r % P.M + 1] != 0; };
+  auto need = [](int) { return true; };
   mlp_tc_tiles(P.clos_w, P.clos_b, nrows, load, store, need, prefetch, err);
 }
 
@@ -403,6 +463,9 @@ void launch_vdif_q_shallow(const Dev& P, cudaStream_t s) {
 }
 
 void launch_closure(const Dev& P, cudaStream_t s, int* err, int grid) {
+  const int nb = P.M / kListBlock + 1;
+  k_clos_count<<<nb, 256, 0, s>>>(P);
+  k_clos_list<<<nb, 256, 0, s>>>(P);
   k_closure_mlp<<<grid, ROWS, S_END, s>>>(P, err);
   k_closure_shallow<<<(P.M + 127) / 128, 128, 0, s>>>(P);
 }

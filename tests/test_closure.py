@@ -65,12 +65,19 @@ def _samples(case, steps=120, every=4):
     return np.concatenate(xs), np.concatenate(ys)
 
 
-def test_trained_network_runs_in_the_step(small_channel):
+@pytest.fixture(scope="module")
+def channel_trained(small_channel):
+    from myfvcomcode_b200 import closure
+    X, Y = _samples(small_channel)
+    tr = closure.train(X, Y, epochs=30, batch=256, lr=3e-3, seed=1)
+    return X, Y, tr
+
+
+def test_trained_network_runs_in_the_step(small_channel, channel_trained):
     from myfvcomcode_b200 import closure
     from myfvcomcode_b200.engine import Fvcom
-    X, Y = _samples(small_channel)
+    X, Y, tr = channel_trained
     assert X.shape[0] > 5000 and np.isfinite(X).all() and (Y >= 0).all()
-    tr = closure.train(X, Y, epochs=30, batch=256, lr=3e-3, seed=1)
     assert tr["history"][-1] < 0.2 * tr["history"][0]
     # accuracy on the samples: trained vs untrained network (FP32 forward)
     inside = closure.inside(X, tr["norm"])
@@ -96,3 +103,47 @@ def test_trained_network_runs_in_the_step(small_channel):
           (rel_rms, np.abs(km_a - km_b).max(), np.abs(km_a).max()))
     assert rel_rms <= 0.6
     assert np.abs(a.get("el") - b.get("el")).max() < 0.02
+
+
+def test_network_coefficients_land_on_their_rows(small_channel, channel_trained):
+    """One step with the network on: on each column on the network, every interior level's
+    KQ, KM, KH equal 0.5*(network(inputs of that level) + value before the step), the
+    inputs read back through the closure samples of the same step and the network
+    evaluated by the FP32 forward pass.  The tensor-core network runs in BF16 on inputs
+    rounded to BF16, hence the percent-level tolerance; a coefficient stored on another
+    node or level would miss by far more."""
+    import ctypes as C
+    import torch
+    from myfvcomcode_b200 import closure
+    from myfvcomcode_b200.engine import Fvcom
+    _, _, tr = channel_trained
+    f = Fvcom(small_channel)
+    closure.attach(f, tr)
+    f.run(20)
+    M, KB = f.M, f.KB
+    S = M * (KB - 2)
+    before = {n: f.get3(n).copy() for n in ("kq", "km", "kh")}
+    buf = torch.zeros(12 * S, dtype=torch.float32, device="cuda")
+    f.lib.fvg_closure_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    assert f.lib.fvg_closure_sample(f.h, buf.data_ptr(), buf.numel()) == 0
+    f.run(1)
+    f.lib.fvg_closure_sample(f.h, None, 0)
+    a = buf.view(12, S).cpu().numpy()
+    X = a[:8].T.astype(np.float32)                         # row (K-2)*M + (I-1)
+    wet = (a[11] > 0.5).reshape(KB - 2, M).all(axis=0)
+    ins = closure.inside(X, tr["norm"]).reshape(KB - 2, M).all(axis=0)
+    on = wet & ins
+    assert on.sum() > 0
+    assert abs(int(on.sum()) - closure.status(f)["columns_on_network"]) <= max(1, on.sum() // 100)
+    rows = np.flatnonzero(np.tile(on, KB - 2))
+    new = closure.predict(tr, X[rows])                    # KN*KAPPA*SM, KN*SM, KN*SH*VPRNU
+    k = rows // M + 2
+    i = rows % M + 1
+    hits = []
+    for c, n in enumerate(("kq", "km", "kh")):
+        want = 0.5 * (new[:, c] + before[n][i, k - 1])
+        got = f.get3(n)[i, k - 1]
+        rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-12)
+        hits.append(rel <= 0.05)
+        assert np.median(rel) <= 0.01, n
+    assert np.mean(np.all(hits, axis=0)) >= 0.99

@@ -107,18 +107,26 @@ def test_staged_momentum_kernels_in_precision_form(small_coastal):
         assert np.abs(x - y).max() <= 1e-4 * scale, n
 
 
-def test_stream_hints_leave_results_bitwise_unchanged(small_coastal):
+def test_stream_hints_and_walks_leave_results_bitwise_unchanged():
     """The external loop's stage kernels load what a stage reads once evict-first in L2
-    (tuning key stream_hints, on by default): a cache hint only, so runs with and without
-    it are bit for bit equal, in the precision form and in plain FP64."""
+    (tuning key stream_hints, on by default) and the compact cell kernel runs as one wave
+    of blocks whose threads walk the cells (ext_grid, 8 by default): neither changes any
+    arithmetic, so runs with both and with neither are bit for bit equal, in the precision
+    form and in plain FP64.  A mesh of 20,000 points with one block per SM: each thread
+    walks two to three cells."""
+    from myfvcomcode_b200 import cases
     from myfvcomcode_b200.engine import Fvcom
+    case = cases.coastal_mesh(npts=20000, kb=7, lx=60000.0, ly=30000.0, seed=5, IRAMP=20)
+    assert case["grid"]["N"] > 2 * 128 * 148
     for prec in ("fp32flux", "fp64"):
-        a, b = Fvcom(small_coastal), Fvcom(small_coastal)
+        a, b = Fvcom(case), Fvcom(case)
         for f in (a, b):
             f.set_precision(prec)
-        assert a.get_tuning("stream_hints") == 1
+        assert a.get_tuning("stream_hints") == 1 and a.get_tuning("ext_grid") == 8
+        a.set_tuning("ext_grid", 1)
         b.set_tuning("stream_hints", 0)
-        assert b.get_tuning("stream_hints") == 0
+        b.set_tuning("ext_grid", 0)
+        assert b.get_tuning("stream_hints") == 0 and b.get_tuning("ext_grid") == 0
         a.run(4)
         b.run(4)
         for n in ("el", "ua", "va", "u", "v", "t1", "s1", "iswetc", "iswetn"):
