@@ -8,7 +8,10 @@ drift of the volume, heat and salt budgets (``fvg_budget``) over the run.  The c
 (two seeds): their differences from FP64 are what perturbations of the size of FP32
 rounding grow to by themselves in this flow.
 
-    python -m myfvcomcode_b200.precision_report [--npts 200000] [--hours 24] [--md FILE]
+    python -m myfvcomcode_b200.precision_report [--npts 200000] [--hours 24] [--md FILE] [--json FILE]
+
+The form with the learned closure ("fp32flux_learned") is run beside the precision form
+alone, with the network the library ships (trained on the 50k-node coastal mesh).
 """
 from __future__ import annotations
 
@@ -77,12 +80,17 @@ def twin_case(case, amplitude=1e-6, seed=17):
 
 
 TWIN_SEEDS = {"fp64_twin": 17, "fp64_twin2": 29}
+# the learned closure of the chosen form: the network trained on the 50k-node coastal mesh
+LEARNED = os.path.join(_HERE, "data", "closure_coastal50k_8seeds.npz")
 
 
-def run(case, steps, modes=("fp64", "fp32flux", "fp64_twin", "fp64_twin2"), chunk=200):
-    """Every mode from the same cold start for ``steps`` internal steps; the twins are
-    FP64 from initial temperatures perturbed by 1e-6 C with different seeds (their
-    spread shows how far this flow's own sensitivity alone moves the fields)."""
+def run(case, steps, modes=("fp64", "fp32flux", "fp32flux_learned", "fp64_twin", "fp64_twin2"), chunk=200):
+    """Every mode from the same cold start for ``steps`` internal steps: "fp32flux" the
+    precision form, "fp32flux_learned" the precision form with the learned closure (MY2.5
+    as its per-column fallback); the twins are FP64 from initial temperatures perturbed by
+    1e-6 C with different seeds (their spread shows how far this flow's own sensitivity
+    alone moves the fields)."""
+    from . import closure
     from .engine import Fvcom
     engines = {}
     budgets = {}
@@ -90,7 +98,9 @@ def run(case, steps, modes=("fp64", "fp32flux", "fp64_twin", "fp64_twin2"), chun
     for m in modes:
         twin = m in TWIN_SEEDS
         f = Fvcom(twin_case(case, seed=TWIN_SEEDS[m]) if twin else case)
-        f.set_precision("fp64" if twin else m)
+        f.set_precision("fp64" if twin else ("fp32flux" if m == "fp32flux_learned" else m))
+        if m == "fp32flux_learned":
+            closure.attach(f, closure.load(LEARNED))
         b0 = f.budget()
         t0 = time.perf_counter()
         done = 0
