@@ -295,8 +295,9 @@ __device__ __forceinline__ void ext_node_job(const Dev& P, const int i, int iext
 }
 
 // One job per thread, 48 registers (five blocks of 256 per SM; at 40 registers it
-// spills).  A grid of five blocks per SM whose threads walk the jobs measured slower
-// (1.14 -> 1.29 ms per step on the 200k-node mesh).
+// spills).  Measured slower on the 200k-node mesh: a grid of five blocks per SM whose
+// threads walk the jobs (1.14 -> 1.29 ms per step), and blocks that each mix three warps
+// of node jobs with five of gradient jobs (1.13 -> 1.45 ms).
 template <bool CS>
 __global__ void __launch_bounds__(256, 5) k_ext_node(const Dev P, int iext, int K, int parts) {
   pdl_enter();

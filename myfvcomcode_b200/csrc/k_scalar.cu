@@ -276,10 +276,21 @@ struct HeCell {
   R vf[3], nn[3];
 };
 
-// Cell data of the half-edge fluxes on layer k, formed in FP64 and rounded to R.
-template <typename R, int MODE>
-__device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell<R>& hc) {
+// The layer-independent part of a cell's half-edge data: its three nodes and their
+// NN_HVC, loaded once per thread for the layers it walks.
+template <typename R>
+__device__ inline void he_cell_static(const Dev& P, int c, HeCell<R>& hc) {
   const size_t n1 = P.N + 1;
+  for (int j = 0; j < 3; ++j) {
+    const int n = P.nv[j * n1 + c];
+    hc.nd[j] = n;
+    hc.nn[j] = (R)P.nn_hvc[n];
+  }
+}
+// Cell data of the half-edge fluxes on layer k, formed in FP64 and rounded to R; with
+// STATIC false, hc already holds he_cell_static's part.
+template <typename R, int MODE, bool STATIC = true>
+__device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell<R>& hc) {
   size_t ck = C3(P, c, k);
   if (MODE == 0) {
     size_t ckm = C3(P, c, k - 1);
@@ -291,11 +302,10 @@ __device__ inline void he_cell_load(const Dev& P, int c, int k, HeCell<R>& hc) {
     hc.vq = (R)P.v[ck];
     hc.dtij = (R)(P.dt1[c] * P.dz1[ck]);
   }
+  if (STATIC) he_cell_static<R>(P, c, hc);
   for (int j = 0; j < 3; ++j) {
-    int n = P.nv[j * n1 + c];
-    hc.nd[j] = n;
-    hc.nn[j] = (R)P.nn_hvc[n];
     if (sizeof(R) == 4) continue;  // FP32: VISCOFH travels in the node records
+    const int n = hc.nd[j];
     size_t q = N3(P, n, k);
     if (MODE == 0) {
       size_t qm = N3(P, n, k - 1);
@@ -399,10 +409,12 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_he_adv(const De
   }
   // Each of the cell's three nodes ends two of its half-edges: its record is loaded once
   // per tracer and layer and handed to both.  The metrics and the fluxes are by position
-  // s*ns + c.
+  // s*ns + c.  For Q2/Q2L the cell's nodes are loaded once for the layers this thread
+  // walks (for T/S, which hold more live values, that spills: they are reloaded per layer).
+  HeCell<R> hc;
+  if (MODE == 0) he_cell_static<R>(P, c, hc);
   for (int k = kb; k <= ke; ++k) {
-    HeCell<R> hc;
-    he_cell_load<R, MODE>(P, c, k, hc);
+    he_cell_load<R, MODE, MODE != 0>(P, c, k, hc);
     R2* EX = Mesh<R>::ex2(P) + (size_t)(k - 1) * P.ncvs + c;
     R e[2][3] = {{0, 0, 0}, {0, 0, 0}};
     for (int t = 0; t < 2; ++t) {
@@ -589,10 +601,10 @@ __device__ inline void vq_stress(const Dev& P, int i, double& utau2, double& wub
 
 // AUX bit 1: the learned closure's inputs are written (P.closure); bit 2: the closure
 // samples (P.clos_samp).  Each combination is its own instantiation, so that the plain
-// step and the learned step carry none of the other paths' registers; with either path
-// every instantiation is held to 64 registers (four blocks per SM).
+// step carries none of the other paths' registers (held to 64 registers, four blocks per
+// SM); with either path 80 registers (three blocks; at 64 they spill).
 template <int AUX>
-__global__ void __launch_bounds__(256, 4) k_vdif_q_levels(const Dev P) {
+__global__ void __launch_bounds__(256, AUX ? 3 : 4) k_vdif_q_levels(const Dev P) {
   using namespace vq;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.M) return;
