@@ -8,16 +8,19 @@
 // whether the node is wet and all its inputs lie inside the training envelope (clos_env,
 // from per-chunk flags of VDIF_Q's level kernel).  VDIF_Q finishes every column outside
 // the envelope with MY2.5 (the per-column fallback) and leaves KQ, KM, KH of the interior
-// levels of the others to k_closure_mlp, which takes the network's prediction and
-// averages with the old value as MY2.5 does: K = 0.5*(new + K_old) (vdif_q.F:489-491).
+// levels of the others to the network: k_clos_count and k_clos_list compact the columns
+// on the network into an ordered list, and k_closure_mlp runs the network on the rows
+// (interior level, listed column) only, takes its prediction and averages with the old
+// value as MY2.5 does: K = 0.5*(new + K_old) (vdif_q.F:489-491).
 //
 // Tile scheme: a CTA of 128 threads owns tiles of 128 rows; thread t owns row t of the
 // tile and TMEM lane t.  For each layer the threads write their row's BF16 activations
 // into shared memory in the canonical no-swizzle K-major layout (core matrices of 8 rows
 // x 16 bytes; core (row group g, k group c) at g*SBO + c*128 bytes), one elected thread
-// issues tcgen05.mma (M=128, N=64 or 16, K=16 per instruction, FP32 accumulate) and
-// commits to an mbarrier, and every thread reads its row back with tcgen05.ld, adds the
-// bias and applies GELU.  Weights are staged once per CTA in the same layout.
+// issues tcgen05.mma (M=128, N=64 or 16, K=16 per instruction, FP32 accumulate), commits
+// to an mbarrier and waits on it while the others wait at the block barrier, and every
+// thread reads its row back with tcgen05.ld, adds the bias (from shared memory) and
+// applies GELU (packed FP16, gelu2_bf16).  Weights and biases are staged once per CTA.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>

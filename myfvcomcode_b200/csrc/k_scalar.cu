@@ -601,10 +601,12 @@ __device__ inline void vq_stress(const Dev& P, int i, double& utau2, double& wub
 
 // AUX bit 1: the learned closure's inputs are written (P.closure); bit 2: the closure
 // samples (P.clos_samp).  Each combination is its own instantiation, so that the plain
-// step carries none of the other paths' registers (held to 64 registers, four blocks per
-// SM); with either path 80 registers (three blocks; at 64 they spill).
+// step carries none of the other paths' registers.  Every instantiation is held to 64
+// registers (four blocks per SM): with the closure's inputs that spills 20 bytes, and
+// still measured faster than 80 registers and three blocks (1.30 against 1.37 ms per
+// step for VDIF_Q on the 200k-node mesh).
 template <int AUX>
-__global__ void __launch_bounds__(256, AUX ? 3 : 4) k_vdif_q_levels(const Dev P) {
+__global__ void __launch_bounds__(256, 4) k_vdif_q_levels(const Dev P) {
   using namespace vq;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > P.M) return;
