@@ -392,12 +392,10 @@ struct Oracle {
       double dij = 0.5 * (d[j1] + d[j2]);
       double elij = 0.5 * (el[j1] + el[j2]);
       if (iswetce[ia] * iswetc[ia] == 1 || iswetce[ib] * iswetc[ib] == 1) {
-        int k1 = NBE(ia, 1), k2 = NBE(ia, 2), k3 = NBE(ia, 3);
         double cofa1, cofa2, cofa5, cofa6;
         cofa(ua.data(), va.data(), ia, cofa1, cofa2, cofa5, cofa6);
         double xija = xijc[i] - xc[ia];
         double yija = yijc[i] - yc[ia];
-        k1 = NBE(ib, 1); k2 = NBE(ib, 2); k3 = NBE(ib, 3);
         double cofa3, cofa4, cofa7, cofa8;
         cofa(ua.data(), va.data(), ib, cofa3, cofa4, cofa7, cofa8);
         double xijb = xijc[i] - xc[ib];
