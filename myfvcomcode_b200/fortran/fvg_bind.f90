@@ -101,6 +101,38 @@ MODULE FVG_BIND
       IMPORT :: C_INT, C_PTR
       TYPE(C_PTR), VALUE :: handle
     END FUNCTION
+    INTEGER(C_INT) FUNCTION fvg_get_ifield(handle, name, dst, cnt) BIND(C, NAME="fvg_get_ifield")
+      IMPORT :: C_INT, C_PTR, C_CHAR, C_INT64_T
+      TYPE(C_PTR), VALUE :: handle
+      CHARACTER(KIND=C_CHAR), DIMENSION(*), INTENT(IN) :: name
+      TYPE(C_PTR), VALUE :: dst
+      INTEGER(C_INT64_T), VALUE :: cnt
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION fvg_set_forcing(handle, forcing) BIND(C, NAME="fvg_set_forcing")
+      IMPORT :: C_INT, C_PTR, FVG_FORCING_T
+      TYPE(C_PTR), VALUE :: handle
+      TYPE(FVG_FORCING_T), INTENT(IN) :: forcing
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION fvg_run(handle, nsteps) BIND(C, NAME="fvg_run")
+      IMPORT :: C_INT, C_PTR, C_INT32_T
+      TYPE(C_PTR), VALUE :: handle
+      INTEGER(C_INT32_T), VALUE :: nsteps
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION fvg_set_precision(handle, mode) BIND(C, NAME="fvg_set_precision")
+      IMPORT :: C_INT, C_PTR, C_INT32_T
+      TYPE(C_PTR), VALUE :: handle
+      INTEGER(C_INT32_T), VALUE :: mode
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION fvg_budget(handle, out) BIND(C, NAME="fvg_budget")
+      IMPORT :: C_INT, C_PTR, C_DOUBLE
+      TYPE(C_PTR), VALUE :: handle
+      REAL(C_DOUBLE), DIMENSION(3), INTENT(OUT) :: out
+    END FUNCTION
+    FUNCTION fvg_last_error(handle) BIND(C, NAME="fvg_last_error")
+      IMPORT :: C_PTR
+      TYPE(C_PTR), VALUE :: handle
+      TYPE(C_PTR) :: fvg_last_error
+    END FUNCTION
   END INTERFACE
 
   TYPE(C_PTR), SAVE :: FVG_HANDLE = C_NULL_PTR
@@ -129,6 +161,16 @@ CONTAINS
     RC = fvg_get_field(FVG_HANDLE, TRIM(NAME)//C_NULL_CHAR, C_LOC(A), INT(SIZE(A), C_INT64_T))
     IF (RC /= 0) CALL FATAL_ERROR("fvg_get_field failed for "//TRIM(NAME))
   END SUBROUTINE PULL
+
+  ! Forcing of the coming internal step (the river, wind and heating arrays BCOND_GCN(8)
+  ! updated on the host, UPDATE_RIVERS / UPDATE_WIND / UPDATE_HEAT), handed over before
+  ! FVG_INTERNAL_STEP; FRC's pointers are C_LOC of FVCOM's arrays, as for FVG_CREATE.
+  SUBROUTINE FVG_FORCE(FRC)
+    TYPE(FVG_FORCING_T), INTENT(IN) :: FRC
+    INTEGER(C_INT) :: RC
+    RC = fvg_set_forcing(FVG_HANDLE, FRC)
+    IF (RC /= 0) CALL FATAL_ERROR("fvg_set_forcing failed")
+  END SUBROUTINE FVG_FORCE
 
   ! Replacement for CALL INTERNAL_STEP at fvcom.F:852.  IntTime was advanced by the caller;
   ! the library advances IINT and ExtTime (ISPLIT*DTE) itself.
